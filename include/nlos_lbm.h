@@ -1,0 +1,249 @@
+/*
+ * nlos_lbm.h -- C-ABI of the B200 D3Q19 lattice-Boltzmann acoustic solver.
+ *
+ * The reference solver has no library interface: its entry points are the
+ * public members of `LBMSolver` in 06_transient_localization_dx1.cpp (and the
+ * identical family-B solvers 05/07/08), called from `main`.  Each function
+ * below replaces one of those members; the comment names the reference
+ * member it stands in for (file:line).  Plain C types only: pointers, sizes,
+ * doubles.  The library owns all device memory; callers own host arrays.
+ *
+ * Error behaviour: every call returns an lbm_status.  0 is success, negative
+ * values are errors (nothing was changed), positive values are warnings for
+ * the cases the reference reports on stdout and then carries on (STL not
+ * loaded, probe inside a solid).  No C++ exceptions cross this boundary.
+ * A handle owns one CUDA stream and is not re-entrant: use one handle per
+ * host thread.
+ *
+ * Lattice: D3Q19 in the reference's family-B velocity order (06:21-31).
+ * Populations are stored on the device as deviations g_q = f_q - w_q from the
+ * rest equilibrium, in FP32 or (scaled) FP16, and collided in FP32.
+ */
+#ifndef NLOS_LBM_H
+#define NLOS_LBM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct lbm_handle lbm_handle;
+
+typedef enum lbm_status
+{
+    LBM_OK = 0,
+    LBM_WARN_STL_NOT_LOADED = 1,   /* 06:397-410: geometry left empty, run continues */
+    LBM_WARN_PROBE_IN_SOLID = 2,   /* 06:432-435: probe cell is SOLID, run continues */
+    LBM_ERR_INVALID_ARGUMENT = -1,
+    LBM_ERR_BAD_CONFIG = -2,
+    LBM_ERR_OUT_OF_MEMORY = -3,
+    LBM_ERR_CUDA = -4,
+    LBM_ERR_NAN = -5,
+    LBM_ERR_STATE = -6,            /* call out of order, e.g. step before init */
+    LBM_ERR_CAPACITY = -7,         /* caller's output buffer too small */
+    LBM_ERR_NO_DEVICE = -8,
+    LBM_ERR_IO = -9,
+    LBM_ERR_UNSUPPORTED = -10
+} lbm_status;
+
+/* Boundary treatment of one face of the box. */
+enum
+{
+    LBM_BC_NSCBC = 0,  /* characteristic open boundary, zero incoming wave (06:684-835) */
+    LBM_BC_REST = 1,   /* halo held at rest equilibrium w_q (06:677-682 with use_nscbc=false) */
+    LBM_BC_WALL = 2    /* SOLID halo: halfway bounce-back (ground plane, 06:520-531) */
+};
+enum { LBM_FACE_XLO = 0, LBM_FACE_XHI, LBM_FACE_YLO, LBM_FACE_YHI, LBM_FACE_ZLO, LBM_FACE_ZHI };
+
+enum { LBM_STORE_F32 = 0, LBM_STORE_F16 = 1 };
+
+/* Source time functions. */
+enum
+{
+    LBM_WAVE_GAUSS = 0,   /* amp*exp(-0.5*((t-t0)/sigma_t)^2)            (06:579-581) */
+    LBM_WAVE_SINE = 1,    /* amp*sin(2*pi*freq*t)                         (08:543) */
+    LBM_WAVE_RICKER = 2,  /* amp*(1-2a)exp(-a), a=(pi*freq*(t-t0))^2 */
+    LBM_WAVE_TABLE = 3    /* amp*table[s], one sample per time step s */
+};
+/* Spatial injection stencils. */
+enum
+{
+    LBM_INJECT_GAUSS = 0,     /* (2R+1)^3 Gaussian, fluid-normalised          (06:587-666) */
+    LBM_INJECT_TRILINEAR = 1  /* 8 cells, trilinear weights, fluid-normalised */
+};
+
+/* Solver configuration: the member fields of LBMSolver (06:244-268), the
+ * constants of init_domain (06:455-458) and UnitConverter (06:195-204), plus
+ * the boundary/sponge/storage choices the reference hard-codes. */
+typedef struct lbm_config
+{
+    double x_min, x_max, y_min, y_max, z_min, z_max; /* 06:250-252 */
+    double dx;                                       /* 06:253 DX */
+    double c_phys;                                   /* 06:198 speed of sound (dt = cs*dx/c) */
+    double tau;                                      /* 06:268 BGK relaxation time */
+    int use_geometry;                                /* 06:248 */
+    int face_bc[6];                                  /* LBM_BC_* per face, LBM_FACE_* order */
+    unsigned sponge_faces;                           /* bit f set: sponge ramps in from face f (06:491-496) */
+    double sponge_width;                             /* in cells (06:455: 20) */
+    double sponge_strength;                          /* 06:456: 0.35 */
+    double sky_z;                                    /* cells above this z are FLUID (06:458,489) */
+    int storage;                                     /* LBM_STORE_F32 or LBM_STORE_F16 */
+    double f16_scale;                                /* FP16 stores (f_q - w_q) * f16_scale */
+    int device;                                      /* CUDA device ordinal */
+    int use_graphs;                                  /* replay multi-step runs as CUDA graphs */
+    int verbose;                                     /* print the reference's progress lines */
+} lbm_config;
+
+/* One sound source: DroneSource (06:211-239) plus its time function. */
+typedef struct lbm_source
+{
+    double sx, sy, sz;      /* path start  (06:213) */
+    double ex, ey, ez;      /* path end    (06:214) */
+    double speed;           /* units / time; 0 = stationary (06:225) */
+    double amp;             /* 06:216 */
+    double freq;            /* 06:217 (sine, Ricker peak frequency) */
+    int waveform;           /* LBM_WAVE_* */
+    double t0, sigma_t;     /* Gaussian centre/width (06:579-580); Ricker delay t0 */
+    int injection;          /* LBM_INJECT_* */
+    double gain;            /* 06:583 source_gain */
+    double sigma_cells;     /* Gaussian stencil width in cells (06:588: 1.25) */
+    int radius;             /* Gaussian stencil radius in cells (06:587: 2), 0..3 */
+    const double* table;    /* LBM_WAVE_TABLE samples (copied at lbm_add_source) */
+    int table_len;
+} lbm_source;
+
+/* Seeded synthetic city: axis-aligned box buildings written as triangles. */
+typedef struct lbm_city_params
+{
+    int nx, ny;             /* plan extent in cells */
+    double dx;              /* cell size (vertex coordinates are multiples of it) */
+    uint64_t seed;
+    int fp_min, fp_max;     /* footprint side, cells */
+    int h_min, h_max;       /* building height, cells */
+    double coverage;        /* target plan-area fraction */
+    int street;             /* minimum gap between buildings, cells */
+    int margin;             /* keep-out band along the plan border, cells */
+} lbm_city_params;
+
+/* ---- defaults ------------------------------------------------------------ */
+
+/* Reference defaults: 06:250-268 fields, 06:455-458 sponge/sky constants,
+ * NSCBC on x-,x+,y-,y+,z+ and ground bounce-back at z- (06:509-531). */
+void lbm_config_default(lbm_config* cfg);
+/* Reference defaults for a source: Gaussian pulse t0=0.05 s, sigma_t=0.005 s
+ * (06:579-580), 5x5x5 Gaussian stencil R=2, sigma 1.25 cells (06:587-588). */
+void lbm_source_default(lbm_source* src);
+const char* lbm_status_string(int status);
+/* Library version string and the CUDA architecture it was built for. */
+const char* lbm_version(void);
+
+/* ---- lifetime ------------------------------------------------------------ */
+
+/* Validates the config and binds the device; no device memory yet.
+ * Replaces constructing LBMSolver and setting its fields (06:1128-1166). */
+int lbm_create(const lbm_config* cfg, lbm_handle** out);
+/* Frees all device and host memory of the handle. */
+int lbm_destroy(lbm_handle* h);
+/* Last error message of this handle (NUL-terminated, may be empty). */
+const char* lbm_last_error(lbm_handle* h);
+
+/* ---- geometry / mask (LBMSolver::init 06:397-413, init_domain 06:453-532) ---- */
+
+/* Binary STL file; vertices * scale + (sx,sy,sz) as GeometryEngine::load
+ * (06:70-111).  Returns LBM_WARN_STL_NOT_LOADED and keeps an empty geometry
+ * when the file cannot be read, as the reference does (06:397-410). */
+int lbm_set_geometry_stl(lbm_handle* h, const char* path, double scale, double sx, double sy, double sz);
+/* Same, from memory: tris holds ntris * 9 floats (v1, v2, v3). */
+int lbm_set_geometry_triangles(lbm_handle* h, const float* tris, int ntris, double scale, double sx,
+                               double sy, double sz);
+/* Override the voxelised mask: nx_t*ny_t*nz_t bytes (0 FLUID, 1 SOLID) in the
+ * reference's halo-inclusive order i + j*nx_t + k*nx_t*ny_t (06:206-209). */
+int lbm_set_mask(lbm_handle* h, const uint8_t* mask, int nx_t, int ny_t, int nz_t);
+
+/* ---- sources and probes ------------------------------------------------- */
+
+/* Adds a source (the reference has exactly one, LBMSolver::drone 06:246). */
+int lbm_add_source(lbm_handle* h, const lbm_source* src);
+int lbm_clear_sources(lbm_handle* h);
+/* Probe positions xyz[3*n] in physical coordinates (LBMSolver::probes
+ * 06:257-266); cell = floor((x - x_min)/dx) (06:417-419). */
+int lbm_set_probes(lbm_handle* h, const double* xyz, int n);
+/* Per probe: owned (inside the grid) and in_solid flags; either may be NULL. */
+int lbm_probe_info(lbm_handle* h, int* owned, int* in_solid);
+
+/* ---- set-up and stepping ------------------------------------------------- */
+
+/* Builds the grid, mask, sponge and rest state on the device
+ * (LBMSolver::init 06:299-450).  May return LBM_WARN_* codes. */
+int lbm_init(lbm_handle* h);
+/* Source injection at time t (LBMSolver::apply_source 06:576-667). */
+int lbm_apply_source(lbm_handle* h, double t);
+/* Open-boundary ghost fill (LBMSolver::exchange_halos 06:671-904, one rank). */
+int lbm_exchange_halos(lbm_handle* h);
+/* Fused pull-stream + bounce-back + BGK + sponge, then buffer swap
+ * (LBMSolver::step_collision_bgk 06:906-972). */
+int lbm_step_collision_bgk(lbm_handle* h);
+/* Appends rho-1 at every owned probe for the last step (06:1085-1092). */
+int lbm_record_probes(lbm_handle* h);
+/* nsteps full time steps s, s+1, ...: apply_source(s*dt), exchange_halos,
+ * step_collision_bgk, record_probes -- the body of LBMSolver::run
+ * (06:1077-1092) without VTK output. */
+int lbm_step(lbm_handle* h, int nsteps);
+/* LBMSolver::run(T_total, Frames) (06:1064-1121): steps s = 0..round(T/dt)
+ * inclusive.  Frames only sets the progress/frame interval (no VTK here). */
+int lbm_run(lbm_handle* h, double T_total, int frames);
+/* Waits for all work queued on the handle's stream. */
+int lbm_synchronize(lbm_handle* h);
+
+/* ---- results ------------------------------------------------------------ */
+
+/* Grid size NXg, NYg, NZg (06:332-334) and halo-inclusive nx_t, ny_t, nz_t. */
+int lbm_get_dims(lbm_handle* h, int* n3, int* n3_halo);
+double lbm_get_dt(lbm_handle* h);
+/* Number of time steps taken so far. */
+long lbm_get_step(lbm_handle* h);
+/* Probe series rho-1, layout [step][probe], FP64 (06:1090, 06:1106-1118);
+ * unowned probes read NaN.  *nsteps receives the number of rows. */
+int lbm_get_probes(lbm_handle* h, double* out, long capacity, long* nsteps);
+/* Per-probe sum over recorded steps of (rho-1)^2, accumulated in FP64. */
+int lbm_get_probe_energy(lbm_handle* h, double* out);
+/* Interior field (float)(rho-1) of the last step, i fastest (06:979-985). */
+int lbm_get_rho(lbm_handle* h, float* out, long capacity);
+/* Populations f_q (FP64, w_q + deviation) in the reference's AoS,
+ * halo-inclusive layout f[idx*19+q] (06:366, 06:206-209). */
+int lbm_get_f(lbm_handle* h, double* out, long capacity);
+int lbm_set_f(lbm_handle* h, const double* in, long count);
+/* Voxelised mask, halo-inclusive, 0 FLUID / 1 SOLID (06:469-531). */
+int lbm_get_mask(lbm_handle* h, uint8_t* out, long capacity);
+
+/* ---- measurement ---------------------------------------------------------- */
+
+/* When enabled, every launch of the fused step kernel is bracketed by CUDA
+ * events on the handle's stream; lbm_get_kernel_time returns the summed
+ * device time (ms) and launch count since the last reset. */
+int lbm_set_kernel_timing(lbm_handle* h, int enable);
+int lbm_get_kernel_time(lbm_handle* h, double* total_ms, long* launches);
+/* Number of CUDA kernels this handle has launched (graph replays counted
+ * per kernel node). */
+long lbm_get_launch_count(lbm_handle* h);
+/* Bytes per cell update the fused step moves by algorithm: 2*19*sizeof(store). */
+int lbm_bytes_per_cell(lbm_handle* h);
+
+/* ---- synthetic geometry -------------------------------------------------- */
+
+/* Fills tris (capacity triangles, 9 floats each) with the city's boxes
+ * (12 triangles per building).  Returns LBM_ERR_CAPACITY with *ntris set to
+ * the required count when tris is too small.  *coverage receives the plan
+ * fraction achieved. */
+int lbm_city_generate(const lbm_city_params* p, float* tris, int capacity, int* ntris, double* coverage);
+/* Writes a binary STL file (80-byte header, uint32 count, 50-byte records;
+ * the format GeometryEngine::load reads, 06:49-58, 06:70-111). */
+int lbm_stl_write(const char* path, const float* tris, int ntris);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NLOS_LBM_H */

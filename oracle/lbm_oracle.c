@@ -1,0 +1,803 @@
+/*
+ * lbm_oracle.c -- FP64 CPU restatement of the reference's family-B D3Q19
+ * acoustic solver.  TEST INFRASTRUCTURE ONLY (see lbm_oracle.h).
+ *
+ * Layout and arithmetic follow the reference one to one so that results are
+ * bit-identical where the reference defines them:
+ *   - AoS populations f[idx*19+q], idx = i + j*nx_t + k*nx_t*ny_t with a
+ *     one-cell halo (06:206-209, 06:361-371);
+ *   - every FP64 expression keeps the reference's operand order (feq 06:286-291,
+ *     macro_at 06:545-568, the NSCBC ghost formulas 06:684-835, the BGK step
+ *     06:906-972, the source 06:576-667, the mask/sponge 06:453-532 and the
+ *     heightmap ray cast 06:144-192).  Compile with -ffp-contract=off.
+ */
+#include "lbm_oracle.h"
+
+#include <math.h>
+#include <omp.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define Q 19
+#define SOLID 1
+#define FLUID 0
+
+static const double CS2 = 1.0 / 3.0;                  /* 06:17 */
+static const double CS = 0.57735026918962576451;      /* 06:18 */
+static const double PI_ = 3.14159265358979323846;     /* 06:19 */
+
+/* Family-B velocity order (06:21-23) and weights (06:25-31). */
+static const int EX[Q] = {0, 1, -1, 0, 0, 0, 0, 1, 1, -1, -1, 1, 1, -1, -1, 0, 0, 0, 0};
+static const int EY[Q] = {0, 0, 0, 1, -1, 0, 0, 1, -1, 1, -1, 0, 0, 0, 0, 1, 1, -1, -1};
+static const int EZ[Q] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1};
+static const double W[Q] = {1.0 / 3.0,
+                            1.0 / 18.0, 1.0 / 18.0, 1.0 / 18.0, 1.0 / 18.0, 1.0 / 18.0, 1.0 / 18.0,
+                            1.0 / 36.0, 1.0 / 36.0, 1.0 / 36.0, 1.0 / 36.0, 1.0 / 36.0, 1.0 / 36.0,
+                            1.0 / 36.0, 1.0 / 36.0, 1.0 / 36.0, 1.0 / 36.0, 1.0 / 36.0, 1.0 / 36.0};
+
+typedef struct { double x, y, z; } pt3;
+typedef struct { pt3 v1, v2, v3, mn, mx; } tri_t;
+
+typedef struct
+{
+    lbm_source s;
+    double* table;   /* owned copy for LBM_WAVE_TABLE */
+    double cx, cy, cz;
+} src_t;
+
+struct orc_handle
+{
+    lbm_config cfg;
+    int inv_q[Q];
+    int NXg, NYg, NZg, nx, ny, nz, nx_t, ny_t, nz_t;
+    size_t Nloc;
+    double dt;
+    double *f_curr, *f_next, *rho, *sponge, *gH;
+    unsigned char* mask;
+    int mask_override;
+    /* geometry (GeometryEngine 06:60-193) */
+    tri_t* tris;
+    int ntris;
+    pt3 gmin, gmax;
+    double cellW, cellH;
+    int* bin_start;   /* 200*200+1 CSR offsets */
+    int* bin_items;
+    /* sources / probes */
+    src_t* srcs;
+    int nsrc;
+    int nprobe;
+    double* probe_xyz;
+    long* probe_idx;   /* -1: not owned */
+    double* series;    /* [steps][nprobe] */
+    long steps_rec, steps_cap;
+    long step;         /* time steps taken by orc_step */
+};
+
+static inline size_t loc(const orc_handle* h, int i, int j, int k)
+{
+    return (size_t)i + (size_t)j * (size_t)h->nx_t + (size_t)k * (size_t)h->nx_t * (size_t)h->ny_t;
+}
+
+/* 06:286-291 */
+static inline double feq(int k, double r, double ux, double uy, double uz)
+{
+    double cu = EX[k] * ux + EY[k] * uy + EZ[k] * uz;
+    double u2 = ux * ux + uy * uy + uz * uz;
+    return W[k] * r * (1.0 + 3.0 * cu + 4.5 * cu * cu - 1.5 * u2);
+}
+
+static double dmin(double a, double b) { return b < a ? b : a; }
+static double dmax(double a, double b) { return a < b ? b : a; }
+static double min3(double a, double b, double c) { return dmin(dmin(a, b), c); }
+static double max3(double a, double b, double c) { return dmax(dmax(a, b), c); }
+
+void orc_set_threads(int n) { omp_set_num_threads(n); }
+
+orc_handle* orc_create(const lbm_config* cfg)
+{
+    orc_handle* h = (orc_handle*)calloc(1, sizeof(orc_handle));
+    h->cfg = *cfg;
+    /* inv_q as computed in LBMSolver::init (06:301-312) */
+    for (int i = 0; i < Q; ++i)
+    {
+        h->inv_q[i] = 0;
+        for (int j = 0; j < Q; ++j)
+            if (EX[i] == -EX[j] && EY[i] == -EY[j] && EZ[i] == -EZ[j]) { h->inv_q[i] = j; break; }
+    }
+    h->gmin.x = h->gmin.y = h->gmin.z = 1e30;
+    h->gmax.x = h->gmax.y = h->gmax.z = -1e30;
+    h->cellW = h->cellH = 1.0;
+    return h;
+}
+
+void orc_destroy(orc_handle* h)
+{
+    if (!h) return;
+    free(h->f_curr); free(h->f_next); free(h->rho); free(h->sponge); free(h->gH); free(h->mask);
+    free(h->tris); free(h->bin_start); free(h->bin_items);
+    for (int i = 0; i < h->nsrc; ++i) free(h->srcs[i].table);
+    free(h->srcs); free(h->probe_xyz); free(h->probe_idx); free(h->series);
+    free(h);
+}
+
+/* ---------------------------------------------------------------- geometry */
+
+/* GeometryEngine::buildGrid (06:113-142) with a 200x200 bin grid. */
+static void build_grid(orc_handle* h)
+{
+    const int R = 200, C = 200;
+    free(h->bin_start); free(h->bin_items);
+    h->bin_start = NULL; h->bin_items = NULL;
+    if (h->ntris == 0) return;
+    h->cellW = (h->gmax.x - h->gmin.x) / R;
+    h->cellH = (h->gmax.y - h->gmin.y) / C;
+    if (h->cellW < 1e-9) h->cellW = 1.0;
+    if (h->cellH < 1e-9) h->cellH = 1.0;
+    int* cnt = (int*)calloc((size_t)R * C + 1, sizeof(int));
+    int* rr = (int*)malloc((size_t)h->ntris * 4 * sizeof(int));
+    for (int i = 0; i < h->ntris; ++i)
+    {
+        const tri_t* t = &h->tris[i];
+        int r1 = (int)((t->mn.x - h->gmin.x) / h->cellW);
+        int r2 = (int)((t->mx.x - h->gmin.x) / h->cellW);
+        int c1 = (int)((t->mn.y - h->gmin.y) / h->cellH);
+        int c2 = (int)((t->mx.y - h->gmin.y) / h->cellH);
+        r1 = r1 < 0 ? 0 : (r1 > R - 1 ? R - 1 : r1);
+        r2 = r2 < 0 ? 0 : (r2 > R - 1 ? R - 1 : r2);
+        c1 = c1 < 0 ? 0 : (c1 > C - 1 ? C - 1 : c1);
+        c2 = c2 < 0 ? 0 : (c2 > C - 1 ? C - 1 : c2);
+        rr[4 * i] = r1; rr[4 * i + 1] = r2; rr[4 * i + 2] = c1; rr[4 * i + 3] = c2;
+        for (int r = r1; r <= r2; ++r)
+            for (int c = c1; c <= c2; ++c) cnt[r * C + c + 1]++;
+    }
+    for (int b = 0; b < R * C; ++b) cnt[b + 1] += cnt[b];
+    h->bin_start = cnt;
+    h->bin_items = (int*)malloc((size_t)(cnt[R * C] > 0 ? cnt[R * C] : 1) * sizeof(int));
+    int* fill = (int*)calloc((size_t)R * C, sizeof(int));
+    for (int i = 0; i < h->ntris; ++i)
+        for (int r = rr[4 * i]; r <= rr[4 * i + 1]; ++r)
+            for (int c = rr[4 * i + 2]; c <= rr[4 * i + 3]; ++c)
+                h->bin_items[cnt[r * C + c] + fill[r * C + c]++] = i;
+    free(fill);
+    free(rr);
+}
+
+/* GeometryEngine::getGroundHeight (06:144-192): highest hit of the down ray. */
+static double ground_height(const orc_handle* h, double x, double y)
+{
+    const int R = 200, C = 200;
+    if (h->ntris == 0) return -1e30;
+    if (x < h->gmin.x || x > h->gmax.x || y < h->gmin.y || y > h->gmax.y) return -1e30;
+    int r = (int)((x - h->gmin.x) / h->cellW);
+    int c = (int)((y - h->gmin.y) / h->cellH);
+    if (r < 0 || r >= R || c < 0 || c >= C) return -1e30;
+    const int b0 = h->bin_start[r * C + c], b1 = h->bin_start[r * C + c + 1];
+    if (b0 == b1) return -1e30;
+    const pt3 ro = {x, y, 10000.0};
+    const pt3 rd = {0.0, 0.0, -1.0};
+    double maxZ = -1e30;
+    for (int b = b0; b < b1; ++b)
+    {
+        const tri_t* tri = &h->tris[h->bin_items[b]];
+        if (tri->mx.x < x - 1e-6 || tri->mn.x > x + 1e-6) continue;
+        if (tri->mx.y < y - 1e-6 || tri->mn.y > y + 1e-6) continue;
+        const double EPS = 1e-9;
+        pt3 e1 = {tri->v2.x - tri->v1.x, tri->v2.y - tri->v1.y, tri->v2.z - tri->v1.z};
+        pt3 e2 = {tri->v3.x - tri->v1.x, tri->v3.y - tri->v1.y, tri->v3.z - tri->v1.z};
+        pt3 hh = {rd.y * e2.z - rd.z * e2.y, rd.z * e2.x - rd.x * e2.z, rd.x * e2.y - rd.y * e2.x};
+        double a = e1.x * hh.x + e1.y * hh.y + e1.z * hh.z;
+        if (fabs(a) < EPS) continue;
+        double f = 1.0 / a;
+        pt3 s = {ro.x - tri->v1.x, ro.y - tri->v1.y, ro.z - tri->v1.z};
+        double u = f * (s.x * hh.x + s.y * hh.y + s.z * hh.z);
+        if (u < 0.0 || u > 1.0) continue;
+        pt3 q = {s.y * e1.z - s.z * e1.y, s.z * e1.x - s.x * e1.z, s.x * e1.y - s.y * e1.x};
+        double v = f * (rd.x * q.x + rd.y * q.y + rd.z * q.z);
+        if (v < 0.0 || (u + v) > 1.0) continue;
+        double t = f * (e2.x * q.x + e2.y * q.y + e2.z * q.z);
+        if (t > EPS)
+        {
+            double hitZ = ro.z + t * rd.z;
+            if (hitZ > maxZ) maxZ = hitZ;
+        }
+    }
+    return maxZ;
+}
+
+static void add_triangle(orc_handle* h, int i, const float* v, double scale, double sx, double sy, double sz)
+{
+    tri_t* t = &h->tris[i];
+    /* GeometryEngine::load (06:90-106) */
+    t->v1.x = v[0] * scale + sx; t->v1.y = v[1] * scale + sy; t->v1.z = v[2] * scale + sz;
+    t->v2.x = v[3] * scale + sx; t->v2.y = v[4] * scale + sy; t->v2.z = v[5] * scale + sz;
+    t->v3.x = v[6] * scale + sx; t->v3.y = v[7] * scale + sy; t->v3.z = v[8] * scale + sz;
+    t->mn.x = min3(t->v1.x, t->v2.x, t->v3.x);
+    t->mn.y = min3(t->v1.y, t->v2.y, t->v3.y);
+    t->mn.z = min3(t->v1.z, t->v2.z, t->v3.z);
+    t->mx.x = max3(t->v1.x, t->v2.x, t->v3.x);
+    t->mx.y = max3(t->v1.y, t->v2.y, t->v3.y);
+    t->mx.z = max3(t->v1.z, t->v2.z, t->v3.z);
+    h->gmin.x = dmin(h->gmin.x, t->mn.x); h->gmin.y = dmin(h->gmin.y, t->mn.y); h->gmin.z = dmin(h->gmin.z, t->mn.z);
+    h->gmax.x = dmax(h->gmax.x, t->mx.x); h->gmax.y = dmax(h->gmax.y, t->mx.y); h->gmax.z = dmax(h->gmax.z, t->mx.z);
+}
+
+int orc_set_geometry_triangles(orc_handle* h, const float* tris, int ntris, double scale, double sx,
+                               double sy, double sz)
+{
+    free(h->tris);
+    h->tris = (tri_t*)calloc((size_t)(ntris > 0 ? ntris : 1), sizeof(tri_t));
+    h->ntris = ntris;
+    h->gmin.x = h->gmin.y = h->gmin.z = 1e30;
+    h->gmax.x = h->gmax.y = h->gmax.z = -1e30;
+    for (int i = 0; i < ntris; ++i) add_triangle(h, i, tris + 9 * (size_t)i, scale, sx, sy, sz);
+    build_grid(h);
+    return LBM_OK;
+}
+
+int orc_set_geometry_stl(orc_handle* h, const char* path, double scale, double sx, double sy, double sz)
+{
+    FILE* fp = fopen(path, "rb");
+    if (!fp)
+    {
+        orc_set_geometry_triangles(h, NULL, 0, scale, sx, sy, sz);
+        return LBM_WARN_STL_NOT_LOADED;
+    }
+    char header[80];
+    uint32_t n = 0;
+    if (fread(header, 1, 80, fp) != 80 || fread(&n, 4, 1, fp) != 1) n = 0;
+    float* v = (float*)calloc((size_t)(n ? n : 1) * 9, sizeof(float));
+    for (uint32_t i = 0; i < n; ++i)
+    {
+        unsigned char rec[50];
+        memset(rec, 0, sizeof rec);
+        size_t got = fread(rec, 1, 50, fp);
+        (void)got;
+        memcpy(v + 9 * (size_t)i, rec + 12, 36);
+    }
+    fclose(fp);
+    orc_set_geometry_triangles(h, v, (int)n, scale, sx, sy, sz);
+    free(v);
+    return LBM_OK;
+}
+
+int orc_set_mask(orc_handle* h, const unsigned char* mask)
+{
+    if (!h->mask) return LBM_ERR_STATE;
+    memcpy(h->mask, mask, h->Nloc);
+    h->mask_override = 1;
+    return LBM_OK;
+}
+
+/* ---------------------------------------------------------- sources/probes */
+
+int orc_add_source(orc_handle* h, const lbm_source* src)
+{
+    h->srcs = (src_t*)realloc(h->srcs, (size_t)(h->nsrc + 1) * sizeof(src_t));
+    src_t* s = &h->srcs[h->nsrc++];
+    memset(s, 0, sizeof *s);
+    s->s = *src;
+    if (src->waveform == LBM_WAVE_TABLE && src->table_len > 0)
+    {
+        s->table = (double*)malloc((size_t)src->table_len * sizeof(double));
+        memcpy(s->table, src->table, (size_t)src->table_len * sizeof(double));
+    }
+    s->s.table = s->table;
+    return LBM_OK;
+}
+
+int orc_set_probes(orc_handle* h, const double* xyz, int n)
+{
+    free(h->probe_xyz);
+    h->probe_xyz = (double*)malloc((size_t)(n > 0 ? n : 1) * 3 * sizeof(double));
+    memcpy(h->probe_xyz, xyz, (size_t)n * 3 * sizeof(double));
+    h->nprobe = n;
+    return LBM_OK;
+}
+
+/* ---------------------------------------------------------------- init */
+
+static void init_domain(orc_handle* h)
+{
+    const lbm_config* c = &h->cfg;
+    const double dx = c->dx;
+    const double sponge_w = c->sponge_width * dx;   /* 06:455 */
+    const double strength = c->sponge_strength;     /* 06:456 */
+    const double sky_z = c->sky_z;                  /* 06:458 */
+    const unsigned sf = c->sponge_faces;
+
+    /* 06:460-467 */
+    #pragma omp parallel for collapse(2)
+    for (int j = 0; j < h->ny_t; ++j)
+        for (int i = 0; i < h->nx_t; ++i)
+        {
+            double x = c->x_min + ((i - 1) + 0.5) * dx;
+            double y = c->y_min + ((j - 1) + 0.5) * dx;
+            h->gH[(size_t)j * h->nx_t + (size_t)i] = ground_height(h, x, y);
+        }
+
+    /* 06:469-507 */
+    #pragma omp parallel for collapse(2)
+    for (int k = 0; k < h->nz_t; ++k)
+        for (int j = 0; j < h->ny_t; ++j)
+            for (int i = 0; i < h->nx_t; ++i)
+            {
+                size_t idx = loc(h, i, j, k);
+                double x = c->x_min + ((i - 1) + 0.5) * dx;
+                double y = c->y_min + ((j - 1) + 0.5) * dx;
+                double z = c->z_min + ((k - 1) + 0.5) * dx;
+                double gH = h->gH[(size_t)j * h->nx_t + (size_t)i];
+                if (!h->mask_override)
+                {
+                    if (!c->use_geometry) h->mask[idx] = FLUID;
+                    else h->mask[idx] = (z < gH) ? SOLID : FLUID;
+                    if (z > sky_z) h->mask[idx] = FLUID;
+                }
+                double d = 1e30;
+                if (sf & (1u << LBM_FACE_XLO)) d = dmin(d, x - c->x_min);
+                if (sf & (1u << LBM_FACE_XHI)) d = dmin(d, c->x_max - x);
+                if (sf & (1u << LBM_FACE_YLO)) d = dmin(d, y - c->y_min);
+                if (sf & (1u << LBM_FACE_YHI)) d = dmin(d, c->y_max - y);
+                if (sf & (1u << LBM_FACE_ZLO)) d = dmin(d, z - c->z_min);
+                if (sf & (1u << LBM_FACE_ZHI)) d = dmin(d, c->z_max - z);
+                if (d < sponge_w)
+                {
+                    double r = (sponge_w - d) / sponge_w;
+                    h->sponge[idx] = strength * r * r;
+                }
+                else
+                {
+                    h->sponge[idx] = 0.0;
+                }
+            }
+
+    if (h->mask_override) return;
+    /* Halo rules (06:509-531): x faces, then y faces, then z faces. */
+    const unsigned char mx0 = c->face_bc[LBM_FACE_XLO] == LBM_BC_WALL ? SOLID : FLUID;
+    const unsigned char mx1 = c->face_bc[LBM_FACE_XHI] == LBM_BC_WALL ? SOLID : FLUID;
+    const unsigned char my0 = c->face_bc[LBM_FACE_YLO] == LBM_BC_WALL ? SOLID : FLUID;
+    const unsigned char my1 = c->face_bc[LBM_FACE_YHI] == LBM_BC_WALL ? SOLID : FLUID;
+    const unsigned char mz0 = c->face_bc[LBM_FACE_ZLO] == LBM_BC_WALL ? SOLID : FLUID;
+    const unsigned char mz1 = c->face_bc[LBM_FACE_ZHI] == LBM_BC_WALL ? SOLID : FLUID;
+    for (int k = 0; k <= h->nz + 1; ++k)
+        for (int j = 0; j <= h->ny + 1; ++j)
+        {
+            h->mask[loc(h, 0, j, k)] = mx0;
+            h->mask[loc(h, h->nx + 1, j, k)] = mx1;
+        }
+    for (int k = 0; k <= h->nz + 1; ++k)
+        for (int i = 0; i <= h->nx + 1; ++i)
+        {
+            h->mask[loc(h, i, 0, k)] = my0;
+            h->mask[loc(h, i, h->ny + 1, k)] = my1;
+        }
+    for (int j = 0; j <= h->ny + 1; ++j)
+        for (int i = 0; i <= h->nx + 1; ++i)
+        {
+            h->mask[loc(h, i, j, 0)] = mz0;
+            h->mask[loc(h, i, j, h->nz + 1)] = mz1;
+        }
+}
+
+int orc_init(orc_handle* h)
+{
+    const lbm_config* c = &h->cfg;
+    /* 06:332-334 */
+    h->NXg = (int)((c->x_max - c->x_min) / c->dx + 0.5);
+    h->NYg = (int)((c->y_max - c->y_min) / c->dx + 0.5);
+    h->NZg = (int)((c->z_max - c->z_min) / c->dx + 0.5);
+    h->nx = h->NXg; h->ny = h->NYg; h->nz = h->NZg;
+    h->nx_t = h->nx + 2; h->ny_t = h->ny + 2; h->nz_t = h->nz + 2;
+    h->Nloc = (size_t)h->nx_t * h->ny_t * h->nz_t;
+    h->dt = (CS * c->dx) / c->c_phys;   /* UnitConverter::get_dt_phys 06:200-203 */
+
+    int had_mask = h->mask != NULL && h->mask_override;
+    unsigned char* keep = NULL;
+    if (had_mask) { keep = h->mask; h->mask = NULL; }
+    free(h->f_curr); free(h->f_next); free(h->rho); free(h->sponge); free(h->gH); free(h->mask);
+    h->f_curr = (double*)malloc(h->Nloc * Q * sizeof(double));
+    h->f_next = (double*)calloc(h->Nloc * Q, sizeof(double));
+    h->rho = (double*)malloc(h->Nloc * sizeof(double));
+    h->sponge = (double*)calloc(h->Nloc, sizeof(double));
+    h->gH = (double*)malloc((size_t)h->nx_t * h->ny_t * sizeof(double));
+    h->mask = keep ? keep : (unsigned char*)calloc(h->Nloc, 1);
+    if (!h->f_curr || !h->f_next || !h->rho || !h->sponge || !h->gH || !h->mask) return LBM_ERR_OUT_OF_MEMORY;
+    for (size_t i = 0; i < h->Nloc; ++i) h->rho[i] = 1.0;
+
+    double feq0[Q];
+    for (int q = 0; q < Q; ++q) feq0[q] = feq(q, 1.0, 0.0, 0.0, 0.0);
+    #pragma omp parallel for
+    for (long i = 0; i < (long)h->Nloc; ++i)
+        for (int q = 0; q < Q; ++q) h->f_curr[(size_t)i * Q + q] = feq0[q];
+
+    init_domain(h);
+
+    int status = LBM_OK;
+    free(h->probe_idx);
+    h->probe_idx = (long*)malloc((size_t)(h->nprobe > 0 ? h->nprobe : 1) * sizeof(long));
+    for (int p = 0; p < h->nprobe; ++p)
+    {
+        /* 06:415-437 */
+        int gi = (int)floor((h->probe_xyz[3 * p] - c->x_min) / c->dx);
+        int gj = (int)floor((h->probe_xyz[3 * p + 1] - c->y_min) / c->dx);
+        int gk = (int)floor((h->probe_xyz[3 * p + 2] - c->z_min) / c->dx);
+        h->probe_idx[p] = -1;
+        if (gi >= 0 && gi < h->nx && gj >= 0 && gj < h->ny && gk >= 0 && gk < h->nz)
+        {
+            h->probe_idx[p] = (long)loc(h, gi + 1, gj + 1, gk + 1);
+            if (h->mask[h->probe_idx[p]] == SOLID) status = LBM_WARN_PROBE_IN_SOLID;
+        }
+    }
+    free(h->series);
+    h->series = NULL;
+    h->steps_rec = h->steps_cap = 0;
+    h->step = 0;
+    return status;
+}
+
+/* ---------------------------------------------------------------- source */
+
+/* DroneSource::update (06:221-238) */
+static void drone_update(src_t* s, double t)
+{
+    double dx = s->s.ex - s->s.sx, dy = s->s.ey - s->s.sy, dz = s->s.ez - s->s.sz;
+    double dist_total = sqrt(dx * dx + dy * dy + dz * dz);
+    if (dist_total < 1e-12 || s->s.speed < 1e-12)
+    {
+        s->cx = s->s.sx; s->cy = s->s.sy; s->cz = s->s.sz;
+        return;
+    }
+    double travel_time = dist_total / s->s.speed;
+    double r = t / travel_time;
+    if (r > 1.0) r = 1.0;
+    s->cx = s->s.sx + r * dx;
+    s->cy = s->s.sy + r * dy;
+    s->cz = s->s.sz + r * dz;
+}
+
+static double source_value(const orc_handle* h, const src_t* s, double t)
+{
+    const lbm_source* p = &s->s;
+    switch (p->waveform)
+    {
+    case LBM_WAVE_GAUSS:   /* 06:579-581 */
+        return p->amp * exp(-0.5 * pow((t - p->t0) / p->sigma_t, 2));
+    case LBM_WAVE_SINE:    /* 08:543 */
+        return p->amp * sin(2.0 * PI_ * p->freq * t);
+    case LBM_WAVE_RICKER:
+    {
+        double a = PI_ * p->freq * (t - p->t0);
+        a = a * a;
+        return p->amp * (1.0 - 2.0 * a) * exp(-a);
+    }
+    case LBM_WAVE_TABLE:
+    {
+        long s_idx = lround(t / h->dt);
+        if (s_idx < 0 || s_idx >= p->table_len) return 0.0;
+        return p->amp * p->table[s_idx];
+    }
+    }
+    return 0.0;
+}
+
+static int cell_in_grid(const orc_handle* h, int gi, int gj, int gk)
+{
+    return !(gi < 0 || gi >= h->NXg || gj < 0 || gj >= h->NYg || gk < 0 || gk >= h->NZg);
+}
+
+/* LBMSolver::apply_source (06:576-667; 08:540-628 for the sine), one source. */
+static void apply_one_source(orc_handle* h, src_t* s, double t)
+{
+    const lbm_config* c = &h->cfg;
+    const double dt = h->dt;
+    const double DX = c->dx;
+    const double val = source_value(h, s, t);
+    const double source_gain = s->s.gain;
+    drone_update(s, t);
+
+    if (s->s.injection == LBM_INJECT_TRILINEAR)
+    {
+        double fx = (s->cx - c->x_min) / DX - 0.5;
+        double fy = (s->cy - c->y_min) / DX - 0.5;
+        double fz = (s->cz - c->z_min) / DX - 0.5;
+        int i0 = (int)floor(fx), j0 = (int)floor(fy), k0 = (int)floor(fz);
+        double tx = fx - i0, ty = fy - j0, tz = fz - k0;
+        double sumw = 0.0;
+        for (int b = 0; b < 8; ++b)
+        {
+            int gi = i0 + (b & 1), gj = j0 + ((b >> 1) & 1), gk = k0 + (b >> 2);
+            if (!cell_in_grid(h, gi, gj, gk)) continue;
+            double ww = ((b & 1) ? tx : 1.0 - tx) * (((b >> 1) & 1) ? ty : 1.0 - ty) * ((b >> 2) ? tz : 1.0 - tz);
+            if (h->mask[loc(h, gi + 1, gj + 1, gk + 1)] == FLUID) sumw += ww;
+        }
+        if (sumw < 1e-30) return;
+        const double A = (val * dt * source_gain) / sumw;
+        for (int b = 0; b < 8; ++b)
+        {
+            int gi = i0 + (b & 1), gj = j0 + ((b >> 1) & 1), gk = k0 + (b >> 2);
+            if (!cell_in_grid(h, gi, gj, gk)) continue;
+            size_t idx = loc(h, gi + 1, gj + 1, gk + 1);
+            if (h->mask[idx] != FLUID) continue;
+            double ww = ((b & 1) ? tx : 1.0 - tx) * (((b >> 1) & 1) ? ty : 1.0 - ty) * ((b >> 2) ? tz : 1.0 - tz);
+            const double add = A * ww;
+            for (int q = 0; q < Q; ++q) h->f_curr[idx * Q + q] += W[q] * add;
+        }
+        return;
+    }
+
+    const int R = s->s.radius;
+    const double sigma_cells = s->s.sigma_cells;
+    const double sigma2 = (sigma_cells * DX) * (sigma_cells * DX);
+    const int ic = (int)floor((s->cx - c->x_min) / DX);
+    const int jc = (int)floor((s->cy - c->y_min) / DX);
+    const int kc = (int)floor((s->cz - c->z_min) / DX);
+    if (ic < -R || ic >= h->NXg + R || jc < -R || jc >= h->NYg + R || kc < -R || kc >= h->NZg + R) return;
+
+    double sumw = 0.0;
+    for (int gk = kc - R; gk <= kc + R; ++gk)
+        for (int gj = jc - R; gj <= jc + R; ++gj)
+            for (int gi = ic - R; gi <= ic + R; ++gi)
+            {
+                if (!cell_in_grid(h, gi, gj, gk)) continue;
+                const double x = c->x_min + (gi + 0.5) * DX;
+                const double y = c->y_min + (gj + 0.5) * DX;
+                const double z = c->z_min + (gk + 0.5) * DX;
+                const double ddx = x - s->cx, ddy = y - s->cy, ddz = z - s->cz;
+                const double r2 = ddx * ddx + ddy * ddy + ddz * ddz;
+                const double ww = exp(-0.5 * r2 / sigma2);
+                if (h->mask[loc(h, gi + 1, gj + 1, gk + 1)] == FLUID) sumw += ww;
+            }
+    if (sumw < 1e-30) return;
+    const double A = (val * dt * source_gain) / sumw;
+    for (int gk = kc - R; gk <= kc + R; ++gk)
+        for (int gj = jc - R; gj <= jc + R; ++gj)
+            for (int gi = ic - R; gi <= ic + R; ++gi)
+            {
+                if (!cell_in_grid(h, gi, gj, gk)) continue;
+                const double x = c->x_min + (gi + 0.5) * DX;
+                const double y = c->y_min + (gj + 0.5) * DX;
+                const double z = c->z_min + (gk + 0.5) * DX;
+                const double ddx = x - s->cx, ddy = y - s->cy, ddz = z - s->cz;
+                const double r2 = ddx * ddx + ddy * ddy + ddz * ddz;
+                const double ww = exp(-0.5 * r2 / sigma2);
+                const size_t idx = loc(h, gi + 1, gj + 1, gk + 1);
+                if (h->mask[idx] != FLUID) continue;
+                const double add = A * ww;
+                for (int q = 0; q < Q; ++q) h->f_curr[idx * Q + q] += W[q] * add;
+            }
+}
+
+void orc_apply_source(orc_handle* h, double t)
+{
+    for (int i = 0; i < h->nsrc; ++i) apply_one_source(h, &h->srcs[i], t);
+}
+
+/* ---------------------------------------------------------------- halos */
+
+/* LBMSolver::macro_at (06:545-568) */
+static void macro_at(const orc_handle* h, size_t idx, double* r, double* ux, double* uy, double* uz)
+{
+    *r = *ux = *uy = *uz = 0.0;
+    const size_t base = idx * Q;
+    for (int q = 0; q < Q; ++q)
+    {
+        const double fq = h->f_curr[base + q];
+        *r += fq;
+        *ux += fq * EX[q];
+        *uy += fq * EY[q];
+        *uz += fq * EZ[q];
+    }
+    if (*r > 1e-30)
+    {
+        *ux /= *r; *uy /= *r; *uz /= *r;
+    }
+    else
+    {
+        *r = 1.0;
+        *ux = *uy = *uz = 0.0;
+    }
+}
+
+/* Ghost populations for one open-face cell from its interior neighbour
+ * (06:689-707 pattern): axis 0/1/2, side 0 = low face, 1 = high face. */
+static void nscbc_ghost(const orc_handle* h, size_t idxI, int axis, int side, double* out)
+{
+    double rI, u[3];
+    macro_at(h, idxI, &rI, &u[0], &u[1], &u[2]);
+    const double pI = CS2 * (rI - 1.0);
+    double Wp, Wm, unB, pB;
+    if (side == 0)
+    {
+        Wp = 0.0;
+        Wm = u[axis] - pI / CS;
+    }
+    else
+    {
+        Wm = 0.0;
+        Wp = u[axis] + pI / CS;
+    }
+    unB = 0.5 * (Wp + Wm);
+    pB = 0.5 * CS * (Wp - Wm);
+    const double rhoB = 1.0 + pB / CS2;
+    double uB[3] = {u[0], u[1], u[2]};
+    uB[axis] = unB;
+    const size_t baseI = idxI * Q;
+    for (int q = 0; q < Q; ++q)
+    {
+        const double feqI = feq(q, rI, u[0], u[1], u[2]);
+        const double feqB = feq(q, rhoB, uB[0], uB[1], uB[2]);
+        out[q] = feqB + (h->f_curr[baseI + q] - feqI);
+    }
+}
+
+/* LBMSolver::exchange_halos (06:671-904) at MPI size 1: every halo cell is
+ * rewritten from interior cells only, so the evaluation order of the faces
+ * does not matter; edge/corner halo cells hold w_q. */
+void orc_exchange_halos(orc_handle* h)
+{
+    const lbm_config* c = &h->cfg;
+    const int nx = h->nx, ny = h->ny, nz = h->nz;
+    double feq0[Q];
+    for (int q = 0; q < Q; ++q) feq0[q] = feq(q, 1.0, 0.0, 0.0, 0.0);
+
+    /* x faces: j 1..ny, k 1..nz (06:684-736, unpack 06:853-859) */
+    for (int side = 0; side < 2; ++side)
+    {
+        const int nscbc = c->face_bc[LBM_FACE_XLO + side] == LBM_BC_NSCBC;
+        const int ig = side ? nx + 1 : 0, ii = side ? nx : 1;
+        #pragma omp parallel for
+        for (int k = 1; k <= nz; ++k)
+            for (int j = 1; j <= ny; ++j)
+            {
+                double g[Q];
+                if (nscbc) nscbc_ghost(h, loc(h, ii, j, k), 0, side, g);
+                else memcpy(g, feq0, sizeof g);
+                double* dst = &h->f_curr[loc(h, ig, j, k) * Q];
+                /* ghosts read only interior cells; writing in place is safe */
+                for (int q = 0; q < Q; ++q) dst[q] = g[q];
+            }
+    }
+    /* y faces: i 0..nx+1 (edges w_q), k 1..nz (06:738-802, unpack 06:875-881) */
+    for (int side = 0; side < 2; ++side)
+    {
+        const int nscbc = c->face_bc[LBM_FACE_YLO + side] == LBM_BC_NSCBC;
+        const int jg = side ? ny + 1 : 0, ji = side ? ny : 1;
+        #pragma omp parallel for
+        for (int k = 1; k <= nz; ++k)
+            for (int i = 0; i <= nx + 1; ++i)
+            {
+                double g[Q];
+                if (nscbc && i != 0 && i != nx + 1) nscbc_ghost(h, loc(h, i, ji, k), 1, side, g);
+                else memcpy(g, feq0, sizeof g);
+                double* dst = &h->f_curr[loc(h, i, jg, k) * Q];
+                for (int q = 0; q < Q; ++q) dst[q] = g[q];
+            }
+    }
+    /* z faces: all i, j (edges w_q) (06:804-835, unpack 06:897-903) */
+    for (int side = 0; side < 2; ++side)
+    {
+        const int nscbc = c->face_bc[LBM_FACE_ZLO + side] == LBM_BC_NSCBC;
+        const int kg = side ? nz + 1 : 0, ki = side ? nz : 1;
+        #pragma omp parallel for
+        for (int j = 0; j <= ny + 1; ++j)
+            for (int i = 0; i <= nx + 1; ++i)
+            {
+                double g[Q];
+                if (nscbc && i != 0 && i != nx + 1 && j != 0 && j != ny + 1)
+                    nscbc_ghost(h, loc(h, i, j, ki), 2, side, g);
+                else memcpy(g, feq0, sizeof g);
+                double* dst = &h->f_curr[loc(h, i, j, kg) * Q];
+                for (int q = 0; q < Q; ++q) dst[q] = g[q];
+            }
+    }
+}
+
+/* ---------------------------------------------------------------- step */
+
+/* LBMSolver::step_collision_bgk (06:906-972) */
+void orc_step_collision_bgk(orc_handle* h)
+{
+    const double omega = 1.0 / h->cfg.tau;
+    const int nx = h->nx, ny = h->ny, nz = h->nz;
+    #pragma omp parallel for collapse(2)
+    for (int k = 1; k <= nz; ++k)
+        for (int j = 1; j <= ny; ++j)
+            for (int i = 1; i <= nx; ++i)
+            {
+                size_t dst = loc(h, i, j, k);
+                double f_in[Q];
+                for (int q = 0; q < Q; ++q)
+                {
+                    size_t src = loc(h, i - EX[q], j - EY[q], k - EZ[q]);
+                    if (h->mask[src] == SOLID) f_in[q] = h->f_curr[dst * Q + h->inv_q[q]];
+                    else f_in[q] = h->f_curr[src * Q + q];
+                }
+                if (h->mask[dst] == SOLID)
+                {
+                    for (int q = 0; q < Q; ++q) h->f_next[dst * Q + q] = f_in[q];
+                    h->rho[dst] = 1.0;
+                    continue;
+                }
+                double r = 0, jx = 0, jy = 0, jz = 0;
+                for (int q = 0; q < Q; ++q)
+                {
+                    r += f_in[q];
+                    jx += f_in[q] * EX[q];
+                    jy += f_in[q] * EY[q];
+                    jz += f_in[q] * EZ[q];
+                }
+                if (r <= 0.0) r = 1e-12;
+                double ux = jx / r, uy = jy / r, uz = jz / r;
+                h->rho[dst] = r;
+                double sponge = h->sponge[dst];
+                for (int q = 0; q < Q; ++q)
+                {
+                    double feq_q = feq(q, r, ux, uy, uz);
+                    double f_post = f_in[q] - omega * (f_in[q] - feq_q);
+                    if (sponge > 1e-12)
+                    {
+                        double feq0 = feq(q, 1.0, 0.0, 0.0, 0.0);
+                        f_post = (1.0 - sponge) * f_post + sponge * feq0;
+                    }
+                    h->f_next[dst * Q + q] = f_post;
+                }
+            }
+    double* t = h->f_curr;
+    h->f_curr = h->f_next;
+    h->f_next = t;
+}
+
+/* Probe record (06:1085-1092) */
+void orc_record_probes(orc_handle* h)
+{
+    if (h->nprobe == 0) return;
+    if (h->steps_rec == h->steps_cap)
+    {
+        h->steps_cap = h->steps_cap ? 2 * h->steps_cap : 1024;
+        h->series = (double*)realloc(h->series, (size_t)h->steps_cap * h->nprobe * sizeof(double));
+    }
+    double* row = h->series + (size_t)h->steps_rec * h->nprobe;
+    for (int p = 0; p < h->nprobe; ++p)
+        row[p] = h->probe_idx[p] >= 0 ? h->rho[h->probe_idx[p]] - 1.0 : NAN;
+    h->steps_rec++;
+}
+
+/* The body of LBMSolver::run (06:1077-1092) for steps s .. s+n-1. */
+void orc_step(orc_handle* h, int nsteps)
+{
+    for (int n = 0; n < nsteps; ++n)
+    {
+        const double t = h->step * h->dt;
+        orc_apply_source(h, t);
+        orc_exchange_halos(h);
+        orc_step_collision_bgk(h);
+        orc_record_probes(h);
+        h->step++;
+    }
+}
+
+/* ---------------------------------------------------------------- access */
+
+void orc_get_dims(orc_handle* h, int* n3, int* n3_halo)
+{
+    if (n3) { n3[0] = h->NXg; n3[1] = h->NYg; n3[2] = h->NZg; }
+    if (n3_halo) { n3_halo[0] = h->nx_t; n3_halo[1] = h->ny_t; n3_halo[2] = h->nz_t; }
+}
+double orc_get_dt(orc_handle* h) { return h->dt; }
+void orc_get_f(orc_handle* h, double* out) { memcpy(out, h->f_curr, h->Nloc * Q * sizeof(double)); }
+void orc_set_f(orc_handle* h, const double* in) { memcpy(h->f_curr, in, h->Nloc * Q * sizeof(double)); }
+void orc_get_mask(orc_handle* h, unsigned char* out) { memcpy(out, h->mask, h->Nloc); }
+void orc_get_rho(orc_handle* h, double* out) { memcpy(out, h->rho, h->Nloc * sizeof(double)); }
+void orc_get_sponge(orc_handle* h, double* out) { memcpy(out, h->sponge, h->Nloc * sizeof(double)); }
+void orc_get_ground_height(orc_handle* h, double* out)
+{
+    memcpy(out, h->gH, (size_t)h->nx_t * h->ny_t * sizeof(double));
+}
+long orc_get_probes(orc_handle* h, double* out, long capacity)
+{
+    long n = h->steps_rec * h->nprobe;
+    if (n > capacity) return -1;
+    if (n) memcpy(out, h->series, (size_t)n * sizeof(double));
+    return h->steps_rec;
+}
