@@ -1,0 +1,363 @@
+"""Benchmark of the fused D3Q19 acoustic step on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step = one full time step of the synthetic-city workload (source
+injection, open-boundary ghost fill, fused stream+bounce-back+BGK+sponge
+kernel, probe sampling).  Headline workload: the 2048x2048x256 synthetic
+city with FP16 deviation storage (1.07 G cells).  Also measured on one GPU:
+FP32 and FP16 storage on the 1024x1024x256 city (the FP16/FP32 ratio) and the
+end-to-end rate through the C-ABI with host buffers.  Multi-GPU runs are
+independent replicas (one per rank, no data exchange), value = all ranks'
+cell updates / the slowest rank's device time.
+
+--impl reference times the reference solver's own CPU step
+(06_transient_localization_dx1.cpp:576-972 via oracle/_ref, or the FP64
+oracle port where the reference was not built) on a bounded sub-domain of the
+same city with all host threads.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "city-scale-nlos-acoustic-engine-code_b200"))
+sys.path.insert(0, REPO)
+
+METRIC = "D3Q19 GLUPS, %HBM peak: FP16-store vs FP32 @<=1e-3 probe L2; adjoint grad/s"
+UNIT = "GLUPS"
+
+
+def measured_peaks():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+            except (ValueError, IndexError):
+                continue
+            for n, v in zip(names, r[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+# ---------------------------------------------------------------------------- our arm
+
+def make_solver(name, storage, device):
+    import nlos_lbm
+    from nlos_lbm import workloads
+
+    w = workloads.build(name, storage=storage)
+    w["cfg"].device = device
+    t0 = time.time()
+    s = nlos_lbm.Solver(w["cfg"], w["sources"], w["probes"], triangles=w["triangles"])
+    return s, w, time.time() - t0
+
+
+def device_timed_steps(solver, steps, torch, barrier):
+    """Runs `steps` steps bracketed by CUDA events on the library's stream."""
+    stream = torch.cuda.ExternalStream(solver.stream)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    solver.synchronize()
+    torch.cuda.synchronize()
+    barrier()
+    e0.record(stream)
+    solver.step(steps)
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    barrier()
+    return e0.elapsed_time(e1)
+
+
+def measure(name, storage, steps, warmup, device, torch, barrier, reduce_max, kernel_timing=True):
+    from nlos_lbm import workloads
+
+    s, w, setup_s = make_solver(name, storage, device)
+    nx, ny, nz = workloads.cells(w["cfg"])
+    ncell = nx * ny * nz
+    s.step(warmup)
+    s.set_kernel_timing(kernel_timing)
+    l0 = s.launch_count
+    ms = device_timed_steps(s, steps, torch, barrier)
+    launches = s.launch_count - l0
+    kms, kn = s.kernel_time()
+    s.set_kernel_timing(False)
+    ms_max = reduce_max(ms)
+    probes = s.get_probes()
+    res = dict(name=name, storage="fp16" if storage == 1 else "fp32", cells=ncell, dims=[nx, ny, nz],
+               steps=steps, ms=ms_max, ms_local=ms, setup_s=setup_s, glups_rank=ncell * steps / (ms_max / 1e3) / 1e9,
+               kernel_ms_avg=kms / max(kn, 1), kernel_launches=kn, launches=launches,
+               bytes_per_cell=s.bytes_per_cell, probes_finite=bool(np.all(np.isfinite(probes))),
+               description=w["description"], coverage=w.get("coverage"))
+    return s, w, res
+
+
+def e2e_measure(solver, w, steps):
+    """Through the C-ABI with host buffers: the source amplitude series goes
+    host->device (lbm_add_source with a table waveform, uploaded inside
+    lbm_step) and the probe series device->host (lbm_get_probes)."""
+    from nlos_lbm import abi
+
+    base = w["sources"][0]
+    s0 = solver.step_count
+    table = np.zeros(s0 + steps)
+    t = np.arange(s0, s0 + steps, dtype=np.float64)
+    table[s0:] = np.sin(2 * np.pi * t / 40.0)
+    solver.get_probes()   # drain earlier rows
+    h0, d0 = solver.transfer_bytes()
+    t0 = time.perf_counter()
+    solver.clear_sources()
+    src = abi.reference_source(sx=base.sx, sy=base.sy, sz=base.sz, ex=base.ex, ey=base.ey, ez=base.ez,
+                               speed=base.speed, amp=base.amp, waveform=abi.LBM_WAVE_TABLE,
+                               injection=base.injection)
+    src.table = table.ctypes.data_as(abi.c_double_p)
+    src.table_len = len(table)
+    solver.add_source(src)
+    solver.step(steps)
+    series = solver.get_probes()
+    t1 = time.perf_counter()
+    h1, d1 = solver.transfer_bytes()
+    assert series.shape[0] >= steps
+    return (t1 - t0) * 1e3, (h1 - h0) / steps, (d1 - d0) / steps
+
+
+def cpu_baseline(steps_hint=None):
+    """Reference CPU step on a bounded sub-domain of the city (rank 0, N=1)."""
+    import oracle
+
+    from nlos_lbm import workloads
+    from nlos_lbm.solver import city_triangles, stl_write
+
+    nx, ny, nz = 256, 256, 128
+    tris, _ = city_triangles(nx, ny, seed=2024, fp=(20, 60), height=(10, 80), coverage=0.40, street=8, margin=40)
+    threads = os.cpu_count() or 1
+    if oracle.ref_available("06"):
+        stl = "/tmp/bench_city_sample.stl"
+        stl_write(stl, tris)
+        ref = oracle.RefSolver("06", (0, nx), (0, ny), (0, nz), 1.0, 0.51, (128.5, 128.5, 2.5, 128.5, 128.5, 2.5,
+                                                                           0.0, 10.0, 0.0), stl=stl)
+        kind = "reference"
+
+        def run(n):
+            ref.step(n)
+    else:
+        cfg = workloads.lattice_config(nx, ny, nz, 0.51)
+        from nlos_lbm import abi
+        src = abi.reference_source(sx=128.5, sy=128.5, sz=2.5, ex=128.5, ey=128.5, ez=2.5, amp=1e-3, t0=40.0,
+                                   sigma_t=8.0)
+        orc = oracle.OracleSolver(cfg, [src], None, triangles=tris)
+        kind = "port"
+
+        def run(n):
+            orc.step(n)
+    run(1)   # warm-up
+    t0 = time.perf_counter()
+    run(2)
+    per = (time.perf_counter() - t0) / 2
+    n = steps_hint or max(2, min(200, int(12.0 / max(per, 1e-6))))
+    t0 = time.perf_counter()
+    run(n)
+    dt = time.perf_counter() - t0
+    cells = nx * ny * nz
+    return dict(value=cells * n / dt / 1e9, unit=UNIT, cores=threads, kind=kind,
+                sample=f"{nx}x{ny}x{nz} sub-domain of the seeded city, {n} full steps "
+                       f"(apply_source+exchange_halos+step_collision_bgk), FP64, {threads} OpenMP threads",
+                seconds=dt, steps=n)
+
+
+def run_reference_arm(args):
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    import oracle
+
+    oracle_kind = "reference" if oracle.ref_available("06") else "port"
+    # warm-up + timed steps on the bounded sample
+    b = cpu_baseline(steps_hint=max(1, args.steps))
+    line = {"metric": METRIC, "value": b["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": b["steps"],
+            "warmup": args.warmup, "ms_per_step": b["seconds"] / b["steps"] * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": "synthetic city (seeded boxes), 256x256x128 sub-domain of the city workload",
+                       "sample": b["sample"]},
+            "cpu_baseline": {"value": b["value"], "unit": UNIT, "cores": b["cores"], "kind": oracle_kind,
+                             "sample": b["sample"]},
+            "e2e": {"value": b["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_our_arm(args):
+    import torch
+
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def reduce_max(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    hbm_peak, peak_kind = measured_peaks()
+    headline = args.workload
+    with ClockSampler(local) as clk:
+        s, w, head = measure(headline, None, args.steps, args.warmup, local, torch, barrier, reduce_max)
+    clocks = clk.summary()
+    # e2e through the C-ABI with host buffers (same workload, same handle)
+    e2e_ms, h2d_ps, d2h_ps = e2e_measure(s, w, args.steps)
+    e2e_ms = reduce_max(e2e_ms)
+    del s
+    import gc
+
+    gc.collect()
+
+    secondary = {}
+    if world == 1 and not args.headline_only:
+        for nm, st in (("city1024", 0), ("city1024", 1)):
+            s2, _, r = measure(nm, st, args.steps, args.warmup, local, torch, barrier, reduce_max)
+            secondary[f"{nm}_{r['storage']}"] = {k: r[k] for k in ("glups_rank", "ms", "kernel_ms_avg", "dims",
+                                                                    "bytes_per_cell")}
+            secondary[f"{nm}_{r['storage']}"]["hbm_frac_kernel"] = (
+                r["cells"] * r["bytes_per_cell"] / (r["kernel_ms_avg"] / 1e3) / 1e9 / hbm_peak)
+            del s2
+            gc.collect()
+
+    n = world
+    cells, steps = head["cells"], head["steps"]
+    value = n * cells * steps / (head["ms"] / 1e3) / 1e9
+    achieved = cells * head["bytes_per_cell"] / (head["kernel_ms_avg"] / 1e3) / 1e9
+    traffic = None
+    tpath = os.path.join(REPO, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as fh:
+            traffic = json.load(fh).get(f"{headline}_{head['storage']}")
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": n, "steps": steps, "warmup": args.warmup,
+        "ms_per_step": head["ms"] / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "fp16-store/fp32-compute" if head["storage"] == "fp16" else "fp32",
+        "data": "synthetic (seeded box city voxelised from STL triangles)",
+        "config": {"workload": f"{headline}: {head['description']}", "grid": head["dims"],
+                   "storage": head["storage"], "plan_coverage": head["coverage"],
+                   "parallelism": f"replicas x{n}" if n > 1 else "single GPU",
+                   "l2": "inputs larger than L2 (populations %.1f GB per step)" % (cells * head["bytes_per_cell"] / 1e9)},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                     "frac": achieved / hbm_peak, "traffic": traffic, "peak_kind": peak_kind,
+                     "kernel": "k_step (fused pull-stream + bounce-back + BGK + sponge)",
+                     "kernel_ms": head["kernel_ms_avg"], "bytes_per_cell": head["bytes_per_cell"]},
+        "e2e": {"value": n * cells * steps / (e2e_ms / 1e3) / 1e9, "unit": UNIT, "h2d_bytes_per_step": h2d_ps,
+                "d2h_bytes_per_step": d2h_ps},
+        "gpu_launches": head["launches"],
+        "clocks": clocks,
+        "probes_finite": head["probes_finite"],
+        "secondary": secondary,
+    }
+    if secondary.get("city1024_fp32") and secondary.get("city1024_fp16"):
+        line["fp16_over_fp32"] = secondary["city1024_fp16"]["glups_rank"] / secondary["city1024_fp32"]["glups_rank"]
+    if world == 1 and rank == 0 and not args.no_cpu:
+        line["cpu_baseline"] = {k: v for k, v in cpu_baseline().items() if k in ("value", "unit", "cores", "kind",
+                                                                                  "sample")}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="city2048", choices=["city2048", "city1024", "lloyd", "scatter"])
+    ap.add_argument("--headline-only", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    return run_our_arm(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

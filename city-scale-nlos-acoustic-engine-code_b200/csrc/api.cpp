@@ -1,0 +1,1274 @@
+// C-ABI of the B200 D3Q19 acoustic solver (include/nlos_lbm.h).
+//
+// Host side of LBMSolver (06_transient_localization_dx1.cpp:241-1122): the
+// grid/mask/sponge/probe set-up of init() and the source schedule of
+// apply_source() are computed here in FP64 exactly as the reference does; the
+// per-cell work runs in the sm_100a kernels of kernels.cu.  Compiled with
+// -ffp-contract=off so the FP64 host arithmetic keeps the reference's
+// rounding.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "device.hpp"
+#include "geometry.hpp"
+#include "lattice.cuh"
+#include "nlos_lbm.h"
+
+using namespace lbm;
+
+namespace {
+
+constexpr int kTableRows = 4096;   // source-schedule rows resident on the device
+constexpr int kProbeRows = 4096;   // probe-series rows buffered on the device
+
+struct SourceState
+{
+    lbm_source s;
+    std::vector<double> table;
+};
+
+template <typename T>
+T* dalloc(size_t n, cudaError_t& err)
+{
+    void* p = nullptr;
+    if (err == cudaSuccess) err = cudaMalloc(&p, n * sizeof(T));
+    return (T*)p;
+}
+
+}  // namespace
+
+struct lbm_handle
+{
+    lbm_config cfg{};
+    std::string err;
+    int storage = LBM_STORE_F32;
+    float scale = 1.0f;
+
+    // geometry / mask
+    HeightField geo;
+    int stl_status = LBM_OK;
+    std::vector<uint8_t> mask_override;
+    int mo_dims[3] = {0, 0, 0};
+
+    std::vector<SourceState> srcs;
+    std::vector<double> probe_xyz;
+
+    // set-up results
+    bool inited = false;
+    int NXg = 0, NYg = 0, NZg = 0;
+    double dt = 0.0;
+    Layout L{};
+    std::vector<uint8_t> mask;           // reference layout, halo-inclusive
+    std::vector<long long> probe_cell;   // device linear cell, -1 unowned
+    std::vector<int> probe_owned, probe_solid;
+
+    // device state
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    void* f_alloc[2] = {nullptr, nullptr};
+    void* f[2] = {nullptr, nullptr};   // origin pointers (alloc + front pad)
+    int cur = 0;
+    uint32_t* links = nullptr;
+    uint32_t* near = nullptr;
+    float* sig = nullptr;              // sig_x | sig_y | sig_z
+    StepArgs sa{};
+    GhostArgs ga{};
+    Control* ctl = nullptr;            // device
+    Control* ctl_host = nullptr;       // pinned staging
+    SourceEntry* d_table = nullptr;
+    SourceEntry* h_table = nullptr;    // pinned
+    long long table_base = 0, table_rows = 0;
+    long long* d_probe_cell = nullptr;
+    double* d_probe_out = nullptr;
+    double* h_probe_out = nullptr;     // pinned
+    double* d_energy = nullptr;
+    long long probe_pending = 0;        // rows recorded on the device, not yet on the host
+    std::vector<double> series;
+    bool halo_dirty = false;
+
+    long long step = 0;                // completed time steps
+    long launches = 0;
+    long h2d_bytes = 0, d2h_bytes = 0;
+
+    // graphs: two full steps starting from buffer 0
+    cudaGraphExec_t graph = nullptr;
+    int graph_kernels = 0;
+
+    // kernel timing
+    bool timing = false;
+    std::vector<cudaEvent_t> ev;
+    size_t ev_used = 0;
+    double kernel_ms = 0.0;
+    long kernel_launches = 0;
+
+    ~lbm_handle() { release(); }
+
+    int fail(int code, const std::string& msg)
+    {
+        err = msg;
+        return code;
+    }
+    int cuda_fail(cudaError_t e, const char* where)
+    {
+        err = std::string(where) + ": " + cudaGetErrorString(e);
+        return e == cudaErrorMemoryAllocation ? LBM_ERR_OUT_OF_MEMORY : LBM_ERR_CUDA;
+    }
+
+    void release()
+    {
+        if (graph) cudaGraphExecDestroy(graph);
+        graph = nullptr;
+        for (auto e : ev) cudaEventDestroy(e);
+        ev.clear();
+        ev_used = 0;
+        for (int b = 0; b < 2; ++b)
+        {
+            if (f_alloc[b]) cudaFree(f_alloc[b]);
+            f_alloc[b] = f[b] = nullptr;
+        }
+        cudaFree(links); links = nullptr;
+        cudaFree(near); near = nullptr;
+        cudaFree(sig); sig = nullptr;
+        cudaFree(ctl); ctl = nullptr;
+        cudaFree(d_table); d_table = nullptr;
+        cudaFree(d_probe_cell); d_probe_cell = nullptr;
+        cudaFree(d_probe_out); d_probe_out = nullptr;
+        cudaFree(d_energy); d_energy = nullptr;
+        if (ctl_host) cudaFreeHost(ctl_host);
+        if (h_table) cudaFreeHost(h_table);
+        if (h_probe_out) cudaFreeHost(h_probe_out);
+        ctl_host = nullptr; h_table = nullptr; h_probe_out = nullptr;
+        if (stream) cudaStreamDestroy(stream);
+        stream = nullptr;
+        inited = false;
+    }
+
+    int nprobe() const { return (int)probe_xyz.size() / 3; }
+};
+
+// ---------------------------------------------------------------- helpers
+
+namespace {
+
+// DroneSource::update (06:221-238).
+void drone_position(const lbm_source& s, double t, double& cx, double& cy, double& cz)
+{
+    double dx = s.ex - s.sx, dy = s.ey - s.sy, dz = s.ez - s.sz;
+    double dist_total = std::sqrt(dx * dx + dy * dy + dz * dz);
+    if (dist_total < 1e-12 || s.speed < 1e-12)
+    {
+        cx = s.sx; cy = s.sy; cz = s.sz;
+        return;
+    }
+    double travel_time = dist_total / s.speed;
+    double r = t / travel_time;
+    if (r > 1.0) r = 1.0;
+    cx = s.sx + r * dx;
+    cy = s.sy + r * dy;
+    cz = s.sz + r * dz;
+}
+
+// Source time function at time t (06:579-581 Gaussian, 08:543 sine, Ricker,
+// per-step table).
+double source_value(const SourceState& st, double t, double dt)
+{
+    const lbm_source& p = st.s;
+    switch (p.waveform)
+    {
+    case LBM_WAVE_GAUSS:
+        return p.amp * std::exp(-0.5 * std::pow((t - p.t0) / p.sigma_t, 2));
+    case LBM_WAVE_SINE:
+        return p.amp * std::sin(2.0 * kPi * p.freq * t);
+    case LBM_WAVE_RICKER:
+    {
+        double a = kPi * p.freq * (t - p.t0);
+        a = a * a;
+        return p.amp * (1.0 - 2.0 * a) * std::exp(-a);
+    }
+    case LBM_WAVE_TABLE:
+    {
+        const long s = std::lround(t / dt);
+        if (s < 0 || s >= (long)st.table.size()) return 0.0;
+        return p.amp * st.table[(size_t)s];
+    }
+    default:
+        return 0.0;
+    }
+}
+
+SourceEntry source_entry(const SourceState& st, double t, double dt)
+{
+    SourceEntry e;
+    const double val = source_value(st, t, dt);
+    drone_position(st.s, t, e.cx, e.cy, e.cz);
+    e.mass = val * dt * st.s.gain;   // numerator of A (06:631)
+    return e;
+}
+
+int validate(const lbm_config& c, std::string& why)
+{
+    if (!(c.dx > 0)) return why = "dx must be > 0", LBM_ERR_BAD_CONFIG;
+    if (!(c.tau > 0.5)) return why = "tau must be > 0.5", LBM_ERR_BAD_CONFIG;
+    if (!(c.c_phys > 0)) return why = "c_phys must be > 0", LBM_ERR_BAD_CONFIG;
+    if (!(c.x_max > c.x_min && c.y_max > c.y_min && c.z_max > c.z_min))
+        return why = "empty domain", LBM_ERR_BAD_CONFIG;
+    for (int f = 0; f < 6; ++f)
+        if (c.face_bc[f] < LBM_BC_NSCBC || c.face_bc[f] > LBM_BC_WALL)
+            return why = "face_bc out of range", LBM_ERR_BAD_CONFIG;
+    if (c.storage != LBM_STORE_F32 && c.storage != LBM_STORE_F16)
+        return why = "storage must be LBM_STORE_F32 or LBM_STORE_F16", LBM_ERR_BAD_CONFIG;
+    if (c.storage == LBM_STORE_F16 && !(c.f16_scale > 0)) return why = "f16_scale must be > 0", LBM_ERR_BAD_CONFIG;
+    if (!(c.sponge_width >= 0)) return why = "sponge_width must be >= 0", LBM_ERR_BAD_CONFIG;
+    return LBM_OK;
+}
+
+// Per-axis sponge strength at interior cell centres (init_domain 06:491-506).
+// sigma(x,y,z) = S((w - d)/w)^2 with d the distance to the nearest sponge
+// face is monotone in d, so the per-cell value equals the maximum of the
+// per-axis values; the kernel takes that maximum.  Values <= 1e-12 are the
+// reference's "no sponge" (06:961) and are stored as 0.
+void sponge_axis(const lbm_config& c, int axis, int n, std::vector<float>& out)
+{
+    const double lo[3] = {c.x_min, c.y_min, c.z_min};
+    const double hi[3] = {c.x_max, c.y_max, c.z_max};
+    const unsigned sf = c.sponge_faces;
+    const double w = c.sponge_width * c.dx;
+    out.resize((size_t)n);
+    for (int i = 1; i <= n; ++i)
+    {
+        const double x = lo[axis] + ((i - 1) + 0.5) * c.dx;
+        double d = 1e30;
+        if (sf & (1u << (2 * axis))) d = std::min(d, x - lo[axis]);
+        if (sf & (1u << (2 * axis + 1))) d = std::min(d, hi[axis] - x);
+        double s = 0.0;
+        if (d < w)
+        {
+            const double r = (w - d) / w;
+            s = c.sponge_strength * r * r;
+        }
+        out[(size_t)i - 1] = s > 1e-12 ? (float)s : 0.0f;
+    }
+}
+
+// The voxelised mask of init_domain (06:460-531) in the reference's
+// halo-inclusive layout: SOLID below the ground height of the column unless
+// above sky_z, then the halo rules x faces, y faces, z faces in that order
+// (a WALL face is SOLID, every other face FLUID).
+void build_mask(const lbm_config& c, const HeightField& geo, int nx, int ny, int nz, uint8_t* m)
+{
+    const int nxt = nx + 2, nyt = ny + 2, nzt = nz + 2;
+    std::vector<double> gH((size_t)nxt * nyt, -1e30);
+    const bool geom = c.use_geometry != 0;
+    if (geom)
+    {
+#pragma omp parallel for collapse(2) schedule(dynamic, 16)
+        for (int j = 0; j < nyt; ++j)
+            for (int i = 0; i < nxt; ++i)
+            {
+                const double x = c.x_min + ((i - 1) + 0.5) * c.dx;
+                const double y = c.y_min + ((j - 1) + 0.5) * c.dx;
+                gH[(size_t)j * nxt + i] = geo.ground_height(x, y);
+            }
+    }
+#pragma omp parallel for collapse(2)
+    for (int k = 0; k < nzt; ++k)
+        for (int j = 0; j < nyt; ++j)
+        {
+            const double z = c.z_min + ((k - 1) + 0.5) * c.dx;
+            for (int i = 0; i < nxt; ++i)
+            {
+                const size_t idx = (size_t)i + (size_t)j * nxt + (size_t)k * nxt * nyt;
+                uint8_t v = geom ? (z < gH[(size_t)j * nxt + i] ? 1 : 0) : 0;
+                if (z > c.sky_z) v = 0;
+                m[idx] = v;
+            }
+        }
+    const auto wall = [&](int f) { return (uint8_t)(c.face_bc[f] == LBM_BC_WALL ? 1 : 0); };
+    for (int k = 0; k < nzt; ++k)
+        for (int j = 0; j < nyt; ++j)
+        {
+            m[(size_t)0 + (size_t)j * nxt + (size_t)k * nxt * nyt] = wall(LBM_FACE_XLO);
+            m[(size_t)(nx + 1) + (size_t)j * nxt + (size_t)k * nxt * nyt] = wall(LBM_FACE_XHI);
+        }
+    for (int k = 0; k < nzt; ++k)
+        for (int i = 0; i < nxt; ++i)
+        {
+            m[(size_t)i + (size_t)k * nxt * nyt] = wall(LBM_FACE_YLO);
+            m[(size_t)i + (size_t)(ny + 1) * nxt + (size_t)k * nxt * nyt] = wall(LBM_FACE_YHI);
+        }
+    for (int j = 0; j < nyt; ++j)
+        for (int i = 0; i < nxt; ++i)
+        {
+            m[(size_t)i + (size_t)j * nxt] = wall(LBM_FACE_ZLO);
+            m[(size_t)i + (size_t)j * nxt + (size_t)(nz + 1) * nxt * nyt] = wall(LBM_FACE_ZHI);
+        }
+}
+
+void grid_size(const lbm_config& c, int& nx, int& ny, int& nz)
+{
+    // 06:332-334
+    nx = (int)((c.x_max - c.x_min) / c.dx + 0.5);
+    ny = (int)((c.y_max - c.y_min) / c.dx + 0.5);
+    nz = (int)((c.z_max - c.z_min) / c.dx + 0.5);
+}
+
+#define CK(expr, where)                                   \
+    do                                                    \
+    {                                                     \
+        cudaError_t e_ = (expr);                          \
+        if (e_ != cudaSuccess) return h->cuda_fail(e_, where); \
+    } while (0)
+
+}  // namespace
+
+// ---------------------------------------------------------------- defaults
+
+extern "C" void lbm_config_default(lbm_config* c)
+{
+    std::memset(c, 0, sizeof *c);
+    c->x_min = 0.0; c->x_max = 1650.0;   // 06:250-252
+    c->y_min = 0.0; c->y_max = 1150.0;
+    c->z_min = 0.0; c->z_max = 250.0;
+    c->dx = 2.0;                         // 06:253
+    c->c_phys = 340.0;                   // 06:198
+    c->tau = 0.55;                       // 06:268
+    c->use_geometry = 1;                 // 06:248
+    for (int f = 0; f < 6; ++f) c->face_bc[f] = LBM_BC_NSCBC;
+    c->face_bc[LBM_FACE_ZLO] = LBM_BC_WALL;   // ground (06:520-531)
+    c->sponge_faces = (1u << LBM_FACE_XLO) | (1u << LBM_FACE_XHI) | (1u << LBM_FACE_YLO) | (1u << LBM_FACE_YHI) |
+                      (1u << LBM_FACE_ZHI);   // 06:491-496
+    c->sponge_width = 20.0;              // 06:455
+    c->sponge_strength = 0.35;           // 06:456
+    c->sky_z = 120.0;                    // 06:458
+    c->storage = LBM_STORE_F32;
+    c->f16_scale = 1.0;
+    c->device = 0;
+    c->use_graphs = 1;
+    c->verbose = 0;
+}
+
+extern "C" void lbm_source_default(lbm_source* s)
+{
+    std::memset(s, 0, sizeof *s);
+    s->waveform = LBM_WAVE_GAUSS;
+    s->t0 = 0.05;          // 06:579
+    s->sigma_t = 0.005;    // 06:580
+    s->injection = LBM_INJECT_GAUSS;
+    s->gain = 1.0;         // 06:583
+    s->sigma_cells = 1.25; // 06:588
+    s->radius = 2;         // 06:587
+}
+
+extern "C" const char* lbm_status_string(int s)
+{
+    switch (s)
+    {
+    case LBM_OK: return "ok";
+    case LBM_WARN_STL_NOT_LOADED: return "warning: STL not loaded, using empty geometry";
+    case LBM_WARN_PROBE_IN_SOLID: return "warning: probe inside a SOLID cell";
+    case LBM_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case LBM_ERR_BAD_CONFIG: return "bad configuration";
+    case LBM_ERR_OUT_OF_MEMORY: return "out of device memory";
+    case LBM_ERR_CUDA: return "CUDA error";
+    case LBM_ERR_NAN: return "non-finite value in probe series";
+    case LBM_ERR_STATE: return "call out of order";
+    case LBM_ERR_CAPACITY: return "output buffer too small";
+    case LBM_ERR_NO_DEVICE: return "no CUDA device";
+    case LBM_ERR_IO: return "I/O error";
+    case LBM_ERR_UNSUPPORTED: return "unsupported";
+    default: return "unknown status";
+    }
+}
+
+extern "C" const char* lbm_version(void) { return "nlos_lbm 0.1 (sm_100a)"; }
+
+// ---------------------------------------------------------------- lifetime
+
+extern "C" int lbm_create(const lbm_config* cfg, lbm_handle** out)
+{
+    if (!cfg || !out) return LBM_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    std::string why;
+    int st = validate(*cfg, why);
+    if (st != LBM_OK) return st;
+    auto* h = new (std::nothrow) lbm_handle();
+    if (!h) return LBM_ERR_OUT_OF_MEMORY;
+    h->cfg = *cfg;
+    h->storage = cfg->storage;
+    h->scale = cfg->storage == LBM_STORE_F16 ? (float)cfg->f16_scale : 1.0f;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    {
+        delete h;
+        return LBM_ERR_NO_DEVICE;
+    }
+    if (cfg->device < 0 || cfg->device >= ndev)
+    {
+        delete h;
+        return LBM_ERR_BAD_CONFIG;
+    }
+    h->device = cfg->device;
+    *out = h;
+    return LBM_OK;
+}
+
+extern "C" int lbm_destroy(lbm_handle* h)
+{
+    if (!h) return LBM_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(h->device);
+    delete h;
+    return LBM_OK;
+}
+
+extern "C" const char* lbm_last_error(lbm_handle* h) { return h ? h->err.c_str() : ""; }
+
+// ---------------------------------------------------------------- geometry
+
+extern "C" int lbm_set_geometry_stl(lbm_handle* h, const char* path, double scale, double sx, double sy, double sz)
+{
+    if (!h || !path) return LBM_ERR_INVALID_ARGUMENT;
+    const bool ok = h->geo.load_stl(path, scale, sx, sy, sz);
+    h->stl_status = ok ? LBM_OK : LBM_WARN_STL_NOT_LOADED;
+    if (!ok) h->err = std::string("STL not loaded: ") + path;
+    return h->stl_status;
+}
+
+extern "C" int lbm_set_geometry_triangles(lbm_handle* h, const float* tris, int ntris, double scale, double sx,
+                                          double sy, double sz)
+{
+    if (!h || ntris < 0 || (ntris > 0 && !tris)) return LBM_ERR_INVALID_ARGUMENT;
+    h->geo.set_triangles(tris, ntris, scale, sx, sy, sz);
+    h->stl_status = LBM_OK;
+    return LBM_OK;
+}
+
+extern "C" int lbm_set_mask(lbm_handle* h, const uint8_t* mask, int nx_t, int ny_t, int nz_t)
+{
+    if (!h || !mask || nx_t < 3 || ny_t < 3 || nz_t < 3) return LBM_ERR_INVALID_ARGUMENT;
+    const size_t n = (size_t)nx_t * ny_t * nz_t;
+    h->mask_override.assign(mask, mask + n);
+    for (auto& m : h->mask_override) m = m ? 1 : 0;
+    h->mo_dims[0] = nx_t; h->mo_dims[1] = ny_t; h->mo_dims[2] = nz_t;
+    return LBM_OK;
+}
+
+// ---------------------------------------------------------------- sources / probes
+
+extern "C" int lbm_add_source(lbm_handle* h, const lbm_source* s)
+{
+    if (!h || !s) return LBM_ERR_INVALID_ARGUMENT;
+    if ((int)h->srcs.size() >= kMaxSources) return h->fail(LBM_ERR_UNSUPPORTED, "at most 8 sources");
+    if (s->injection == LBM_INJECT_GAUSS && (s->radius < 0 || s->radius > 3 || !(s->sigma_cells > 0)))
+        return h->fail(LBM_ERR_INVALID_ARGUMENT, "Gaussian stencil needs radius 0..3 and sigma_cells > 0");
+    if (s->injection != LBM_INJECT_GAUSS && s->injection != LBM_INJECT_TRILINEAR)
+        return h->fail(LBM_ERR_INVALID_ARGUMENT, "unknown injection");
+    if (s->waveform < LBM_WAVE_GAUSS || s->waveform > LBM_WAVE_TABLE)
+        return h->fail(LBM_ERR_INVALID_ARGUMENT, "unknown waveform");
+    if (s->waveform == LBM_WAVE_TABLE && (s->table_len < 0 || (s->table_len > 0 && !s->table)))
+        return h->fail(LBM_ERR_INVALID_ARGUMENT, "table waveform needs table samples");
+    SourceState st;
+    st.s = *s;
+    if (s->waveform == LBM_WAVE_TABLE) st.table.assign(s->table, s->table + s->table_len);
+    st.s.table = nullptr;
+    h->srcs.push_back(std::move(st));
+    h->table_rows = 0;   // schedule must be rebuilt
+    if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; }
+    return LBM_OK;
+}
+
+extern "C" int lbm_clear_sources(lbm_handle* h)
+{
+    if (!h) return LBM_ERR_INVALID_ARGUMENT;
+    h->srcs.clear();
+    h->table_rows = 0;
+    if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; }
+    return LBM_OK;
+}
+
+extern "C" int lbm_set_probes(lbm_handle* h, const double* xyz, int n)
+{
+    if (!h || n < 0 || (n > 0 && !xyz)) return LBM_ERR_INVALID_ARGUMENT;
+    if (h->inited) return h->fail(LBM_ERR_STATE, "probes are fixed at lbm_init");
+    h->probe_xyz.assign(xyz, xyz + 3 * (size_t)n);
+    return LBM_OK;
+}
+
+extern "C" int lbm_probe_info(lbm_handle* h, int* owned, int* in_solid)
+{
+    if (!h) return LBM_ERR_INVALID_ARGUMENT;
+    if (!h->inited) return LBM_ERR_STATE;
+    for (int p = 0; p < h->nprobe(); ++p)
+    {
+        if (owned) owned[p] = h->probe_owned[p];
+        if (in_solid) in_solid[p] = h->probe_solid[p];
+    }
+    return LBM_OK;
+}
+
+// ---------------------------------------------------------------- init
+
+extern "C" int lbm_init(lbm_handle* h)
+{
+    if (!h) return LBM_ERR_INVALID_ARGUMENT;
+    const lbm_config& c = h->cfg;
+    h->release();
+    CK(cudaSetDevice(h->device), "cudaSetDevice");
+
+    // Grid (06:330-334, MPI size 1: one block, off = 0) and time step (06:200-203).
+    grid_size(c, h->NXg, h->NYg, h->NZg);
+    h->dt = (kCs * c.dx) / c.c_phys;
+    const int nx = h->NXg, ny = h->NYg, nz = h->NZg;
+    if (nx < 1 || ny < 1 || nz < 1) return h->fail(LBM_ERR_BAD_CONFIG, "grid has no cells");
+    const int nxt = nx + 2, nyt = ny + 2, nzt = nz + 2;
+    const size_t nloc = (size_t)nxt * nyt * nzt;
+
+    Layout& L = h->L;
+    L.nx = nx; L.ny = ny; L.nz = nz;
+    L.pitch = (nx + 2 + 31) / 32 * 32;
+    L.words_per_row = L.pitch / 32;
+    L.plane = (long long)L.pitch * nyt;
+    L.pop_stride = ((long long)kFrontPad + L.plane * nzt + 32 + 63) / 64 * 64;
+    if (L.pop_stride >= (1ll << 31)) return h->fail(LBM_ERR_UNSUPPORTED, "grid too large for one GPU");
+
+    // Mask (init_domain 06:453-532).
+    if (!h->mask_override.empty())
+    {
+        if (h->mo_dims[0] != nxt || h->mo_dims[1] != nyt || h->mo_dims[2] != nzt)
+            return h->fail(LBM_ERR_INVALID_ARGUMENT, "lbm_set_mask dimensions do not match the grid");
+        h->mask = h->mask_override;
+    }
+    else
+    {
+        try
+        {
+            h->mask.assign(nloc, 0);
+        }
+        catch (const std::bad_alloc&)
+        {
+            return h->fail(LBM_ERR_OUT_OF_MEMORY, "host mask");
+        }
+        build_mask(c, h->geo, nx, ny, nz, h->mask.data());
+    }
+
+    // Sponge profiles.
+    std::vector<float> sx, sy, sz;
+    sponge_axis(c, 0, nx, sx);
+    sponge_axis(c, 1, ny, sy);
+    sponge_axis(c, 2, nz, sz);
+
+    // Device buffers.
+    CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    const size_t esz = h->storage == LBM_STORE_F16 ? 2 : 4;
+    const size_t pop_bytes = (size_t)Q * (size_t)L.pop_stride * esz;
+    cudaError_t e = cudaSuccess;
+    for (int b = 0; b < 2; ++b)
+    {
+        if (e == cudaSuccess) e = cudaMalloc(&h->f_alloc[b], pop_bytes);
+        if (e == cudaSuccess) e = cudaMemsetAsync(h->f_alloc[b], 0, pop_bytes, h->stream);   // g = 0: rest state (06:388-395)
+        if (e == cudaSuccess) h->f[b] = (char*)h->f_alloc[b] + kFrontPad * esz;
+    }
+    const size_t cells = (size_t)L.pop_stride;
+    h->links = dalloc<uint32_t>(cells, e);
+    const size_t near_words = (size_t)nzt * nyt * L.words_per_row;
+    h->near = dalloc<uint32_t>(near_words, e);
+    h->sig = dalloc<float>((size_t)nx + ny + nz, e);
+    h->ctl = dalloc<Control>(1, e);
+    if (e != cudaSuccess) return h->cuda_fail(e, "device allocation");
+    CK(cudaMemsetAsync(h->links, 0, cells * sizeof(uint32_t), h->stream), "memset links");
+    CK(cudaMemsetAsync(h->near, 0, near_words * sizeof(uint32_t), h->stream), "memset near");
+    CK(cudaMallocHost(&h->ctl_host, sizeof(Control)), "cudaMallocHost");
+    CK(cudaMemcpyAsync(h->sig, sx.data(), sx.size() * 4, cudaMemcpyHostToDevice, h->stream), "upload sponge");
+    CK(cudaMemcpyAsync(h->sig + nx, sy.data(), sy.size() * 4, cudaMemcpyHostToDevice, h->stream), "upload sponge");
+    CK(cudaMemcpyAsync(h->sig + nx + ny, sz.data(), sz.size() * 4, cudaMemcpyHostToDevice, h->stream),
+       "upload sponge");
+    {
+        uint8_t* d_mask = nullptr;
+        CK(cudaMalloc(&d_mask, nloc), "mask upload buffer");
+        e = cudaMemcpyAsync(d_mask, h->mask.data(), nloc, cudaMemcpyHostToDevice, h->stream);
+        // links[c] belongs to the cell with linear index c (interior cells only)
+        if (e == cudaSuccess) e = launch_build_links(d_mask, h->links, h->near, L, h->stream);
+        cudaError_t e2 = cudaStreamSynchronize(h->stream);
+        cudaFree(d_mask);
+        if (e == cudaSuccess) e = e2;
+        if (e != cudaSuccess) return h->cuda_fail(e, "build links");
+        h->launches += 1;
+    }
+
+    h->sa.links = h->links;
+    h->sa.near = h->near;
+    h->sa.sig_x = h->sig;
+    h->sa.sig_y = h->sig + nx;
+    h->sa.sig_z = h->sig + nx + ny;
+    h->sa.omega = (float)(1.0 / c.tau);
+
+    // Open faces for the ghost kernel.
+    h->ga = GhostArgs{};
+    h->ga.scale = h->scale;
+    long long first = 0;
+    for (int f = 0; f < 6; ++f)
+    {
+        if (c.face_bc[f] != LBM_BC_NSCBC) continue;
+        GhostFace gf;
+        gf.axis = f / 2;
+        gf.side = f % 2;
+        gf.nu = gf.axis == 0 ? ny : nx;
+        gf.nv = gf.axis == 2 ? ny : nz;
+        gf.first = first;
+        first += (long long)gf.nu * gf.nv;
+        h->ga.face[h->ga.nfaces++] = gf;
+    }
+    h->ga.total = first;
+
+    // Probes (06:415-437).
+    int status = h->stl_status;
+    const int np = h->nprobe();
+    h->probe_cell.assign((size_t)np, -1);
+    h->probe_owned.assign((size_t)np, 0);
+    h->probe_solid.assign((size_t)np, 0);
+    for (int p = 0; p < np; ++p)
+    {
+        const int gi = (int)std::floor((h->probe_xyz[3 * p] - c.x_min) / c.dx);
+        const int gj = (int)std::floor((h->probe_xyz[3 * p + 1] - c.y_min) / c.dx);
+        const int gk = (int)std::floor((h->probe_xyz[3 * p + 2] - c.z_min) / c.dx);
+        if (gi >= 0 && gi < nx && gj >= 0 && gj < ny && gk >= 0 && gk < nz)
+        {
+            h->probe_owned[p] = 1;
+            h->probe_cell[p] = L.cell(gi + 1, gj + 1, gk + 1);
+            const size_t idx = (size_t)(gi + 1) + (size_t)(gj + 1) * nxt + (size_t)(gk + 1) * nxt * nyt;
+            if (h->mask[idx])
+            {
+                h->probe_solid[p] = 1;
+                if (status == LBM_OK) status = LBM_WARN_PROBE_IN_SOLID;
+                if (c.verbose) std::printf("WARNING: Probe %d is trapped inside SOLID building!\n", p);
+            }
+        }
+    }
+    const int npa = std::max(np, 1);
+    h->d_probe_cell = dalloc<long long>((size_t)npa, e);
+    h->d_probe_out = dalloc<double>((size_t)npa * kProbeRows, e);
+    h->d_energy = dalloc<double>((size_t)npa, e);
+    if (e != cudaSuccess) return h->cuda_fail(e, "probe buffers");
+    CK(cudaMallocHost(&h->h_probe_out, (size_t)npa * kProbeRows * sizeof(double)), "cudaMallocHost");
+    if (np) CK(cudaMemcpyAsync(h->d_probe_cell, h->probe_cell.data(), (size_t)np * 8, cudaMemcpyHostToDevice, h->stream),
+               "upload probes");
+    CK(cudaMemsetAsync(h->d_energy, 0, (size_t)npa * 8, h->stream), "memset energy");
+
+    // Source schedule buffers (sized for the maximum source count so sources
+    // may change after init).
+    const size_t ns = kMaxSources;
+    h->d_table = dalloc<SourceEntry>(ns * kTableRows, e);
+    if (e != cudaSuccess) return h->cuda_fail(e, "source table");
+    CK(cudaMallocHost(&h->h_table, ns * kTableRows * sizeof(SourceEntry)), "cudaMallocHost");
+    h->table_base = 0;
+    h->table_rows = 0;
+
+    h->series.clear();
+    h->probe_pending = 0;
+    h->step = 0;
+    h->cur = 0;
+    h->halo_dirty = false;
+    CK(cudaStreamSynchronize(h->stream), "init sync");
+    h->h2d_bytes = h->d2h_bytes = 0;
+    h->inited = true;
+    if (c.verbose)
+        std::printf("Grid: %d x %d x %d  (dx=%g m)\ndt=%g s\n", nx, ny, nz, c.dx, h->dt);
+    return status;
+}
+
+// ---------------------------------------------------------------- stepping internals
+
+namespace {
+
+SourceArgs source_args(lbm_handle* h, bool batched)
+{
+    SourceArgs a{};
+    a.nsrc = (int)h->srcs.size();
+    for (int s = 0; s < a.nsrc; ++s)
+    {
+        const lbm_source& p = h->srcs[s].s;
+        a.st[s].injection = p.injection;
+        a.st[s].radius = p.radius;
+        a.st[s].sigma2 = (p.sigma_cells * h->cfg.dx) * (p.sigma_cells * h->cfg.dx);   // 06:589
+    }
+    a.table = batched ? h->d_table : nullptr;
+    a.ctl = batched ? h->ctl : nullptr;
+    a.x_min = h->cfg.x_min;
+    a.y_min = h->cfg.y_min;
+    a.z_min = h->cfg.z_min;
+    a.dx = h->cfg.dx;
+    a.scale = h->scale;
+    return a;
+}
+
+ProbeArgs probe_args(lbm_handle* h, bool batched, long long direct_row)
+{
+    ProbeArgs a{};
+    a.n = h->nprobe();
+    a.cell = h->d_probe_cell;
+    a.out = h->d_probe_out;
+    a.energy = h->d_energy;
+    a.ctl = batched ? h->ctl : nullptr;
+    a.direct_row = direct_row;
+    a.scale = h->scale;
+    return a;
+}
+
+cudaError_t timed_step_launch(lbm_handle* h, const void* fin, void* fout)
+{
+    cudaError_t e;
+    if (h->timing)
+    {
+        if (h->ev_used + 2 > h->ev.size())
+        {
+            for (int n = 0; n < 64; ++n)
+            {
+                cudaEvent_t x;
+                e = cudaEventCreate(&x);
+                if (e != cudaSuccess) return e;
+                h->ev.push_back(x);
+            }
+        }
+        e = cudaEventRecord(h->ev[h->ev_used], h->stream);
+        if (e != cudaSuccess) return e;
+        e = launch_step(h->storage, fin, fout, h->L, h->sa, h->scale, h->stream);
+        if (e != cudaSuccess) return e;
+        e = cudaEventRecord(h->ev[h->ev_used + 1], h->stream);
+        h->ev_used += 2;
+        return e;
+    }
+    return launch_step(h->storage, fin, fout, h->L, h->sa, h->scale, h->stream);
+}
+
+// Collect the kernel times recorded since the last harvest (synchronises).
+int harvest_timing(lbm_handle* h)
+{
+    if (!h->timing || h->ev_used == 0) return LBM_OK;
+    cudaError_t e = cudaEventSynchronize(h->ev[h->ev_used - 1]);
+    if (e != cudaSuccess) return h->cuda_fail(e, "timing");
+    for (size_t n = 0; n < h->ev_used; n += 2)
+    {
+        float ms = 0.f;
+        e = cudaEventElapsedTime(&ms, h->ev[n], h->ev[n + 1]);
+        if (e != cudaSuccess) return h->cuda_fail(e, "timing");
+        h->kernel_ms += ms;
+        h->kernel_launches += 1;
+    }
+    h->ev_used = 0;
+    return LBM_OK;
+}
+
+// One full time step on the device (source -> ghosts -> fused step ->
+// probes), reading the step index from the device control block.
+cudaError_t enqueue_batched_step(lbm_handle* h, int parity, int& kernels)
+{
+    cudaError_t e = cudaSuccess;
+    void* fc = h->f[parity];
+    void* fn = h->f[parity ^ 1];
+    kernels = 0;
+    if (!h->srcs.empty())
+    {
+        e = launch_source(h->storage, fc, h->L, h->sa, source_args(h, true), h->stream);
+        if (e != cudaSuccess) return e;
+        kernels++;
+    }
+    if (h->ga.total > 0)
+    {
+        e = launch_ghost(h->storage, fc, h->L, h->ga, h->stream);
+        if (e != cudaSuccess) return e;
+        kernels++;
+    }
+    e = timed_step_launch(h, fc, fn);
+    if (e != cudaSuccess) return e;
+    kernels++;
+    e = launch_probe(h->storage, fc, h->L, h->sa, probe_args(h, true, 0), h->stream);
+    kernels++;
+    return e;
+}
+
+int build_graph(lbm_handle* h)
+{
+    if (h->graph) return LBM_OK;
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return h->cuda_fail(e, "begin capture");
+    int k0 = 0, k1 = 0;
+    cudaError_t le = enqueue_batched_step(h, 0, k0);
+    if (le == cudaSuccess) le = enqueue_batched_step(h, 1, k1);
+    e = cudaStreamEndCapture(h->stream, &g);
+    if (le != cudaSuccess) e = le;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&h->graph, g, 0);
+    if (g) cudaGraphDestroy(g);
+    if (e != cudaSuccess)
+    {
+        h->graph = nullptr;
+        return h->cuda_fail(e, "graph capture");
+    }
+    h->graph_kernels = k0 + k1;
+    return LBM_OK;
+}
+
+// Moves the probe rows buffered on the device to the host series.
+int drain_probes(lbm_handle* h)
+{
+    const int np = h->nprobe();
+    if (np == 0 || h->probe_pending == 0) return LBM_OK;
+    const size_t n = (size_t)h->probe_pending * np;
+    CK(cudaMemcpyAsync(h->h_probe_out, h->d_probe_out, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream),
+       "probe download");
+    h->d2h_bytes += (long)(n * sizeof(double));
+    CK(cudaStreamSynchronize(h->stream), "probe download");
+    h->series.insert(h->series.end(), h->h_probe_out, h->h_probe_out + n);
+    h->probe_pending = 0;
+    for (size_t i = 0; i < n; ++i)
+        if (h->probe_owned[i % np] && !std::isfinite(h->h_probe_out[i]))
+            return h->fail(LBM_ERR_NAN, "non-finite probe value");
+    return LBM_OK;
+}
+
+// Fills the device source schedule with rows for steps [s0, s0 + rows).
+int fill_table(lbm_handle* h, long long s0)
+{
+    const size_t ns = h->srcs.size();
+    if (ns == 0) return LBM_OK;
+    CK(cudaStreamSynchronize(h->stream), "table refill");   // staging buffer reuse
+    for (long long r = 0; r < kTableRows; ++r)
+    {
+        const double t = (double)(s0 + r) * h->dt;   // t = s * dt (06:1079)
+        for (size_t s = 0; s < ns; ++s) h->h_table[r * ns + s] = source_entry(h->srcs[s], t, h->dt);
+    }
+    CK(cudaMemcpyAsync(h->d_table, h->h_table, ns * kTableRows * sizeof(SourceEntry), cudaMemcpyHostToDevice,
+                       h->stream),
+       "table upload");
+    h->h2d_bytes += (long)(ns * kTableRows * sizeof(SourceEntry));
+    h->table_base = s0;
+    h->table_rows = kTableRows;
+    return LBM_OK;
+}
+
+int check_ready(lbm_handle* h)
+{
+    if (!h) return LBM_ERR_INVALID_ARGUMENT;
+    if (!h->inited) return h->fail(LBM_ERR_STATE, "lbm_init has not run");
+    return LBM_OK;
+}
+
+int reset_halos_if_dirty(lbm_handle* h)
+{
+    if (!h->halo_dirty) return LBM_OK;
+    // All halo cells return to rest (w_q) before the open faces are refilled,
+    // as exchange_halos rewrites every halo cell (06:677-682, 06:853-903).
+    const Layout& L = h->L;
+    const size_t esz = h->storage == LBM_STORE_F16 ? 2 : 4;
+    std::vector<double> tmp;   // host round trip is fine: only after lbm_set_f
+    const size_t nloc = (size_t)(L.nx + 2) * (L.ny + 2) * (L.nz + 2);
+    double* d = nullptr;
+    CK(cudaMalloc(&d, nloc * Q * sizeof(double)), "halo reset");
+    cudaError_t e = launch_export_f(h->storage, h->f[h->cur], d, L, h->scale, h->stream);
+    if (e == cudaSuccess)
+    {
+        tmp.resize(nloc * Q);
+        e = cudaMemcpyAsync(tmp.data(), d, nloc * Q * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    }
+    if (e == cudaSuccess)
+    {
+        const int nxt = L.nx + 2, nyt = L.ny + 2, nzt = L.nz + 2;
+        for (int k = 0; k < nzt; ++k)
+            for (int j = 0; j < nyt; ++j)
+                for (int i = 0; i < nxt; ++i)
+                {
+                    if (i > 0 && i <= L.nx && j > 0 && j <= L.ny && k > 0 && k <= L.nz) continue;
+                    const size_t idx = (size_t)i + (size_t)j * nxt + (size_t)k * nxt * nyt;
+                    for (int q = 0; q < Q; ++q) tmp[idx * Q + q] = wd(q);
+                }
+        e = cudaMemcpyAsync(d, tmp.data(), nloc * Q * sizeof(double), cudaMemcpyHostToDevice, h->stream);
+        if (e == cudaSuccess) e = launch_import_f(h->storage, h->f[h->cur], d, L, h->scale, h->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    }
+    cudaFree(d);
+    (void)esz;
+    if (e != cudaSuccess) return h->cuda_fail(e, "halo reset");
+    h->halo_dirty = false;
+    return LBM_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- stepping API
+
+extern "C" int lbm_apply_source(lbm_handle* h, double t)
+{
+    int st = check_ready(h);
+    if (st) return st;
+    if (h->srcs.empty()) return LBM_OK;
+    CK(cudaSetDevice(h->device), "cudaSetDevice");
+    SourceArgs a = source_args(h, false);
+    for (size_t s = 0; s < h->srcs.size(); ++s) a.direct[s] = source_entry(h->srcs[s], t, h->dt);
+    CK(launch_source(h->storage, h->f[h->cur], h->L, h->sa, a, h->stream), "source kernel");
+    h->launches++;
+    return LBM_OK;
+}
+
+extern "C" int lbm_exchange_halos(lbm_handle* h)
+{
+    int st = check_ready(h);
+    if (st) return st;
+    CK(cudaSetDevice(h->device), "cudaSetDevice");
+    st = reset_halos_if_dirty(h);
+    if (st) return st;
+    if (h->ga.total > 0)
+    {
+        CK(launch_ghost(h->storage, h->f[h->cur], h->L, h->ga, h->stream), "ghost kernel");
+        h->launches++;
+    }
+    return LBM_OK;
+}
+
+extern "C" int lbm_step_collision_bgk(lbm_handle* h)
+{
+    int st = check_ready(h);
+    if (st) return st;
+    CK(cudaSetDevice(h->device), "cudaSetDevice");
+    CK(timed_step_launch(h, h->f[h->cur], h->f[h->cur ^ 1]), "step kernel");
+    h->launches++;
+    h->cur ^= 1;
+    h->step++;
+    return harvest_timing(h);
+}
+
+extern "C" int lbm_record_probes(lbm_handle* h)
+{
+    int st = check_ready(h);
+    if (st) return st;
+    if (h->nprobe() == 0) return LBM_OK;
+    if (h->step == 0) return h->fail(LBM_ERR_STATE, "no step taken yet");
+    CK(cudaSetDevice(h->device), "cudaSetDevice");
+    if (h->probe_pending >= kProbeRows)
+    {
+        st = drain_probes(h);
+        if (st) return st;
+    }
+    // the pre-step buffer of the last collision step is intact until the next one
+    CK(launch_probe(h->storage, h->f[h->cur ^ 1], h->L, h->sa, probe_args(h, false, h->probe_pending), h->stream),
+       "probe kernel");
+    h->launches++;
+    h->probe_pending++;
+    return LBM_OK;
+}
+
+extern "C" int lbm_step(lbm_handle* h, int nsteps)
+{
+    int st = check_ready(h);
+    if (st) return st;
+    if (nsteps < 0) return LBM_ERR_INVALID_ARGUMENT;
+    CK(cudaSetDevice(h->device), "cudaSetDevice");
+    st = reset_halos_if_dirty(h);
+    if (st) return st;
+    const int np = h->nprobe();
+    const bool use_graph = h->cfg.use_graphs && !h->timing;
+    long long left = nsteps;
+    while (left > 0)
+    {
+        if (!h->srcs.empty() && (h->step < h->table_base || h->step >= h->table_base + h->table_rows))
+        {
+            st = fill_table(h, h->step);
+            if (st) return st;
+        }
+        long long chunk = left;
+        if (!h->srcs.empty()) chunk = std::min(chunk, h->table_base + h->table_rows - h->step);
+        if (np) chunk = std::min<long long>(chunk, kProbeRows - h->probe_pending);
+        if (chunk <= 0)
+        {
+            st = drain_probes(h);
+            if (st) return st;
+            continue;
+        }
+        h->ctl_host->step = h->step;
+        h->ctl_host->table_base = h->table_base;
+        // the probe row of step s is s - probe_base: rows continue after the
+        // ones already buffered
+        h->ctl_host->probe_base = h->step - h->probe_pending;
+        CK(cudaMemcpyAsync(h->ctl, h->ctl_host, sizeof(Control), cudaMemcpyHostToDevice, h->stream), "control");
+        h->h2d_bytes += (long)sizeof(Control);
+        long long done = 0;
+        while (done < chunk)
+        {
+            if (use_graph && h->cur == 0 && chunk - done >= 2)
+            {
+                st = build_graph(h);
+                if (st) return st;
+                CK(cudaGraphLaunch(h->graph, h->stream), "graph launch");
+                h->launches += h->graph_kernels;
+                done += 2;
+            }
+            else
+            {
+                int k = 0;
+                CK(enqueue_batched_step(h, h->cur, k), "step launch");
+                h->launches += k;
+                h->cur ^= 1;
+                done += 1;
+            }
+        }
+        // the control block upload must not be overwritten before the copy ran
+        CK(cudaStreamSynchronize(h->stream), "step sync");
+        h->step += chunk;
+        if (np) h->probe_pending += chunk;
+        left -= chunk;
+        st = harvest_timing(h);
+        if (st) return st;
+        if (np && h->probe_pending >= kProbeRows)
+        {
+            st = drain_probes(h);
+            if (st) return st;
+        }
+    }
+    return LBM_OK;
+}
+
+extern "C" int lbm_run(lbm_handle* h, double T_total, int frames)
+{
+    int st = check_ready(h);
+    if (st) return st;
+    // 06:1066-1068; steps s = 0..total_steps inclusive (06:1077).
+    const int total_steps = (int)std::round(T_total / h->dt);
+    const int out_interval = std::max(1, total_steps / std::max(frames, 1));
+    if (h->cfg.verbose)
+        std::printf("Run: T_total=%g s, Frames=%d, total_steps=%d, out_interval=%d\n", T_total, frames, total_steps,
+                    out_interval);
+    int left = total_steps + 1;
+    while (left > 0)
+    {
+        const int n = std::min(left, 200);
+        st = lbm_step(h, n);
+        if (st) return st;
+        left -= n;
+        if (h->cfg.verbose) std::printf("Step %lld/%d\r", h->step - 1, total_steps);
+    }
+    if (h->cfg.verbose) std::printf("\nDone.\n");
+    return LBM_OK;
+}
+
+extern "C" int lbm_synchronize(lbm_handle* h)
+{
+    int st = check_ready(h);
+    if (st) return st;
+    CK(cudaStreamSynchronize(h->stream), "synchronize");
+    return LBM_OK;
+}
+
+// ---------------------------------------------------------------- results
+
+extern "C" int lbm_get_dims(lbm_handle* h, int* n3, int* n3h)
+{
+    int st = check_ready(h);
+    if (st) return st;
+    if (n3) { n3[0] = h->NXg; n3[1] = h->NYg; n3[2] = h->NZg; }
+    if (n3h) { n3h[0] = h->NXg + 2; n3h[1] = h->NYg + 2; n3h[2] = h->NZg + 2; }
+    return LBM_OK;
+}
+
+extern "C" double lbm_get_dt(lbm_handle* h)
+{
+    if (!h) return 0.0;
+    return (kCs * h->cfg.dx) / h->cfg.c_phys;
+}
+
+extern "C" long lbm_get_step(lbm_handle* h) { return h ? (long)h->step : -1; }
+
+extern "C" int lbm_get_probes(lbm_handle* h, double* out, long capacity, long* nsteps)
+{
+    int st = check_ready(h);
+    if (st) return st;
+    CK(cudaSetDevice(h->device), "cudaSetDevice");
+    st = drain_probes(h);
+    const int np = h->nprobe();
+    const long rows = np ? (long)(h->series.size() / np) : 0;
+    if (nsteps) *nsteps = rows;
+    if (!out) return st;
+    if ((long)h->series.size() > capacity) return h->fail(LBM_ERR_CAPACITY, "probe buffer too small");
+    std::copy(h->series.begin(), h->series.end(), out);
+    return st;
+}
+
+extern "C" int lbm_get_probe_energy(lbm_handle* h, double* out)
+{
+    int st = check_ready(h);
+    if (st) return st;
+    if (!out) return LBM_ERR_INVALID_ARGUMENT;
+    const int np = h->nprobe();
+    if (np == 0) return LBM_OK;
+    CK(cudaMemcpyAsync(out, h->d_energy, (size_t)np * 8, cudaMemcpyDeviceToHost, h->stream), "energy");
+    h->d2h_bytes += (long)np * 8;
+    CK(cudaStreamSynchronize(h->stream), "energy");
+    for (int p = 0; p < np; ++p)
+        if (!h->probe_owned[p]) out[p] = NAN;
+    return LBM_OK;
+}
+
+extern "C" int lbm_get_rho(lbm_handle* h, float* out, long capacity)
+{
+    int st = check_ready(h);
+    if (st) return st;
+    const Layout& L = h->L;
+    const size_t n = (size_t)L.nx * L.ny * L.nz;
+    if (!out || (long)n > capacity) return h->fail(LBM_ERR_CAPACITY, "rho buffer too small");
+    if (h->step == 0)
+    {
+        std::fill(out, out + n, 0.0f);   // rho initialised to 1 (06:368)
+        return LBM_OK;
+    }
+    CK(cudaSetDevice(h->device), "cudaSetDevice");
+    float* d = nullptr;
+    CK(cudaMalloc(&d, n * sizeof(float)), "rho buffer");
+    cudaError_t e = launch_field_rho(h->storage, h->f[h->cur ^ 1], d, L, h->sa, h->scale, h->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, d, n * sizeof(float), cudaMemcpyDeviceToHost, h->stream);
+    h->d2h_bytes += (long)(n * sizeof(float));
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    cudaFree(d);
+    if (e != cudaSuccess) return h->cuda_fail(e, "get_rho");
+    h->launches++;
+    return LBM_OK;
+}
+
+extern "C" int lbm_get_f(lbm_handle* h, double* out, long capacity)
+{
+    int st = check_ready(h);
+    if (st) return st;
+    const Layout& L = h->L;
+    const size_t n = (size_t)(L.nx + 2) * (L.ny + 2) * (L.nz + 2) * Q;
+    if (!out || (long)n > capacity) return h->fail(LBM_ERR_CAPACITY, "f buffer too small");
+    CK(cudaSetDevice(h->device), "cudaSetDevice");
+    double* d = nullptr;
+    CK(cudaMalloc(&d, n * sizeof(double)), "f export buffer");
+    cudaError_t e = launch_export_f(h->storage, h->f[h->cur], d, L, h->scale, h->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, d, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+    h->d2h_bytes += (long)(n * sizeof(double));
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    cudaFree(d);
+    if (e != cudaSuccess) return h->cuda_fail(e, "get_f");
+    h->launches++;
+    return LBM_OK;
+}
+
+extern "C" int lbm_set_f(lbm_handle* h, const double* in, long count)
+{
+    int st = check_ready(h);
+    if (st) return st;
+    const Layout& L = h->L;
+    const size_t n = (size_t)(L.nx + 2) * (L.ny + 2) * (L.nz + 2) * Q;
+    if (!in || count != (long)n) return h->fail(LBM_ERR_INVALID_ARGUMENT, "f size mismatch");
+    CK(cudaSetDevice(h->device), "cudaSetDevice");
+    double* d = nullptr;
+    CK(cudaMalloc(&d, n * sizeof(double)), "f import buffer");
+    cudaError_t e = cudaMemcpyAsync(d, in, n * sizeof(double), cudaMemcpyHostToDevice, h->stream);
+    h->h2d_bytes += (long)(n * sizeof(double));
+    if (e == cudaSuccess) e = launch_import_f(h->storage, h->f[h->cur], d, L, h->scale, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    cudaFree(d);
+    if (e != cudaSuccess) return h->cuda_fail(e, "set_f");
+    h->launches++;
+    h->halo_dirty = true;
+    return LBM_OK;
+}
+
+extern "C" int lbm_get_mask(lbm_handle* h, uint8_t* out, long capacity)
+{
+    int st = check_ready(h);
+    if (st) return st;
+    if (!out || (long)h->mask.size() > capacity) return h->fail(LBM_ERR_CAPACITY, "mask buffer too small");
+    std::copy(h->mask.begin(), h->mask.end(), out);
+    return LBM_OK;
+}
+
+// ---------------------------------------------------------------- measurement
+
+extern "C" int lbm_set_kernel_timing(lbm_handle* h, int enable)
+{
+    if (!h) return LBM_ERR_INVALID_ARGUMENT;
+    h->timing = enable != 0;
+    h->kernel_ms = 0.0;
+    h->kernel_launches = 0;
+    h->ev_used = 0;
+    return LBM_OK;
+}
+
+extern "C" int lbm_get_kernel_time(lbm_handle* h, double* total_ms, long* launches)
+{
+    if (!h) return LBM_ERR_INVALID_ARGUMENT;
+    int st = harvest_timing(h);
+    if (total_ms) *total_ms = h->kernel_ms;
+    if (launches) *launches = h->kernel_launches;
+    return st;
+}
+
+extern "C" long lbm_get_launch_count(lbm_handle* h) { return h ? h->launches : -1; }
+
+extern "C" void* lbm_get_stream(lbm_handle* h) { return h ? (void*)h->stream : nullptr; }
+
+extern "C" int lbm_get_transfer_bytes(lbm_handle* h, long* h2d, long* d2h)
+{
+    if (!h) return LBM_ERR_INVALID_ARGUMENT;
+    if (h2d) *h2d = h->h2d_bytes;
+    if (d2h) *d2h = h->d2h_bytes;
+    return LBM_OK;
+}
+
+extern "C" int lbm_bytes_per_cell(lbm_handle* h)
+{
+    if (!h) return 0;
+    return 2 * Q * (h->storage == LBM_STORE_F16 ? 2 : 4);
+}
+
+// ---------------------------------------------------------------- synthetic geometry
+
+extern "C" int lbm_city_generate(const lbm_city_params* p, float* tris, int capacity, int* ntris, double* coverage)
+{
+    if (!p || !ntris) return LBM_ERR_INVALID_ARGUMENT;
+    if (p->nx <= 0 || p->ny <= 0 || p->fp_min <= 0 || p->fp_max < p->fp_min || p->h_min <= 0 ||
+        p->h_max < p->h_min || p->street < 0 || p->margin < 0 || !(p->dx > 0))
+        return LBM_ERR_INVALID_ARGUMENT;
+    std::vector<float> t;
+    const double cov = city_generate(*p, t);
+    const int n = (int)(t.size() / 9);
+    *ntris = n;
+    if (coverage) *coverage = cov;
+    if (!tris || capacity < n) return LBM_ERR_CAPACITY;
+    std::copy(t.begin(), t.end(), tris);
+    return LBM_OK;
+}
+
+extern "C" int lbm_stl_write(const char* path, const float* tris, int ntris)
+{
+    if (!path || ntris < 0 || (ntris > 0 && !tris)) return LBM_ERR_INVALID_ARGUMENT;
+    return stl_write(path, tris, ntris) ? LBM_OK : LBM_ERR_IO;
+}
+
+extern "C" int lbm_voxelize(const lbm_config* cfg, const float* tris, int ntris, double scale, double sx, double sy,
+                            double sz, uint8_t* mask, long capacity, int* n3_halo)
+{
+    if (!cfg || ntris < 0 || (ntris > 0 && !tris)) return LBM_ERR_INVALID_ARGUMENT;
+    std::string why;
+    if (validate(*cfg, why) != LBM_OK) return LBM_ERR_BAD_CONFIG;
+    int nx, ny, nz;
+    grid_size(*cfg, nx, ny, nz);
+    if (nx < 1 || ny < 1 || nz < 1) return LBM_ERR_BAD_CONFIG;
+    if (n3_halo)
+    {
+        n3_halo[0] = nx + 2; n3_halo[1] = ny + 2; n3_halo[2] = nz + 2;
+    }
+    const long n = (long)(nx + 2) * (ny + 2) * (nz + 2);
+    if (!mask || capacity < n) return LBM_ERR_CAPACITY;
+    HeightField geo;
+    geo.set_triangles(tris, ntris, scale, sx, sy, sz);
+    build_mask(*cfg, geo, nx, ny, nz, mask);
+    return LBM_OK;
+}

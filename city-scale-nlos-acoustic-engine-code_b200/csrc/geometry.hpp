@@ -1,0 +1,49 @@
+// Host geometry: binary STL, the heightmap voxeliser of the reference's
+// GeometryEngine (06_transient_localization_dx1.cpp:60-193) and a seeded
+// synthetic city generator.  Built with -ffp-contract=off: every FP64
+// expression of the ray cast keeps the reference's operation order so the
+// voxelised mask is bit-identical.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+struct lbm_city_params;
+
+namespace lbm {
+
+class HeightField
+{
+public:
+    // GeometryEngine::load (06:70-111) from memory: 9 floats per triangle,
+    // vertex * scale + offset in FP64.
+    void set_triangles(const float* tris, int ntris, double scale, double sx, double sy, double sz);
+    // Returns false (and leaves the geometry empty) when the file cannot be opened.
+    bool load_stl(const std::string& path, double scale, double sx, double sy, double sz);
+    // GeometryEngine::getGroundHeight (06:144-192): highest hit of the ray
+    // from z = 10000 straight down, -1e30 when there is none.
+    double ground_height(double x, double y) const;
+    size_t triangle_count() const { return tris_.size(); }
+
+private:
+    struct Tri
+    {
+        double v1[3], v2[3], v3[3], mn[3], mx[3];
+    };
+    void build_bins();   // GeometryEngine::buildGrid (06:113-142), 200 x 200 bins
+
+    std::vector<Tri> tris_;
+    double gmin_[3] = {1e30, 1e30, 1e30};
+    double gmax_[3] = {-1e30, -1e30, -1e30};
+    double cell_w_ = 1.0, cell_h_ = 1.0;
+    std::vector<int> bin_start_;   // CSR offsets, 200*200+1
+    std::vector<int> bin_items_;
+};
+
+// Seeded city of axis-aligned box buildings on a street grid; 12 triangles
+// per box, vertices on multiples of dx.  Returns the plan coverage reached.
+double city_generate(const lbm_city_params& p, std::vector<float>& tris);
+bool stl_write(const char* path, const float* tris, int ntris);
+
+}  // namespace lbm

@@ -182,9 +182,13 @@ def bind_product(lib):
         "lbm_get_kernel_time": (ctypes.c_int, [P, c_double_p, c_long_p]),
         "lbm_get_launch_count": (ctypes.c_long, [P]),
         "lbm_bytes_per_cell": (ctypes.c_int, [P]),
+        "lbm_get_stream": (ctypes.c_void_p, [P]),
+        "lbm_get_transfer_bytes": (ctypes.c_int, [P, c_long_p, c_long_p]),
         "lbm_city_generate": (ctypes.c_int, [ctypes.POINTER(LbmCityParams), c_float_p, ctypes.c_int,
                                              c_int_p, c_double_p]),
         "lbm_stl_write": (ctypes.c_int, [ctypes.c_char_p, c_float_p, ctypes.c_int]),
+        "lbm_voxelize": (ctypes.c_int, [ctypes.POINTER(LbmConfig), c_float_p, ctypes.c_int] + [ctypes.c_double] * 4
+                         + [c_uint8_p, ctypes.c_long, c_int_p]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

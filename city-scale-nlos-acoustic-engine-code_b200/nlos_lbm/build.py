@@ -1,0 +1,85 @@
+"""Build recipe of the in-tree shared library ``nlos_lbm/liblbm_b200.so``.
+
+kernels.cu is compiled by nvcc for sm_100a only; the host C++ (api.cpp,
+geometry.cpp) by g++ with -ffp-contract=off so its FP64 arithmetic matches the
+reference's rounding.  The CUDA runtime is linked statically, so the library
+needs only the driver at run time.  Run ``python -m nlos_lbm.build`` or call
+``build()``.
+"""
+import os
+import shutil
+import subprocess
+import sys
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)                      # city-scale-nlos-acoustic-engine-code_b200/
+REPO = os.path.dirname(ROOT)
+CSRC = os.path.join(ROOT, "csrc")
+INCLUDE = os.path.join(REPO, "include")
+BUILD = os.path.join(ROOT, "_build")
+LIB = os.path.join(PKG, "liblbm_b200.so")
+
+CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
+NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
+CXX = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+CU_SOURCES = ["kernels.cu"]
+CXX_SOURCES = ["api.cpp", "geometry.cpp"]
+HEADERS = ["device.hpp", "geometry.hpp", "lattice.cuh"]
+
+
+def _newer(target, deps):
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def _run(cmd, verbose):
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("build step failed:\n" + " ".join(cmd) + "\n" + r.stdout + r.stderr)
+    if verbose and (r.stdout or r.stderr):
+        print(r.stdout + r.stderr, flush=True)
+    return r.stdout + r.stderr
+
+
+def build(verbose=False, force=False, ptxas_verbose=False):
+    """Compile the library if any source is newer than it; returns its path."""
+    os.makedirs(BUILD, exist_ok=True)
+    headers = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(INCLUDE, "nlos_lbm.h")]
+    objs = []
+    log = ""
+    for src in CU_SOURCES:
+        s = os.path.join(CSRC, src)
+        o = os.path.join(BUILD, src + ".o")
+        objs.append(o)
+        if force or _newer(o, [s] + headers):
+            cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-ccbin", CXX, "-Xcompiler", "-fPIC",
+                   "-I" + INCLUDE, "-I" + CSRC, "-c", s, "-o", o]
+            if ptxas_verbose:
+                cmd.insert(1, "-Xptxas=-v")
+            log += _run(cmd, verbose)
+    for src in CXX_SOURCES:
+        s = os.path.join(CSRC, src)
+        o = os.path.join(BUILD, src + ".o")
+        objs.append(o)
+        if force or _newer(o, [s] + headers):
+            cmd = [CXX, "-O2", "-std=c++17", "-fPIC", "-fopenmp", "-ffp-contract=off", "-fno-fast-math",
+                   "-Wall", "-Wno-unknown-pragmas", "-I" + INCLUDE, "-I" + CSRC,
+                   "-I" + os.path.join(CUDA_HOME, "include"), "-c", s, "-o", o]
+            log += _run(cmd, verbose)
+    if force or _newer(LIB, objs):
+        tmp = LIB + ".tmp"
+        cmd = [NVCC, *ARCH, "-shared", "-ccbin", CXX, "-Xcompiler", "-fopenmp", "-o", tmp, *objs, "-lgomp"]
+        log += _run(cmd, verbose)
+        shutil.move(tmp, LIB)
+    return LIB if not ptxas_verbose else (LIB, log)
+
+
+if __name__ == "__main__":
+    res = build(verbose=True, force="--force" in sys.argv, ptxas_verbose="-v" in sys.argv)
+    print(res if isinstance(res, str) else res[1])

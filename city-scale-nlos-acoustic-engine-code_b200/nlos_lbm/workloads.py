@@ -1,0 +1,122 @@
+"""Seeded synthetic workloads at full size.
+
+Lattice units throughout (dx = 1, c_phys = cs, so dt = 1 and times count
+steps).  The city workloads stand in for the reference's real-city STL
+(csx_model_binary.stl, 06:1131), which is not distributed: buildings are
+seeded axis-aligned boxes written as triangles and voxelised by the
+reference's heightmap ray cast.
+
+  scatter    128^3 open box, rigid 16^3 cube, Gaussian pulse, 20-cell sponge
+  lloyd      256x128x128, ground wall, moving sine source (Mach 0.1), trilinear
+  city1024   1024x1024x256 city, 4 Ricker sources at street level, 256 probes
+  city2048   2048x2048x256 city, one source flying at z = 120 at Mach 0.15,
+             512 probes (FP16 deviation storage, scale 1/amplitude)
+"""
+import numpy as np
+
+from . import abi
+
+ALL_FACES = (1 << 6) - 1
+FIVE_FACES = ALL_FACES & ~(1 << abi.FACE_ZLO)
+MACH_TO_CELLS = abi.CS   # cells/step per unit Mach (c = cs in lattice units)
+
+
+def lattice_config(nx, ny, nz, tau, **kw):
+    base = dict(x_min=0.0, x_max=float(nx), y_min=0.0, y_max=float(ny), z_min=0.0, z_max=float(nz), dx=1.0,
+                c_phys=abi.CS, tau=tau, sky_z=1e30)
+    base.update(kw)
+    return abi.reference_config(**base)
+
+
+def footprints(tris):
+    b = np.asarray(tris, dtype=np.float64).reshape(-1, 12, 3, 3)
+    return b.min(axis=(1, 2)), b.max(axis=(1, 2))
+
+
+def street_points(tris, nx, ny, n, z, seed, margin=40, clearance=2.0):
+    """n random points at height z that lie in the streets (outside every
+    building footprint by `clearance` cells) and `margin` cells inside the plan."""
+    lo, hi = footprints(tris)
+    rng = np.random.default_rng(seed)
+    out = []
+    while len(out) < n:
+        c = np.stack([rng.uniform(margin, nx - margin, 4 * n), rng.uniform(margin, ny - margin, 4 * n)], 1)
+        inside = ((c[:, None, 0] > lo[None, :, 0] - clearance) & (c[:, None, 0] < hi[None, :, 0] + clearance)
+                  & (c[:, None, 1] > lo[None, :, 1] - clearance) & (c[:, None, 1] < hi[None, :, 1] + clearance))
+        ok = c[~inside.any(1)]
+        out.extend(ok.tolist())
+    pts = np.array(out[:n])
+    return np.concatenate([pts, np.full((n, 1), z)], 1)
+
+
+def city(nx, ny, nz, seed, storage, tau=0.51, sponge=32):
+    from .solver import city_triangles
+
+    tris, cov = city_triangles(nx, ny, seed=seed, fp=(20, 60), height=(10, 80), coverage=0.40, street=8,
+                               margin=sponge + 8)
+    amp = 1e-3
+    cfg = lattice_config(nx, ny, nz, tau, sponge_width=float(sponge), sponge_faces=FIVE_FACES, storage=storage,
+                         f16_scale=1.0 / amp)
+    return cfg, tris, cov, amp
+
+
+def build(name, storage=None, seed=2024):
+    """dict(cfg, sources, probes, triangles, steps, description)."""
+    if name == "scatter":
+        n = 128
+        cfg = lattice_config(n, n, n, 0.55, face_bc=(abi.LBM_BC_NSCBC,) * 6, sponge_faces=ALL_FACES,
+                             sponge_width=20.0, sponge_strength=0.5,
+                             storage=abi.LBM_STORE_F32 if storage is None else storage, f16_scale=1e3)
+        c = n / 2
+        tris = _cube(c - 8, c + 8)
+        src = abi.reference_source(sx=c - 24 + 0.5, sy=c + 0.5, sz=c + 0.5, ex=c - 24 + 0.5, ey=c + 0.5,
+                                   ez=c + 0.5, amp=1e-3, t0=40.0, sigma_t=8.0)
+        a = 2 * np.pi * np.arange(8) / 8
+        probes = np.stack([c + 40 * np.cos(a), c + 40 * np.sin(a), np.full(8, c)], 1)
+        return dict(cfg=cfg, sources=[src], probes=probes, triangles=tris, steps=2000,
+                    description="acoustic scattering 128^3, cube 16^3, Gaussian pulse")
+    if name == "lloyd":
+        cfg = lattice_config(256, 128, 128, 0.52, sponge_width=16.0, sponge_faces=FIVE_FACES,
+                             storage=abi.LBM_STORE_F32 if storage is None else storage, f16_scale=2e3)
+        v = 0.1 * MACH_TO_CELLS
+        src = abi.reference_source(sx=40.0, sy=64.0, sz=20.0, ex=250.0, ey=64.0, ez=20.0, speed=v, amp=5e-4,
+                                   freq=1 / 50.0, waveform=abi.LBM_WAVE_SINE, injection=abi.LBM_INJECT_TRILINEAR)
+        probes = np.stack([np.linspace(8.5, 247.5, 64), np.full(64, 64.5), np.full(64, 10.5)], 1)
+        return dict(cfg=cfg, sources=[src], probes=probes, triangles=None, steps=6000,
+                    description="Lloyd's mirror 256x128x128, moving sine source Mach 0.1, trilinear")
+    if name == "city1024":
+        st = abi.LBM_STORE_F32 if storage is None else storage
+        cfg, tris, cov, amp = city(1024, 1024, 256, seed, st)
+        pts = street_points(tris, 1024, 1024, 4 + 256, 2.5, seed)
+        srcs = [abi.reference_source(sx=p[0], sy=p[1], sz=p[2], ex=p[0], ey=p[1], ez=p[2], amp=amp, freq=1 / 40.0,
+                                     t0=60.0, waveform=abi.LBM_WAVE_RICKER, injection=abi.LBM_INJECT_TRILINEAR)
+                for p in pts[:4]]
+        return dict(cfg=cfg, sources=srcs, probes=pts[4:], triangles=tris, steps=4000, coverage=cov,
+                    description="synthetic city 1024x1024x256, 4 Ricker sources, 256 street probes")
+    if name == "city2048":
+        st = abi.LBM_STORE_F16 if storage is None else storage
+        cfg, tris, cov, amp = city(2048, 2048, 256, seed, st)
+        probes = street_points(tris, 2048, 2048, 512, 2.5, seed)
+        v = 0.15 * MACH_TO_CELLS
+        src = abi.reference_source(sx=400.0, sy=600.0, sz=120.0, ex=1650.0, ey=1450.0, ez=120.0, speed=v, amp=amp,
+                                   freq=1 / 40.0, waveform=abi.LBM_WAVE_SINE, injection=abi.LBM_INJECT_TRILINEAR)
+        return dict(cfg=cfg, sources=[src], probes=probes, triangles=tris, steps=4000, coverage=cov,
+                    description="synthetic city 2048x2048x256, source flying at z=120 Mach 0.15, 512 probes")
+    raise KeyError(name)
+
+
+def _cube(a, b):
+    v = [(a, a, a), (b, a, a), (b, b, a), (a, b, a), (a, a, b), (b, a, b), (b, b, b), (a, b, b)]
+    quads = [(0, 3, 2, 1), (4, 5, 6, 7), (0, 1, 5, 4), (1, 2, 6, 5), (2, 3, 7, 6), (3, 0, 4, 7)]
+    out = []
+    for q in quads:
+        out.append(v[q[0]] + v[q[1]] + v[q[2]])
+        out.append(v[q[0]] + v[q[2]] + v[q[3]])
+    return np.asarray(out, dtype=np.float32)
+
+
+def cells(cfg):
+    nx = int((cfg.x_max - cfg.x_min) / cfg.dx + 0.5)
+    ny = int((cfg.y_max - cfg.y_min) / cfg.dx + 0.5)
+    nz = int((cfg.z_max - cfg.z_min) / cfg.dx + 0.5)
+    return nx, ny, nz

@@ -162,6 +162,12 @@ int lbm_set_geometry_triangles(lbm_handle* h, const float* tris, int ntris, doub
  * reference's halo-inclusive order i + j*nx_t + k*nx_t*ny_t (06:206-209). */
 int lbm_set_mask(lbm_handle* h, const uint8_t* mask, int nx_t, int ny_t, int nz_t);
 
+/* The mask lbm_init builds for this config and triangle set (init_domain
+ * 06:453-532), computed on the host; needs no device.  n3_halo receives
+ * nx_t, ny_t, nz_t; mask needs nx_t*ny_t*nz_t bytes. */
+int lbm_voxelize(const lbm_config* cfg, const float* tris, int ntris, double scale, double sx, double sy, double sz,
+                 uint8_t* mask, long capacity, int* n3_halo);
+
 /* ---- sources and probes ------------------------------------------------- */
 
 /* Adds a source (the reference has exactly one, LBMSolver::drone 06:246). */
@@ -230,6 +236,12 @@ int lbm_get_kernel_time(lbm_handle* h, double* total_ms, long* launches);
 long lbm_get_launch_count(lbm_handle* h);
 /* Bytes per cell update the fused step moves by algorithm: 2*19*sizeof(store). */
 int lbm_bytes_per_cell(lbm_handle* h);
+/* The handle's CUDA stream (a cudaStream_t), for callers that record their
+ * own CUDA events around library calls. */
+void* lbm_get_stream(lbm_handle* h);
+/* Host<->device bytes the handle has copied since lbm_init (source
+ * schedules, control blocks and uploads in; probe series and results out). */
+int lbm_get_transfer_bytes(lbm_handle* h, long* h2d, long* d2h);
 
 /* ---- synthetic geometry -------------------------------------------------- */
 

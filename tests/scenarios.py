@@ -1,0 +1,109 @@
+"""Seeded parity scenarios shared by the GPU tests, the fixture generator and
+the smoke check.  Each scenario is a small version of one workload the solver
+is run on (reference-native set-ups of 06/08 and reduced versions of the
+scattering / Lloyd's-mirror / synthetic-city workloads); both the CUDA solver
+and the FP64 oracle are built from the same description.
+"""
+import numpy as np
+
+from nlos_lbm import abi
+
+ALL_FACES = (1 << 6) - 1
+FIVE_FACES = ALL_FACES & ~(1 << abi.FACE_ZLO)
+
+
+def boxes_to_triangles(boxes):
+    from oracle import box_triangles
+
+    return box_triangles(boxes)
+
+
+def lattice_config(nx, ny, nz, tau, **kw):
+    """Lattice units: dx = 1 and c_phys = cs, so dt = 1 and t counts steps."""
+    base = dict(x_min=0.0, x_max=float(nx), y_min=0.0, y_max=float(ny), z_min=0.0, z_max=float(nz), dx=1.0,
+                c_phys=abi.CS, tau=tau, sky_z=1e30)
+    base.update(kw)
+    return abi.reference_config(**base)
+
+
+def ring_probes(center, radius, n, z):
+    a = 2 * np.pi * np.arange(n) / n
+    return np.stack([center[0] + radius * np.cos(a), center[1] + radius * np.sin(a), np.full(n, z)], 1)
+
+
+def scenario(name, storage=abi.LBM_STORE_F32, f16_scale=1.0):
+    """Returns dict(cfg, sources, probes, triangles, steps)."""
+    if name == "ref06_box":
+        # 06 physics: physical units, dx = 1 m, Gaussian pulse (06:579-581), ground wall,
+        # NSCBC on the other faces, 20-cell sponge at strength 0.35.
+        cfg = abi.reference_config(x_min=0, x_max=48, y_min=0, y_max=32, z_min=0, z_max=30, dx=1.0, tau=0.55)
+        src = abi.reference_source(sx=24.3, sy=16.2, sz=12.7, ex=24.3, ey=16.2, ez=12.7, amp=10.0)
+        tris = boxes_to_triangles([(10, 8, 0, 22, 20, 12), (30, 5, 0, 41, 14, 7), (26, 20, 0, 38, 30, 16)])
+        probes = np.array([[20.5, 16.5, 10.5], [30.5, 16.5, 20.5], [5.2, 3.3, 2.1], [15.0, 12.0, 5.0]])
+        return dict(cfg=cfg, sources=[src], probes=probes, triangles=tris, steps=80)
+    if name == "ref08_moving":
+        # 08 physics: sine source flying across the domain (08:543, 06:221-238).
+        cfg = abi.reference_config(x_min=0, x_max=48, y_min=0, y_max=32, z_min=0, z_max=30, dx=1.0, tau=0.55)
+        src = abi.reference_source(sx=5.0, sy=6.0, sz=20.0, ex=40.0, ey=25.0, ez=22.0, speed=300.0, amp=0.5,
+                                   freq=20.0, waveform=abi.LBM_WAVE_SINE)
+        tris = boxes_to_triangles([(10, 8, 0, 22, 20, 12), (30, 5, 0, 41, 14, 7)])
+        probes = np.array([[20.5, 16.5, 14.5], [40.5, 26.5, 20.5], [8.0, 28.0, 3.0]])
+        return dict(cfg=cfg, sources=[src], probes=probes, triangles=tris, steps=60)
+    if name == "scatter_small":
+        # Acoustic scattering: open box (NSCBC on all six faces), rigid cube at the
+        # centre, Gaussian pulse 12 cells away, sponge on every face ramping to 0.5.
+        n = 48
+        cfg = lattice_config(n, n, n, 0.55, face_bc=(abi.LBM_BC_NSCBC,) * 6, sponge_faces=ALL_FACES,
+                             sponge_width=10.0, sponge_strength=0.5, storage=storage, f16_scale=f16_scale)
+        c = n / 2
+        tris = boxes_to_triangles([(c - 4, c - 4, c - 4, c + 4, c + 4, c + 4)])
+        src = abi.reference_source(sx=c - 12.0 + 0.3, sy=c + 0.2, sz=c + 0.1, ex=c - 11.7, ey=c + 0.2, ez=c + 0.1,
+                                   amp=1e-3, t0=20.0, sigma_t=4.0)
+        probes = ring_probes((c, c), 16.0, 8, c)
+        return dict(cfg=cfg, sources=[src], probes=probes, triangles=tris, steps=240)
+    if name == "lloyd_small":
+        # Lloyd's mirror: ground wall, moving sine source, trilinear injection, probe line.
+        cfg = lattice_config(64, 32, 32, 0.52, sponge_width=8.0, sponge_faces=FIVE_FACES, storage=storage,
+                             f16_scale=f16_scale)
+        src = abi.reference_source(sx=12.0, sy=16.0, sz=10.0, ex=60.0, ey=16.0, ez=10.0, speed=0.0577, amp=5e-4,
+                                   freq=1.0 / 50.0, waveform=abi.LBM_WAVE_SINE, injection=abi.LBM_INJECT_TRILINEAR)
+        probes = np.stack([np.linspace(4.5, 59.5, 16), np.full(16, 16.5), np.full(16, 5.5)], 1)
+        return dict(cfg=cfg, sources=[src], probes=probes, triangles=None, steps=300)
+    if name == "city_small":
+        # Synthetic city: seeded box buildings (STL triangles -> voxeliser), ground wall,
+        # sponge on sides and top, two Ricker sources at street level.
+        import nlos_lbm
+
+        nx, ny, nz = 96, 80, 40
+        tris, _ = nlos_lbm.city_triangles(nx, ny, seed=7, fp=(12, 24), height=(6, 30), street=6, margin=4)
+        cfg = lattice_config(nx, ny, nz, 0.51, sponge_width=10.0, sponge_faces=FIVE_FACES, storage=storage,
+                             f16_scale=f16_scale)
+        mask = nlos_lbm.voxelize(cfg, tris).reshape(nz + 2, ny + 2, nx + 2)
+        rng = np.random.default_rng(7)
+        pts = []
+        while len(pts) < 2 + 12:
+            x, y = rng.uniform(6, nx - 6), rng.uniform(6, ny - 6)
+            if mask[3, int(y) + 1, int(x) + 1] == 0:
+                pts.append((x, y, 2.5))
+        srcs = [abi.reference_source(sx=p[0], sy=p[1], sz=p[2], ex=p[0], ey=p[1], ez=p[2], amp=1e-3, freq=1 / 40.0,
+                                     t0=40.0, waveform=abi.LBM_WAVE_RICKER, injection=abi.LBM_INJECT_TRILINEAR)
+                for p in pts[:2]]
+        probes = np.array(pts[2:])
+        return dict(cfg=cfg, sources=srcs, probes=probes, triangles=tris, steps=200)
+    raise KeyError(name)
+
+
+def build_pair(sc):
+    """(CUDA solver, FP64 oracle) for one scenario."""
+    from nlos_lbm import Solver
+    from oracle import OracleSolver
+
+    g = Solver(sc["cfg"], sc["sources"], sc["probes"], triangles=sc["triangles"])
+    o = OracleSolver(sc["cfg"], sc["sources"], sc["probes"], triangles=sc["triangles"])
+    return g, o
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
