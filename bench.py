@@ -148,7 +148,7 @@ def measure(name, storage, steps, warmup, device, torch, barrier, reduce_max, ke
     s.set_kernel_timing(False)
     ms_max = reduce_max(ms)
     probes = s.get_probes()
-    res = dict(name=name, storage="fp16" if storage == 1 else "fp32", cells=ncell, dims=[nx, ny, nz],
+    res = dict(name=name, storage="fp16" if s.bytes_per_cell == 76 else "fp32", cells=ncell, dims=[nx, ny, nz],
                steps=steps, ms=ms_max, ms_local=ms, setup_s=setup_s, glups_rank=ncell * steps / (ms_max / 1e3) / 1e9,
                kernel_ms_avg=kms / max(kn, 1), kernel_launches=kn, launches=launches,
                bytes_per_cell=s.bytes_per_cell, probes_finite=bool(np.all(np.isfinite(probes))),
@@ -279,7 +279,8 @@ def run_our_arm(args):
     hbm_peak, peak_kind = measured_peaks()
     headline = args.workload
     with ClockSampler(local) as clk:
-        s, w, head = measure(headline, None, args.steps, args.warmup, local, torch, barrier, reduce_max)
+        storage = None if args.storage is None else (1 if args.storage == "fp16" else 0)
+        s, w, head = measure(headline, storage, args.steps, args.warmup, local, torch, barrier, reduce_max)
     clocks = clk.summary()
     # e2e through the C-ABI with host buffers (same workload, same handle)
     e2e_ms, h2d_ps, d2h_ps = e2e_measure(s, w, args.steps)
@@ -348,7 +349,9 @@ def main():
     ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="city2048", choices=["city2048", "city1024", "lloyd", "scatter"])
+    ap.add_argument("--workload", default="city2048", choices=["city2048", "city1024", "city512", "lloyd", "scatter"])
+    ap.add_argument("--storage", default=None, choices=["fp32", "fp16"],
+                    help="population storage of the headline workload (default: the workload's own)")
     ap.add_argument("--headline-only", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()

@@ -79,6 +79,7 @@ struct lbm_handle
     uint32_t* links = nullptr;
     uint32_t* near = nullptr;
     float* sig = nullptr;              // sig_x | sig_y | sig_z
+    XFace xf{nullptr, nullptr};        // x-face exports and ghosts
     StepArgs sa{};
     GhostArgs ga{};
     Control* ctl = nullptr;            // device
@@ -137,6 +138,8 @@ struct lbm_handle
         cudaFree(links); links = nullptr;
         cudaFree(near); near = nullptr;
         cudaFree(sig); sig = nullptr;
+        cudaFree(xf.xexp); xf.xexp = nullptr;
+        cudaFree(xf.xgh); xf.xgh = nullptr;
         cudaFree(ctl); ctl = nullptr;
         cudaFree(d_table); d_table = nullptr;
         cudaFree(d_probe_cell); d_probe_cell = nullptr;
@@ -580,10 +583,15 @@ extern "C" int lbm_init(lbm_handle* h)
     const size_t near_words = (size_t)nzt * nyt * L.words_per_row;
     h->near = dalloc<uint32_t>(near_words, e);
     h->sig = dalloc<float>((size_t)nx + ny + nz, e);
+    const size_t n_xexp = (size_t)2 * Q * ny * nz, n_xgh = (size_t)2 * Q * nyt * nzt;
+    h->xf.xexp = dalloc<float>(n_xexp, e);
+    h->xf.xgh = dalloc<float>(n_xgh, e);
     h->ctl = dalloc<Control>(1, e);
     if (e != cudaSuccess) return h->cuda_fail(e, "device allocation");
     CK(cudaMemsetAsync(h->links, 0, cells * sizeof(uint32_t), h->stream), "memset links");
     CK(cudaMemsetAsync(h->near, 0, near_words * sizeof(uint32_t), h->stream), "memset near");
+    CK(cudaMemsetAsync(h->xf.xexp, 0, n_xexp * sizeof(float), h->stream), "memset x faces");
+    CK(cudaMemsetAsync(h->xf.xgh, 0, n_xgh * sizeof(float), h->stream), "memset x faces");
     CK(cudaMallocHost(&h->ctl_host, sizeof(Control)), "cudaMallocHost");
     CK(cudaMemcpyAsync(h->sig, sx.data(), sx.size() * 4, cudaMemcpyHostToDevice, h->stream), "upload sponge");
     CK(cudaMemcpyAsync(h->sig + nx, sy.data(), sy.size() * 4, cudaMemcpyHostToDevice, h->stream), "upload sponge");
@@ -608,10 +616,12 @@ extern "C" int lbm_init(lbm_handle* h)
     h->sa.sig_y = h->sig + nx;
     h->sa.sig_z = h->sig + nx + ny;
     h->sa.omega = (float)(1.0 / c.tau);
+    h->sa.xf = h->xf;
 
     // Open faces for the ghost kernel.
     h->ga = GhostArgs{};
     h->ga.scale = h->scale;
+    h->ga.xf = h->xf;
     long long first = 0;
     for (int f = 0; f < 6; ++f)
     {
@@ -871,7 +881,7 @@ int reset_halos_if_dirty(lbm_handle* h)
     const size_t nloc = (size_t)(L.nx + 2) * (L.ny + 2) * (L.nz + 2);
     double* d = nullptr;
     CK(cudaMalloc(&d, nloc * Q * sizeof(double)), "halo reset");
-    cudaError_t e = launch_export_f(h->storage, h->f[h->cur], d, L, h->scale, h->stream);
+    cudaError_t e = launch_export_f(h->storage, h->f[h->cur], d, L, h->xf, h->scale, h->stream);
     if (e == cudaSuccess)
     {
         tmp.resize(nloc * Q);
@@ -890,7 +900,7 @@ int reset_halos_if_dirty(lbm_handle* h)
                     for (int q = 0; q < Q; ++q) tmp[idx * Q + q] = wd(q);
                 }
         e = cudaMemcpyAsync(d, tmp.data(), nloc * Q * sizeof(double), cudaMemcpyHostToDevice, h->stream);
-        if (e == cudaSuccess) e = launch_import_f(h->storage, h->f[h->cur], d, L, h->scale, h->stream);
+        if (e == cudaSuccess) e = launch_import_f(h->storage, h->f[h->cur], d, L, h->xf, h->scale, h->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     }
     cudaFree(d);
@@ -1149,7 +1159,7 @@ extern "C" int lbm_get_f(lbm_handle* h, double* out, long capacity)
     CK(cudaSetDevice(h->device), "cudaSetDevice");
     double* d = nullptr;
     CK(cudaMalloc(&d, n * sizeof(double)), "f export buffer");
-    cudaError_t e = launch_export_f(h->storage, h->f[h->cur], d, L, h->scale, h->stream);
+    cudaError_t e = launch_export_f(h->storage, h->f[h->cur], d, L, h->xf, h->scale, h->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(out, d, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
     h->d2h_bytes += (long)(n * sizeof(double));
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
@@ -1171,7 +1181,7 @@ extern "C" int lbm_set_f(lbm_handle* h, const double* in, long count)
     CK(cudaMalloc(&d, n * sizeof(double)), "f import buffer");
     cudaError_t e = cudaMemcpyAsync(d, in, n * sizeof(double), cudaMemcpyHostToDevice, h->stream);
     h->h2d_bytes += (long)(n * sizeof(double));
-    if (e == cudaSuccess) e = launch_import_f(h->storage, h->f[h->cur], d, L, h->scale, h->stream);
+    if (e == cudaSuccess) e = launch_import_f(h->storage, h->f[h->cur], d, L, h->xf, h->scale, h->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     cudaFree(d);
     if (e != cudaSuccess) return h->cuda_fail(e, "set_f");

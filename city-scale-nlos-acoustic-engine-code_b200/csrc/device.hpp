@@ -75,12 +75,35 @@ struct GhostFace
     long long first;       // first thread index of this face
 };
 
+// x-face buffers (float, stored deviation units).  The x-halo columns of the
+// population arrays are not used: the fused step exports the post-collision
+// populations of the cells next to the x faces into `xexp`, the ghost kernel
+// turns them into the open-boundary ghosts `xgh`, and the step reads those
+// for the first and last cell of each row.  Both are [side][q][k][j] and
+// coalesced along j, so no strided column of the populations is touched.
+//   xexp: side 0/1 = cells i = 1 / i = nx, j = 1..ny, k = 1..nz  -> [2][Q][nz][ny]
+//   xgh : side 0/1 = halo i = 0 / i = nx+1, j = 0..ny+1, k = 0..nz+1 -> [2][Q][nz+2][ny+2]
+struct XFace
+{
+    float* xexp;
+    float* xgh;
+    __host__ __device__ long long exp_index(int side, int q, int j, int k, int ny, int nz) const
+    {
+        return ((long long)(side * 19 + q) * nz + (k - 1)) * ny + (j - 1);
+    }
+    __host__ __device__ long long gh_index(int side, int q, int j, int k, int ny, int nz) const
+    {
+        return ((long long)(side * 19 + q) * (nz + 2) + k) * (ny + 2) + j;
+    }
+};
+
 struct GhostArgs
 {
     int nfaces;
     GhostFace face[6];
     long long total;
     float scale;
+    XFace xf;
 };
 
 struct StepArgs
@@ -91,6 +114,7 @@ struct StepArgs
     const float* sig_y;
     const float* sig_z;
     float omega;               // 1 / tau
+    XFace xf;
 };
 
 struct ProbeArgs
@@ -120,9 +144,9 @@ cudaError_t launch_field_rho(int storage, const void* f, float* out, const Layou
                              float scale, cudaStream_t stream);
 // Conversions between the stored deviations and FP64 f in the reference's
 // AoS halo-inclusive layout (f[idx*19+q]).
-cudaError_t launch_export_f(int storage, const void* f, double* out, const Layout& L, float scale,
+cudaError_t launch_export_f(int storage, const void* f, double* out, const Layout& L, const XFace& xf, float scale,
                             cudaStream_t stream);
-cudaError_t launch_import_f(int storage, void* f, const double* in, const Layout& L, float scale,
+cudaError_t launch_import_f(int storage, void* f, const double* in, const Layout& L, const XFace& xf, float scale,
                             cudaStream_t stream);
 
 }  // namespace lbm

@@ -8,6 +8,7 @@ reference's heightmap ray cast.
 
   scatter    128^3 open box, rigid 16^3 cube, Gaussian pulse, 20-cell sponge
   lloyd      256x128x128, ground wall, moving sine source (Mach 0.1), trilinear
+  city512    512x512x128 city (profiler-sized), 2 Ricker sources, 64 probes
   city1024   1024x1024x256 city, 4 Ricker sources at street level, 256 probes
   city2048   2048x2048x256 city, one source flying at z = 120 at Mach 0.15,
              512 probes (FP16 deviation storage, scale 1/amplitude)
@@ -93,6 +94,16 @@ def build(name, storage=None, seed=2024):
                 for p in pts[:4]]
         return dict(cfg=cfg, sources=srcs, probes=pts[4:], triangles=tris, steps=4000, coverage=cov,
                     description="synthetic city 1024x1024x256, 4 Ricker sources, 256 street probes")
+    if name == "city512":
+        # a few-GB version of the city for profiler captures
+        st = abi.LBM_STORE_F32 if storage is None else storage
+        cfg, tris, cov, amp = city(512, 512, 128, seed, st)
+        pts = street_points(tris, 512, 512, 2 + 64, 2.5, seed)
+        srcs = [abi.reference_source(sx=p[0], sy=p[1], sz=p[2], ex=p[0], ey=p[1], ez=p[2], amp=amp, freq=1 / 40.0,
+                                     t0=60.0, waveform=abi.LBM_WAVE_RICKER, injection=abi.LBM_INJECT_TRILINEAR)
+                for p in pts[:2]]
+        return dict(cfg=cfg, sources=srcs, probes=pts[2:], triangles=tris, steps=4000, coverage=cov,
+                    description="synthetic city 512x512x128, 2 Ricker sources, 64 street probes")
     if name == "city2048":
         st = abi.LBM_STORE_F16 if storage is None else storage
         cfg, tris, cov, amp = city(2048, 2048, 256, seed, st)

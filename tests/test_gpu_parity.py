@@ -20,8 +20,8 @@ pytestmark = pytest.mark.gpu
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
-# probe relative-L2 error vs the FP64 oracle, FP32 deviation storage
-FP32_PROBE_TOL = 1e-4
+# probe relative-L2 error vs the FP64 oracle, FP32 deviation storage (measured <= 3e-6)
+FP32_PROBE_TOL = 1e-5
 # largest population deviation error, relative to the largest deviation
 FP32_STATE_TOL = 1e-4
 # FP16 deviation storage with scale 1/amplitude: the 1e-3 probe target
@@ -158,10 +158,15 @@ def test_probe_flags_and_solid_probe(gpu):
     assert abi.LBM_WARN_PROBE_IN_SOLID in g.warnings
     owned, solid = g.probe_info()
     assert list(owned) == [True] * 5 + [False]
-    assert list(solid) == [False] * 4 + [True, False]
+    nx, ny, nz = g.dims_halo
+    m = g.get_mask().reshape(nz, ny, nx)
+    ijk = np.floor(probes[:5]).astype(int) + 1
+    expect = [bool(m[k, j, i]) for i, j, k in ijk]
+    assert expect[4] and list(solid) == expect + [False]
     g.step(40)
     p = g.get_probes()
-    assert np.all(p[:, 4] == 0.0) and np.all(np.isnan(p[:, 5]))
+    assert np.all(p[:, np.array(expect + [False])] == 0.0) and np.all(np.isnan(p[:, 5]))
+    assert np.max(np.abs(p[:, 1])) > 0
     e = g.get_probe_energy()
     np.testing.assert_allclose(e[:5], (p[:, :5] ** 2).sum(0), rtol=1e-12)
 
