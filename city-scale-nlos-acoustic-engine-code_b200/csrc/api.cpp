@@ -11,6 +11,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <new>
@@ -28,6 +29,8 @@ namespace {
 
 constexpr int kTableRows = 4096;   // source-schedule rows resident on the device
 constexpr int kProbeRows = 4096;   // probe-series rows buffered on the device
+constexpr int kDefaultStepVariant = 0;
+constexpr int kDefaultPrefetchRows = 0;
 
 struct SourceState
 {
@@ -51,6 +54,9 @@ struct lbm_handle
     std::string err;
     int storage = LBM_STORE_F32;
     float scale = 1.0f;
+    int step_variant = kDefaultStepVariant;   // fused-step implementation (NLOS_LBM_STEP_VARIANT)
+    int step_grid = 0;                 // persistent grid of the staged variants
+    int* d_error = nullptr;            // kernel error word (bounded waits)
 
     // geometry / mask
     HeightField geo;
@@ -141,6 +147,7 @@ struct lbm_handle
         cudaFree(xf.xexp); xf.xexp = nullptr;
         cudaFree(xf.xgh); xf.xgh = nullptr;
         cudaFree(ctl); ctl = nullptr;
+        cudaFree(d_error); d_error = nullptr;
         cudaFree(d_table); d_table = nullptr;
         cudaFree(d_probe_cell); d_probe_cell = nullptr;
         cudaFree(d_probe_out); d_probe_out = nullptr;
@@ -387,6 +394,7 @@ extern "C" const char* lbm_status_string(int s)
     case LBM_ERR_NO_DEVICE: return "no CUDA device";
     case LBM_ERR_IO: return "I/O error";
     case LBM_ERR_UNSUPPORTED: return "unsupported";
+    case LBM_ERR_TIMEOUT: return "kernel wait timed out";
     default: return "unknown status";
     }
 }
@@ -538,7 +546,7 @@ extern "C" int lbm_init(lbm_handle* h)
     L.pitch = (nx + 2 + 31) / 32 * 32;
     L.words_per_row = L.pitch / 32;
     L.plane = (long long)L.pitch * nyt;
-    L.pop_stride = ((long long)kFrontPad + L.plane * nzt + 32 + 63) / 64 * 64;
+    L.pop_stride = ((long long)kFrontPad + L.plane * nzt + kBackPad + 63) / 64 * 64;
     if (L.pop_stride >= (1ll << 31)) return h->fail(LBM_ERR_UNSUPPORTED, "grid too large for one GPU");
 
     // Mask (init_domain 06:453-532).
@@ -587,11 +595,13 @@ extern "C" int lbm_init(lbm_handle* h)
     h->xf.xexp = dalloc<float>(n_xexp, e);
     h->xf.xgh = dalloc<float>(n_xgh, e);
     h->ctl = dalloc<Control>(1, e);
+    h->d_error = dalloc<int>(1, e);
     if (e != cudaSuccess) return h->cuda_fail(e, "device allocation");
     CK(cudaMemsetAsync(h->links, 0, cells * sizeof(uint32_t), h->stream), "memset links");
     CK(cudaMemsetAsync(h->near, 0, near_words * sizeof(uint32_t), h->stream), "memset near");
     CK(cudaMemsetAsync(h->xf.xexp, 0, n_xexp * sizeof(float), h->stream), "memset x faces");
     CK(cudaMemsetAsync(h->xf.xgh, 0, n_xgh * sizeof(float), h->stream), "memset x faces");
+    CK(cudaMemsetAsync(h->d_error, 0, sizeof(int), h->stream), "memset error");
     CK(cudaMallocHost(&h->ctl_host, sizeof(Control)), "cudaMallocHost");
     CK(cudaMemcpyAsync(h->sig, sx.data(), sx.size() * 4, cudaMemcpyHostToDevice, h->stream), "upload sponge");
     CK(cudaMemcpyAsync(h->sig + nx, sy.data(), sy.size() * 4, cudaMemcpyHostToDevice, h->stream), "upload sponge");
@@ -617,6 +627,17 @@ extern "C" int lbm_init(lbm_handle* h)
     h->sa.sig_z = h->sig + nx + ny;
     h->sa.omega = (float)(1.0 / c.tau);
     h->sa.xf = h->xf;
+    if (const char* v = std::getenv("NLOS_LBM_STEP_VARIANT")) h->step_variant = std::atoi(v);
+    if (h->step_variant < 0 || h->step_variant > 12) return h->fail(LBM_ERR_BAD_CONFIG, "NLOS_LBM_STEP_VARIANT out of range");
+    h->sa.prefetch_rows = kDefaultPrefetchRows;
+    if (const char* v = std::getenv("NLOS_LBM_PREFETCH_ROWS")) h->sa.prefetch_rows = std::max(0, std::atoi(v));
+    CK(prepare_step(h->storage, h->step_variant, h->device, &h->step_grid), "prepare step kernel");
+    h->sa.error = h->d_error;
+    for (int q = 0; q < Q; ++q)
+    {
+        h->sa.pop_off[q] = (long long)q * L.pop_stride;
+        h->sa.pull_off[q] = (long long)q * L.pop_stride - ((long long)ey(q) * L.pitch + (long long)ez(q) * L.plane);
+    }
 
     // Open faces for the ghost kernel.
     h->ga = GhostArgs{};
@@ -748,13 +769,13 @@ cudaError_t timed_step_launch(lbm_handle* h, const void* fin, void* fout)
         }
         e = cudaEventRecord(h->ev[h->ev_used], h->stream);
         if (e != cudaSuccess) return e;
-        e = launch_step(h->storage, fin, fout, h->L, h->sa, h->scale, h->stream);
+        e = launch_step(h->storage, fin, fout, h->L, h->sa, h->scale, h->step_variant, h->step_grid, h->stream);
         if (e != cudaSuccess) return e;
         e = cudaEventRecord(h->ev[h->ev_used + 1], h->stream);
         h->ev_used += 2;
         return e;
     }
-    return launch_step(h->storage, fin, fout, h->L, h->sa, h->scale, h->stream);
+    return launch_step(h->storage, fin, fout, h->L, h->sa, h->scale, h->step_variant, h->step_grid, h->stream);
 }
 
 // Collect the kernel times recorded since the last harvest (synchronises).
@@ -861,6 +882,16 @@ int fill_table(lbm_handle* h, long long s0)
     h->table_base = s0;
     h->table_rows = kTableRows;
     return LBM_OK;
+}
+
+// A kernel that gave up a bounded wait leaves a code in the error word.
+int check_kernel_error(lbm_handle* h)
+{
+    int code = 0;
+    CK(cudaMemcpy(&code, h->d_error, sizeof(int), cudaMemcpyDeviceToHost), "error word");
+    if (code == 0) return LBM_OK;
+    cudaMemset(h->d_error, 0, sizeof(int));
+    return h->fail(LBM_ERR_TIMEOUT, "a staged-copy wait in the step kernel timed out");
 }
 
 int check_ready(lbm_handle* h)
@@ -1030,6 +1061,8 @@ extern "C" int lbm_step(lbm_handle* h, int nsteps)
         }
         // the control block upload must not be overwritten before the copy ran
         CK(cudaStreamSynchronize(h->stream), "step sync");
+        st = check_kernel_error(h);
+        if (st) return st;
         h->step += chunk;
         if (np) h->probe_pending += chunk;
         left -= chunk;

@@ -24,6 +24,9 @@ namespace lbm {
 
 constexpr int kMaxSources = 8;
 constexpr int kFrontPad = 32;
+// Elements after the last plane: a staged row copy of the last row may run
+// up to one tile (<= 512 elements) plus its alignment margin past it.
+constexpr int kBackPad = 1024;
 
 struct Layout
 {
@@ -115,7 +118,15 @@ struct StepArgs
     const float* sig_z;
     float omega;               // 1 / tau
     XFace xf;
+    // Per direction, in elements (warp-uniform address offsets):
+    long long pull_off[19];    // q * pop_stride - (ey * pitch + ez * plane): aligned source of a pair
+    long long pop_off[19];     // q * pop_stride
+    int* error;                // set when a bounded wait in a kernel gives up (0 = fine)
+    int prefetch_rows;         // > 0: each block prefetches into L2 the source rows of the row this far ahead
 };
+
+// Error codes a kernel writes to StepArgs::error.
+constexpr int kErrStageTimeout = 1;   // staged-copy barrier wait exceeded its limit
 
 struct ProbeArgs
 {
@@ -135,8 +146,20 @@ cudaError_t launch_build_links(const uint8_t* mask_ref, uint32_t* links, uint32_
 cudaError_t launch_source(int storage, void* f, const Layout& L, const StepArgs& sa, const SourceArgs& a,
                           cudaStream_t stream);
 cudaError_t launch_ghost(int storage, void* f, const Layout& L, const GhostArgs& a, cudaStream_t stream);
+// variant: implementation / launch shape of the fused step; all do the same
+// work.  0-3: register-resident pairs with lane shuffles (0: 128 threads,
+// 1: 128 threads with at most 64 registers, 2: 256 threads, 3: 64 threads);
+// 4-7: persistent CTAs staging rows in shared memory with bulk async copies
+// (tile width / stages 256/3, 256/2, 128/4, 512/2); 8, 9: four cells per
+// thread with 8-byte vectors (FP16 storage; 9 caps registers at 80; FP32
+// storage runs variant 3); 10-12: pair kernel with 32-bit per-thread offsets
+// (128 threads, 128 threads with at most 64 registers, 64 threads).  `grid` is the persistent
+// grid from prepare_step (ignored by 0-3).
 cudaError_t launch_step(int storage, const void* fin, void* fout, const Layout& L, const StepArgs& a,
-                        float scale, cudaStream_t stream);
+                        float scale, int variant, int grid, cudaStream_t stream);
+// Per-variant set-up (shared-memory opt-in, persistent grid size); call
+// once per device before the first launch and outside stream capture.
+cudaError_t prepare_step(int storage, int variant, int device, int* grid);
 cudaError_t launch_probe(int storage, const void* f, const Layout& L, const StepArgs& sa, const ProbeArgs& a,
                          cudaStream_t stream);
 // (float)(rho - 1) of every interior cell, pulled from the pre-step buffer `f`.

@@ -4,8 +4,10 @@
 // with FP64 for the source-weight reduction and the probe accumulators.
 #include <cuda_fp16.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <type_traits>
 
 #include "device.hpp"
 #include "lattice.cuh"
@@ -36,77 +38,6 @@ struct Io<__half>
     static __device__ __forceinline__ float ldw(const __half* p) { return __half2float(*p); }
     static __device__ __forceinline__ void st(__half* p, float v) { *p = __float2half_rn(v); }
     static __device__ __forceinline__ float rnd(float v) { return __half2float(__float2half_rn(v)); }
-};
-
-// Two x-adjacent cells as one aligned vector: float2 (8 B) or half2 (4 B).
-// `V` is the raw register form that is shuffled between lanes.
-template <typename S>
-struct Pair;
-
-template <>
-struct Pair<float>
-{
-    using V = float2;
-    static __device__ __forceinline__ V ld(const float* p) { return __ldg(reinterpret_cast<const float2*>(p)); }
-    static __device__ __forceinline__ void st(float* p, float a, float b)
-    {
-        *reinterpret_cast<float2*>(p) = make_float2(a, b);
-    }
-    static __device__ __forceinline__ float lo(V v) { return v.x; }
-    static __device__ __forceinline__ float hi(V v) { return v.y; }
-    static __device__ __forceinline__ V up(V v)   // element 1 of lane - 1 (element 0 unused)
-    {
-        return make_float2(v.x, __shfl_up_sync(kFull, v.y, 1));
-    }
-    static __device__ __forceinline__ V down(V v)   // element 0 of lane + 1 (element 1 unused)
-    {
-        return make_float2(__shfl_down_sync(kFull, v.x, 1), v.y);
-    }
-    // cells (c-1, c) from prev = (c-2, c-1) and cur = (c, c+1)
-    static __device__ __forceinline__ void left(V prev, V cur, float& a, float& b)
-    {
-        a = prev.y;
-        b = cur.x;
-    }
-    // cells (c+1, c+2) from cur = (c, c+1) and next = (c+2, c+3)
-    static __device__ __forceinline__ void right(V cur, V next, float& a, float& b)
-    {
-        a = cur.y;
-        b = next.x;
-    }
-};
-
-template <>
-struct Pair<__half>
-{
-    using V = unsigned;
-    static __device__ __forceinline__ V ld(const __half* p) { return __ldg(reinterpret_cast<const unsigned*>(p)); }
-    static __device__ __forceinline__ void st(__half* p, float a, float b)
-    {
-        *reinterpret_cast<__half2*>(p) = __floats2half2_rn(a, b);
-    }
-    static __device__ __forceinline__ float2 f2(unsigned u)
-    {
-        __half2 h;
-        *reinterpret_cast<unsigned*>(&h) = u;
-        return __half22float2(h);
-    }
-    static __device__ __forceinline__ float lo(V v) { return f2(v).x; }
-    static __device__ __forceinline__ float hi(V v) { return f2(v).y; }
-    static __device__ __forceinline__ V up(V v) { return __shfl_up_sync(kFull, v, 1); }
-    static __device__ __forceinline__ V down(V v) { return __shfl_down_sync(kFull, v, 1); }
-    static __device__ __forceinline__ void left(V prev, V cur, float& a, float& b)
-    {
-        const float2 r = f2(__byte_perm(prev, cur, 0x5432));
-        a = r.x;
-        b = r.y;
-    }
-    static __device__ __forceinline__ void right(V cur, V next, float& a, float& b)
-    {
-        const float2 r = f2(__byte_perm(cur, next, 0x5432));
-        a = r.x;
-        b = r.y;
-    }
 };
 
 // Row part of the pull offset of direction q: src = dst - ex(q) - row_off(q).
@@ -202,18 +133,144 @@ __device__ __forceinline__ void pull_cell(const S* __restrict__ f, const Layout&
 }
 
 // ---------------------------------------------------------------- step
+// Packed FP32x2 arithmetic (sm_100): both cells of a thread's pair in one
+// instruction.
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, f2(-1.0f), a); }
+
+// Pair version of collide(): the same BGK + sponge update of two cells, in
+// lockstep.  A SOLID cell gets cA = 1, cB = 0, so its pulled values pass
+// through unchanged (06:933-938).
+__device__ __forceinline__ void collide2(float2 (&G)[Q], float inv_scale, float omega, float2 sigma, bool solid0,
+                                         bool solid1)
+{
+    // rho' and J in the family-B order (06:21-23)
+    const float2 rho = add2(add2(add2(add2(G[0], G[1]), add2(G[2], G[3])), add2(add2(G[4], G[5]), add2(G[6], G[7]))),
+                            add2(add2(add2(G[8], G[9]), add2(G[10], G[11])),
+                                 add2(add2(add2(G[12], G[13]), add2(G[14], G[15])), add2(add2(G[16], G[17]), G[18]))));
+    const float2 jx = sub2(add2(add2(add2(G[1], G[7]), add2(G[8], G[11])), G[12]),
+                           add2(add2(add2(G[2], G[9]), add2(G[10], G[13])), G[14]));
+    const float2 jy = sub2(add2(add2(add2(G[3], G[7]), add2(G[9], G[15])), G[16]),
+                           add2(add2(add2(G[4], G[8]), add2(G[10], G[17])), G[18]));
+    const float2 jz = sub2(add2(add2(add2(G[5], G[11]), add2(G[13], G[15])), G[17]),
+                           add2(add2(add2(G[6], G[12]), add2(G[14], G[16])), G[18]));
+    float2 r = fma2(rho, f2(inv_scale), f2(1.0f));
+    if (r.x <= 0.f) r.x = 1e-12f;   // 06:948
+    if (r.y <= 0.f) r.y = 1e-12f;
+    const float2 irs = make_float2(__fdividef(inv_scale, r.x), __fdividef(inv_scale, r.y));
+    const float2 j2 = fma2(jz, jz, fma2(jy, jy, mul2(jx, jx)));
+    const float2 base = fma2(mul2(irs, j2), f2(-1.5f), rho);
+    const float2 k45 = mul2(irs, f2(4.5f));
+    const float2 keep = sub2(f2(1.0f), sigma);
+    float2 cA = mul2(keep, f2(1.0f - omega));
+    float2 cB = mul2(keep, f2(omega));
+    if (solid0) cA.x = 1.0f, cB.x = 0.0f;
+    if (solid1) cA.y = 1.0f, cB.y = 0.0f;
+    const float2 cBw1 = mul2(cB, f2(wf(1))), cBw2 = mul2(cB, f2(wf(7)));
+    const float2 cBt1 = mul2(cB, f2(3.0f * wf(1))), cBt2 = mul2(cB, f2(3.0f * wf(7)));
+    G[0] = fma2(cA, G[0], mul2(mul2(cB, f2(wf(0))), base));
+#pragma unroll
+    for (int p = 0; p < 9; ++p)
+    {
+        const int q = pair_head(p);
+        const int qb = inv(q);
+        float2 cj;
+        if (p == 0) cj = jx;                  // q = 1  ( 1, 0, 0)
+        else if (p == 1) cj = jy;             // q = 3  ( 0, 1, 0)
+        else if (p == 2) cj = jz;             // q = 5  ( 0, 0, 1)
+        else if (p == 3) cj = add2(jx, jy);   // q = 7  ( 1, 1, 0)
+        else if (p == 4) cj = sub2(jx, jy);   // q = 8  ( 1,-1, 0)
+        else if (p == 5) cj = add2(jx, jz);   // q = 11 ( 1, 0, 1)
+        else if (p == 6) cj = sub2(jx, jz);   // q = 12 ( 1, 0,-1)
+        else if (p == 7) cj = add2(jy, jz);   // q = 15 ( 0, 1, 1)
+        else cj = sub2(jy, jz);               // q = 16 ( 0, 1,-1)
+        const float2 cBw = q < 7 ? cBw1 : cBw2;
+        const float2 cBt = q < 7 ? cBt1 : cBt2;
+        const float2 e = mul2(cBw, fma2(k45, mul2(cj, cj), base));
+        const float2 o = mul2(cBt, cj);
+        G[q] = fma2(cA, G[q], add2(e, o));
+        G[qb] = fma2(cA, G[qb], sub2(e, o));
+    }
+}
+
+template <typename S>
+struct PairIo;
+
+template <>
+struct PairIo<float>
+{
+    using V = float2;
+    static __device__ __forceinline__ V ld(const float* p) { return __ldg(reinterpret_cast<const float2*>(p)); }
+    static __device__ __forceinline__ void st(float* p, float2 v) { *reinterpret_cast<float2*>(p) = v; }
+    static __device__ __forceinline__ float2 cvt(V v) { return v; }
+    static __device__ __forceinline__ V up(V v) { return make_float2(v.x, __shfl_up_sync(kFull, v.y, 1)); }
+    static __device__ __forceinline__ V down(V v) { return make_float2(__shfl_down_sync(kFull, v.x, 1), v.y); }
+    static __device__ __forceinline__ float2 left(V prev, V cur) { return make_float2(prev.y, cur.x); }
+    static __device__ __forceinline__ float2 right(V cur, V next) { return make_float2(cur.y, next.x); }
+    static __device__ __forceinline__ float rnd(float v) { return v; }
+};
+
+template <>
+struct PairIo<__half>
+{
+    using V = unsigned;
+    static __device__ __forceinline__ V ld(const __half* p) { return __ldg(reinterpret_cast<const unsigned*>(p)); }
+    static __device__ __forceinline__ void st(__half* p, float2 v)
+    {
+        *reinterpret_cast<__half2*>(p) = __float22half2_rn(v);
+    }
+    static __device__ __forceinline__ float2 cvt(V u)
+    {
+        __half2 h;
+        *reinterpret_cast<unsigned*>(&h) = u;
+        return __half22float2(h);
+    }
+    static __device__ __forceinline__ V up(V v) { return __shfl_up_sync(kFull, v, 1); }
+    static __device__ __forceinline__ V down(V v) { return __shfl_down_sync(kFull, v, 1); }
+    static __device__ __forceinline__ float2 left(V prev, V cur) { return cvt(__byte_perm(prev, cur, 0x5432)); }
+    static __device__ __forceinline__ float2 right(V cur, V next) { return cvt(__byte_perm(cur, next, 0x5432)); }
+    static __device__ __forceinline__ float rnd(float v) { return __half2float(__float2half_rn(v)); }
+};
+
+__device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes)
+{
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
+// One thread of the block asks L2 for the 19 source row segments the same
+// block position needs `prefetch_rows` rows later, so that by the time that
+// block runs its loads hit L2 instead of HBM.  Segments are widened to
+// 16-byte boundaries (the bulk-prefetch alignment rule).
+template <typename S>
+__device__ __forceinline__ void prefetch_ahead(const S* fin, const Layout& L, const StepArgs& a, int j, int k,
+                                               int col0, int ncols)
+{
+    const long long r = (long long)(k - 1) * L.ny + (j - 1) + a.prefetch_rows;
+    if (r >= (long long)L.ny * L.nz) return;
+    const int jj = 1 + (int)(r % L.ny), kk = 1 + (int)(r / L.ny);
+    constexpr int PADE = 16 / (int)sizeof(S);
+    const long long cell0 = (long long)kk * L.plane + (long long)jj * L.pitch + col0;
+    const uint32_t bytes = (uint32_t)((ncols + 2 * PADE) * (int)sizeof(S) + 15) & ~15u;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) prefetch_l2(fin + cell0 + a.pull_off[q] - PADE, bytes);
+}
+
 // Fused pull-stream + halfway bounce-back + BGK + sponge (06:906-972), two
 // x-adjacent cells per thread.  Each direction is read as one aligned vector
 // per thread; the +-1 x shift of directions with ex != 0 takes the missing
 // neighbour element from the adjacent lane (warp shuffle) and, at the warp
-// edge, from one extra aligned load.  SOLID cells copy the pulled values
-// (06:933-938).  Cells next to the x faces take their x-halo sources from
-// the x-face ghosts and export their results for the next ghost fill.
-template <typename S>
-__global__ void __launch_bounds__(128) k_step(const S* __restrict__ fin, S* __restrict__ fout, Layout L,
-                                              StepArgs a, float inv_scale)
+// edge, from one extra aligned load.  The collision runs on the pair with
+// packed FP32x2 instructions.  Cells next to the x faces take their x-halo
+// sources from the x-face ghosts and export their results for the next ghost
+// fill.
+template <typename S, int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) k_step(const S* __restrict__ fin, S* __restrict__ fout, Layout L,
+                                                      StepArgs a, float inv_scale)
 {
-    using P = Pair<S>;
+    using P = PairIo<S>;
     const int lane = threadIdx.x & 31;
     const int c0r = 2 * (blockIdx.x * blockDim.x + threadIdx.x);   // first column of the pair
     const bool active = c0r < L.nx;
@@ -221,6 +278,12 @@ __global__ void __launch_bounds__(128) k_step(const S* __restrict__ fin, S* __re
     const int j = blockIdx.y + 1;
     const int k = blockIdx.z + 1;
     const long long cell = (long long)k * L.plane + (long long)j * L.pitch + c0;
+    const S* tin = fin + cell;
+    if (a.prefetch_rows > 0 && threadIdx.x == 0)
+    {
+        const int col0 = 2 * blockIdx.x * BLOCK;
+        prefetch_ahead<S>(fin, L, a, j, k, col0, min(2 * BLOCK, L.nx - col0));
+    }
 
     uint32_t lk0 = 0, lk1 = 0;
     if (active)
@@ -232,28 +295,27 @@ __global__ void __launch_bounds__(128) k_step(const S* __restrict__ fin, S* __re
     }
     const bool any_link = __any_sync(kFull, (lk0 | lk1) != 0u);
 
-    float G0[Q], G1[Q];
+    float2 G[Q];
 #pragma unroll
     for (int q = 0; q < Q; ++q)
     {
-        const S* src = fin + (long long)q * L.pop_stride + cell - row_off(q, L);
+        const S* src = tin + a.pull_off[q];
         const typename P::V cur = P::ld(src);
         if (ex(q) == 0)
         {
-            G0[q] = P::lo(cur);
-            G1[q] = P::hi(cur);
+            G[q] = P::cvt(cur);
         }
         else if (ex(q) > 0)
         {
             typename P::V prev = P::up(cur);
             if (lane == 0) prev = P::ld(src - 2);
-            P::left(prev, cur, G0[q], G1[q]);
+            G[q] = P::left(prev, cur);
         }
         else
         {
             typename P::V next = P::down(cur);
             if (lane == 31) next = P::ld(src + 2);
-            P::right(cur, next, G0[q], G1[q]);
+            G[q] = P::right(cur, next);
         }
     }
     if (any_link)
@@ -263,9 +325,9 @@ __global__ void __launch_bounds__(128) k_step(const S* __restrict__ fin, S* __re
         {
             if (((lk0 | lk1) >> q) & 1u)
             {
-                const typename P::V own = P::ld(fin + (long long)inv(q) * L.pop_stride + cell);
-                if ((lk0 >> q) & 1u) G0[q] = P::lo(own);
-                if ((lk1 >> q) & 1u) G1[q] = P::hi(own);
+                const float2 own = P::cvt(P::ld(tin + a.pop_off[inv(q)]));
+                if ((lk0 >> q) & 1u) G[q].x = own.x;
+                if ((lk1 >> q) & 1u) G[q].y = own.y;
             }
         }
     }
@@ -280,30 +342,470 @@ __global__ void __launch_bounds__(128) k_step(const S* __restrict__ fin, S* __re
         {
             if (ex(q) == 0) continue;
             const float g = a.xf.xgh[a.xf.gh_index(ex(q) > 0 ? 0 : 1, q, j - ey(q), k - ez(q), L.ny, L.nz)];
-            if (ex(q) > 0 && xlo && !((lk0 >> q) & 1u)) G0[q] = g;
-            if (ex(q) < 0 && xhi0 && !((lk0 >> q) & 1u)) G0[q] = g;
-            if (ex(q) < 0 && xhi1 && !((lk1 >> q) & 1u)) G1[q] = g;
+            if (ex(q) > 0 && xlo && !((lk0 >> q) & 1u)) G[q].x = g;
+            if (ex(q) < 0 && xhi0 && !((lk0 >> q) & 1u)) G[q].x = g;
+            if (ex(q) < 0 && xhi1 && !((lk1 >> q) & 1u)) G[q].y = g;
         }
     }
     if (!active) return;
 
     const float syz = fmaxf(a.sig_y[j - 1], a.sig_z[k - 1]);
-    const float s0 = fmaxf(a.sig_x[c0], syz);
-    const float s1 = fmaxf(c0 + 1 < L.nx ? a.sig_x[c0 + 1] : 0.f, syz);
-    if (!(lk0 & kSolidSelfBit)) collide(G0, inv_scale, a.omega, s0);
-    if (!(lk1 & kSolidSelfBit)) collide(G1, inv_scale, a.omega, s1);
+    const float2 sg = make_float2(fmaxf(a.sig_x[c0], syz), fmaxf(c0 + 1 < L.nx ? a.sig_x[c0 + 1] : 0.f, syz));
+    collide2(G, inv_scale, a.omega, sg, (lk0 & kSolidSelfBit) != 0u, (lk1 & kSolidSelfBit) != 0u);
 
+    S* tout = fout + cell;
 #pragma unroll
-    for (int q = 0; q < Q; ++q) P::st(fout + (long long)q * L.pop_stride + cell, G0[q], G1[q]);
+    for (int q = 0; q < Q; ++q) P::st(tout + a.pop_off[q], G[q]);
 
     if (xlo | xhi0 | xhi1)
     {
 #pragma unroll
         for (int q = 0; q < Q; ++q)
         {
-            if (xlo) a.xf.xexp[a.xf.exp_index(0, q, j, k, L.ny, L.nz)] = Io<S>::rnd(G0[q]);
-            if (xhi0) a.xf.xexp[a.xf.exp_index(1, q, j, k, L.ny, L.nz)] = Io<S>::rnd(G0[q]);
-            if (xhi1) a.xf.xexp[a.xf.exp_index(1, q, j, k, L.ny, L.nz)] = Io<S>::rnd(G1[q]);
+            if (xlo) a.xf.xexp[a.xf.exp_index(0, q, j, k, L.ny, L.nz)] = P::rnd(G[q].x);
+            if (xhi0) a.xf.xexp[a.xf.exp_index(1, q, j, k, L.ny, L.nz)] = P::rnd(G[q].x);
+            if (xhi1) a.xf.xexp[a.xf.exp_index(1, q, j, k, L.ny, L.nz)] = P::rnd(G[q].y);
+        }
+    }
+}
+
+// Pair kernel with 32-bit per-thread element offsets: every address is a
+// warp-uniform per-direction base pointer (fin + q * pop_stride, from kernel
+// parameters) plus a 32-bit cell offset, so per-thread address arithmetic
+// stays 32-bit.  The host guarantees pop_stride < 2^31.
+template <typename S, int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) k_step32(const S* __restrict__ fin, S* __restrict__ fout, Layout L,
+                                                        StepArgs a, float inv_scale)
+{
+    using P = PairIo<S>;
+    const int lane = threadIdx.x & 31;
+    const int c0r = 2 * (blockIdx.x * BLOCK + threadIdx.x);
+    const bool active = c0r < L.nx;
+    const int c0 = active ? c0r : ((L.nx - 1) & ~1);
+    const int j = blockIdx.y + 1;
+    const int k = blockIdx.z + 1;
+    const uint32_t pitch = (uint32_t)L.pitch, plane = (uint32_t)L.plane;
+    const uint32_t cell = (uint32_t)k * plane + (uint32_t)j * pitch + (uint32_t)c0;
+    const size_t ps = (size_t)L.pop_stride;
+    if (a.prefetch_rows > 0 && threadIdx.x == 0)
+    {
+        const int col0 = 2 * blockIdx.x * BLOCK;
+        prefetch_ahead<S>(fin, L, a, j, k, col0, min(2 * BLOCK, L.nx - col0));
+    }
+    uint32_t lk0 = 0, lk1 = 0;
+    if (active)
+    {
+        const uint32_t b = (near_word(a, L, c0, j, k) >> (c0 & 31)) & 3u;
+        if (b & 1u) lk0 = a.links[cell];
+        if (b & 2u) lk1 = a.links[cell + 1];
+    }
+    const bool any_link = __any_sync(kFull, (lk0 | lk1) != 0u);
+
+    float2 G[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q)
+    {
+        const S* __restrict__ Pq = fin + q * ps;
+        const uint32_t src = cell - (uint32_t)(ey(q) * (int)pitch + ez(q) * (int)plane);
+        const typename P::V cur = P::ld(Pq + src);
+        if (ex(q) == 0)
+        {
+            G[q] = P::cvt(cur);
+        }
+        else if (ex(q) > 0)
+        {
+            typename P::V prev = P::up(cur);
+            if (lane == 0) prev = P::ld(Pq + (src - 2u));
+            G[q] = P::left(prev, cur);
+        }
+        else
+        {
+            typename P::V next = P::down(cur);
+            if (lane == 31) next = P::ld(Pq + (src + 2u));
+            G[q] = P::right(cur, next);
+        }
+    }
+    if (any_link)
+    {
+#pragma unroll
+        for (int q = 0; q < Q; ++q)
+        {
+            if (((lk0 | lk1) >> q) & 1u)
+            {
+                const float2 own = P::cvt(P::ld(fin + inv(q) * ps + cell));
+                if ((lk0 >> q) & 1u) G[q].x = own.x;
+                if ((lk1 >> q) & 1u) G[q].y = own.y;
+            }
+        }
+    }
+    const bool xlo = active && c0 == 0;
+    const bool xhi0 = active && c0 == L.nx - 1;
+    const bool xhi1 = active && c0 + 1 == L.nx - 1;
+    if (xlo | xhi0 | xhi1)
+    {
+#pragma unroll
+        for (int q = 0; q < Q; ++q)
+        {
+            if (ex(q) == 0) continue;
+            const float g = a.xf.xgh[a.xf.gh_index(ex(q) > 0 ? 0 : 1, q, j - ey(q), k - ez(q), L.ny, L.nz)];
+            if (ex(q) > 0 && xlo && !((lk0 >> q) & 1u)) G[q].x = g;
+            if (ex(q) < 0 && xhi0 && !((lk0 >> q) & 1u)) G[q].x = g;
+            if (ex(q) < 0 && xhi1 && !((lk1 >> q) & 1u)) G[q].y = g;
+        }
+    }
+    if (!active) return;
+
+    const float syz = fmaxf(a.sig_y[j - 1], a.sig_z[k - 1]);
+    const float2 sg = make_float2(fmaxf(a.sig_x[c0], syz), fmaxf(c0 + 1 < L.nx ? a.sig_x[c0 + 1] : 0.f, syz));
+    collide2(G, inv_scale, a.omega, sg, (lk0 & kSolidSelfBit) != 0u, (lk1 & kSolidSelfBit) != 0u);
+#pragma unroll
+    for (int q = 0; q < Q; ++q) P::st(fout + q * ps + cell, G[q]);
+    if (xlo | xhi0 | xhi1)
+    {
+#pragma unroll
+        for (int q = 0; q < Q; ++q)
+        {
+            if (xlo) a.xf.xexp[a.xf.exp_index(0, q, j, k, L.ny, L.nz)] = P::rnd(G[q].x);
+            if (xhi0) a.xf.xexp[a.xf.exp_index(1, q, j, k, L.ny, L.nz)] = P::rnd(G[q].x);
+            if (xhi1) a.xf.xexp[a.xf.exp_index(1, q, j, k, L.ny, L.nz)] = P::rnd(G[q].y);
+        }
+    }
+}
+
+// Four x-adjacent cells per thread, FP16 storage: every direction is one
+// aligned 8-byte vector (two half2 words) per thread, so each thread keeps
+// twice the bytes in flight of the pair kernel for about the same register
+// budget.  The two pairs are collided one after the other (packed FP32x2).
+__device__ __forceinline__ uint2 ld_quad(const __half* p) { return __ldg(reinterpret_cast<const uint2*>(p)); }
+
+template <int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) k_step_quad(const __half* __restrict__ fin, __half* __restrict__ fout,
+                                                           Layout L, StepArgs a, float inv_scale)
+{
+    using P = PairIo<__half>;
+    const int lane = threadIdx.x & 31;
+    const int c0r = 4 * (blockIdx.x * BLOCK + threadIdx.x);
+    const bool active = c0r < L.nx;
+    const int c0 = active ? c0r : ((L.nx - 1) & ~3);
+    const int j = blockIdx.y + 1;
+    const int k = blockIdx.z + 1;
+    const long long cell = (long long)k * L.plane + (long long)j * L.pitch + c0;
+    const __half* tin = fin + cell;
+    if (a.prefetch_rows > 0 && threadIdx.x == 0)
+    {
+        const int col0 = 4 * blockIdx.x * BLOCK;
+        prefetch_ahead<__half>(fin, L, a, j, k, col0, min(4 * BLOCK, L.nx - col0));
+    }
+    uint32_t lk[4] = {0, 0, 0, 0};
+    if (active)
+    {
+        const uint32_t b = (near_word(a, L, c0, j, k) >> (c0 & 31)) & 15u;
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+            if ((b >> c) & 1u) lk[c] = a.links[cell + c];
+    }
+    const bool any_link = __any_sync(kFull, (lk[0] | lk[1] | lk[2] | lk[3]) != 0u);
+
+    // words: w[q].x = cells (c0, c0+1), w[q].y = cells (c0+2, c0+3), shifted per direction
+    uint2 w[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q)
+    {
+        const __half* src = tin + a.pull_off[q];
+        const uint2 cur = ld_quad(src);
+        if (ex(q) == 0)
+        {
+            w[q] = cur;
+        }
+        else if (ex(q) > 0)
+        {
+            unsigned prev = __shfl_up_sync(kFull, cur.y, 1);   // cells (c0-2, c0-1)
+            if (lane == 0) prev = ld_quad(src - 4).y;
+            w[q] = make_uint2(__byte_perm(prev, cur.x, 0x5432), __byte_perm(cur.x, cur.y, 0x5432));
+        }
+        else
+        {
+            unsigned next = __shfl_down_sync(kFull, cur.x, 1);   // cells (c0+4, c0+5)
+            if (lane == 31) next = ld_quad(src + 4).x;
+            w[q] = make_uint2(__byte_perm(cur.x, cur.y, 0x5432), __byte_perm(cur.y, next, 0x5432));
+        }
+    }
+    if (any_link)
+    {
+        const uint32_t la = lk[0] | lk[1] | lk[2] | lk[3];
+#pragma unroll
+        for (int q = 0; q < Q; ++q)
+        {
+            if ((la >> q) & 1u)
+            {
+                const uint2 own = ld_quad(tin + a.pop_off[inv(q)]);
+                // halfword select: cell c takes `own` when its link bit q is set
+                const unsigned m0 = (((lk[0] >> q) & 1u) ? 0x0000ffffu : 0u) | (((lk[1] >> q) & 1u) ? 0xffff0000u : 0u);
+                const unsigned m1 = (((lk[2] >> q) & 1u) ? 0x0000ffffu : 0u) | (((lk[3] >> q) & 1u) ? 0xffff0000u : 0u);
+                w[q].x = (w[q].x & ~m0) | (own.x & m0);
+                w[q].y = (w[q].y & ~m1) | (own.y & m1);
+            }
+        }
+    }
+    // x faces (ghost values are float; patched after conversion below)
+    const int last = L.nx - 1 - c0;   // position of cell nx-1 in this quad when 0..3
+    const bool xlo = active && c0 == 0;
+    const bool xhi = active && last >= 0 && last < 4;
+    if (!active) return;
+
+    const float syz = fmaxf(a.sig_y[j - 1], a.sig_z[k - 1]);
+    __half* tout = fout + cell;
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
+    {
+        float2 G[Q];
+#pragma unroll
+        for (int q = 0; q < Q; ++q) G[q] = P::cvt(h == 0 ? w[q].x : w[q].y);
+        const int ca = c0 + 2 * h;
+        if (xlo | xhi)
+        {
+#pragma unroll
+            for (int q = 0; q < Q; ++q)
+            {
+                if (ex(q) == 0) continue;
+                const float g = a.xf.xgh[a.xf.gh_index(ex(q) > 0 ? 0 : 1, q, j - ey(q), k - ez(q), L.ny, L.nz)];
+                if (ex(q) > 0 && xlo && h == 0 && !((lk[0] >> q) & 1u)) G[q].x = g;
+                if (ex(q) < 0 && xhi && last == 2 * h && !((lk[2 * h] >> q) & 1u)) G[q].x = g;
+                if (ex(q) < 0 && xhi && last == 2 * h + 1 && !((lk[2 * h + 1] >> q) & 1u)) G[q].y = g;
+            }
+        }
+        const float2 sg = make_float2(fmaxf(ca < L.nx ? a.sig_x[ca] : 0.f, syz),
+                                      fmaxf(ca + 1 < L.nx ? a.sig_x[ca + 1] : 0.f, syz));
+        collide2(G, inv_scale, a.omega, sg, (lk[2 * h] & kSolidSelfBit) != 0u, (lk[2 * h + 1] & kSolidSelfBit) != 0u);
+#pragma unroll
+        for (int q = 0; q < Q; ++q) P::st(tout + a.pop_off[q] + 2 * h, G[q]);
+        if (xlo | xhi)
+        {
+#pragma unroll
+            for (int q = 0; q < Q; ++q)
+            {
+                if (xlo && h == 0) a.xf.xexp[a.xf.exp_index(0, q, j, k, L.ny, L.nz)] = P::rnd(G[q].x);
+                if (xhi && last == 2 * h) a.xf.xexp[a.xf.exp_index(1, q, j, k, L.ny, L.nz)] = P::rnd(G[q].x);
+                if (xhi && last == 2 * h + 1) a.xf.xexp[a.xf.exp_index(1, q, j, k, L.ny, L.nz)] = P::rnd(G[q].y);
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------- staged step
+// Bulk asynchronous copies (cp.async.bulk, completion counted on an mbarrier)
+// stage, for every direction q, the source row segment of a tile in shared
+// memory; a persistent CTA keeps NS tiles in flight while it collides the
+// oldest one.  Memory-level parallelism no longer depends on registers.
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0u;
+}
+// Waits for phase `parity` of the barrier, giving up after `limit` polls.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int limit)
+{
+    for (int n = 0; n < limit; ++n)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void fence_mbarrier_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+// Reads of a staged row (p points at the element of the pair's first cell).
+template <typename S>
+struct Staged;
+
+template <>
+struct Staged<float>
+{
+    static __device__ __forceinline__ float2 pair(const float* p) { return *reinterpret_cast<const float2*>(p); }
+    static __device__ __forceinline__ float2 left(const float* p) { return make_float2(p[-1], p[0]); }
+    static __device__ __forceinline__ float2 right(const float* p) { return make_float2(p[1], p[2]); }
+};
+
+template <>
+struct Staged<__half>
+{
+    static __device__ __forceinline__ unsigned word(const __half* p) { return *reinterpret_cast<const unsigned*>(p); }
+    static __device__ __forceinline__ float2 pair(const __half* p) { return PairIo<__half>::cvt(word(p)); }
+    static __device__ __forceinline__ float2 left(const __half* p)
+    {
+        return PairIo<__half>::cvt(__byte_perm(word(p - 2), word(p), 0x5432));
+    }
+    static __device__ __forceinline__ float2 right(const __half* p)
+    {
+        return PairIo<__half>::cvt(__byte_perm(word(p), word(p + 2), 0x5432));
+    }
+};
+
+constexpr int kStageWaitLimit = 1 << 22;   // mbarrier polls before a stage wait gives up
+
+template <typename S, int TW, int NS>
+__global__ void __launch_bounds__(TW / 2) k_step_staged(const S* __restrict__ fin, S* __restrict__ fout, Layout L,
+                                                       StepArgs a, float inv_scale, int tiles_per_row,
+                                                       long long ntiles)
+{
+    using P = PairIo<S>;
+    using T = Staged<S>;
+    constexpr int PADE = 16 / (int)sizeof(S);   // 16-byte alignment margin on both sides of a row
+    constexpr int ROW = TW + 2 * PADE;          // staged elements per direction
+    constexpr uint32_t ROW_BYTES = ROW * sizeof(S);
+    constexpr uint32_t STAGE_BYTES = Q * ROW_BYTES;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    S* const stages = reinterpret_cast<S*>(smem_raw);
+    __shared__ __align__(8) uint64_t full[NS];
+
+    const int tid = threadIdx.x;
+    if (tid == 0)
+    {
+        for (int s = 0; s < NS; ++s) mbar_init(&full[s], 1);
+        fence_mbarrier_init();
+    }
+    __syncthreads();
+
+    // One elected thread stages all 19 source rows of a tile.
+    auto issue = [&](int s, long long tile) {
+        const long long r = tile / tiles_per_row;
+        const int seg = (int)(tile - r * tiles_per_row);
+        const int j = 1 + (int)(r % L.ny), k = 1 + (int)(r / L.ny);
+        const long long cell0 = (long long)k * L.plane + (long long)j * L.pitch + (long long)seg * TW;
+        S* dst = stages + (size_t)s * Q * ROW;
+        mbar_expect_tx(&full[s], STAGE_BYTES);
+#pragma unroll
+        for (int q = 0; q < Q; ++q) bulk_copy_g2s(dst + q * ROW, fin + cell0 + a.pull_off[q] - PADE, ROW_BYTES, &full[s]);
+    };
+    if (tid == 0)
+        for (int s = 0; s < NS; ++s)
+        {
+            const long long t = blockIdx.x + (long long)s * gridDim.x;
+            if (t < ntiles) issue(s, t);
+        }
+
+    int it = 0;
+    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it)
+    {
+        const int s = it % NS;
+        const uint32_t parity = (uint32_t)(it / NS) & 1u;
+        const bool ok = mbar_wait_bounded(&full[s], parity, kStageWaitLimit);
+
+        const long long r = tile / tiles_per_row;
+        const int seg = (int)(tile - r * tiles_per_row);
+        const int j = 1 + (int)(r % L.ny), k = 1 + (int)(r / L.ny);
+        const int c0 = seg * TW + 2 * tid;
+        const bool active = ok && c0 < L.nx;
+        if (active)
+        {
+            const long long cell = (long long)k * L.plane + (long long)j * L.pitch + c0;
+            uint32_t lk0 = 0, lk1 = 0;
+            const uint32_t b = (near_word(a, L, c0, j, k) >> (c0 & 31)) & 3u;
+            if (b & 1u) lk0 = a.links[cell];
+            if (b & 2u) lk1 = a.links[cell + 1];
+            const S* sp = stages + (size_t)s * Q * ROW + PADE + 2 * tid;
+            float2 G[Q];
+#pragma unroll
+            for (int q = 0; q < Q; ++q)
+            {
+                if (ex(q) == 0) G[q] = T::pair(sp + q * ROW);
+                else if (ex(q) > 0) G[q] = T::left(sp + q * ROW);
+                else G[q] = T::right(sp + q * ROW);
+            }
+            const S* tin = fin + cell;
+            if (lk0 | lk1)
+            {
+#pragma unroll
+                for (int q = 0; q < Q; ++q)
+                {
+                    if (((lk0 | lk1) >> q) & 1u)
+                    {
+                        const float2 own = P::cvt(P::ld(tin + a.pop_off[inv(q)]));
+                        if ((lk0 >> q) & 1u) G[q].x = own.x;
+                        if ((lk1 >> q) & 1u) G[q].y = own.y;
+                    }
+                }
+            }
+            const bool xlo = c0 == 0;
+            const bool xhi0 = c0 == L.nx - 1;
+            const bool xhi1 = c0 + 1 == L.nx - 1;
+            if (xlo | xhi0 | xhi1)
+            {
+#pragma unroll
+                for (int q = 0; q < Q; ++q)
+                {
+                    if (ex(q) == 0) continue;
+                    const float g = a.xf.xgh[a.xf.gh_index(ex(q) > 0 ? 0 : 1, q, j - ey(q), k - ez(q), L.ny, L.nz)];
+                    if (ex(q) > 0 && xlo && !((lk0 >> q) & 1u)) G[q].x = g;
+                    if (ex(q) < 0 && xhi0 && !((lk0 >> q) & 1u)) G[q].x = g;
+                    if (ex(q) < 0 && xhi1 && !((lk1 >> q) & 1u)) G[q].y = g;
+                }
+            }
+            const float syz = fmaxf(a.sig_y[j - 1], a.sig_z[k - 1]);
+            const float2 sg =
+                make_float2(fmaxf(a.sig_x[c0], syz), fmaxf(c0 + 1 < L.nx ? a.sig_x[c0 + 1] : 0.f, syz));
+            collide2(G, inv_scale, a.omega, sg, (lk0 & kSolidSelfBit) != 0u, (lk1 & kSolidSelfBit) != 0u);
+            S* tout = fout + cell;
+#pragma unroll
+            for (int q = 0; q < Q; ++q) P::st(tout + a.pop_off[q], G[q]);
+            if (xlo | xhi0 | xhi1)
+            {
+#pragma unroll
+                for (int q = 0; q < Q; ++q)
+                {
+                    if (xlo) a.xf.xexp[a.xf.exp_index(0, q, j, k, L.ny, L.nz)] = P::rnd(G[q].x);
+                    if (xhi0) a.xf.xexp[a.xf.exp_index(1, q, j, k, L.ny, L.nz)] = P::rnd(G[q].x);
+                    if (xhi1) a.xf.xexp[a.xf.exp_index(1, q, j, k, L.ny, L.nz)] = P::rnd(G[q].y);
+                }
+            }
+        }
+        // every thread is done with stage s (and agrees on whether the wait failed)
+        const int failed = __syncthreads_or(!ok);
+        if (failed)
+        {
+            if (tid == 0)
+            {
+                atomicExch(a.error, kErrStageTimeout);
+                // let the copies already in flight land before the CTA exits
+                for (int d = 0; d < NS; ++d)
+                {
+                    const long long t = tile + (long long)d * gridDim.x;
+                    if (t < ntiles) mbar_wait_bounded(&full[(it + d) % NS], (uint32_t)((it + d) / NS) & 1u, kStageWaitLimit);
+                }
+            }
+            return;
+        }
+        if (tid == 0)
+        {
+            const long long next = tile + (long long)NS * gridDim.x;
+            if (next < ntiles)
+            {
+                fence_proxy_async_smem();   // generic-proxy reads of stage s before the async-proxy refill
+                issue(s, next);
+            }
         }
     }
 }
@@ -670,9 +1172,85 @@ __global__ void k_import_f(S* __restrict__ f, const double* __restrict__ in, Lay
 }
 
 dim3 row_grid(const Layout& L) { return dim3((unsigned)((L.nx + 127) / 128), (unsigned)L.ny, (unsigned)L.nz); }
-dim3 pair_grid(const Layout& L)
+dim3 pair_grid(const Layout& L, int block)
 {
-    return dim3((unsigned)(((L.nx + 1) / 2 + 127) / 128), (unsigned)L.ny, (unsigned)L.nz);
+    return dim3((unsigned)(((L.nx + 1) / 2 + block - 1) / block), (unsigned)L.ny, (unsigned)L.nz);
+}
+
+template <typename S, int TW, int NS>
+constexpr size_t staged_smem()
+{
+    return (size_t)NS * Q * (TW + 2 * (16 / sizeof(S))) * sizeof(S);
+}
+
+template <typename S, int TW, int NS>
+cudaError_t launch_staged(const S* fin, S* fout, const Layout& L, const StepArgs& a, float inv_scale, int grid,
+                          cudaStream_t stream)
+{
+    const int tpr = (L.nx + TW - 1) / TW;
+    const long long ntiles = (long long)tpr * L.ny * L.nz;
+    const int g = (int)std::min<long long>(grid, ntiles);
+    k_step_staged<S, TW, NS><<<g, TW / 2, staged_smem<S, TW, NS>(), stream>>>(fin, fout, L, a, inv_scale, tpr, ntiles);
+    return cudaGetLastError();
+}
+
+template <typename S, int TW, int NS>
+cudaError_t prepare_staged(int device, int* grid)
+{
+    const size_t smem = staged_smem<S, TW, NS>();
+    cudaError_t e = cudaFuncSetAttribute(k_step_staged<S, TW, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0, sms = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_staged<S, TW, NS>, TW / 2, smem);
+    if (e != cudaSuccess) return e;
+    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    if (e != cudaSuccess) return e;
+    *grid = std::max(1, per_sm) * sms;
+    return cudaSuccess;
+}
+
+template <typename S>
+cudaError_t launch_step_t(const S* fin, S* fout, const Layout& L, const StepArgs& a, float inv_scale, int variant,
+                          int grid, cudaStream_t stream)
+{
+    switch (variant)
+    {
+    case 4: return launch_staged<S, 256, 3>(fin, fout, L, a, inv_scale, grid, stream);
+    case 5: return launch_staged<S, 256, 2>(fin, fout, L, a, inv_scale, grid, stream);
+    case 6: return launch_staged<S, 128, 4>(fin, fout, L, a, inv_scale, grid, stream);
+    case 7: return launch_staged<S, 512, 2>(fin, fout, L, a, inv_scale, grid, stream);
+    case 8:
+        if constexpr (std::is_same<S, __half>::value)
+        {
+            const dim3 g((unsigned)(((L.nx + 3) / 4 + 127) / 128), (unsigned)L.ny, (unsigned)L.nz);
+            k_step_quad<128, 0><<<g, 128, 0, stream>>>(fin, fout, L, a, inv_scale);
+            return cudaGetLastError();
+        }
+        variant = 3;
+        break;
+    case 10: k_step32<S, 128, 0><<<pair_grid(L, 128), 128, 0, stream>>>(fin, fout, L, a, inv_scale); return cudaGetLastError();
+    case 11: k_step32<S, 128, 8><<<pair_grid(L, 128), 128, 0, stream>>>(fin, fout, L, a, inv_scale); return cudaGetLastError();
+    case 12: k_step32<S, 64, 0><<<pair_grid(L, 64), 64, 0, stream>>>(fin, fout, L, a, inv_scale); return cudaGetLastError();
+    case 9:
+        if constexpr (std::is_same<S, __half>::value)
+        {
+            const dim3 g((unsigned)(((L.nx + 3) / 4 + 127) / 128), (unsigned)L.ny, (unsigned)L.nz);
+            k_step_quad<128, 6><<<g, 128, 0, stream>>>(fin, fout, L, a, inv_scale);
+            return cudaGetLastError();
+        }
+        variant = 3;
+        break;
+    default: break;
+    }
+    switch (variant)
+    {
+    case 1: k_step<S, 128, 8><<<pair_grid(L, 128), 128, 0, stream>>>(fin, fout, L, a, inv_scale); break;
+    case 2: k_step<S, 256, 4><<<pair_grid(L, 256), 256, 0, stream>>>(fin, fout, L, a, inv_scale); break;
+    case 3: k_step<S, 64, 0><<<pair_grid(L, 64), 64, 0, stream>>>(fin, fout, L, a, inv_scale); break;
+    default: k_step<S, 128, 0><<<pair_grid(L, 128), 128, 0, stream>>>(fin, fout, L, a, inv_scale); break;
+    }
+    return cudaGetLastError();
 }
 
 }  // namespace
@@ -685,13 +1263,25 @@ cudaError_t launch_build_links(const uint8_t* mask_ref, uint32_t* links, uint32_
 }
 
 cudaError_t launch_step(int storage, const void* fin, void* fout, const Layout& L, const StepArgs& a,
-                        float scale, cudaStream_t stream)
+                        float scale, int variant, int grid, cudaStream_t stream)
 {
     if (storage == 0)
-        k_step<float><<<pair_grid(L), 128, 0, stream>>>((const float*)fin, (float*)fout, L, a, 1.0f);
-    else
-        k_step<__half><<<pair_grid(L), 128, 0, stream>>>((const __half*)fin, (__half*)fout, L, a, 1.0f / scale);
-    return cudaGetLastError();
+        return launch_step_t<float>((const float*)fin, (float*)fout, L, a, 1.0f, variant, grid, stream);
+    return launch_step_t<__half>((const __half*)fin, (__half*)fout, L, a, 1.0f / scale, variant, grid, stream);
+}
+
+cudaError_t prepare_step(int storage, int variant, int device, int* grid)
+{
+    *grid = 0;
+    const bool h = storage != 0;
+    switch (variant)
+    {
+    case 4: return h ? prepare_staged<__half, 256, 3>(device, grid) : prepare_staged<float, 256, 3>(device, grid);
+    case 5: return h ? prepare_staged<__half, 256, 2>(device, grid) : prepare_staged<float, 256, 2>(device, grid);
+    case 6: return h ? prepare_staged<__half, 128, 4>(device, grid) : prepare_staged<float, 128, 4>(device, grid);
+    case 7: return h ? prepare_staged<__half, 512, 2>(device, grid) : prepare_staged<float, 512, 2>(device, grid);
+    default: return cudaSuccess;
+    }
 }
 
 cudaError_t launch_source(int storage, void* f, const Layout& L, const StepArgs& sa, const SourceArgs& a,
