@@ -29,8 +29,12 @@ namespace {
 
 constexpr int kTableRows = 4096;   // source-schedule rows resident on the device
 constexpr int kProbeRows = 4096;   // probe-series rows buffered on the device
-constexpr int kDefaultStepVariant = 0;
-constexpr int kDefaultPrefetchRows = 0;
+// Fused-step implementation and L2 prefetch distance per storage type, from
+// launch-shape sweeps on the 1024x1024x256 city (B200): FP32 is fastest with
+// the plain pair kernel; FP16 with the packed pair kernel at a 64-register
+// cap plus line prefetches 96 rows ahead.
+constexpr int kDefaultStepVariant[2] = {0, 4};
+constexpr int kDefaultPrefetchRows[2] = {0, 96};
 
 struct SourceState
 {
@@ -54,9 +58,7 @@ struct lbm_handle
     std::string err;
     int storage = LBM_STORE_F32;
     float scale = 1.0f;
-    int step_variant = kDefaultStepVariant;   // fused-step implementation (NLOS_LBM_STEP_VARIANT)
-    int step_grid = 0;                 // persistent grid of the staged variants
-    int* d_error = nullptr;            // kernel error word (bounded waits)
+    int step_variant = 0;              // fused-step implementation (NLOS_LBM_STEP_VARIANT overrides)
 
     // geometry / mask
     HeightField geo;
@@ -73,14 +75,13 @@ struct lbm_handle
     double dt = 0.0;
     Layout L{};
     std::vector<uint8_t> mask;           // reference layout, halo-inclusive
-    std::vector<long long> probe_cell;   // device linear cell, -1 unowned
+    std::vector<int> probe_ijk;          // halo-inclusive cell coordinates, i = -1 unowned
     std::vector<int> probe_owned, probe_solid;
 
     // device state
     int device = 0;
     cudaStream_t stream = nullptr;
-    void* f_alloc[2] = {nullptr, nullptr};
-    void* f[2] = {nullptr, nullptr};   // origin pointers (alloc + front pad)
+    void* f[2] = {nullptr, nullptr};   // population buffers (block-interleaved layout)
     int cur = 0;
     uint32_t* links = nullptr;
     uint32_t* near = nullptr;
@@ -93,7 +94,7 @@ struct lbm_handle
     SourceEntry* d_table = nullptr;
     SourceEntry* h_table = nullptr;    // pinned
     long long table_base = 0, table_rows = 0;
-    long long* d_probe_cell = nullptr;
+    int* d_probe_ijk = nullptr;
     double* d_probe_out = nullptr;
     double* h_probe_out = nullptr;     // pinned
     double* d_energy = nullptr;
@@ -138,8 +139,8 @@ struct lbm_handle
         ev_used = 0;
         for (int b = 0; b < 2; ++b)
         {
-            if (f_alloc[b]) cudaFree(f_alloc[b]);
-            f_alloc[b] = f[b] = nullptr;
+            if (f[b]) cudaFree(f[b]);
+            f[b] = nullptr;
         }
         cudaFree(links); links = nullptr;
         cudaFree(near); near = nullptr;
@@ -147,9 +148,8 @@ struct lbm_handle
         cudaFree(xf.xexp); xf.xexp = nullptr;
         cudaFree(xf.xgh); xf.xgh = nullptr;
         cudaFree(ctl); ctl = nullptr;
-        cudaFree(d_error); d_error = nullptr;
         cudaFree(d_table); d_table = nullptr;
-        cudaFree(d_probe_cell); d_probe_cell = nullptr;
+        cudaFree(d_probe_ijk); d_probe_ijk = nullptr;
         cudaFree(d_probe_out); d_probe_out = nullptr;
         cudaFree(d_energy); d_energy = nullptr;
         if (ctl_host) cudaFreeHost(ctl_host);
@@ -394,7 +394,6 @@ extern "C" const char* lbm_status_string(int s)
     case LBM_ERR_NO_DEVICE: return "no CUDA device";
     case LBM_ERR_IO: return "I/O error";
     case LBM_ERR_UNSUPPORTED: return "unsupported";
-    case LBM_ERR_TIMEOUT: return "kernel wait timed out";
     default: return "unknown status";
     }
 }
@@ -546,8 +545,12 @@ extern "C" int lbm_init(lbm_handle* h)
     L.pitch = (nx + 2 + 31) / 32 * 32;
     L.words_per_row = L.pitch / 32;
     L.plane = (long long)L.pitch * nyt;
-    L.pop_stride = ((long long)kFrontPad + L.plane * nzt + kBackPad + 63) / 64 * 64;
-    if (L.pop_stride >= (1ll << 31)) return h->fail(LBM_ERR_UNSUPPORTED, "grid too large for one GPU");
+    L.bc = block_cells(h->storage == LBM_STORE_F16 ? 2 : 4);
+    L.bc_shift = L.bc == 64 ? 6 : 5;
+    L.nb = (nx + L.bc - 1) / L.bc;
+    L.row_stride = (long long)L.nb * Q * L.bc;
+    L.plane_stride = L.row_stride * nyt;
+    L.total = kFrontElems + L.plane_stride * nzt + kBackElems;
 
     // Mask (init_domain 06:453-532).
     if (!h->mask_override.empty())
@@ -578,15 +581,14 @@ extern "C" int lbm_init(lbm_handle* h)
     // Device buffers.
     CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "cudaStreamCreate");
     const size_t esz = h->storage == LBM_STORE_F16 ? 2 : 4;
-    const size_t pop_bytes = (size_t)Q * (size_t)L.pop_stride * esz;
+    const size_t pop_bytes = (size_t)L.total * esz;
     cudaError_t e = cudaSuccess;
     for (int b = 0; b < 2; ++b)
     {
-        if (e == cudaSuccess) e = cudaMalloc(&h->f_alloc[b], pop_bytes);
-        if (e == cudaSuccess) e = cudaMemsetAsync(h->f_alloc[b], 0, pop_bytes, h->stream);   // g = 0: rest state (06:388-395)
-        if (e == cudaSuccess) h->f[b] = (char*)h->f_alloc[b] + kFrontPad * esz;
+        if (e == cudaSuccess) e = cudaMalloc(&h->f[b], pop_bytes);
+        if (e == cudaSuccess) e = cudaMemsetAsync(h->f[b], 0, pop_bytes, h->stream);   // g = 0: rest state (06:388-395)
     }
-    const size_t cells = (size_t)L.pop_stride;
+    const size_t cells = (size_t)L.plane * nzt;
     h->links = dalloc<uint32_t>(cells, e);
     const size_t near_words = (size_t)nzt * nyt * L.words_per_row;
     h->near = dalloc<uint32_t>(near_words, e);
@@ -595,13 +597,11 @@ extern "C" int lbm_init(lbm_handle* h)
     h->xf.xexp = dalloc<float>(n_xexp, e);
     h->xf.xgh = dalloc<float>(n_xgh, e);
     h->ctl = dalloc<Control>(1, e);
-    h->d_error = dalloc<int>(1, e);
     if (e != cudaSuccess) return h->cuda_fail(e, "device allocation");
     CK(cudaMemsetAsync(h->links, 0, cells * sizeof(uint32_t), h->stream), "memset links");
     CK(cudaMemsetAsync(h->near, 0, near_words * sizeof(uint32_t), h->stream), "memset near");
     CK(cudaMemsetAsync(h->xf.xexp, 0, n_xexp * sizeof(float), h->stream), "memset x faces");
     CK(cudaMemsetAsync(h->xf.xgh, 0, n_xgh * sizeof(float), h->stream), "memset x faces");
-    CK(cudaMemsetAsync(h->d_error, 0, sizeof(int), h->stream), "memset error");
     CK(cudaMallocHost(&h->ctl_host, sizeof(Control)), "cudaMallocHost");
     CK(cudaMemcpyAsync(h->sig, sx.data(), sx.size() * 4, cudaMemcpyHostToDevice, h->stream), "upload sponge");
     CK(cudaMemcpyAsync(h->sig + nx, sy.data(), sy.size() * 4, cudaMemcpyHostToDevice, h->stream), "upload sponge");
@@ -627,17 +627,12 @@ extern "C" int lbm_init(lbm_handle* h)
     h->sa.sig_z = h->sig + nx + ny;
     h->sa.omega = (float)(1.0 / c.tau);
     h->sa.xf = h->xf;
+    const int si = h->storage == LBM_STORE_F16 ? 1 : 0;
+    h->step_variant = kDefaultStepVariant[si];
     if (const char* v = std::getenv("NLOS_LBM_STEP_VARIANT")) h->step_variant = std::atoi(v);
-    if (h->step_variant < 0 || h->step_variant > 12) return h->fail(LBM_ERR_BAD_CONFIG, "NLOS_LBM_STEP_VARIANT out of range");
-    h->sa.prefetch_rows = kDefaultPrefetchRows;
+    if (h->step_variant < 0 || h->step_variant > 7) return h->fail(LBM_ERR_BAD_CONFIG, "NLOS_LBM_STEP_VARIANT out of range");
+    h->sa.prefetch_rows = kDefaultPrefetchRows[si];
     if (const char* v = std::getenv("NLOS_LBM_PREFETCH_ROWS")) h->sa.prefetch_rows = std::max(0, std::atoi(v));
-    CK(prepare_step(h->storage, h->step_variant, h->device, &h->step_grid), "prepare step kernel");
-    h->sa.error = h->d_error;
-    for (int q = 0; q < Q; ++q)
-    {
-        h->sa.pop_off[q] = (long long)q * L.pop_stride;
-        h->sa.pull_off[q] = (long long)q * L.pop_stride - ((long long)ey(q) * L.pitch + (long long)ez(q) * L.plane);
-    }
 
     // Open faces for the ghost kernel.
     h->ga = GhostArgs{};
@@ -661,7 +656,7 @@ extern "C" int lbm_init(lbm_handle* h)
     // Probes (06:415-437).
     int status = h->stl_status;
     const int np = h->nprobe();
-    h->probe_cell.assign((size_t)np, -1);
+    h->probe_ijk.assign((size_t)np * 3, -1);
     h->probe_owned.assign((size_t)np, 0);
     h->probe_solid.assign((size_t)np, 0);
     for (int p = 0; p < np; ++p)
@@ -672,7 +667,9 @@ extern "C" int lbm_init(lbm_handle* h)
         if (gi >= 0 && gi < nx && gj >= 0 && gj < ny && gk >= 0 && gk < nz)
         {
             h->probe_owned[p] = 1;
-            h->probe_cell[p] = L.cell(gi + 1, gj + 1, gk + 1);
+            h->probe_ijk[3 * p] = gi + 1;
+            h->probe_ijk[3 * p + 1] = gj + 1;
+            h->probe_ijk[3 * p + 2] = gk + 1;
             const size_t idx = (size_t)(gi + 1) + (size_t)(gj + 1) * nxt + (size_t)(gk + 1) * nxt * nyt;
             if (h->mask[idx])
             {
@@ -683,13 +680,15 @@ extern "C" int lbm_init(lbm_handle* h)
         }
     }
     const int npa = std::max(np, 1);
-    h->d_probe_cell = dalloc<long long>((size_t)npa, e);
+    h->d_probe_ijk = dalloc<int>((size_t)npa * 3, e);
     h->d_probe_out = dalloc<double>((size_t)npa * kProbeRows, e);
     h->d_energy = dalloc<double>((size_t)npa, e);
     if (e != cudaSuccess) return h->cuda_fail(e, "probe buffers");
     CK(cudaMallocHost(&h->h_probe_out, (size_t)npa * kProbeRows * sizeof(double)), "cudaMallocHost");
-    if (np) CK(cudaMemcpyAsync(h->d_probe_cell, h->probe_cell.data(), (size_t)np * 8, cudaMemcpyHostToDevice, h->stream),
-               "upload probes");
+    if (np)
+        CK(cudaMemcpyAsync(h->d_probe_ijk, h->probe_ijk.data(), (size_t)np * 3 * sizeof(int), cudaMemcpyHostToDevice,
+                           h->stream),
+           "upload probes");
     CK(cudaMemsetAsync(h->d_energy, 0, (size_t)npa * 8, h->stream), "memset energy");
 
     // Source schedule buffers (sized for the maximum source count so sources
@@ -743,7 +742,7 @@ ProbeArgs probe_args(lbm_handle* h, bool batched, long long direct_row)
 {
     ProbeArgs a{};
     a.n = h->nprobe();
-    a.cell = h->d_probe_cell;
+    a.ijk = h->d_probe_ijk;
     a.out = h->d_probe_out;
     a.energy = h->d_energy;
     a.ctl = batched ? h->ctl : nullptr;
@@ -769,13 +768,13 @@ cudaError_t timed_step_launch(lbm_handle* h, const void* fin, void* fout)
         }
         e = cudaEventRecord(h->ev[h->ev_used], h->stream);
         if (e != cudaSuccess) return e;
-        e = launch_step(h->storage, fin, fout, h->L, h->sa, h->scale, h->step_variant, h->step_grid, h->stream);
+        e = launch_step(h->storage, fin, fout, h->L, h->sa, h->scale, h->step_variant, h->stream);
         if (e != cudaSuccess) return e;
         e = cudaEventRecord(h->ev[h->ev_used + 1], h->stream);
         h->ev_used += 2;
         return e;
     }
-    return launch_step(h->storage, fin, fout, h->L, h->sa, h->scale, h->step_variant, h->step_grid, h->stream);
+    return launch_step(h->storage, fin, fout, h->L, h->sa, h->scale, h->step_variant, h->stream);
 }
 
 // Collect the kernel times recorded since the last harvest (synchronises).
@@ -882,16 +881,6 @@ int fill_table(lbm_handle* h, long long s0)
     h->table_base = s0;
     h->table_rows = kTableRows;
     return LBM_OK;
-}
-
-// A kernel that gave up a bounded wait leaves a code in the error word.
-int check_kernel_error(lbm_handle* h)
-{
-    int code = 0;
-    CK(cudaMemcpy(&code, h->d_error, sizeof(int), cudaMemcpyDeviceToHost), "error word");
-    if (code == 0) return LBM_OK;
-    cudaMemset(h->d_error, 0, sizeof(int));
-    return h->fail(LBM_ERR_TIMEOUT, "a staged-copy wait in the step kernel timed out");
 }
 
 int check_ready(lbm_handle* h)
@@ -1061,8 +1050,6 @@ extern "C" int lbm_step(lbm_handle* h, int nsteps)
         }
         // the control block upload must not be overwritten before the copy ran
         CK(cudaStreamSynchronize(h->stream), "step sync");
-        st = check_kernel_error(h);
-        if (st) return st;
         h->step += chunk;
         if (np) h->probe_pending += chunk;
         left -= chunk;

@@ -1,18 +1,24 @@
 // Device-side data layout and kernel launchers of the D3Q19 acoustic step.
 // Included by the host C++ (api.cpp, built with g++) and by kernels.cu.
 //
-// Population layout in HBM (structure of arrays, one array per direction q):
-//   element (i, j, k) of direction q, in the reference's halo-inclusive cell
-//   coordinates i = 0..nx+1, j = 0..ny+1, k = 0..nz+1 (06:206-209), lives at
-//       base + q * pop_stride + k * plane + j * pitch + (i - 1)
-//   pitch = round_up(nx + 2, 32), plane = pitch * (ny + 2).
-//   Interior rows therefore start on a 128-byte (FP32) / 64-byte (FP16)
-//   boundary, the x-high halo sits at column nx, and the x-low halo of row j
-//   occupies the last (padding) column of row j-1; one 32-element pad before
-//   the origin holds the x-low halo of (j=0, k=0).  Pull offsets are the same
-//   for every cell: src = dst - (ex + ey * pitch + ez * plane).
+// Population layout in HBM: block-interleaved ("array of structures of
+// arrays").  Each row (j, k) of the halo-inclusive grid, j = 0..ny+1,
+// k = 0..nz+1 (06:206-209), holds nb = ceil(nx/bc) blocks of bc cells along
+// x, bc = 128 bytes / element size (32 FP32 or 64 FP16 cells); a block
+// stores its 19 directions one after the other, bc elements each, so every
+// direction of a block is exactly one 128-byte line:
+//     elem(q, i, j, k) = kFrontElems + (k * (ny+2) + j) * row_stride
+//                        + ((i-1) / bc) * 19 bc + q * bc + ((i-1) % bc)
+// for interior columns i = 1..nx, with row_stride = nb * 19 bc.  A thread's
+// 19 loads or stores for one row therefore differ by compile-time
+// immediates (q * bc), and a warp-wide access of one direction reads or
+// writes whole lines.  The x-halo columns are not stored: open x
+// faces keep their ghosts in the compact x-face buffers (XFace).
 // Stored values are deviations from rest equilibrium, g_q = f_q - w_q, times
 // `scale` (1 for FP32; the per-run FP16 scale otherwise).
+//
+// Per-cell side arrays (links words, near-solid bits) use a plain padded
+// layout: cell(i, j, k) = k * plane + j * pitch + (i - 1).
 #pragma once
 
 #include <cstddef>
@@ -23,20 +29,35 @@
 namespace lbm {
 
 constexpr int kMaxSources = 8;
-constexpr int kFrontPad = 32;
-// Elements after the last plane: a staged row copy of the last row may run
-// up to one tile (<= 512 elements) plus its alignment margin past it.
-constexpr int kBackPad = 1024;
+constexpr int kLineBytes = 128;
+// cells per interleaved block for an element size in bytes (one line per direction)
+__host__ __device__ constexpr int block_cells(int esz) { return kLineBytes / esz; }
+constexpr long long kFrontElems = 19 * 64 + 64;   // pad before the first row (>= one block)
+constexpr long long kBackElems = 19 * 64 + 64;    // pad after the last row
 
 struct Layout
 {
-    int nx, ny, nz;        // interior cells
-    int pitch;             // x pitch, elements
-    int words_per_row;     // pitch / 32 (near-solid bitmap)
-    long long plane;       // pitch * (ny + 2)
-    long long pop_stride;  // elements per direction array, incl. pads
-    // Linear cell index of halo-inclusive coordinates (relative to the origin).
-    long long cell(int i, int j, int k) const { return (long long)k * plane + (long long)j * pitch + (i - 1); }
+    int nx, ny, nz;          // interior cells
+    int pitch;               // x pitch of the side arrays, round_up(nx + 2, 32)
+    int words_per_row;       // pitch / 32 (near-solid bitmap)
+    long long plane;         // pitch * (ny + 2)
+    int bc;                  // cells per interleaved block (32 FP32, 64 FP16)
+    int bc_shift;            // log2(bc)
+    int nb;                  // blocks per row
+    long long row_stride;    // nb * 19 * bc population elements per row
+    long long plane_stride;  // (ny + 2) * row_stride
+    long long total;         // population elements per buffer, pads included
+
+    __host__ __device__ long long cell(int i, int j, int k) const
+    {
+        return (long long)k * plane + (long long)j * pitch + (i - 1);
+    }
+    __host__ __device__ long long elem(int q, int i, int j, int k) const
+    {
+        const int c = i - 1;
+        return kFrontElems + ((long long)k * (ny + 2) + j) * row_stride +
+               (long long)(c >> bc_shift) * (19 * bc) + q * bc + (c & (bc - 1));
+    }
 };
 
 // Device control block: read by the kernels of a batched (graph) step.
@@ -78,12 +99,11 @@ struct GhostFace
     long long first;       // first thread index of this face
 };
 
-// x-face buffers (float, stored deviation units).  The x-halo columns of the
-// population arrays are not used: the fused step exports the post-collision
-// populations of the cells next to the x faces into `xexp`, the ghost kernel
-// turns them into the open-boundary ghosts `xgh`, and the step reads those
-// for the first and last cell of each row.  Both are [side][q][k][j] and
-// coalesced along j, so no strided column of the populations is touched.
+// x-face buffers (float, stored deviation units).  The fused step exports
+// the post-collision populations of the cells next to the x faces into
+// `xexp`, the ghost kernel turns them into the open-boundary ghosts `xgh`,
+// and the step reads those for the first and last cell of each row.  Both
+// are [side][q][k][j], coalesced along j.
 //   xexp: side 0/1 = cells i = 1 / i = nx, j = 1..ny, k = 1..nz  -> [2][Q][nz][ny]
 //   xgh : side 0/1 = halo i = 0 / i = nx+1, j = 0..ny+1, k = 0..nz+1 -> [2][Q][nz+2][ny+2]
 struct XFace
@@ -118,20 +138,13 @@ struct StepArgs
     const float* sig_z;
     float omega;               // 1 / tau
     XFace xf;
-    // Per direction, in elements (warp-uniform address offsets):
-    long long pull_off[19];    // q * pop_stride - (ey * pitch + ez * plane): aligned source of a pair
-    long long pop_off[19];     // q * pop_stride
-    int* error;                // set when a bounded wait in a kernel gives up (0 = fine)
-    int prefetch_rows;         // > 0: each block prefetches into L2 the source rows of the row this far ahead
+    int prefetch_rows;         // > 0: each block prefetches into L2 the lines the row this far ahead will read
 };
-
-// Error codes a kernel writes to StepArgs::error.
-constexpr int kErrStageTimeout = 1;   // staged-copy barrier wait exceeded its limit
 
 struct ProbeArgs
 {
     int n;
-    const long long* cell;     // linear index, -1 = not owned
+    const int* ijk;            // [n][3] halo-inclusive cell coordinates; i = -1: not owned
     double* out;               // [row][n], row = step - probe_base
     double* energy;            // [n] running sum of p^2 (FP64)
     Control* ctl;              // nullptr: row = direct_row, no counter update
@@ -146,20 +159,14 @@ cudaError_t launch_build_links(const uint8_t* mask_ref, uint32_t* links, uint32_
 cudaError_t launch_source(int storage, void* f, const Layout& L, const StepArgs& sa, const SourceArgs& a,
                           cudaStream_t stream);
 cudaError_t launch_ghost(int storage, void* f, const Layout& L, const GhostArgs& a, cudaStream_t stream);
-// variant: implementation / launch shape of the fused step; all do the same
-// work.  0-3: register-resident pairs with lane shuffles (0: 128 threads,
-// 1: 128 threads with at most 64 registers, 2: 256 threads, 3: 64 threads);
-// 4-7: persistent CTAs staging rows in shared memory with bulk async copies
-// (tile width / stages 256/3, 256/2, 128/4, 512/2); 8, 9: four cells per
-// thread with 8-byte vectors (FP16 storage; 9 caps registers at 80; FP32
-// storage runs variant 3); 10-12: pair kernel with 32-bit per-thread offsets
-// (128 threads, 128 threads with at most 64 registers, 64 threads).  `grid` is the persistent
-// grid from prepare_step (ignored by 0-3).
+// variant: implementation of the fused step, same work in all.  0-3: two
+// cells per thread (0: 128 threads, 1: 128 threads with at most 64
+// registers, 2: 256 threads, 3: 64 threads); 4-7: FP16 storage only, kept
+// packed as half2 through the update (cells per thread / register cap:
+// 4: 2/64, 5: 4/85, 6: 2/51, 7: 4/102, 128 threads); FP32 storage runs
+// variant 0 instead.
 cudaError_t launch_step(int storage, const void* fin, void* fout, const Layout& L, const StepArgs& a,
-                        float scale, int variant, int grid, cudaStream_t stream);
-// Per-variant set-up (shared-memory opt-in, persistent grid size); call
-// once per device before the first launch and outside stream capture.
-cudaError_t prepare_step(int storage, int variant, int device, int* grid);
+                        float scale, int variant, cudaStream_t stream);
 cudaError_t launch_probe(int storage, const void* f, const Layout& L, const StepArgs& sa, const ProbeArgs& a,
                          cudaStream_t stream);
 // (float)(rho - 1) of every interior cell, pulled from the pre-step buffer `f`.

@@ -1,10 +1,10 @@
 // sm_100a kernels of the D3Q19 acoustic step (family-B semantics of
 // 06_transient_localization_dx1.cpp).  Storage is FP32 or FP16 deviations from
-// rest equilibrium (see device.hpp for the HBM layout); arithmetic is FP32,
-// with FP64 for the source-weight reduction and the probe accumulators.
+// rest equilibrium in the block-interleaved layout of device.hpp; arithmetic
+// is FP32 (packed FP32x2 where two cells go together), with FP64 for the
+// source-weight reduction and the probe accumulators.
 #include <cuda_fp16.h>
 
-#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <type_traits>
@@ -28,7 +28,6 @@ struct Io<float>
     static __device__ __forceinline__ float ld(const float* p) { return __ldg(p); }
     static __device__ __forceinline__ float ldw(const float* p) { return *p; }
     static __device__ __forceinline__ void st(float* p, float v) { *p = v; }
-    static __device__ __forceinline__ float rnd(float v) { return v; }   // value as stored
 };
 
 template <>
@@ -37,14 +36,51 @@ struct Io<__half>
     static __device__ __forceinline__ float ld(const __half* p) { return __half2float(__ldg(p)); }
     static __device__ __forceinline__ float ldw(const __half* p) { return __half2float(*p); }
     static __device__ __forceinline__ void st(__half* p, float v) { *p = __float2half_rn(v); }
-    static __device__ __forceinline__ float rnd(float v) { return __half2float(__float2half_rn(v)); }
 };
 
-// Row part of the pull offset of direction q: src = dst - ex(q) - row_off(q).
-__device__ __forceinline__ long long row_off(int q, const Layout& L)
+// Two x-adjacent cells as one aligned vector: float2 (8 B) or half2 (4 B).
+// `V` is the raw register form that is shuffled between lanes.
+template <typename S>
+struct PairIo;
+
+template <>
+struct PairIo<float>
 {
-    return (long long)ey(q) * L.pitch + (long long)ez(q) * L.plane;
-}
+    using V = float2;
+    static __device__ __forceinline__ V ld(const float* p) { return __ldg(reinterpret_cast<const float2*>(p)); }
+    static __device__ __forceinline__ void st(float* p, float2 v) { *reinterpret_cast<float2*>(p) = v; }
+    static __device__ __forceinline__ float2 cvt(V v) { return v; }
+    static __device__ __forceinline__ float hi_of(V v) { return v.y; }
+    static __device__ __forceinline__ float lo_of(V v) { return v.x; }
+    // cells (c-1, c) from the previous pair's high element and cur = (c, c+1)
+    static __device__ __forceinline__ float2 left(float prev_hi, V cur) { return make_float2(prev_hi, cur.x); }
+    // cells (c+1, c+2) from cur = (c, c+1) and the next pair's low element
+    static __device__ __forceinline__ float2 right(V cur, float next_lo) { return make_float2(cur.y, next_lo); }
+    static __device__ __forceinline__ float rnd(float v) { return v; }   // value as stored
+};
+
+template <>
+struct PairIo<__half>
+{
+    using V = unsigned;
+    static __device__ __forceinline__ V ld(const __half* p) { return __ldg(reinterpret_cast<const unsigned*>(p)); }
+    static __device__ __forceinline__ void st(__half* p, float2 v)
+    {
+        *reinterpret_cast<__half2*>(p) = __float22half2_rn(v);
+    }
+    static __device__ __forceinline__ float2 cvt(V u)
+    {
+        __half2 h;
+        *reinterpret_cast<unsigned*>(&h) = u;
+        return __half22float2(h);
+    }
+    // the whole 32-bit word is shuffled; the byte permute picks the half
+    static __device__ __forceinline__ unsigned hi_of(V v) { return v; }
+    static __device__ __forceinline__ unsigned lo_of(V v) { return v; }
+    static __device__ __forceinline__ float2 left(unsigned prev, V cur) { return cvt(__byte_perm(prev, cur, 0x5432)); }
+    static __device__ __forceinline__ float2 right(V cur, unsigned next) { return cvt(__byte_perm(cur, next, 0x5432)); }
+    static __device__ __forceinline__ float rnd(float v) { return __half2float(__float2half_rn(v)); }
+};
 
 __device__ __forceinline__ void moments(const float (&G)[Q], float& rho, float& jx, float& jy, float& jz)
 {
@@ -75,40 +111,9 @@ __device__ __forceinline__ float dot_c(int q, float x, float y, float z)
     return r;
 }
 
-// BGK + sponge in deviation form, in place (06:940-967).  With stored
-// G = scale * (f - w):
-//   rho' = sum G, J = sum c G, r = 1 + rho'/scale (guard r <= 0 -> 1e-12, 06:948)
-//   Geq_q = w_q (rho' + 3 c.J + (4.5 (c.J)^2 - 1.5 J^2) / (scale r))
-//   G'    = (1 - sigma) (G - omega (G - Geq))      [sponge blend toward w_q, 06:955-965]
-__device__ __forceinline__ void collide(float (&G)[Q], float inv_scale, float omega, float sigma)
+__device__ __forceinline__ uint32_t near_bits(const StepArgs& a, const Layout& L, int col, int j, int k)
 {
-    float rho, jx, jy, jz;
-    moments(G, rho, jx, jy, jz);
-    float r = fmaf(rho, inv_scale, 1.0f);
-    if (r <= 0.f) r = 1e-12f;
-    const float irs = inv_scale / r;
-    const float base = rho - 1.5f * irs * (jx * jx + jy * jy + jz * jz);
-    const float k45 = 4.5f * irs;
-    const float keep = 1.0f - sigma;
-    const float cA = keep * (1.0f - omega);
-    const float cB = keep * omega;
-    G[0] = fmaf(cA, G[0], cB * wf(0) * base);
-#pragma unroll
-    for (int p = 0; p < 9; ++p)
-    {
-        const int q = pair_head(p);
-        const int qb = inv(q);
-        const float cj = dot_c(q, jx, jy, jz);
-        const float e = cB * wf(q) * fmaf(k45, cj * cj, base);
-        const float o = cB * (3.0f * wf(q)) * cj;
-        G[q] = fmaf(cA, G[q], e + o);
-        G[qb] = fmaf(cA, G[qb], e - o);
-    }
-}
-
-__device__ __forceinline__ uint32_t near_word(const StepArgs& a, const Layout& L, int col, int j, int k)
-{
-    return a.near[((long long)k * (L.ny + 2) + j) * L.words_per_row + (col >> 5)];
+    return a.near[((long long)k * (L.ny + 2) + j) * L.words_per_row + (col >> 5)] >> (col & 31);
 }
 
 // Pulled populations of one cell (halo-inclusive coordinates i, j, k),
@@ -118,17 +123,43 @@ template <typename S>
 __device__ __forceinline__ void pull_cell(const S* __restrict__ f, const Layout& L, const StepArgs& sa, int i, int j,
                                           int k, float (&G)[Q], bool& solid)
 {
-    const long long cell = (long long)k * L.plane + (long long)j * L.pitch + (i - 1);
-    const uint32_t lk = sa.links[cell];
+    const uint32_t lk = sa.links[L.cell(i, j, k)];
     solid = (lk & kSolidSelfBit) != 0u;
 #pragma unroll
     for (int q = 0; q < Q; ++q)
     {
         const int si = i - ex(q);
-        if ((lk >> q) & 1u) G[q] = Io<S>::ld(f + (long long)inv(q) * L.pop_stride + cell);
+        if ((lk >> q) & 1u) G[q] = Io<S>::ld(f + L.elem(inv(q), i, j, k));
         else if (si == 0) G[q] = sa.xf.xgh[sa.xf.gh_index(0, q, j - ey(q), k - ez(q), L.ny, L.nz)];
         else if (si == L.nx + 1) G[q] = sa.xf.xgh[sa.xf.gh_index(1, q, j - ey(q), k - ez(q), L.ny, L.nz)];
-        else G[q] = Io<S>::ld(f + (long long)q * L.pop_stride + cell - ex(q) - row_off(q, L));
+        else G[q] = Io<S>::ld(f + L.elem(q, si, j - ey(q), k - ez(q)));
+    }
+}
+
+// ---------------------------------------------------------------- L2 prefetch
+__constant__ signed char c_ey[19] = {0, 0, 0, 1, -1, 0, 0, 1, -1, 1, -1, 0, 0, 0, 0, 1, 1, -1, -1};
+__constant__ signed char c_ez[19] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1};
+
+// Each thread of a block asks L2 for one (or more) of the lines that the
+// same block position `prefetch_rows` rows later will load: direction q of
+// each interleaved block of the tile, from source row (j - ey, k - ez).
+// Prefetches hold no registers, so they add memory-level parallelism that
+// the register-bound demand loads cannot; those later loads then hit L2.
+template <typename S, int CELLS_PER_BLOCK>
+__device__ __forceinline__ void prefetch_rows_ahead(const S* f, const Layout& L, int dist, int j, int k, int col0)
+{
+    constexpr int BC = block_cells(sizeof(S));
+    constexpr int NBLK = (CELLS_PER_BLOCK + BC - 1) / BC;   // interleaved blocks in this tile
+    const long long r = (long long)(k - 1) * L.ny + (j - 1) + dist;
+    if (r >= (long long)L.ny * L.nz) return;
+    const int jj = 1 + (int)(r % L.ny), kk = 1 + (int)(r / L.ny);
+    for (int t = threadIdx.x; t < 19 * NBLK; t += blockDim.x)
+    {
+        const int q = t / NBLK, b = t - q * NBLK;
+        const int col = col0 + b * BC;
+        if (col >= L.nx) continue;
+        const S* p = f + L.elem(q, col + 1, jj - c_ey[q], kk - c_ez[q]);
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
     }
 }
 
@@ -141,9 +172,13 @@ __device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a
 __device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
 __device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, f2(-1.0f), a); }
 
-// Pair version of collide(): the same BGK + sponge update of two cells, in
-// lockstep.  A SOLID cell gets cA = 1, cB = 0, so its pulled values pass
-// through unchanged (06:933-938).
+// BGK + sponge of two cells in lockstep, in place, deviation form (06:940-967).
+// With stored G = scale * (f - w):
+//   rho' = sum G, J = sum c G, r = 1 + rho'/scale (guard r <= 0 -> 1e-12, 06:948)
+//   Geq_q = w_q (rho' + 3 c.J + (4.5 (c.J)^2 - 1.5 J^2) / (scale r))
+//   G'    = (1 - sigma) (G - omega (G - Geq))      [sponge blend toward w_q, 06:955-965]
+// A SOLID cell gets cA = 1, cB = 0, so its pulled values pass through
+// unchanged (06:933-938).
 __device__ __forceinline__ void collide2(float2 (&G)[Q], float inv_scale, float omega, float2 sigma, bool solid0,
                                          bool solid1)
 {
@@ -196,102 +231,39 @@ __device__ __forceinline__ void collide2(float2 (&G)[Q], float inv_scale, float 
     }
 }
 
-template <typename S>
-struct PairIo;
-
-template <>
-struct PairIo<float>
-{
-    using V = float2;
-    static __device__ __forceinline__ V ld(const float* p) { return __ldg(reinterpret_cast<const float2*>(p)); }
-    static __device__ __forceinline__ void st(float* p, float2 v) { *reinterpret_cast<float2*>(p) = v; }
-    static __device__ __forceinline__ float2 cvt(V v) { return v; }
-    static __device__ __forceinline__ V up(V v) { return make_float2(v.x, __shfl_up_sync(kFull, v.y, 1)); }
-    static __device__ __forceinline__ V down(V v) { return make_float2(__shfl_down_sync(kFull, v.x, 1), v.y); }
-    static __device__ __forceinline__ float2 left(V prev, V cur) { return make_float2(prev.y, cur.x); }
-    static __device__ __forceinline__ float2 right(V cur, V next) { return make_float2(cur.y, next.x); }
-    static __device__ __forceinline__ float rnd(float v) { return v; }
-};
-
-template <>
-struct PairIo<__half>
-{
-    using V = unsigned;
-    static __device__ __forceinline__ V ld(const __half* p) { return __ldg(reinterpret_cast<const unsigned*>(p)); }
-    static __device__ __forceinline__ void st(__half* p, float2 v)
-    {
-        *reinterpret_cast<__half2*>(p) = __float22half2_rn(v);
-    }
-    static __device__ __forceinline__ float2 cvt(V u)
-    {
-        __half2 h;
-        *reinterpret_cast<unsigned*>(&h) = u;
-        return __half22float2(h);
-    }
-    static __device__ __forceinline__ V up(V v) { return __shfl_up_sync(kFull, v, 1); }
-    static __device__ __forceinline__ V down(V v) { return __shfl_down_sync(kFull, v, 1); }
-    static __device__ __forceinline__ float2 left(V prev, V cur) { return cvt(__byte_perm(prev, cur, 0x5432)); }
-    static __device__ __forceinline__ float2 right(V cur, V next) { return cvt(__byte_perm(cur, next, 0x5432)); }
-    static __device__ __forceinline__ float rnd(float v) { return __half2float(__float2half_rn(v)); }
-};
-
-__device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes)
-{
-    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
-}
-
-// One thread of the block asks L2 for the 19 source row segments the same
-// block position needs `prefetch_rows` rows later, so that by the time that
-// block runs its loads hit L2 instead of HBM.  Segments are widened to
-// 16-byte boundaries (the bulk-prefetch alignment rule).
-template <typename S>
-__device__ __forceinline__ void prefetch_ahead(const S* fin, const Layout& L, const StepArgs& a, int j, int k,
-                                               int col0, int ncols)
-{
-    const long long r = (long long)(k - 1) * L.ny + (j - 1) + a.prefetch_rows;
-    if (r >= (long long)L.ny * L.nz) return;
-    const int jj = 1 + (int)(r % L.ny), kk = 1 + (int)(r / L.ny);
-    constexpr int PADE = 16 / (int)sizeof(S);
-    const long long cell0 = (long long)kk * L.plane + (long long)jj * L.pitch + col0;
-    const uint32_t bytes = (uint32_t)((ncols + 2 * PADE) * (int)sizeof(S) + 15) & ~15u;
-#pragma unroll
-    for (int q = 0; q < Q; ++q) prefetch_l2(fin + cell0 + a.pull_off[q] - PADE, bytes);
-}
-
 // Fused pull-stream + halfway bounce-back + BGK + sponge (06:906-972), two
-// x-adjacent cells per thread.  Each direction is read as one aligned vector
-// per thread; the +-1 x shift of directions with ex != 0 takes the missing
-// neighbour element from the adjacent lane (warp shuffle) and, at the warp
-// edge, from one extra aligned load.  The collision runs on the pair with
-// packed FP32x2 instructions.  Cells next to the x faces take their x-halo
-// sources from the x-face ghosts and export their results for the next ghost
-// fill.
+// x-adjacent cells per thread.  Direction q of the pair comes from the row
+// (j - ey, k - ez) of the block-interleaved layout as one aligned vector at
+// a compile-time offset from that row's base; the +-1 x shift of directions
+// with ex != 0 takes the missing neighbour element from the adjacent lane
+// (warp shuffle) and, at the warp edge, from one extra aligned load.  Cells
+// next to the x faces take their x-halo sources from the x-face ghosts and
+// export their results for the next ghost fill.
 template <typename S, int BLOCK, int MINB>
 __global__ void __launch_bounds__(BLOCK, MINB) k_step(const S* __restrict__ fin, S* __restrict__ fout, Layout L,
                                                       StepArgs a, float inv_scale)
 {
     using P = PairIo<S>;
+    constexpr int BC = block_cells(sizeof(S));   // cells per interleaved block
+    constexpr int BE = 19 * BC;                   // elements per block
     const int lane = threadIdx.x & 31;
-    const int c0r = 2 * (blockIdx.x * blockDim.x + threadIdx.x);   // first column of the pair
+    const int c0r = 2 * (blockIdx.x * BLOCK + threadIdx.x);   // first column (0-based) of the pair
     const bool active = c0r < L.nx;
-    const int c0 = active ? c0r : ((L.nx - 1) & ~1);              // inactive lanes shadow a valid pair
+    const int c0 = active ? c0r : ((L.nx - 1) & ~1);         // inactive lanes shadow a valid pair
     const int j = blockIdx.y + 1;
     const int k = blockIdx.z + 1;
-    const long long cell = (long long)k * L.plane + (long long)j * L.pitch + c0;
-    const S* tin = fin + cell;
-    if (a.prefetch_rows > 0 && threadIdx.x == 0)
-    {
-        const int col0 = 2 * blockIdx.x * BLOCK;
-        prefetch_ahead<S>(fin, L, a, j, k, col0, min(2 * BLOCK, L.nx - col0));
-    }
+    const long long e0 = L.elem(0, c0 + 1, j, k);
+    const S* own = fin + e0;
+    const long long rs = L.row_stride, ps = L.plane_stride;
+    if (a.prefetch_rows > 0) prefetch_rows_ahead<S, 2 * BLOCK>(fin, L, a.prefetch_rows, j, k, 2 * BLOCK * blockIdx.x);
 
     uint32_t lk0 = 0, lk1 = 0;
     if (active)
     {
-        const uint32_t nw = near_word(a, L, c0, j, k);
-        const uint32_t b = (nw >> (c0 & 31)) & 3u;
-        if (b & 1u) lk0 = a.links[cell];
-        if (b & 2u) lk1 = a.links[cell + 1];
+        const uint32_t b = near_bits(a, L, c0, j, k) & 3u;
+        const long long cl = L.cell(c0 + 1, j, k);
+        if (b & 1u) lk0 = a.links[cl];
+        if (b & 2u) lk1 = a.links[cl + 1];
     }
     const bool any_link = __any_sync(kFull, (lk0 | lk1) != 0u);
 
@@ -299,22 +271,26 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step(const S* __restrict__ fin,
 #pragma unroll
     for (int q = 0; q < Q; ++q)
     {
-        const S* src = tin + a.pull_off[q];
-        const typename P::V cur = P::ld(src);
+        const S* row = own - (ey(q) * rs + ez(q) * ps);
+        const typename P::V cur = P::ld(row + q * BC);
         if (ex(q) == 0)
         {
             G[q] = P::cvt(cur);
         }
         else if (ex(q) > 0)
         {
-            typename P::V prev = P::up(cur);
-            if (lane == 0) prev = P::ld(src - 2);
+            // lane 0 sits at the start of a block: its left neighbour pair is
+            // the last pair of the previous block
+            auto prev = __shfl_up_sync(kFull, P::hi_of(cur), 1);
+            if (lane == 0) prev = P::hi_of(P::ld(row + q * BC - BE + (BC - 2)));
             G[q] = P::left(prev, cur);
         }
         else
         {
-            typename P::V next = P::down(cur);
-            if (lane == 31) next = P::ld(src + 2);
+            // lane 31 sits at the last pair of a block: its right neighbour
+            // pair is the first pair of the next block
+            auto next = __shfl_down_sync(kFull, P::lo_of(cur), 1);
+            if (lane == 31) next = P::lo_of(P::ld(row + q * BC + BE - (BC - 2)));
             G[q] = P::right(cur, next);
         }
     }
@@ -325,9 +301,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step(const S* __restrict__ fin,
         {
             if (((lk0 | lk1) >> q) & 1u)
             {
-                const float2 own = P::cvt(P::ld(tin + a.pop_off[inv(q)]));
-                if ((lk0 >> q) & 1u) G[q].x = own.x;
-                if ((lk1 >> q) & 1u) G[q].y = own.y;
+                const float2 o = P::cvt(P::ld(own + inv(q) * BC));
+                if ((lk0 >> q) & 1u) G[q].x = o.x;
+                if ((lk1 >> q) & 1u) G[q].y = o.y;
             }
         }
     }
@@ -353,9 +329,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step(const S* __restrict__ fin,
     const float2 sg = make_float2(fmaxf(a.sig_x[c0], syz), fmaxf(c0 + 1 < L.nx ? a.sig_x[c0 + 1] : 0.f, syz));
     collide2(G, inv_scale, a.omega, sg, (lk0 & kSolidSelfBit) != 0u, (lk1 & kSolidSelfBit) != 0u);
 
-    S* tout = fout + cell;
+    S* out = fout + e0;
 #pragma unroll
-    for (int q = 0; q < Q; ++q) P::st(tout + a.pop_off[q], G[q]);
+    for (int q = 0; q < Q; ++q) P::st(out + q * BC, G[q]);
 
     if (xlo | xhi0 | xhi1)
     {
@@ -369,60 +345,164 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step(const S* __restrict__ fin,
     }
 }
 
-// Pair kernel with 32-bit per-thread element offsets: every address is a
-// warp-uniform per-direction base pointer (fin + q * pop_stride, from kernel
-// parameters) plus a 32-bit cell offset, so per-thread address arithmetic
-// stays 32-bit.  The host guarantees pop_stride < 2^31.
-template <typename S, int BLOCK, int MINB>
-__global__ void __launch_bounds__(BLOCK, MINB) k_step32(const S* __restrict__ fin, S* __restrict__ fout, Layout L,
-                                                        StepArgs a, float inv_scale)
+// ---------------------------------------------------------------- FP16 step
+// FP16 storage keeps the 19 directions of a cell pair packed as half2 words
+// through the whole update: the moment pass and the update pass each convert
+// a word to float2 right before use, so no 19 x float2 array is ever live and
+// the kernel needs far fewer registers (more warps, more loads in flight).
+__device__ __forceinline__ float2 h2f(unsigned u) { return PairIo<__half>::cvt(u); }
+__device__ __forceinline__ unsigned f2h(float2 v)
 {
-    using P = PairIo<S>;
+    const __half2 h = __float22half2_rn(v);
+    return *reinterpret_cast<const unsigned*>(&h);
+}
+__device__ __forceinline__ unsigned set_lo(unsigned w, float v)
+{
+    return (w & 0xffff0000u) | (unsigned)__half_as_ushort(__float2half_rn(v));
+}
+__device__ __forceinline__ unsigned set_hi(unsigned w, float v)
+{
+    return (w & 0x0000ffffu) | ((unsigned)__half_as_ushort(__float2half_rn(v)) << 16);
+}
+
+// collide2() on packed words (same formulas, FP32x2 arithmetic).
+__device__ __forceinline__ void collide2_packed(unsigned (&w)[Q], float inv_scale, float omega, float2 sigma,
+                                                bool solid0, bool solid1)
+{
+    float2 rho = h2f(w[0]);
+    float2 jx = f2(0.f), jy = f2(0.f), jz = f2(0.f);
+#pragma unroll
+    for (int q = 1; q < Q; ++q)
+    {
+        const float2 g = h2f(w[q]);
+        rho = add2(rho, g);
+        if (ex(q) > 0) jx = add2(jx, g);
+        if (ex(q) < 0) jx = sub2(jx, g);
+        if (ey(q) > 0) jy = add2(jy, g);
+        if (ey(q) < 0) jy = sub2(jy, g);
+        if (ez(q) > 0) jz = add2(jz, g);
+        if (ez(q) < 0) jz = sub2(jz, g);
+    }
+    float2 r = fma2(rho, f2(inv_scale), f2(1.0f));
+    if (r.x <= 0.f) r.x = 1e-12f;   // 06:948
+    if (r.y <= 0.f) r.y = 1e-12f;
+    const float2 irs = make_float2(__fdividef(inv_scale, r.x), __fdividef(inv_scale, r.y));
+    const float2 j2 = fma2(jz, jz, fma2(jy, jy, mul2(jx, jx)));
+    const float2 base = fma2(mul2(irs, j2), f2(-1.5f), rho);
+    const float2 k45 = mul2(irs, f2(4.5f));
+    const float2 keep = sub2(f2(1.0f), sigma);
+    float2 cA = mul2(keep, f2(1.0f - omega));
+    float2 cB = mul2(keep, f2(omega));
+    if (solid0) cA.x = 1.0f, cB.x = 0.0f;
+    if (solid1) cA.y = 1.0f, cB.y = 0.0f;
+    const float2 cBw1 = mul2(cB, f2(wf(1))), cBw2 = mul2(cB, f2(wf(7)));
+    const float2 cBt1 = mul2(cB, f2(3.0f * wf(1))), cBt2 = mul2(cB, f2(3.0f * wf(7)));
+    w[0] = f2h(fma2(cA, h2f(w[0]), mul2(mul2(cB, f2(wf(0))), base)));
+#pragma unroll
+    for (int p = 0; p < 9; ++p)
+    {
+        const int q = pair_head(p);
+        const int qb = inv(q);
+        float2 cj;
+        if (p == 0) cj = jx;
+        else if (p == 1) cj = jy;
+        else if (p == 2) cj = jz;
+        else if (p == 3) cj = add2(jx, jy);
+        else if (p == 4) cj = sub2(jx, jy);
+        else if (p == 5) cj = add2(jx, jz);
+        else if (p == 6) cj = sub2(jx, jz);
+        else if (p == 7) cj = add2(jy, jz);
+        else cj = sub2(jy, jz);
+        const float2 cBw = q < 7 ? cBw1 : cBw2;
+        const float2 cBt = q < 7 ? cBt1 : cBt2;
+        const float2 e = mul2(cBw, fma2(k45, mul2(cj, cj), base));
+        const float2 o = mul2(cBt, cj);
+        w[q] = f2h(fma2(cA, h2f(w[q]), add2(e, o)));
+        w[qb] = f2h(fma2(cA, h2f(w[qb]), sub2(e, o)));
+    }
+}
+
+// FP16 fused step, CELLS = 2 or 4 x-adjacent cells per thread (one aligned
+// 4- or 8-byte vector per direction).  Same pull / bounce-back / x-face /
+// collision semantics as k_step.
+template <int CELLS, int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) k_step_h(const __half* __restrict__ fin, __half* __restrict__ fout,
+                                                        Layout L, StepArgs a, float inv_scale)
+{
+    constexpr int NW = CELLS / 2;   // half2 words per direction
+    constexpr int BC = block_cells(2);   // cells per interleaved block
+    constexpr int BE = 19 * BC;          // elements per block
     const int lane = threadIdx.x & 31;
-    const int c0r = 2 * (blockIdx.x * BLOCK + threadIdx.x);
+    const int c0r = CELLS * (blockIdx.x * BLOCK + threadIdx.x);
     const bool active = c0r < L.nx;
-    const int c0 = active ? c0r : ((L.nx - 1) & ~1);
+    const int c0 = active ? c0r : ((L.nx - 1) & ~(CELLS - 1));
     const int j = blockIdx.y + 1;
     const int k = blockIdx.z + 1;
-    const uint32_t pitch = (uint32_t)L.pitch, plane = (uint32_t)L.plane;
-    const uint32_t cell = (uint32_t)k * plane + (uint32_t)j * pitch + (uint32_t)c0;
-    const size_t ps = (size_t)L.pop_stride;
-    if (a.prefetch_rows > 0 && threadIdx.x == 0)
-    {
-        const int col0 = 2 * blockIdx.x * BLOCK;
-        prefetch_ahead<S>(fin, L, a, j, k, col0, min(2 * BLOCK, L.nx - col0));
-    }
-    uint32_t lk0 = 0, lk1 = 0;
+    const long long e0 = L.elem(0, c0 + 1, j, k);
+    const __half* own = fin + e0;
+    const long long rs = L.row_stride, ps = L.plane_stride;
+    if (a.prefetch_rows > 0)
+        prefetch_rows_ahead<__half, CELLS * BLOCK>(fin, L, a.prefetch_rows, j, k, CELLS * BLOCK * blockIdx.x);
+
+    uint32_t lk[CELLS];
+#pragma unroll
+    for (int c = 0; c < CELLS; ++c) lk[c] = 0u;
     if (active)
     {
-        const uint32_t b = (near_word(a, L, c0, j, k) >> (c0 & 31)) & 3u;
-        if (b & 1u) lk0 = a.links[cell];
-        if (b & 2u) lk1 = a.links[cell + 1];
+        const uint32_t b = near_bits(a, L, c0, j, k) & ((1u << CELLS) - 1u);
+        if (b)
+        {
+            const long long cl = L.cell(c0 + 1, j, k);
+#pragma unroll
+            for (int c = 0; c < CELLS; ++c)
+                if ((b >> c) & 1u) lk[c] = a.links[cl + c];
+        }
     }
-    const bool any_link = __any_sync(kFull, (lk0 | lk1) != 0u);
+    uint32_t lka = 0u;
+#pragma unroll
+    for (int c = 0; c < CELLS; ++c) lka |= lk[c];
+    const bool any_link = __any_sync(kFull, lka != 0u);
 
-    float2 G[Q];
+    // w[h][q]: cells (c0 + 2h, c0 + 2h + 1) of direction q, already shifted
+    unsigned w[NW][Q];
 #pragma unroll
     for (int q = 0; q < Q; ++q)
     {
-        const S* __restrict__ Pq = fin + q * ps;
-        const uint32_t src = cell - (uint32_t)(ey(q) * (int)pitch + ez(q) * (int)plane);
-        const typename P::V cur = P::ld(Pq + src);
-        if (ex(q) == 0)
+        const __half* row = own - (ey(q) * rs + ez(q) * ps) + q * BC;
+        unsigned cur[NW];
+        if constexpr (NW == 1)
         {
-            G[q] = P::cvt(cur);
-        }
-        else if (ex(q) > 0)
-        {
-            typename P::V prev = P::up(cur);
-            if (lane == 0) prev = P::ld(Pq + (src - 2u));
-            G[q] = P::left(prev, cur);
+            cur[0] = __ldg(reinterpret_cast<const unsigned*>(row));
         }
         else
         {
-            typename P::V next = P::down(cur);
-            if (lane == 31) next = P::ld(Pq + (src + 2u));
-            G[q] = P::right(cur, next);
+            const uint2 v = __ldg(reinterpret_cast<const uint2*>(row));
+            cur[0] = v.x;
+            cur[1] = v.y;
+        }
+        if (ex(q) == 0)
+        {
+#pragma unroll
+            for (int h = 0; h < NW; ++h) w[h][q] = cur[h];
+        }
+        else if (ex(q) > 0)
+        {
+            // lane 0 starts a block: its left neighbour is the previous block's last pair
+            unsigned prev = __shfl_up_sync(kFull, cur[NW - 1], 1);
+            if (lane == 0) prev = __ldg(reinterpret_cast<const unsigned*>(row - BE + (BC - 2)));
+            w[0][q] = __byte_perm(prev, cur[0], 0x5432);
+#pragma unroll
+            for (int h = 1; h < NW; ++h) w[h][q] = __byte_perm(cur[h - 1], cur[h], 0x5432);
+        }
+        else
+        {
+            // lane 31 ends a block: its right neighbour is the next block's first pair
+            unsigned next = __shfl_down_sync(kFull, cur[0], 1);
+            if (lane == 31)
+                next = __ldg(reinterpret_cast<const unsigned*>(row + BE - (BC - CELLS)));
+#pragma unroll
+            for (int h = 0; h < NW - 1; ++h) w[h][q] = __byte_perm(cur[h], cur[h + 1], 0x5432);
+            w[NW - 1][q] = __byte_perm(cur[NW - 1], next, 0x5432);
         }
     }
     if (any_link)
@@ -430,381 +510,71 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step32(const S* __restrict__ fi
 #pragma unroll
         for (int q = 0; q < Q; ++q)
         {
-            if (((lk0 | lk1) >> q) & 1u)
+            if ((lka >> q) & 1u)
             {
-                const float2 own = P::cvt(P::ld(fin + inv(q) * ps + cell));
-                if ((lk0 >> q) & 1u) G[q].x = own.x;
-                if ((lk1 >> q) & 1u) G[q].y = own.y;
+#pragma unroll
+                for (int h = 0; h < NW; ++h)
+                {
+                    const unsigned o = __ldg(reinterpret_cast<const unsigned*>(own + inv(q) * BC + 2 * h));
+                    const unsigned m = (((lk[2 * h] >> q) & 1u) ? 0x0000ffffu : 0u) |
+                                       (((lk[2 * h + 1] >> q) & 1u) ? 0xffff0000u : 0u);
+                    w[h][q] = (w[h][q] & ~m) | (o & m);
+                }
             }
         }
     }
-    const bool xlo = active && c0 == 0;
-    const bool xhi0 = active && c0 == L.nx - 1;
-    const bool xhi1 = active && c0 + 1 == L.nx - 1;
-    if (xlo | xhi0 | xhi1)
+    if (!active) return;
+
+    // x faces: sources in the x halo come from the x-face ghosts.
+    const int last = L.nx - 1 - c0;   // position of cell nx-1 in this group when in 0..CELLS-1
+    const bool xlo = c0 == 0;
+    const bool xhi = last >= 0 && last < CELLS;
+    if (xlo | xhi)
     {
 #pragma unroll
         for (int q = 0; q < Q; ++q)
         {
             if (ex(q) == 0) continue;
             const float g = a.xf.xgh[a.xf.gh_index(ex(q) > 0 ? 0 : 1, q, j - ey(q), k - ez(q), L.ny, L.nz)];
-            if (ex(q) > 0 && xlo && !((lk0 >> q) & 1u)) G[q].x = g;
-            if (ex(q) < 0 && xhi0 && !((lk0 >> q) & 1u)) G[q].x = g;
-            if (ex(q) < 0 && xhi1 && !((lk1 >> q) & 1u)) G[q].y = g;
+            if (ex(q) > 0 && xlo && !((lk[0] >> q) & 1u)) w[0][q] = set_lo(w[0][q], g);
+#pragma unroll
+            for (int h = 0; h < NW; ++h)
+            {
+                if (ex(q) < 0 && xhi && last == 2 * h && !((lk[2 * h] >> q) & 1u)) w[h][q] = set_lo(w[h][q], g);
+                if (ex(q) < 0 && xhi && last == 2 * h + 1 && !((lk[2 * h + 1] >> q) & 1u))
+                    w[h][q] = set_hi(w[h][q], g);
+            }
         }
     }
-    if (!active) return;
 
     const float syz = fmaxf(a.sig_y[j - 1], a.sig_z[k - 1]);
-    const float2 sg = make_float2(fmaxf(a.sig_x[c0], syz), fmaxf(c0 + 1 < L.nx ? a.sig_x[c0 + 1] : 0.f, syz));
-    collide2(G, inv_scale, a.omega, sg, (lk0 & kSolidSelfBit) != 0u, (lk1 & kSolidSelfBit) != 0u);
 #pragma unroll
-    for (int q = 0; q < Q; ++q) P::st(fout + q * ps + cell, G[q]);
-    if (xlo | xhi0 | xhi1)
+    for (int h = 0; h < NW; ++h)
     {
-#pragma unroll
-        for (int q = 0; q < Q; ++q)
-        {
-            if (xlo) a.xf.xexp[a.xf.exp_index(0, q, j, k, L.ny, L.nz)] = P::rnd(G[q].x);
-            if (xhi0) a.xf.xexp[a.xf.exp_index(1, q, j, k, L.ny, L.nz)] = P::rnd(G[q].x);
-            if (xhi1) a.xf.xexp[a.xf.exp_index(1, q, j, k, L.ny, L.nz)] = P::rnd(G[q].y);
-        }
+        const int ca = c0 + 2 * h;
+        const float2 sg = make_float2(fmaxf(ca < L.nx ? a.sig_x[ca] : 0.f, syz),
+                                      fmaxf(ca + 1 < L.nx ? a.sig_x[ca + 1] : 0.f, syz));
+        collide2_packed(w[h], inv_scale, a.omega, sg, (lk[2 * h] & kSolidSelfBit) != 0u,
+                        (lk[2 * h + 1] & kSolidSelfBit) != 0u);
     }
-}
-
-// Four x-adjacent cells per thread, FP16 storage: every direction is one
-// aligned 8-byte vector (two half2 words) per thread, so each thread keeps
-// twice the bytes in flight of the pair kernel for about the same register
-// budget.  The two pairs are collided one after the other (packed FP32x2).
-__device__ __forceinline__ uint2 ld_quad(const __half* p) { return __ldg(reinterpret_cast<const uint2*>(p)); }
-
-template <int BLOCK, int MINB>
-__global__ void __launch_bounds__(BLOCK, MINB) k_step_quad(const __half* __restrict__ fin, __half* __restrict__ fout,
-                                                           Layout L, StepArgs a, float inv_scale)
-{
-    using P = PairIo<__half>;
-    const int lane = threadIdx.x & 31;
-    const int c0r = 4 * (blockIdx.x * BLOCK + threadIdx.x);
-    const bool active = c0r < L.nx;
-    const int c0 = active ? c0r : ((L.nx - 1) & ~3);
-    const int j = blockIdx.y + 1;
-    const int k = blockIdx.z + 1;
-    const long long cell = (long long)k * L.plane + (long long)j * L.pitch + c0;
-    const __half* tin = fin + cell;
-    if (a.prefetch_rows > 0 && threadIdx.x == 0)
-    {
-        const int col0 = 4 * blockIdx.x * BLOCK;
-        prefetch_ahead<__half>(fin, L, a, j, k, col0, min(4 * BLOCK, L.nx - col0));
-    }
-    uint32_t lk[4] = {0, 0, 0, 0};
-    if (active)
-    {
-        const uint32_t b = (near_word(a, L, c0, j, k) >> (c0 & 31)) & 15u;
-#pragma unroll
-        for (int c = 0; c < 4; ++c)
-            if ((b >> c) & 1u) lk[c] = a.links[cell + c];
-    }
-    const bool any_link = __any_sync(kFull, (lk[0] | lk[1] | lk[2] | lk[3]) != 0u);
-
-    // words: w[q].x = cells (c0, c0+1), w[q].y = cells (c0+2, c0+3), shifted per direction
-    uint2 w[Q];
+    __half* out = fout + e0;
 #pragma unroll
     for (int q = 0; q < Q; ++q)
     {
-        const __half* src = tin + a.pull_off[q];
-        const uint2 cur = ld_quad(src);
-        if (ex(q) == 0)
-        {
-            w[q] = cur;
-        }
-        else if (ex(q) > 0)
-        {
-            unsigned prev = __shfl_up_sync(kFull, cur.y, 1);   // cells (c0-2, c0-1)
-            if (lane == 0) prev = ld_quad(src - 4).y;
-            w[q] = make_uint2(__byte_perm(prev, cur.x, 0x5432), __byte_perm(cur.x, cur.y, 0x5432));
-        }
-        else
-        {
-            unsigned next = __shfl_down_sync(kFull, cur.x, 1);   // cells (c0+4, c0+5)
-            if (lane == 31) next = ld_quad(src + 4).x;
-            w[q] = make_uint2(__byte_perm(cur.x, cur.y, 0x5432), __byte_perm(cur.y, next, 0x5432));
-        }
+        if constexpr (NW == 1) *reinterpret_cast<unsigned*>(out + q * BC) = w[0][q];
+        else *reinterpret_cast<uint2*>(out + q * BC) = make_uint2(w[0][q], w[1][q]);
     }
-    if (any_link)
+    if (xlo | xhi)
     {
-        const uint32_t la = lk[0] | lk[1] | lk[2] | lk[3];
 #pragma unroll
         for (int q = 0; q < Q; ++q)
         {
-            if ((la >> q) & 1u)
+            if (xlo) a.xf.xexp[a.xf.exp_index(0, q, j, k, L.ny, L.nz)] = h2f(w[0][q]).x;
+#pragma unroll
+            for (int h = 0; h < NW; ++h)
             {
-                const uint2 own = ld_quad(tin + a.pop_off[inv(q)]);
-                // halfword select: cell c takes `own` when its link bit q is set
-                const unsigned m0 = (((lk[0] >> q) & 1u) ? 0x0000ffffu : 0u) | (((lk[1] >> q) & 1u) ? 0xffff0000u : 0u);
-                const unsigned m1 = (((lk[2] >> q) & 1u) ? 0x0000ffffu : 0u) | (((lk[3] >> q) & 1u) ? 0xffff0000u : 0u);
-                w[q].x = (w[q].x & ~m0) | (own.x & m0);
-                w[q].y = (w[q].y & ~m1) | (own.y & m1);
-            }
-        }
-    }
-    // x faces (ghost values are float; patched after conversion below)
-    const int last = L.nx - 1 - c0;   // position of cell nx-1 in this quad when 0..3
-    const bool xlo = active && c0 == 0;
-    const bool xhi = active && last >= 0 && last < 4;
-    if (!active) return;
-
-    const float syz = fmaxf(a.sig_y[j - 1], a.sig_z[k - 1]);
-    __half* tout = fout + cell;
-#pragma unroll
-    for (int h = 0; h < 2; ++h)
-    {
-        float2 G[Q];
-#pragma unroll
-        for (int q = 0; q < Q; ++q) G[q] = P::cvt(h == 0 ? w[q].x : w[q].y);
-        const int ca = c0 + 2 * h;
-        if (xlo | xhi)
-        {
-#pragma unroll
-            for (int q = 0; q < Q; ++q)
-            {
-                if (ex(q) == 0) continue;
-                const float g = a.xf.xgh[a.xf.gh_index(ex(q) > 0 ? 0 : 1, q, j - ey(q), k - ez(q), L.ny, L.nz)];
-                if (ex(q) > 0 && xlo && h == 0 && !((lk[0] >> q) & 1u)) G[q].x = g;
-                if (ex(q) < 0 && xhi && last == 2 * h && !((lk[2 * h] >> q) & 1u)) G[q].x = g;
-                if (ex(q) < 0 && xhi && last == 2 * h + 1 && !((lk[2 * h + 1] >> q) & 1u)) G[q].y = g;
-            }
-        }
-        const float2 sg = make_float2(fmaxf(ca < L.nx ? a.sig_x[ca] : 0.f, syz),
-                                      fmaxf(ca + 1 < L.nx ? a.sig_x[ca + 1] : 0.f, syz));
-        collide2(G, inv_scale, a.omega, sg, (lk[2 * h] & kSolidSelfBit) != 0u, (lk[2 * h + 1] & kSolidSelfBit) != 0u);
-#pragma unroll
-        for (int q = 0; q < Q; ++q) P::st(tout + a.pop_off[q] + 2 * h, G[q]);
-        if (xlo | xhi)
-        {
-#pragma unroll
-            for (int q = 0; q < Q; ++q)
-            {
-                if (xlo && h == 0) a.xf.xexp[a.xf.exp_index(0, q, j, k, L.ny, L.nz)] = P::rnd(G[q].x);
-                if (xhi && last == 2 * h) a.xf.xexp[a.xf.exp_index(1, q, j, k, L.ny, L.nz)] = P::rnd(G[q].x);
-                if (xhi && last == 2 * h + 1) a.xf.xexp[a.xf.exp_index(1, q, j, k, L.ny, L.nz)] = P::rnd(G[q].y);
-            }
-        }
-    }
-}
-
-// ---------------------------------------------------------------- staged step
-// Bulk asynchronous copies (cp.async.bulk, completion counted on an mbarrier)
-// stage, for every direction q, the source row segment of a tile in shared
-// memory; a persistent CTA keeps NS tiles in flight while it collides the
-// oldest one.  Memory-level parallelism no longer depends on registers.
-__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-                 : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
-{
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0u;
-}
-// Waits for phase `parity` of the barrier, giving up after `limit` polls.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int limit)
-{
-    for (int n = 0; n < limit; ++n)
-        if (mbar_try_wait(bar, parity)) return true;
-    return false;
-}
-__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
-{
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                     smem_u32(dst)),
-                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
-                 : "memory");
-}
-__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-__device__ __forceinline__ void fence_mbarrier_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
-
-// Reads of a staged row (p points at the element of the pair's first cell).
-template <typename S>
-struct Staged;
-
-template <>
-struct Staged<float>
-{
-    static __device__ __forceinline__ float2 pair(const float* p) { return *reinterpret_cast<const float2*>(p); }
-    static __device__ __forceinline__ float2 left(const float* p) { return make_float2(p[-1], p[0]); }
-    static __device__ __forceinline__ float2 right(const float* p) { return make_float2(p[1], p[2]); }
-};
-
-template <>
-struct Staged<__half>
-{
-    static __device__ __forceinline__ unsigned word(const __half* p) { return *reinterpret_cast<const unsigned*>(p); }
-    static __device__ __forceinline__ float2 pair(const __half* p) { return PairIo<__half>::cvt(word(p)); }
-    static __device__ __forceinline__ float2 left(const __half* p)
-    {
-        return PairIo<__half>::cvt(__byte_perm(word(p - 2), word(p), 0x5432));
-    }
-    static __device__ __forceinline__ float2 right(const __half* p)
-    {
-        return PairIo<__half>::cvt(__byte_perm(word(p), word(p + 2), 0x5432));
-    }
-};
-
-constexpr int kStageWaitLimit = 1 << 22;   // mbarrier polls before a stage wait gives up
-
-template <typename S, int TW, int NS>
-__global__ void __launch_bounds__(TW / 2) k_step_staged(const S* __restrict__ fin, S* __restrict__ fout, Layout L,
-                                                       StepArgs a, float inv_scale, int tiles_per_row,
-                                                       long long ntiles)
-{
-    using P = PairIo<S>;
-    using T = Staged<S>;
-    constexpr int PADE = 16 / (int)sizeof(S);   // 16-byte alignment margin on both sides of a row
-    constexpr int ROW = TW + 2 * PADE;          // staged elements per direction
-    constexpr uint32_t ROW_BYTES = ROW * sizeof(S);
-    constexpr uint32_t STAGE_BYTES = Q * ROW_BYTES;
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    S* const stages = reinterpret_cast<S*>(smem_raw);
-    __shared__ __align__(8) uint64_t full[NS];
-
-    const int tid = threadIdx.x;
-    if (tid == 0)
-    {
-        for (int s = 0; s < NS; ++s) mbar_init(&full[s], 1);
-        fence_mbarrier_init();
-    }
-    __syncthreads();
-
-    // One elected thread stages all 19 source rows of a tile.
-    auto issue = [&](int s, long long tile) {
-        const long long r = tile / tiles_per_row;
-        const int seg = (int)(tile - r * tiles_per_row);
-        const int j = 1 + (int)(r % L.ny), k = 1 + (int)(r / L.ny);
-        const long long cell0 = (long long)k * L.plane + (long long)j * L.pitch + (long long)seg * TW;
-        S* dst = stages + (size_t)s * Q * ROW;
-        mbar_expect_tx(&full[s], STAGE_BYTES);
-#pragma unroll
-        for (int q = 0; q < Q; ++q) bulk_copy_g2s(dst + q * ROW, fin + cell0 + a.pull_off[q] - PADE, ROW_BYTES, &full[s]);
-    };
-    if (tid == 0)
-        for (int s = 0; s < NS; ++s)
-        {
-            const long long t = blockIdx.x + (long long)s * gridDim.x;
-            if (t < ntiles) issue(s, t);
-        }
-
-    int it = 0;
-    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it)
-    {
-        const int s = it % NS;
-        const uint32_t parity = (uint32_t)(it / NS) & 1u;
-        const bool ok = mbar_wait_bounded(&full[s], parity, kStageWaitLimit);
-
-        const long long r = tile / tiles_per_row;
-        const int seg = (int)(tile - r * tiles_per_row);
-        const int j = 1 + (int)(r % L.ny), k = 1 + (int)(r / L.ny);
-        const int c0 = seg * TW + 2 * tid;
-        const bool active = ok && c0 < L.nx;
-        if (active)
-        {
-            const long long cell = (long long)k * L.plane + (long long)j * L.pitch + c0;
-            uint32_t lk0 = 0, lk1 = 0;
-            const uint32_t b = (near_word(a, L, c0, j, k) >> (c0 & 31)) & 3u;
-            if (b & 1u) lk0 = a.links[cell];
-            if (b & 2u) lk1 = a.links[cell + 1];
-            const S* sp = stages + (size_t)s * Q * ROW + PADE + 2 * tid;
-            float2 G[Q];
-#pragma unroll
-            for (int q = 0; q < Q; ++q)
-            {
-                if (ex(q) == 0) G[q] = T::pair(sp + q * ROW);
-                else if (ex(q) > 0) G[q] = T::left(sp + q * ROW);
-                else G[q] = T::right(sp + q * ROW);
-            }
-            const S* tin = fin + cell;
-            if (lk0 | lk1)
-            {
-#pragma unroll
-                for (int q = 0; q < Q; ++q)
-                {
-                    if (((lk0 | lk1) >> q) & 1u)
-                    {
-                        const float2 own = P::cvt(P::ld(tin + a.pop_off[inv(q)]));
-                        if ((lk0 >> q) & 1u) G[q].x = own.x;
-                        if ((lk1 >> q) & 1u) G[q].y = own.y;
-                    }
-                }
-            }
-            const bool xlo = c0 == 0;
-            const bool xhi0 = c0 == L.nx - 1;
-            const bool xhi1 = c0 + 1 == L.nx - 1;
-            if (xlo | xhi0 | xhi1)
-            {
-#pragma unroll
-                for (int q = 0; q < Q; ++q)
-                {
-                    if (ex(q) == 0) continue;
-                    const float g = a.xf.xgh[a.xf.gh_index(ex(q) > 0 ? 0 : 1, q, j - ey(q), k - ez(q), L.ny, L.nz)];
-                    if (ex(q) > 0 && xlo && !((lk0 >> q) & 1u)) G[q].x = g;
-                    if (ex(q) < 0 && xhi0 && !((lk0 >> q) & 1u)) G[q].x = g;
-                    if (ex(q) < 0 && xhi1 && !((lk1 >> q) & 1u)) G[q].y = g;
-                }
-            }
-            const float syz = fmaxf(a.sig_y[j - 1], a.sig_z[k - 1]);
-            const float2 sg =
-                make_float2(fmaxf(a.sig_x[c0], syz), fmaxf(c0 + 1 < L.nx ? a.sig_x[c0 + 1] : 0.f, syz));
-            collide2(G, inv_scale, a.omega, sg, (lk0 & kSolidSelfBit) != 0u, (lk1 & kSolidSelfBit) != 0u);
-            S* tout = fout + cell;
-#pragma unroll
-            for (int q = 0; q < Q; ++q) P::st(tout + a.pop_off[q], G[q]);
-            if (xlo | xhi0 | xhi1)
-            {
-#pragma unroll
-                for (int q = 0; q < Q; ++q)
-                {
-                    if (xlo) a.xf.xexp[a.xf.exp_index(0, q, j, k, L.ny, L.nz)] = P::rnd(G[q].x);
-                    if (xhi0) a.xf.xexp[a.xf.exp_index(1, q, j, k, L.ny, L.nz)] = P::rnd(G[q].x);
-                    if (xhi1) a.xf.xexp[a.xf.exp_index(1, q, j, k, L.ny, L.nz)] = P::rnd(G[q].y);
-                }
-            }
-        }
-        // every thread is done with stage s (and agrees on whether the wait failed)
-        const int failed = __syncthreads_or(!ok);
-        if (failed)
-        {
-            if (tid == 0)
-            {
-                atomicExch(a.error, kErrStageTimeout);
-                // let the copies already in flight land before the CTA exits
-                for (int d = 0; d < NS; ++d)
-                {
-                    const long long t = tile + (long long)d * gridDim.x;
-                    if (t < ntiles) mbar_wait_bounded(&full[(it + d) % NS], (uint32_t)((it + d) / NS) & 1u, kStageWaitLimit);
-                }
-            }
-            return;
-        }
-        if (tid == 0)
-        {
-            const long long next = tile + (long long)NS * gridDim.x;
-            if (next < ntiles)
-            {
-                fence_proxy_async_smem();   // generic-proxy reads of stage s before the async-proxy refill
-                issue(s, next);
+                if (xhi && last == 2 * h) a.xf.xexp[a.xf.exp_index(1, q, j, k, L.ny, L.nz)] = h2f(w[h][q]).x;
+                if (xhi && last == 2 * h + 1) a.xf.xexp[a.xf.exp_index(1, q, j, k, L.ny, L.nz)] = h2f(w[h][q]).y;
             }
         }
     }
@@ -834,7 +604,7 @@ __global__ void __launch_bounds__(128) k_build_links(const uint8_t* __restrict__
             if (m[src]) lk |= 1u << q;
         }
         if (m[(long long)i + (long long)j * nxt + (long long)k * nxt * nyt]) lk |= kSolidSelfBit;
-        links[(long long)k * L.plane + (long long)j * L.pitch + i0] = lk;
+        links[L.cell(i, j, k)] = lk;
     }
     const uint32_t ball = __ballot_sync(kFull, active && lk != 0u);
     if ((threadIdx.x & 31) == 0 && i0 < L.pitch)
@@ -919,13 +689,9 @@ __global__ void __launch_bounds__(512) k_source(S* __restrict__ f, Layout L, Ste
                 in = true;
             }
         }
-        long long cell = 0;
         bool fluid = false;
         if (in && gi >= 0 && gi < L.nx && gj >= 0 && gj < L.ny && gk >= 0 && gk < L.nz)
-        {
-            cell = (long long)(gk + 1) * L.plane + (long long)(gj + 1) * L.pitch + gi;
-            fluid = (sa.links[cell] & kSolidSelfBit) == 0u;
-        }
+            fluid = (sa.links[L.cell(gi + 1, gj + 1, gk + 1)] & kSolidSelfBit) == 0u;
         const double sum = block_sum(fluid ? ww : 0.0, red);
         if (sum < 1e-30) continue;
         const double A = e.mass / sum;
@@ -935,7 +701,7 @@ __global__ void __launch_bounds__(512) k_source(S* __restrict__ f, Layout L, Ste
 #pragma unroll
             for (int q = 0; q < Q; ++q)
             {
-                S* p = f + (long long)q * L.pop_stride + cell;
+                S* p = f + L.elem(q, gi + 1, gj + 1, gk + 1);
                 Io<S>::st(p, Io<S>::ldw(p) + (float)(wd(q) * add));
                 if (gi == 0 || gi == L.nx - 1)
                 {
@@ -1044,13 +810,14 @@ __global__ void __launch_bounds__(128) k_ghost(S* __restrict__ f, Layout L, Ghos
         ck = F.side ? L.nz : 1;
         gk = F.side ? L.nz + 1 : 0;
     }
-    const long long cI = (long long)ck * L.plane + (long long)cj * L.pitch + (ci - 1);
-    const long long cB = (long long)gk * L.plane + (long long)gj * L.pitch + (ci - 1);
+    constexpr int BC = block_cells(sizeof(S));
+    const S* I = f + L.elem(0, ci, cj, ck);
+    S* B = f + L.elem(0, ci, gj, gk);
 #pragma unroll
-    for (int q = 0; q < Q; ++q) G[q] = Io<S>::ld(f + (long long)q * L.pop_stride + cI);
+    for (int q = 0; q < Q; ++q) G[q] = Io<S>::ld(I + q * BC);
     nscbc(G, F.axis, F.side, inv_scale);
 #pragma unroll
-    for (int q = 0; q < Q; ++q) Io<S>::st(f + (long long)q * L.pop_stride + cB, G[q]);
+    for (int q = 0; q < Q; ++q) Io<S>::st(B + q * BC, G[q]);
 }
 
 // ---------------------------------------------------------------- probes
@@ -1063,18 +830,14 @@ __global__ void __launch_bounds__(256) k_probe(const S* __restrict__ f, Layout L
     const float inv_scale = 1.0f / a.scale;
     for (int p = threadIdx.x; p < a.n; p += blockDim.x)
     {
-        const long long c = a.cell[p];
+        const int i = a.ijk[3 * p], j = a.ijk[3 * p + 1], k = a.ijk[3 * p + 2];
         double val;
-        if (c < 0)
+        if (i < 0)
         {
             val = __longlong_as_double(0x7ff8000000000000LL);
         }
         else
         {
-            const int k = (int)(c / L.plane);
-            const long long rem = c - (long long)k * L.plane;
-            const int j = (int)(rem / L.pitch);
-            const int i = (int)(rem - (long long)j * L.pitch) + 1;
             bool solid;
             float G[Q];
             pull_cell<S>(f, L, sa, i, j, k, G, solid);
@@ -1123,14 +886,13 @@ __global__ void k_export_f(const S* __restrict__ f, double* __restrict__ out, La
         const int i = (int)(idx % nxt);
         const int j = (int)((idx / nxt) % nyt);
         const int k = (int)(idx / (nxt * nyt));
-        const long long c = (long long)k * L.plane + (long long)j * L.pitch + (i - 1);
 #pragma unroll
         for (int q = 0; q < Q; ++q)
         {
             float g;
             if (i == 0) g = xf.xgh[xf.gh_index(0, q, j, k, L.ny, L.nz)];
             else if (i == L.nx + 1) g = xf.xgh[xf.gh_index(1, q, j, k, L.ny, L.nz)];
-            else g = Io<S>::ld(f + (long long)q * L.pop_stride + c);
+            else g = Io<S>::ld(f + L.elem(q, i, j, k));
             out[idx * Q + q] = wd(q) + (double)g * (double)inv_scale;
         }
     }
@@ -1146,7 +908,6 @@ __global__ void k_import_f(S* __restrict__ f, const double* __restrict__ in, Lay
         const int i = (int)(idx % nxt);
         const int j = (int)((idx / nxt) % nyt);
         const int k = (int)(idx / (nxt * nyt));
-        const long long c = (long long)k * L.plane + (long long)j * L.pitch + (i - 1);
         const bool inner = j >= 1 && j <= L.ny && k >= 1 && k <= L.nz;
 #pragma unroll
         for (int q = 0; q < Q; ++q)
@@ -1162,7 +923,7 @@ __global__ void k_import_f(S* __restrict__ f, const double* __restrict__ in, Lay
                 xf.xgh[xf.gh_index(1, q, j, k, L.ny, L.nz)] = g;
                 continue;
             }
-            S* p = f + (long long)q * L.pop_stride + c;
+            S* p = f + L.elem(q, i, j, k);
             Io<S>::st(p, g);
             const float gs = Io<S>::ldw(p);   // the stored (rounded) value
             if (inner && i == 1) xf.xexp[xf.exp_index(0, q, j, k, L.ny, L.nz)] = gs;
@@ -1177,71 +938,25 @@ dim3 pair_grid(const Layout& L, int block)
     return dim3((unsigned)(((L.nx + 1) / 2 + block - 1) / block), (unsigned)L.ny, (unsigned)L.nz);
 }
 
-template <typename S, int TW, int NS>
-constexpr size_t staged_smem()
+dim3 grid_n(const Layout& L, int cells, int block)
 {
-    return (size_t)NS * Q * (TW + 2 * (16 / sizeof(S))) * sizeof(S);
-}
-
-template <typename S, int TW, int NS>
-cudaError_t launch_staged(const S* fin, S* fout, const Layout& L, const StepArgs& a, float inv_scale, int grid,
-                          cudaStream_t stream)
-{
-    const int tpr = (L.nx + TW - 1) / TW;
-    const long long ntiles = (long long)tpr * L.ny * L.nz;
-    const int g = (int)std::min<long long>(grid, ntiles);
-    k_step_staged<S, TW, NS><<<g, TW / 2, staged_smem<S, TW, NS>(), stream>>>(fin, fout, L, a, inv_scale, tpr, ntiles);
-    return cudaGetLastError();
-}
-
-template <typename S, int TW, int NS>
-cudaError_t prepare_staged(int device, int* grid)
-{
-    const size_t smem = staged_smem<S, TW, NS>();
-    cudaError_t e = cudaFuncSetAttribute(k_step_staged<S, TW, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
-    if (e != cudaSuccess) return e;
-    int per_sm = 0, sms = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_staged<S, TW, NS>, TW / 2, smem);
-    if (e != cudaSuccess) return e;
-    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    if (e != cudaSuccess) return e;
-    *grid = std::max(1, per_sm) * sms;
-    return cudaSuccess;
+    return dim3((unsigned)(((L.nx + cells - 1) / cells + block - 1) / block), (unsigned)L.ny, (unsigned)L.nz);
 }
 
 template <typename S>
 cudaError_t launch_step_t(const S* fin, S* fout, const Layout& L, const StepArgs& a, float inv_scale, int variant,
-                          int grid, cudaStream_t stream)
+                          cudaStream_t stream)
 {
-    switch (variant)
+    if constexpr (std::is_same<S, __half>::value)
     {
-    case 4: return launch_staged<S, 256, 3>(fin, fout, L, a, inv_scale, grid, stream);
-    case 5: return launch_staged<S, 256, 2>(fin, fout, L, a, inv_scale, grid, stream);
-    case 6: return launch_staged<S, 128, 4>(fin, fout, L, a, inv_scale, grid, stream);
-    case 7: return launch_staged<S, 512, 2>(fin, fout, L, a, inv_scale, grid, stream);
-    case 8:
-        if constexpr (std::is_same<S, __half>::value)
+        switch (variant)
         {
-            const dim3 g((unsigned)(((L.nx + 3) / 4 + 127) / 128), (unsigned)L.ny, (unsigned)L.nz);
-            k_step_quad<128, 0><<<g, 128, 0, stream>>>(fin, fout, L, a, inv_scale);
-            return cudaGetLastError();
+        case 4: k_step_h<2, 128, 8><<<grid_n(L, 2, 128), 128, 0, stream>>>(fin, fout, L, a, inv_scale); return cudaGetLastError();
+        case 5: k_step_h<4, 128, 6><<<grid_n(L, 4, 128), 128, 0, stream>>>(fin, fout, L, a, inv_scale); return cudaGetLastError();
+        case 6: k_step_h<2, 128, 10><<<grid_n(L, 2, 128), 128, 0, stream>>>(fin, fout, L, a, inv_scale); return cudaGetLastError();
+        case 7: k_step_h<4, 128, 5><<<grid_n(L, 4, 128), 128, 0, stream>>>(fin, fout, L, a, inv_scale); return cudaGetLastError();
+        default: break;
         }
-        variant = 3;
-        break;
-    case 10: k_step32<S, 128, 0><<<pair_grid(L, 128), 128, 0, stream>>>(fin, fout, L, a, inv_scale); return cudaGetLastError();
-    case 11: k_step32<S, 128, 8><<<pair_grid(L, 128), 128, 0, stream>>>(fin, fout, L, a, inv_scale); return cudaGetLastError();
-    case 12: k_step32<S, 64, 0><<<pair_grid(L, 64), 64, 0, stream>>>(fin, fout, L, a, inv_scale); return cudaGetLastError();
-    case 9:
-        if constexpr (std::is_same<S, __half>::value)
-        {
-            const dim3 g((unsigned)(((L.nx + 3) / 4 + 127) / 128), (unsigned)L.ny, (unsigned)L.nz);
-            k_step_quad<128, 6><<<g, 128, 0, stream>>>(fin, fout, L, a, inv_scale);
-            return cudaGetLastError();
-        }
-        variant = 3;
-        break;
-    default: break;
     }
     switch (variant)
     {
@@ -1263,25 +978,10 @@ cudaError_t launch_build_links(const uint8_t* mask_ref, uint32_t* links, uint32_
 }
 
 cudaError_t launch_step(int storage, const void* fin, void* fout, const Layout& L, const StepArgs& a,
-                        float scale, int variant, int grid, cudaStream_t stream)
+                        float scale, int variant, cudaStream_t stream)
 {
-    if (storage == 0)
-        return launch_step_t<float>((const float*)fin, (float*)fout, L, a, 1.0f, variant, grid, stream);
-    return launch_step_t<__half>((const __half*)fin, (__half*)fout, L, a, 1.0f / scale, variant, grid, stream);
-}
-
-cudaError_t prepare_step(int storage, int variant, int device, int* grid)
-{
-    *grid = 0;
-    const bool h = storage != 0;
-    switch (variant)
-    {
-    case 4: return h ? prepare_staged<__half, 256, 3>(device, grid) : prepare_staged<float, 256, 3>(device, grid);
-    case 5: return h ? prepare_staged<__half, 256, 2>(device, grid) : prepare_staged<float, 256, 2>(device, grid);
-    case 6: return h ? prepare_staged<__half, 128, 4>(device, grid) : prepare_staged<float, 128, 4>(device, grid);
-    case 7: return h ? prepare_staged<__half, 512, 2>(device, grid) : prepare_staged<float, 512, 2>(device, grid);
-    default: return cudaSuccess;
-    }
+    if (storage == 0) return launch_step_t<float>((const float*)fin, (float*)fout, L, a, 1.0f, variant, stream);
+    return launch_step_t<__half>((const __half*)fin, (__half*)fout, L, a, 1.0f / scale, variant, stream);
 }
 
 cudaError_t launch_source(int storage, void* f, const Layout& L, const StepArgs& sa, const SourceArgs& a,

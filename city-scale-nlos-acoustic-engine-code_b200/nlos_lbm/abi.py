@@ -26,7 +26,6 @@ LBM_ERR_CAPACITY = -7
 LBM_ERR_NO_DEVICE = -8
 LBM_ERR_IO = -9
 LBM_ERR_UNSUPPORTED = -10
-LBM_ERR_TIMEOUT = -11
 
 LBM_BC_NSCBC, LBM_BC_REST, LBM_BC_WALL = 0, 1, 2
 FACE_XLO, FACE_XHI, FACE_YLO, FACE_YHI, FACE_ZLO, FACE_ZHI = range(6)

@@ -45,8 +45,7 @@ typedef enum lbm_status
     LBM_ERR_CAPACITY = -7,         /* caller's output buffer too small */
     LBM_ERR_NO_DEVICE = -8,
     LBM_ERR_IO = -9,
-    LBM_ERR_UNSUPPORTED = -10,
-    LBM_ERR_TIMEOUT = -11          /* a bounded wait inside a kernel gave up */
+    LBM_ERR_UNSUPPORTED = -10
 } lbm_status;
 
 /* Boundary treatment of one face of the box. */
