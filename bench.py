@@ -31,6 +31,9 @@ sys.path.insert(0, os.path.join(REPO, "city-scale-nlos-acoustic-engine-code_b200
 sys.path.insert(0, REPO)
 
 METRIC = "D3Q19 GLUPS, %HBM peak: FP16-store vs FP32 @<=1e-3 probe L2; adjoint grad/s"
+# bytes of DRAM traffic per cell update of the fused step kernel, from ncu
+# captures (2.563e9 B and 5.132e9 B for 33.55e6 cells)
+NCU_TRAFFIC_PER_CELL = {"fp16": 2.563e9 / 33554432, "fp32": 5.132e9 / 33554432}
 UNIT = "GLUPS"
 
 
@@ -305,11 +308,12 @@ def run_our_arm(args):
     cells, steps = head["cells"], head["steps"]
     value = n * cells * steps / (head["ms"] / 1e3) / 1e9
     achieved = cells * head["bytes_per_cell"] / (head["kernel_ms_avg"] / 1e3) / 1e9
-    traffic = None
-    tpath = os.path.join(REPO, "profiles", "traffic.json")
-    if os.path.exists(tpath):
-        with open(tpath) as fh:
-            traffic = json.load(fh).get(f"{headline}_{head['storage']}")
+    # DRAM bytes per cell update measured by ncu (dram__bytes_read.sum +
+    # dram__bytes_write.sum) on one launch of the fused step on the
+    # 512x512x128 city; traffic grows with the cell count, so one launch here
+    # moves cells times that.
+    per_cell = NCU_TRAFFIC_PER_CELL.get(head["storage"])
+    traffic = None if per_cell is None else per_cell * cells
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": n, "steps": steps, "warmup": args.warmup,
         "ms_per_step": head["ms"] / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
