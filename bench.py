@@ -108,6 +108,30 @@ def dist_env():
 
 # ---------------------------------------------------------------------------- our arm
 
+def make_reducers(dist, device):
+    """barrier() and reduce_max(x) over the ranks (identity without a process group)."""
+    import torch
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def reduce_max(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    return barrier, reduce_max
+
+
+def replica_glups(world, cells, steps, ms_max):
+    """Whole-job rate of `world` independent replicas: every rank updates
+    cells x steps; the job takes as long as the slowest rank."""
+    return world * cells * steps / (ms_max / 1e3) / 1e9
+
+
 def make_solver(name, storage, device):
     import nlos_lbm
     from nlos_lbm import workloads
@@ -268,16 +292,7 @@ def run_our_arm(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
 
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-
-    def reduce_max(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    barrier, reduce_max = make_reducers(dist, "cuda")
 
     hbm_peak, peak_kind = measured_peaks()
     headline = args.workload
@@ -306,7 +321,7 @@ def run_our_arm(args):
 
     n = world
     cells, steps = head["cells"], head["steps"]
-    value = n * cells * steps / (head["ms"] / 1e3) / 1e9
+    value = replica_glups(n, cells, steps, head["ms"])
     achieved = cells * head["bytes_per_cell"] / (head["kernel_ms_avg"] / 1e3) / 1e9
     # DRAM bytes per cell update measured by ncu (dram__bytes_read.sum +
     # dram__bytes_write.sum) on one launch of the fused step on the
