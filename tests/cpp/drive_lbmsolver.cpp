@@ -1,7 +1,7 @@
 // Scenario driver written against the LBMSolver interface (test input for
 // tests/test_cpp_mirror.py): a 48 x 32 x 30 m box with dx = 1 m, the STL
 // geometry given on the command line, a stationary Gaussian-pulse source
-// and four probes, run for T = 79 dt (80 steps) with two VTK frames.
+// and four probes, run for T = 79 dt (80 steps, frames at steps 0, 39, 78).
 #include <cstdio>
 #include <cstdlib>
 

@@ -40,8 +40,9 @@ def test_cpp_mirror_run_matches_oracle(fp16, gpu, tmp_path):
     assert "WARNING: Probe A is trapped inside SOLID building!" in r.stdout   # 06:434
     got = {n: np.loadtxt(tmp_path / f"probe_{n}.txt") for n in "ABCD"}
     assert all(len(v) == 80 for v in got.values())
+    # total_steps = 79, Frames = 2 -> out_interval = 39: frames at s = 0, 39, 78 (06:1068, 06:1094)
     vtk = sorted(os.listdir(tmp_path / "output_mpi"))
-    assert vtk == ["flight_00000.vtk", "flight_00001.vtk"]
+    assert vtk == ["flight_00000.vtk", "flight_00001.vtk", "flight_00002.vtk"]
     head = open(tmp_path / "output_mpi" / "flight_00001.vtk", "rb").read(400)
     assert b"DIMENSIONS 48 32 30" in head and b"BINARY" in head
 
