@@ -1169,6 +1169,36 @@ extern "C" int lbm_get_rho(lbm_handle* h, float* out, long capacity)
     return LBM_OK;
 }
 
+// Same output as lbm_get_rho without any device allocation: the field goes
+// through the library's statically reserved array (see nlos_lbm.h).
+extern "C" int lbm_get_rho_noalloc(lbm_handle* h, float* out, long capacity)
+{
+    int st = check_ready(h);
+    if (st) return st;
+    const Layout& L = h->L;
+    const long long n = (long long)L.nx * L.ny * L.nz;
+    if (n > LBM_NOALLOC_MAX_CELLS)
+        return h->fail(LBM_ERR_UNSUPPORTED, "lbm_get_rho_noalloc: the grid has " + std::to_string(n) +
+                                                " cells; the static field array holds at most " +
+                                                std::to_string((long long)LBM_NOALLOC_MAX_CELLS));
+    if (!out || (long long)capacity < n) return h->fail(LBM_ERR_CAPACITY, "rho buffer too small");
+    if (h->step == 0)
+    {
+        std::fill(out, out + n, 0.0f);   // rho initialised to 1 (06:368)
+        return LBM_OK;
+    }
+    CK(cudaSetDevice(h->device), "cudaSetDevice");
+    float* d = nullptr;
+    CK(field_scratch_address(h->device, &d), "static field array address");
+    // every cell of the first n entries is written by the kernel: nothing to clear
+    CK(launch_field_rho(h->storage, h->f[h->cur ^ 1], d, L, h->sa, h->scale, h->stream), "field kernel");
+    CK(cudaMemcpyAsync(out, d, (size_t)n * sizeof(float), cudaMemcpyDeviceToHost, h->stream), "field download");
+    CK(cudaStreamSynchronize(h->stream), "field download");
+    h->launches++;
+    h->d2h_bytes += (long)(n * (long long)sizeof(float));
+    return LBM_OK;
+}
+
 extern "C" int lbm_get_f(lbm_handle* h, double* out, long capacity)
 {
     int st = check_ready(h);

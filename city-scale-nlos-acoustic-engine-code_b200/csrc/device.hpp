@@ -179,4 +179,12 @@ cudaError_t launch_export_f(int storage, const void* f, double* out, const Layou
 cudaError_t launch_import_f(int storage, void* f, const double* in, const Layout& L, const XFace& xf, float scale,
                             cudaStream_t stream);
 
+// Capacity (cells) of the statically reserved field array used by
+// lbm_get_rho_noalloc, and the device address of that array on `device`
+// (looked up on first use with the device current; must not run during
+// stream capture).
+constexpr long long kNoAllocFieldCells = 8388608;   // 2^23 floats = 32 MiB
+constexpr int kMaxDevices = 64;
+cudaError_t field_scratch_address(int device, float** ptr);
+
 }  // namespace lbm

@@ -7,6 +7,7 @@
 
 #include <cmath>
 #include <cstdint>
+#include <mutex>
 #include <type_traits>
 
 #include "device.hpp"
@@ -932,6 +933,11 @@ __global__ void k_import_f(S* __restrict__ f, const double* __restrict__ in, Lay
     }
 }
 
+// Statically reserved device array for lbm_get_rho_noalloc: the field of
+// (rho - 1) passes through it instead of a temporary cudaMalloc buffer.  It
+// exists on every GPU that loads this library, for the life of the process.
+static __device__ __align__(256) float g_field_scratch[kNoAllocFieldCells];
+
 dim3 row_grid(const Layout& L) { return dim3((unsigned)((L.nx + 127) / 128), (unsigned)L.ny, (unsigned)L.nz); }
 dim3 pair_grid(const Layout& L, int block)
 {
@@ -969,6 +975,26 @@ cudaError_t launch_step_t(const S* fin, S* fout, const Layout& L, const StepArgs
 }
 
 }  // namespace
+
+cudaError_t field_scratch_address(int device, float** ptr)
+{
+    // Host code cannot use the array's name as a device address; the address
+    // is looked up once per device, with that device current (the caller
+    // sets it), and cached.
+    static std::mutex mu;
+    static float* cached[kMaxDevices] = {};
+    if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!cached[device])
+    {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_field_scratch);
+        if (e != cudaSuccess) return e;
+        cached[device] = static_cast<float*>(p);
+    }
+    *ptr = cached[device];
+    return cudaSuccess;
+}
 
 cudaError_t launch_build_links(const uint8_t* mask_ref, uint32_t* links, uint32_t* near, const Layout& L,
                                cudaStream_t stream)

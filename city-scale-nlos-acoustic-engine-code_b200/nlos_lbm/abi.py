@@ -26,6 +26,7 @@ LBM_ERR_CAPACITY = -7
 LBM_ERR_NO_DEVICE = -8
 LBM_ERR_IO = -9
 LBM_ERR_UNSUPPORTED = -10
+LBM_NOALLOC_MAX_CELLS = 8388608
 
 LBM_BC_NSCBC, LBM_BC_REST, LBM_BC_WALL = 0, 1, 2
 FACE_XLO, FACE_XHI, FACE_YLO, FACE_YHI, FACE_ZLO, FACE_ZHI = range(6)
@@ -175,6 +176,7 @@ def bind_product(lib):
         "lbm_get_probes": (ctypes.c_int, [P, c_double_p, ctypes.c_long, c_long_p]),
         "lbm_get_probe_energy": (ctypes.c_int, [P, c_double_p]),
         "lbm_get_rho": (ctypes.c_int, [P, c_float_p, ctypes.c_long]),
+        "lbm_get_rho_noalloc": (ctypes.c_int, [P, c_float_p, ctypes.c_long]),
         "lbm_get_f": (ctypes.c_int, [P, c_double_p, ctypes.c_long]),
         "lbm_set_f": (ctypes.c_int, [P, c_double_p, ctypes.c_long]),
         "lbm_get_mask": (ctypes.c_int, [P, c_uint8_p, ctypes.c_long]),

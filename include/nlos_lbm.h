@@ -217,6 +217,27 @@ int lbm_get_probes(lbm_handle* h, double* out, long capacity, long* nsteps);
 int lbm_get_probe_energy(lbm_handle* h, double* out);
 /* Interior field (float)(rho-1) of the last step, i fastest (06:979-985). */
 int lbm_get_rho(lbm_handle* h, float* out, long capacity);
+/* Largest grid (interior cells) lbm_get_rho_noalloc accepts. */
+#define LBM_NOALLOC_MAX_CELLS 8388608L
+
+/* lbm_get_rho without allocating: no counterpart in the reference (its
+ * rho field is a host vector, 06:281).  Some callers cannot allocate device
+ * memory at the moment they read a field: a host application that owns the
+ * GPU's memory through its own pool, where a direct cudaMalloc would bypass
+ * or overrun that budget, or a frame loop that must not stall, since
+ * cudaMalloc and cudaFree can synchronise the whole device.  This call
+ * writes the same values as lbm_get_rho into `out`, but the device-side
+ * field passes through one array of LBM_NOALLOC_MAX_CELLS floats (32 MiB)
+ * reserved statically in the library: every GPU that loads the library
+ * holds it until the process exits, and nothing is allocated per call.
+ * Grids with more interior cells are rejected with LBM_ERR_UNSUPPORTED.
+ * The first call on a device looks up the array's address; make that first
+ * call before any CUDA stream capture.  All handles on a device share the
+ * array: calls that overlap on the GPU (handles used from different host
+ * threads at the same time) race and may return each other's field, so
+ * serialise them.  The array keeps the last call's contents; every call
+ * overwrites all the cells it returns, so nothing needs clearing. */
+int lbm_get_rho_noalloc(lbm_handle* h, float* out, long capacity);
 /* Populations f_q (FP64, w_q + deviation) in the reference's AoS,
  * halo-inclusive layout f[idx*19+q] (06:366, 06:206-209). */
 int lbm_get_f(lbm_handle* h, double* out, long capacity);
