@@ -212,6 +212,42 @@ def e2e_measure(solver, w, steps):
     return (t1 - t0) * 1e3, (h1 - h0) / steps, (d1 - d0) / steps
 
 
+def adjoint_measure(device, torch, reps=1, ckpt=(200, 20)):
+    """Gradients per second of lbm_adjoint_grad on the 256x256x128 patch
+    (3000 steps, 64 receivers): observed series from a forward run of the
+    true source, then the misfit gradient at the trial source, timed with CUDA
+    events on the library's stream around whole lbm_adjoint_grad calls."""
+    import nlos_lbm
+    from nlos_lbm import workloads
+
+    w = workloads.build("adjoint256")
+    w["cfg"].device = device
+    truth = nlos_lbm.Solver(w["cfg"], [w["true_source"]], w["probes"], triangles=w["triangles"])
+    truth.step(w["steps"])
+    observed = truth.get_probes()
+    truth.close()
+    s = nlos_lbm.Solver(w["cfg"], w["sources"], w["probes"], triangles=w["triangles"])
+    stream = torch.cuda.ExternalStream(s.stream)
+    s.adjoint_grad(observed[:100], *ckpt)   # warm-up (allocations, first launches)
+    times = []
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        l0 = s.launch_count
+        e0.record(stream)
+        loss, gpos, gsig, _ = s.adjoint_grad(observed, *ckpt)
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+        launches = s.launch_count - l0
+    nx, ny, nz = workloads.cells(w["cfg"])
+    ms = float(np.median(times))
+    return {"workload": "adjoint256: " + w["description"], "grad_per_s": 1e3 / ms, "ms_per_grad": ms,
+            "steps": w["steps"], "cells": nx * ny * nz, "ckpt_outer_inner": list(ckpt), "loss": loss,
+            "grad_pos": [float(v) for v in gpos], "grad_signal_norm": float(np.linalg.norm(gsig)),
+            "launches": launches, "fwd_equiv_glups": nx * ny * nz * w["steps"] / (ms / 1e3) / 1e9}
+
+
 def cpu_baseline(steps_hint=None):
     """Reference CPU step on a bounded sub-domain of the city (rank 0, N=1)."""
     import oracle
@@ -319,6 +355,11 @@ def run_our_arm(args):
             del s2
             gc.collect()
 
+    adjoint = None
+    if world == 1 and not args.headline_only and not args.no_adjoint:
+        adjoint = adjoint_measure(local, torch)
+        gc.collect()
+
     n = world
     cells, steps = head["cells"], head["steps"]
     value = replica_glups(n, cells, steps, head["ms"])
@@ -349,6 +390,8 @@ def run_our_arm(args):
         "probes_finite": head["probes_finite"],
         "secondary": secondary,
     }
+    if adjoint is not None:
+        line["adjoint"] = adjoint
     if secondary.get("city1024_fp32") and secondary.get("city1024_fp16"):
         line["fp16_over_fp32"] = secondary["city1024_fp16"]["glups_rank"] / secondary["city1024_fp32"]["glups_rank"]
     if world == 1 and rank == 0 and not args.no_cpu:
@@ -373,6 +416,7 @@ def main():
                     help="population storage of the headline workload (default: the workload's own)")
     ap.add_argument("--headline-only", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -18,6 +18,7 @@
 #include <string>
 #include <vector>
 
+#include "adjoint.hpp"
 #include "device.hpp"
 #include "geometry.hpp"
 #include "lattice.cuh"
@@ -1331,4 +1332,372 @@ extern "C" int lbm_voxelize(const lbm_config* cfg, const float* tris, int ntris,
     geo.set_triangles(tris, ntris, scale, sx, sy, sz);
     build_mask(*cfg, geo, nx, ny, nz, mask);
     return LBM_OK;
+}
+
+// ---------------------------------------------------------------- adjoint
+
+namespace {
+
+// Device memory of one adjoint evaluation, freed on every exit path.
+struct DevScratch
+{
+    std::vector<void*> ptrs;
+    ~DevScratch()
+    {
+        for (void* p : ptrs) cudaFree(p);
+    }
+    template <typename T>
+    T* get(size_t n, cudaError_t& e)
+    {
+        void* p = nullptr;
+        if (e == cudaSuccess) e = cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T));
+        if (e == cudaSuccess) ptrs.push_back(p);
+        return (T*)p;
+    }
+};
+
+// n stored forward states, each a population buffer plus one x-face array
+// (the x-face exports for a checkpoint of G, the x-face ghosts for a stored Ht).
+struct StateSlots
+{
+    float* base = nullptr;
+    size_t pop = 0, face = 0;   // floats, rounded up to 64
+    float* pop_of(long long s) const { return base + (size_t)s * (pop + face); }
+    float* face_of(long long s) const { return pop_of(s) + pop; }
+};
+
+// All lattice cells are back at rest and the step counter at 0.
+int rest_state(lbm_handle* h)
+{
+    const size_t pop_bytes = (size_t)h->L.total * (h->storage == LBM_STORE_F16 ? 2 : 4);
+    const size_t n_xexp = (size_t)2 * Q * h->L.ny * h->L.nz, n_xgh = (size_t)2 * Q * (h->L.ny + 2) * (h->L.nz + 2);
+    for (int b = 0; b < 2; ++b) CK(cudaMemsetAsync(h->f[b], 0, pop_bytes, h->stream), "rest state");
+    CK(cudaMemsetAsync(h->xf.xexp, 0, n_xexp * sizeof(float), h->stream), "rest state");
+    CK(cudaMemsetAsync(h->xf.xgh, 0, n_xgh * sizeof(float), h->stream), "rest state");
+    CK(cudaMemsetAsync(h->d_energy, 0, (size_t)std::max(h->nprobe(), 1) * sizeof(double), h->stream), "rest state");
+    CK(cudaStreamSynchronize(h->stream), "rest state");
+    h->step = 0;
+    h->cur = 0;
+    h->series.clear();
+    h->probe_pending = 0;
+    h->halo_dirty = false;
+    return LBM_OK;
+}
+
+// Injection cells of the single source at one step with their normalised
+// weights and the weights' derivatives with respect to the source position
+// (metres).  Same cell set, fluid test and normalisation as k_source.
+void source_cells(const lbm_handle* h, const lbm_source& p, const SourceEntry& e, int ncell, AdjSourceCell* out)
+{
+    const lbm_config& c = h->cfg;
+    const Layout& L = h->L;
+    const int nxt = L.nx + 2, nyt = L.ny + 2;
+    std::vector<double> ww((size_t)ncell, 0.0), dw((size_t)ncell * 3, 0.0);
+    std::vector<int> ijk((size_t)ncell * 3, 0);
+    std::vector<char> fluid((size_t)ncell, 0);
+    for (int b = 0; b < ncell; ++b) out[b] = AdjSourceCell{-1, 0, 0, 0, 0.0, {0.0, 0.0, 0.0}};
+    const auto is_fluid = [&](int gi, int gj, int gk) {
+        if (gi < 0 || gi >= L.nx || gj < 0 || gj >= L.ny || gk < 0 || gk >= L.nz) return false;
+        return h->mask[(size_t)(gi + 1) + (size_t)(gj + 1) * nxt + (size_t)(gk + 1) * nxt * nyt] == 0;
+    };
+    if (p.injection == LBM_INJECT_TRILINEAR)
+    {
+        const double fx = (e.cx - c.x_min) / c.dx - 0.5;
+        const double fy = (e.cy - c.y_min) / c.dx - 0.5;
+        const double fz = (e.cz - c.z_min) / c.dx - 0.5;
+        const int i0 = (int)std::floor(fx), j0 = (int)std::floor(fy), k0 = (int)std::floor(fz);
+        const double tx = fx - i0, ty = fy - j0, tz = fz - k0;
+        for (int b = 0; b < 8; ++b)
+        {
+            const int bx = b & 1, by = (b >> 1) & 1, bz = b >> 2;
+            const double wx = bx ? tx : 1.0 - tx, wy = by ? ty : 1.0 - ty, wz = bz ? tz : 1.0 - tz;
+            const double sx = (bx ? 1.0 : -1.0) / c.dx, sy = (by ? 1.0 : -1.0) / c.dx, sz = (bz ? 1.0 : -1.0) / c.dx;
+            ijk[3 * b] = i0 + bx;
+            ijk[3 * b + 1] = j0 + by;
+            ijk[3 * b + 2] = k0 + bz;
+            ww[b] = wx * wy * wz;
+            dw[3 * b] = sx * wy * wz;
+            dw[3 * b + 1] = wx * sy * wz;
+            dw[3 * b + 2] = wx * wy * sz;
+            fluid[b] = is_fluid(ijk[3 * b], ijk[3 * b + 1], ijk[3 * b + 2]);
+        }
+    }
+    else
+    {
+        const int R = p.radius, n = 2 * R + 1;
+        const double sigma2 = (p.sigma_cells * c.dx) * (p.sigma_cells * c.dx);
+        const int ic = (int)std::floor((e.cx - c.x_min) / c.dx);
+        const int jc = (int)std::floor((e.cy - c.y_min) / c.dx);
+        const int kc = (int)std::floor((e.cz - c.z_min) / c.dx);
+        if (ic < -R || ic >= L.nx + R || jc < -R || jc >= L.ny + R || kc < -R || kc >= L.nz + R) return;
+        for (int b = 0; b < ncell; ++b)
+        {
+            const int gi = ic + b % n - R, gj = jc + (b / n) % n - R, gk = kc + b / (n * n) - R;
+            const double x = c.x_min + (gi + 0.5) * c.dx, y = c.y_min + (gj + 0.5) * c.dx,
+                         z = c.z_min + (gk + 0.5) * c.dx;
+            const double ddx = x - e.cx, ddy = y - e.cy, ddz = z - e.cz;
+            const double w = std::exp(-0.5 * (ddx * ddx + ddy * ddy + ddz * ddz) / sigma2);
+            ijk[3 * b] = gi;
+            ijk[3 * b + 1] = gj;
+            ijk[3 * b + 2] = gk;
+            ww[b] = w;
+            dw[3 * b] = w * ddx / sigma2;   // d/dcx exp(-(x-cx)^2 / 2s^2)
+            dw[3 * b + 1] = w * ddy / sigma2;
+            dw[3 * b + 2] = w * ddz / sigma2;
+            fluid[b] = is_fluid(gi, gj, gk);
+        }
+    }
+    double S = 0.0, dS[3] = {0.0, 0.0, 0.0};
+    for (int b = 0; b < ncell; ++b)
+        if (fluid[b])
+        {
+            S += ww[b];
+            for (int a = 0; a < 3; ++a) dS[a] += dw[3 * b + a];
+        }
+    if (S < 1e-30) return;
+    for (int b = 0; b < ncell; ++b)
+    {
+        if (!fluid[b]) continue;
+        AdjSourceCell& o = out[b];
+        o.i = ijk[3 * b] + 1;
+        o.j = ijk[3 * b + 1] + 1;
+        o.k = ijk[3 * b + 2] + 1;
+        o.what = ww[b] / S;
+        for (int a = 0; a < 3; ++a) o.dwhat[a] = (dw[3 * b + a] * S - ww[b] * dS[a]) / (S * S);
+    }
+}
+
+}  // namespace
+
+extern "C" int lbm_adjoint_grad(lbm_handle* h, int nsteps, const double* observed, int ckpt_outer, int ckpt_inner,
+                                double* loss, double* grad_pos, double* grad_signal, double* predicted)
+{
+    int st = check_ready(h);
+    if (st) return st;
+    if (h->storage != LBM_STORE_F32) return h->fail(LBM_ERR_UNSUPPORTED, "the adjoint runs on FP32 storage");
+    if (h->srcs.size() != 1) return h->fail(LBM_ERR_UNSUPPORTED, "the adjoint needs exactly one source");
+    const int np = h->nprobe();
+    if (np < 1) return h->fail(LBM_ERR_STATE, "the adjoint needs probes");
+    if (nsteps < 1 || !observed || !loss) return h->fail(LBM_ERR_INVALID_ARGUMENT, "nsteps, observed or loss");
+    CK(cudaSetDevice(h->device), "cudaSetDevice");
+    st = rest_state(h);
+    if (st) return st;
+
+    const int T = nsteps;
+    const int K1 = std::min(ckpt_outer > 0 ? ckpt_outer : 200, T);
+    const int K2 = std::min(ckpt_inner > 0 ? ckpt_inner : 20, K1);
+    const Layout& L = h->L;
+    const int M = (T + K1 - 1) / K1;          // outer checkpoints
+    const int NI = (K1 + K2 - 1) / K2;        // inner checkpoints per outer segment
+    const size_t n_xexp = (size_t)2 * Q * L.ny * L.nz, n_xgh = (size_t)2 * Q * (L.ny + 2) * (L.nz + 2);
+    const auto r64 = [](size_t n) { return (n + 63) / 64 * 64; };
+    const size_t pop = r64((size_t)L.total);
+    const SourceState& src = h->srcs[0];
+    const int ncell = src.s.injection == LBM_INJECT_TRILINEAR
+                          ? 8
+                          : (2 * src.s.radius + 1) * (2 * src.s.radius + 1) * (2 * src.s.radius + 1);
+
+    // Source schedule and injection cells of every step (host, FP64).
+    std::vector<SourceEntry> entries((size_t)T);
+    std::vector<AdjSourceCell> cells((size_t)T * ncell);
+    for (int s = 0; s < T; ++s)
+    {
+        entries[s] = source_entry(src, (double)s * h->dt, h->dt);
+        source_cells(h, src.s, entries[s], ncell, &cells[(size_t)s * ncell]);
+    }
+
+    // Open faces of the ghost adjoint.
+    long long gadj_off[6] = {-1, -1, -1, -1, -1, -1};
+    long long gadj_n = 0;
+    for (int f = 0; f < h->ga.nfaces; ++f)
+    {
+        const GhostFace& F = h->ga.face[f];
+        gadj_off[F.axis * 2 + F.side] = gadj_n;
+        gadj_n += (long long)Q * F.nu * F.nv;
+    }
+
+    DevScratch mem;
+    cudaError_t e = cudaSuccess;
+    StateSlots outer{mem.get<float>((size_t)M * (pop + r64(n_xexp)), e), pop, r64(n_xexp)};
+    StateSlots inner{mem.get<float>((size_t)NI * (pop + r64(n_xexp)), e), pop, r64(n_xexp)};
+    StateSlots store{mem.get<float>((size_t)(K2 + 1) * (pop + r64(n_xgh)), e), pop, r64(n_xgh)};
+    float* lam[2] = {mem.get<float>(pop, e), mem.get<float>(pop, e)};
+    float* gadj = mem.get<float>((size_t)gadj_n, e);
+    double* d_pred = mem.get<double>((size_t)T * np, e);
+    double* d_resid = mem.get<double>((size_t)T * np, e);
+    AdjSourceCell* d_cells = mem.get<AdjSourceCell>(cells.size(), e);
+    double* d_out = mem.get<double>((size_t)T * 4, e);
+    if (e != cudaSuccess) return h->cuda_fail(e, "adjoint buffers");
+    CK(cudaMemcpyAsync(d_cells, cells.data(), cells.size() * sizeof(AdjSourceCell), cudaMemcpyHostToDevice, h->stream),
+       "adjoint upload");
+    CK(cudaMemsetAsync(d_out, 0, (size_t)T * 4 * sizeof(double), h->stream), "adjoint memset");
+
+    const size_t pop_bytes = (size_t)L.total * sizeof(float);
+    SourceArgs sargs = source_args(h, false);
+    long kernels = 0;
+    const auto save_g = [&](const StateSlots& sl, long long idx) {
+        cudaError_t r = cudaMemcpyAsync(sl.pop_of(idx), h->f[h->cur], pop_bytes, cudaMemcpyDeviceToDevice, h->stream);
+        if (r == cudaSuccess)
+            r = cudaMemcpyAsync(sl.face_of(idx), h->xf.xexp, n_xexp * sizeof(float), cudaMemcpyDeviceToDevice,
+                                h->stream);
+        return r;
+    };
+    const auto restore_g = [&](const StateSlots& sl, long long idx) {
+        h->cur = 0;
+        cudaError_t r = cudaMemcpyAsync(h->f[0], sl.pop_of(idx), pop_bytes, cudaMemcpyDeviceToDevice, h->stream);
+        if (r == cudaSuccess)
+            r = cudaMemcpyAsync(h->xf.xexp, sl.face_of(idx), n_xexp * sizeof(float), cudaMemcpyDeviceToDevice,
+                                h->stream);
+        return r;
+    };
+    const auto save_ht = [&](long long idx) {
+        cudaError_t r =
+            cudaMemcpyAsync(store.pop_of(idx), h->f[h->cur], pop_bytes, cudaMemcpyDeviceToDevice, h->stream);
+        if (r == cudaSuccess)
+            r = cudaMemcpyAsync(store.face_of(idx), h->xf.xgh, n_xgh * sizeof(float), cudaMemcpyDeviceToDevice,
+                                h->stream);
+        return r;
+    };
+    // source + ghost fill of step s on the current buffer (G^s -> Ht^s)
+    const auto source_ghost = [&](int s) {
+        sargs.direct[0] = entries[s];
+        cudaError_t r = launch_source(h->storage, h->f[h->cur], L, h->sa, sargs, h->stream);
+        kernels++;
+        if (r == cudaSuccess && h->ga.total > 0)
+        {
+            r = launch_ghost(h->storage, h->f[h->cur], L, h->ga, h->stream);
+            kernels++;
+        }
+        return r;
+    };
+    // pull + collide of step s (Ht^s -> G^{s+1}), optionally with its probe record
+    const auto collide = [&](int s, bool probe) {
+        cudaError_t r = launch_step(h->storage, h->f[h->cur], h->f[h->cur ^ 1], L, h->sa, h->scale, h->step_variant,
+                                    h->stream);
+        kernels++;
+        if (r == cudaSuccess && probe)
+        {
+            ProbeArgs pa = probe_args(h, false, s);
+            pa.out = d_pred;
+            r = launch_probe(h->storage, h->f[h->cur], L, h->sa, pa, h->stream);
+            kernels++;
+        }
+        h->cur ^= 1;
+        return r;
+    };
+    const auto ckpt_pos = [&](long long boundary) { return std::max(boundary - 1, 0LL); };
+
+    // ---- forward pass: probe predictions and outer checkpoints G^{max(mK1-1,0)}
+    {
+        int m = 0;
+        for (int s = 0; s < T; ++s)
+        {
+            while (m < M && ckpt_pos((long long)m * K1) == s)
+            {
+                CK(save_g(outer, m), "checkpoint");
+                ++m;
+            }
+            CK(source_ghost(s), "adjoint forward");
+            CK(collide(s, true), "adjoint forward");
+        }
+    }
+
+    // ---- misfit (FP64 on the host) and residuals
+    std::vector<double> pred((size_t)T * np), resid((size_t)T * np, 0.0);
+    CK(cudaMemcpyAsync(pred.data(), d_pred, pred.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream),
+       "prediction download");
+    CK(cudaStreamSynchronize(h->stream), "prediction download");
+    double Lsum = 0.0;
+    for (int s = 0; s < T; ++s)
+        for (int p = 0; p < np; ++p)
+        {
+            const size_t n = (size_t)s * np + p;
+            if (!h->probe_owned[p] || !std::isfinite(observed[n])) continue;
+            if (!std::isfinite(pred[n])) return h->fail(LBM_ERR_NAN, "non-finite forward probe value");
+            const double r = pred[n] - observed[n];
+            Lsum += 0.5 * r * r;
+            if (!h->probe_solid[p]) resid[n] = r;   // a SOLID probe reads 0 whatever the state
+        }
+    CK(cudaMemcpyAsync(d_resid, resid.data(), resid.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream),
+       "residual upload");
+
+    // ---- reverse pass
+    for (int b = 0; b < 2; ++b) CK(cudaMemsetAsync(lam[b], 0, pop * sizeof(float), h->stream), "adjoint memset");
+    int la = 0;
+    AdjProbeArgs pa{np, h->d_probe_ijk, nullptr, L};
+    pa.resid = d_resid + (size_t)(T - 1) * np;
+    CK(launch_adj_probe(lam[la], pa, h->stream), "adjoint probe");
+    kernels++;
+    for (int m = M - 1; m >= 0; --m)
+    {
+        const int O = m * K1, E = std::min(O + K1, T);
+        const int N = (E - O + K2 - 1) / K2;
+        CK(restore_g(outer, m), "restore");
+        long long at = ckpt_pos(O);   // the current buffer holds G^at
+        for (int n = 0; n < N; ++n)
+        {
+            const long long cn = ckpt_pos((long long)O + (long long)n * K2);
+            for (; at < cn; ++at)
+            {
+                CK(source_ghost((int)at), "recompute");
+                CK(collide((int)at, false), "recompute");
+            }
+            CK(save_g(inner, n), "checkpoint");
+        }
+        for (int n = N - 1; n >= 0; --n)
+        {
+            const int a0 = O + n * K2, a1 = std::min(a0 + K2, E);
+            const int cn = (int)ckpt_pos(a0);
+            CK(restore_g(inner, n), "restore");
+            for (int s = cn; s < a1; ++s)
+            {
+                CK(source_ghost(s), "recompute");
+                CK(save_ht(s - cn), "store");
+                if (s + 1 < a1) CK(collide(s, false), "recompute");
+            }
+            for (int s = a1 - 1; s >= a0; --s)
+            {
+                if (h->ga.total > 0)
+                {
+                    AdjGhostArgs ga{L, h->ga, h->links, lam[la], store.pop_of(s - cn), gadj, {}};
+                    std::copy(gadj_off, gadj_off + 6, ga.gadj_off);
+                    CK(launch_adj_ghost(ga, h->stream), "adjoint ghost");
+                    kernels++;
+                }
+                AdjSourceArgs sa{L, h->links, lam[la], gadj, {}, d_cells, ncell, s, d_out};
+                std::copy(gadj_off, gadj_off + 6, sa.gadj_off);
+                CK(launch_adj_source(sa, h->stream), "adjoint source");
+                kernels++;
+                if (s == 0) continue;
+                AdjStepArgs as{L, h->sa, lam[la], lam[la ^ 1], store.pop_of(s - 1 - cn), store.face_of(s - 1 - cn),
+                               gadj, {}};
+                std::copy(gadj_off, gadj_off + 6, as.gadj_off);
+                CK(launch_adj_step(as, h->stream), "adjoint step");
+                kernels++;
+                la ^= 1;
+                pa.resid = d_resid + (size_t)(s - 1) * np;
+                CK(launch_adj_probe(lam[la], pa, h->stream), "adjoint probe");
+                kernels++;
+            }
+        }
+    }
+
+    // ---- gradients: d L / d val_s = mu_s dt gain; d L / d pos = sum_s mass_s nu_s
+    std::vector<double> out((size_t)T * 4);
+    CK(cudaMemcpyAsync(out.data(), d_out, out.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream),
+       "gradient download");
+    CK(cudaStreamSynchronize(h->stream), "gradient download");
+    h->launches += kernels;
+    double gp[3] = {0.0, 0.0, 0.0};
+    for (int s = 0; s < T; ++s)
+    {
+        for (int a = 0; a < 3; ++a) gp[a] += entries[s].mass * out[(size_t)s * 4 + 1 + a];
+        if (grad_signal) grad_signal[s] = out[(size_t)s * 4] * h->dt * src.s.gain;
+    }
+    for (int s = 0; s < T; ++s)
+        if (!std::isfinite(out[(size_t)s * 4])) return h->fail(LBM_ERR_NAN, "non-finite adjoint");
+    if (grad_pos) std::copy(gp, gp + 3, grad_pos);
+    if (predicted) std::copy(pred.begin(), pred.end(), predicted);
+    *loss = Lsum;
+    return rest_state(h);
 }

@@ -196,6 +196,24 @@ class Solver:
                     "lbm_get_transfer_bytes")
         return h2d.value, d2h.value
 
+    # -- adjoint
+    def adjoint_grad(self, observed, ckpt_outer=0, ckpt_inner=0):
+        """Misfit and its gradient for the probe series `observed` [nsteps, nprobe]
+        (lbm_adjoint_grad): returns (loss, grad_pos[3], grad_signal[nsteps],
+        predicted[nsteps, nprobe]).  The solver is left at the rest state."""
+        obs = np.ascontiguousarray(observed, dtype=np.float64)
+        if obs.ndim != 2 or obs.shape[1] != self.nprobe:
+            raise ValueError("observed must be [nsteps, nprobe]")
+        T = obs.shape[0]
+        loss = ctypes.c_double()
+        gpos = np.zeros(3)
+        gsig = np.zeros(T)
+        pred = np.zeros((T, self.nprobe))
+        self._check(self.lib.lbm_adjoint_grad(self.h, T, _ptr(obs), int(ckpt_outer), int(ckpt_inner),
+                                              ctypes.byref(loss), _ptr(gpos), _ptr(gsig), _ptr(pred)),
+                    "lbm_adjoint_grad")
+        return loss.value, gpos, gsig, pred
+
     def clear_sources(self):
         self._check(self.lib.lbm_clear_sources(self.h), "lbm_clear_sources")
 

@@ -12,6 +12,10 @@ reference's heightmap ray cast.
   city1024   1024x1024x256 city, 4 Ricker sources at street level, 256 probes
   city2048   2048x2048x256 city, one source flying at z = 120 at Mach 0.15,
              512 probes (FP16 deviation storage, scale 1/amplitude)
+  adjoint256 256x256x128 city patch, tau 0.52, true source at street level
+             emitting a Ricker wavelet (period 30 steps), 64 street-level
+             receivers, 3000 steps; the trial source (the unknown of the
+             localisation) sits a few cells away
 """
 import numpy as np
 
@@ -113,6 +117,26 @@ def build(name, storage=None, seed=2024):
                                    freq=1 / 40.0, waveform=abi.LBM_WAVE_SINE, injection=abi.LBM_INJECT_TRILINEAR)
         return dict(cfg=cfg, sources=[src], probes=probes, triangles=tris, steps=4000, coverage=cov,
                     description="synthetic city 2048x2048x256, source flying at z=120 Mach 0.15, 512 probes")
+    if name == "adjoint256":
+        from .solver import city_triangles
+
+        nx, ny, nz = 256, 256, 128
+        tris, cov = city_triangles(nx, ny, seed=seed, fp=(20, 60), height=(10, 80), coverage=0.40, street=8,
+                                   margin=24)
+        cfg = lattice_config(nx, ny, nz, 0.52, sponge_width=16.0, sponge_faces=FIVE_FACES,
+                             storage=abi.LBM_STORE_F32 if storage is None else storage)
+        pts = street_points(tris, nx, ny, 1 + 64, 2.5, seed, margin=24, clearance=3.0)
+        true_xyz = pts[0] + np.array([0.0, 0.0, 1.1])
+        trial_xyz = true_xyz + np.array([2.37, -1.61, 0.83])
+
+        def ricker(x):
+            return abi.reference_source(sx=x[0], sy=x[1], sz=x[2], ex=x[0], ey=x[1], ez=x[2], amp=1e-3,
+                                        freq=1 / 30.0, t0=45.0, waveform=abi.LBM_WAVE_RICKER,
+                                        injection=abi.LBM_INJECT_TRILINEAR)
+        return dict(cfg=cfg, sources=[ricker(trial_xyz)], true_source=ricker(true_xyz), probes=pts[1:],
+                    triangles=tris, steps=3000, coverage=cov,
+                    description="transient localisation 256x256x128 city patch, Ricker period 30, 64 receivers, "
+                                "3000 steps")
     raise KeyError(name)
 
 

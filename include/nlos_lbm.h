@@ -245,6 +245,30 @@ int lbm_set_f(lbm_handle* h, const double* in, long count);
 /* Voxelised mask, halo-inclusive, 0 FLUID / 1 SOLID (06:469-531). */
 int lbm_get_mask(lbm_handle* h, uint8_t* out, long capacity);
 
+/* ---- adjoint ---------------------------------------------------------------- */
+
+/* Gradient of the receiver misfit
+ *     L = 1/2 sum_{s < nsteps} sum_p (p_s[p] - observed[s * nprobe + p])^2
+ * of an nsteps-step run from the rest state, with respect to a rigid shift of
+ * the source path (grad_pos[3], per metre) and to the source signal value at
+ * every step (grad_signal[nsteps]: dL/dval_s, val_s = amp * waveform(t_s) as in
+ * 06:579-581, so dL/dtable[s] = amp * grad_signal[s] for LBM_WAVE_TABLE).
+ * No counterpart in the reference, which has no adjoint or inverse solver;
+ * the forward model is exactly lbm_step's (same kernels, FP32 storage).
+ * A reverse-time discrete adjoint of the fused step: the forward pass keeps a
+ * checkpoint every ckpt_outer steps (<= 0: 200), each segment is recomputed
+ * with inner checkpoints every ckpt_inner steps (<= 0: 20), and each inner
+ * segment once more, storing its states, before it is run backwards.  Device
+ * memory: about (nsteps/ckpt_outer + ckpt_outer/ckpt_inner + ckpt_inner + 3)
+ * population buffers.  Requires FP32 storage, exactly one source and at least
+ * one probe.  Observed entries that are NaN, probes outside the grid and the
+ * probe rows of SOLID cells (which read 0 whatever the state) contribute no
+ * gradient.  Starts from and returns to the rest state (step 0, empty probe
+ * series); `predicted` (optional, nsteps * nprobe) receives the forward probe
+ * series.  grad_pos, grad_signal and predicted may be NULL. */
+int lbm_adjoint_grad(lbm_handle* h, int nsteps, const double* observed, int ckpt_outer, int ckpt_inner,
+                     double* loss, double* grad_pos, double* grad_signal, double* predicted);
+
 /* ---- measurement ---------------------------------------------------------- */
 
 /* When enabled, every launch of the fused step kernel is bracketed by CUDA

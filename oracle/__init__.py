@@ -69,6 +69,7 @@ def _load():
             "orc_get_sponge": (None, [P, _dp]),
             "orc_get_ground_height": (None, [P, _dp]),
             "orc_get_probes": (ctypes.c_long, [P, _dp, ctypes.c_long]),
+            "orc_adjoint_grad": (ctypes.c_int, [P, ctypes.c_int, _dp, ctypes.c_int, _dp, _dp, _dp, _dp]),
         }
         for n, (r, a) in sig.items():
             fn = getattr(lib, n)
@@ -195,6 +196,20 @@ class OracleSolver:
         out = np.empty(nx * ny)
         self.lib.orc_get_ground_height(self.h, _ptr(out))
         return out
+
+    def adjoint_grad(self, observed, K=0):
+        """FP64 discrete adjoint (orc_adjoint_grad): (loss, grad_pos[3],
+        grad_signal[nsteps], predicted[nsteps, nprobe]); needs the state right
+        after construction and restores it."""
+        obs = np.ascontiguousarray(observed, dtype=np.float64)
+        T = obs.shape[0]
+        loss = ctypes.c_double()
+        gpos, gsig, pred = np.zeros(3), np.zeros(T), np.zeros((T, self.nprobe))
+        st = self.lib.orc_adjoint_grad(self.h, T, _ptr(obs), int(K), ctypes.byref(loss), _ptr(gpos), _ptr(gsig),
+                                       _ptr(pred))
+        if st != 0:
+            raise RuntimeError("orc_adjoint_grad failed: %d" % st)
+        return loss.value, gpos, gsig, pred
 
     def get_probes(self):
         cap = 1

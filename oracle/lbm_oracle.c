@@ -801,3 +801,328 @@ long orc_get_probes(orc_handle* h, double* out, long capacity)
     if (n) memcpy(out, h->series, (size_t)n * sizeof(double));
     return h->steps_rec;
 }
+
+/* ---------------------------------------------------------------- adjoint (FP64)
+ *
+ * Discrete adjoint of orc_step for the misfit
+ *     L = 1/2 sum_s sum_p (probe_s[p] - observed[s][p])^2,
+ * the checker of the GPU adjoint.  The reference has no adjoint; this is
+ * derived here from the forward restatement above and shares no code with
+ * the GPU version: the transposed pull is a scatter, the BGK and ghost
+ * Jacobians are differentiated in (rho, u) variables in full-population form,
+ * and one checkpoint level (every K steps) is recomputed with all its states
+ * stored.  Per step s, going backwards, with lamG = dL/d(post-collision
+ * populations of step s):
+ *   lamF  = J_bgk(F)^T lamG (+ residual at the probe cells, every q)
+ *   lamHt = pull^T lamF                                 (halo included)
+ *   lamH  = lamHt(interior) + J_ghost^T lamHt(open-face halo)
+ *   dL/dmass_s = sum_c w_hat_c sum_q W_q lamH[c][q]; lamG(s-1) = lamH.
+ */
+
+/* Normalised injection weights of source s at its current position and their
+ * derivatives with respect to the position; returns the cell count. */
+static int adj_source_cells(const orc_handle* h, const src_t* s, size_t* idx, double* wh, double* dwh)
+{
+    const lbm_config* c = &h->cfg;
+    const double DX = c->dx;
+    double w[125], dw[375];
+    int n = 0;
+    if (s->s.injection == LBM_INJECT_TRILINEAR)
+    {
+        const double fx = (s->cx - c->x_min) / DX - 0.5, fy = (s->cy - c->y_min) / DX - 0.5,
+                     fz = (s->cz - c->z_min) / DX - 0.5;
+        const int i0 = (int)floor(fx), j0 = (int)floor(fy), k0 = (int)floor(fz);
+        const double t[3] = {fx - i0, fy - j0, fz - k0};
+        for (int b = 0; b < 8; ++b)
+        {
+            const int o[3] = {b & 1, (b >> 1) & 1, b >> 2};
+            const int gi = i0 + o[0], gj = j0 + o[1], gk = k0 + o[2];
+            if (!cell_in_grid(h, gi, gj, gk)) continue;
+            const size_t id = loc(h, gi + 1, gj + 1, gk + 1);
+            if (h->mask[id] != FLUID) continue;
+            double f1[3], d1[3];
+            for (int a = 0; a < 3; ++a)
+            {
+                f1[a] = o[a] ? t[a] : 1.0 - t[a];
+                d1[a] = (o[a] ? 1.0 : -1.0) / DX;
+            }
+            idx[n] = id;
+            w[n] = f1[0] * f1[1] * f1[2];
+            dw[3 * n] = d1[0] * f1[1] * f1[2];
+            dw[3 * n + 1] = f1[0] * d1[1] * f1[2];
+            dw[3 * n + 2] = f1[0] * f1[1] * d1[2];
+            ++n;
+        }
+    }
+    else
+    {
+        const int R = s->s.radius;
+        const double sig2 = (s->s.sigma_cells * DX) * (s->s.sigma_cells * DX);
+        const int ic = (int)floor((s->cx - c->x_min) / DX), jc = (int)floor((s->cy - c->y_min) / DX),
+                  kc = (int)floor((s->cz - c->z_min) / DX);
+        if (ic < -R || ic >= h->NXg + R || jc < -R || jc >= h->NYg + R || kc < -R || kc >= h->NZg + R) return 0;
+        for (int gk = kc - R; gk <= kc + R; ++gk)
+            for (int gj = jc - R; gj <= jc + R; ++gj)
+                for (int gi = ic - R; gi <= ic + R; ++gi)
+                {
+                    if (!cell_in_grid(h, gi, gj, gk)) continue;
+                    const size_t id = loc(h, gi + 1, gj + 1, gk + 1);
+                    if (h->mask[id] != FLUID) continue;
+                    const double d[3] = {c->x_min + (gi + 0.5) * DX - s->cx, c->y_min + (gj + 0.5) * DX - s->cy,
+                                         c->z_min + (gk + 0.5) * DX - s->cz};
+                    idx[n] = id;
+                    w[n] = exp(-0.5 * (d[0] * d[0] + d[1] * d[1] + d[2] * d[2]) / sig2);
+                    for (int a = 0; a < 3; ++a) dw[3 * n + a] = w[n] * d[a] / sig2;
+                    ++n;
+                }
+    }
+    double S = 0.0, dS[3] = {0.0, 0.0, 0.0};
+    for (int m = 0; m < n; ++m)
+    {
+        S += w[m];
+        for (int a = 0; a < 3; ++a) dS[a] += dw[3 * m + a];
+    }
+    if (S < 1e-30) return 0;
+    for (int m = 0; m < n; ++m)
+    {
+        wh[m] = w[m] / S;
+        for (int a = 0; a < 3; ++a) dwh[3 * m + a] = dw[3 * m + a] / S - w[m] * dS[a] / (S * S);
+    }
+    return n;
+}
+
+/* macroscopic state of populations g: r = sum g, u = sum c g / r */
+static void adj_macro(const double* g, double* r, double* u)
+{
+    double s = 0.0, m[3] = {0.0, 0.0, 0.0};
+    for (int q = 0; q < Q; ++q)
+    {
+        s += g[q];
+        m[0] += g[q] * EX[q];
+        m[1] += g[q] * EY[q];
+        m[2] += g[q] * EZ[q];
+    }
+    *r = s;
+    for (int a = 0; a < 3; ++a) u[a] = m[a] / s;
+}
+
+/* For weights lam: a = sum_q lam_q feq_q(r,u) / r and
+ * b_a = sum_q lam_q W_q r (3 c_qa + 9 (c_q.u) c_qa - 3 u_a), so that
+ * sum_q lam_q d feq_q / d g_p = a d r/d g_p + b . d u / d g_p. */
+static void adj_feq_weights(const double* lam, double r, const double* u, double* a, double* b)
+{
+    *a = 0.0;
+    b[0] = b[1] = b[2] = 0.0;
+    for (int q = 0; q < Q; ++q)
+    {
+        const double cq[3] = {EX[q], EY[q], EZ[q]};
+        const double cu = cq[0] * u[0] + cq[1] * u[1] + cq[2] * u[2];
+        *a += lam[q] * feq(q, r, u[0], u[1], u[2]) / r;
+        for (int k = 0; k < 3; ++k) b[k] += lam[q] * W[q] * r * (3.0 * cq[k] + 9.0 * cu * cq[k] - 3.0 * u[k]);
+    }
+}
+
+/* lamF = J_bgk(F)^T lamG at one FLUID cell (sponge s, omega om). */
+static void adj_bgk(const double* F, const double* lamG, double om, double s, double* lamF)
+{
+    double r, u[3], a, b[3];
+    adj_macro(F, &r, u);
+    adj_feq_weights(lamG, r, u, &a, b);
+    const double keep = s > 1e-12 ? 1.0 - s : 1.0;
+    for (int p = 0; p < Q; ++p)
+    {
+        const double cp[3] = {EX[p], EY[p], EZ[p]};
+        double t = a;
+        for (int k = 0; k < 3; ++k) t += b[k] * (cp[k] - u[k]) / r;
+        lamF[p] = keep * ((1.0 - om) * lamG[p] + om * t);
+    }
+}
+
+/* Adds J_ghost^T lamB to lamI for the open-boundary ghost built from
+ * interior populations gI (nscbc_ghost). */
+static void adj_ghost(const double* gI, const double* lamB, int axis, int side, double* lamI)
+{
+    double rI, u[3];
+    adj_macro(gI, &rI, u);
+    const double pI = CS2 * (rI - 1.0);
+    const double W_ = side == 0 ? u[axis] - pI / CS : u[axis] + pI / CS;
+    const double pB = side == 0 ? -0.5 * CS * W_ : 0.5 * CS * W_;
+    const double rhoB = 1.0 + pB / CS2;
+    double uB[3] = {u[0], u[1], u[2]};
+    uB[axis] = 0.5 * W_;
+    double aB, bB[3], aI, bI[3];
+    adj_feq_weights(lamB, rhoB, uB, &aB, bB);
+    adj_feq_weights(lamB, rI, u, &aI, bI);
+    for (int p = 0; p < Q; ++p)
+    {
+        const double cp[3] = {EX[p], EY[p], EZ[p]};
+        double du[3];
+        for (int k = 0; k < 3; ++k) du[k] = (cp[k] - u[k]) / rI;   /* d u_k / d g_p */
+        const double dW = du[axis] + (side == 0 ? -CS : CS);       /* dp_I/dg_p = CS2, / CS */
+        const double drhoB = (side == 0 ? -0.5 : 0.5) * CS * dW / CS2;
+        double duB[3] = {du[0], du[1], du[2]};
+        duB[axis] = 0.5 * dW;
+        double t = lamB[p] + aB * drhoB - aI;
+        for (int k = 0; k < 3; ++k) t += bB[k] * duB[k] - bI[k] * du[k];
+        lamI[p] += t;
+    }
+}
+
+int orc_adjoint_grad(orc_handle* h, int nsteps, const double* observed, int K, double* loss, double* grad_pos,
+                     double* grad_signal, double* predicted)
+{
+    if (h->nsrc != 1 || h->nprobe < 1 || nsteps < 1 || h->step != 0) return LBM_ERR_STATE;
+    if (K < 1) K = (int)ceil(sqrt((double)nsteps));
+    if (K > nsteps) K = nsteps;
+    const int T = nsteps, NC = (T + K - 1) / K, np = h->nprobe;
+    const int nx = h->nx, ny = h->ny, nz = h->nz;
+    const size_t NF = h->Nloc * Q;
+    const double om = 1.0 / h->cfg.tau;
+    const lbm_config* c = &h->cfg;
+    src_t* S = &h->srcs[0];
+    double* rest = (double*)malloc(NF * sizeof(double));
+    double* ck = (double*)malloc((size_t)NC * NF * sizeof(double));
+    double* store = (double*)malloc((size_t)K * NF * sizeof(double));
+    double* lamG = (double*)calloc(NF, sizeof(double));
+    double* lamF = (double*)calloc(NF, sizeof(double));
+    double* lamH = (double*)calloc(NF, sizeof(double));
+    double* pred = (double*)malloc((size_t)T * np * sizeof(double));
+    double* res = (double*)calloc((size_t)T * np, sizeof(double));
+    double* mass = (double*)malloc((size_t)T * sizeof(double));
+    if (!rest || !ck || !store || !lamG || !lamF || !lamH || !pred || !res || !mass)
+    {
+        free(rest); free(ck); free(store); free(lamG); free(lamF); free(lamH); free(pred); free(res); free(mass);
+        return LBM_ERR_OUT_OF_MEMORY;
+    }
+    memcpy(rest, h->f_curr, NF * sizeof(double));
+
+    /* forward: checkpoints before the source of steps 0, K, 2K, ... */
+    for (int s = 0; s < T; ++s)
+    {
+        if (s % K == 0) memcpy(ck + (size_t)(s / K) * NF, h->f_curr, NF * sizeof(double));
+        const double t = s * h->dt;
+        mass[s] = source_value(h, S, t) * h->dt * S->s.gain;
+        orc_apply_source(h, t);
+        orc_exchange_halos(h);
+        orc_step_collision_bgk(h);
+        for (int p = 0; p < np; ++p)
+            pred[(size_t)s * np + p] = h->probe_idx[p] >= 0 ? h->rho[h->probe_idx[p]] - 1.0 : NAN;
+    }
+    double Ls = 0.0;
+    for (int s = 0; s < T; ++s)
+        for (int p = 0; p < np; ++p)
+        {
+            const size_t n = (size_t)s * np + p;
+            if (h->probe_idx[p] < 0 || isnan(observed[n])) continue;
+            const double r = pred[n] - observed[n];
+            Ls += 0.5 * r * r;
+            if (h->mask[h->probe_idx[p]] == FLUID) res[n] = r;
+        }
+
+    /* backward, one checkpoint segment at a time */
+    size_t cidx[125];
+    double wh[125], dwh[375];
+    double gp[3] = {0.0, 0.0, 0.0};
+    for (int g = NC - 1; g >= 0; --g)
+    {
+        const int a0 = g * K, a1 = (a0 + K < T) ? a0 + K : T;
+        memcpy(h->f_curr, ck + (size_t)g * NF, NF * sizeof(double));
+        for (int s = a0; s < a1; ++s)
+        {
+            orc_apply_source(h, s * h->dt);
+            orc_exchange_halos(h);
+            memcpy(store + (size_t)(s - a0) * NF, h->f_curr, NF * sizeof(double));
+            if (s + 1 < a1) orc_step_collision_bgk(h);
+        }
+        for (int s = a1 - 1; s >= a0; --s)
+        {
+            const double* Ht = store + (size_t)(s - a0) * NF;
+            /* lamF = J_bgk^T lamG; SOLID cells pass through */
+            #pragma omp parallel for collapse(2)
+            for (int k = 1; k <= nz; ++k)
+                for (int j = 1; j <= ny; ++j)
+                    for (int i = 1; i <= nx; ++i)
+                    {
+                        const size_t y = loc(h, i, j, k);
+                        if (h->mask[y] == SOLID)
+                        {
+                            for (int q = 0; q < Q; ++q) lamF[y * Q + q] = lamG[y * Q + q];
+                            continue;
+                        }
+                        double F[Q];
+                        for (int q = 0; q < Q; ++q)
+                        {
+                            const size_t src = loc(h, i - EX[q], j - EY[q], k - EZ[q]);
+                            F[q] = h->mask[src] == SOLID ? Ht[y * Q + h->inv_q[q]] : Ht[src * Q + q];
+                        }
+                        adj_bgk(F, lamG + y * Q, om, h->sponge[y], lamF + y * Q);
+                    }
+            for (int p = 0; p < np; ++p)
+                if (h->probe_idx[p] >= 0)
+                    for (int q = 0; q < Q; ++q) lamF[(size_t)h->probe_idx[p] * Q + q] += res[(size_t)s * np + p];
+            /* lamHt = pull^T lamF (scatter, serial: targets overlap) */
+            memset(lamH, 0, NF * sizeof(double));
+            for (int k = 1; k <= nz; ++k)
+                for (int j = 1; j <= ny; ++j)
+                    for (int i = 1; i <= nx; ++i)
+                    {
+                        const size_t y = loc(h, i, j, k);
+                        for (int q = 0; q < Q; ++q)
+                        {
+                            const size_t src = loc(h, i - EX[q], j - EY[q], k - EZ[q]);
+                            if (h->mask[src] == SOLID) lamH[y * Q + h->inv_q[q]] += lamF[y * Q + q];
+                            else lamH[src * Q + q] += lamF[y * Q + q];
+                        }
+                    }
+            /* ghosts of the open faces back onto their interior cells */
+            for (int f = 0; f < 6; ++f)
+            {
+                if (c->face_bc[f] != LBM_BC_NSCBC) continue;
+                const int axis = f / 2, side = f % 2;
+                const int n0 = axis == 0 ? ny : nx, n1 = axis == 2 ? ny : nz;
+                for (int v = 1; v <= n1; ++v)
+                    for (int u = 1; u <= n0; ++u)
+                    {
+                        int I[3], G[3];
+                        if (axis == 0) { I[1] = G[1] = u; I[2] = G[2] = v; }
+                        else if (axis == 1) { I[0] = G[0] = u; I[2] = G[2] = v; }
+                        else { I[0] = G[0] = u; I[1] = G[1] = v; }
+                        const int nn[3] = {nx, ny, nz};
+                        I[axis] = side ? nn[axis] : 1;
+                        G[axis] = side ? nn[axis] + 1 : 0;
+                        const size_t iI = loc(h, I[0], I[1], I[2]), iG = loc(h, G[0], G[1], G[2]);
+                        adj_ghost(Ht + iI * Q, lamH + iG * Q, axis, side, lamH + iI * Q);
+                    }
+            }
+            /* source: mu_s and nu_s; lamG of step s-1 = lamH on interior cells */
+            drone_update(S, s * h->dt);
+            const int n = adj_source_cells(h, S, cidx, wh, dwh);
+            double mu = 0.0, nu[3] = {0.0, 0.0, 0.0};
+            for (int m = 0; m < n; ++m)
+            {
+                double lw = 0.0;
+                for (int q = 0; q < Q; ++q) lw += W[q] * lamH[cidx[m] * Q + q];
+                mu += wh[m] * lw;
+                for (int a = 0; a < 3; ++a) nu[a] += dwh[3 * m + a] * lw;
+            }
+            if (grad_signal) grad_signal[s] = mu * h->dt * S->s.gain;
+            for (int a = 0; a < 3; ++a) gp[a] += mass[s] * nu[a];
+            memset(lamG, 0, NF * sizeof(double));
+            for (int k = 1; k <= nz; ++k)
+                for (int j = 1; j <= ny; ++j)
+                    for (int i = 1; i <= nx; ++i)
+                    {
+                        const size_t y = loc(h, i, j, k);
+                        for (int q = 0; q < Q; ++q) lamG[y * Q + q] = lamH[y * Q + q];
+                    }
+        }
+    }
+    if (grad_pos) for (int a = 0; a < 3; ++a) grad_pos[a] = gp[a];
+    if (predicted) memcpy(predicted, pred, (size_t)T * np * sizeof(double));
+    *loss = Ls;
+    memcpy(h->f_curr, rest, NF * sizeof(double));
+    for (size_t i = 0; i < h->Nloc; ++i) h->rho[i] = 1.0;
+    h->step = 0;
+    free(rest); free(ck); free(store); free(lamG); free(lamF); free(lamH); free(pred); free(res); free(mass);
+    return LBM_OK;
+}

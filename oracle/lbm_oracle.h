@@ -41,6 +41,13 @@ void orc_step_collision_bgk(orc_handle* h);
 void orc_record_probes(orc_handle* h);
 void orc_step(orc_handle* h, int nsteps);
 void orc_set_threads(int n);
+/* FP64 discrete adjoint of orc_step for L = 1/2 sum (probe - observed)^2 over
+ * nsteps steps from the state after orc_init (no counterpart in the
+ * reference); K: checkpoint interval (<= 0: sqrt(nsteps)).  grad_signal[s] =
+ * dL/d(source value at step s), grad_pos = dL/d(rigid shift of the source
+ * path).  Restores the initial state. */
+int orc_adjoint_grad(orc_handle* h, int nsteps, const double* observed, int K, double* loss, double* grad_pos,
+                     double* grad_signal, double* predicted);
 
 void orc_get_dims(orc_handle* h, int* n3, int* n3_halo);
 double orc_get_dt(orc_handle* h);

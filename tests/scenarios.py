@@ -93,6 +93,83 @@ def scenario(name, storage=abi.LBM_STORE_F32, f16_scale=1.0):
     raise KeyError(name)
 
 
+def adjoint_scenario(nx=48, ny=40, nz=24, steps=160, injection=abi.LBM_INJECT_TRILINEAR, speed=0.0, nprobe=16,
+                     seed=11):
+    """Transient localisation on a synthetic-city patch (a reduced version of
+    the 256x256x128, 3000-step case): a true source at street level emits a
+    Ricker wavelet (period 30 steps); receivers at street level record it; the
+    trial source sits 1-2 cells away.  Returns dict(cfg, true, trial, probes,
+    triangles, steps, observed) with `observed` from the FP64 oracle."""
+    import nlos_lbm
+    from oracle import OracleSolver
+
+    tris, _ = nlos_lbm.city_triangles(nx, ny, seed=seed, fp=(8, 14), height=(4, 16), street=5, margin=3)
+    cfg = lattice_config(nx, ny, nz, 0.52, sponge_width=6.0, sponge_faces=FIVE_FACES)
+    mask = nlos_lbm.voxelize(cfg, tris).reshape(nz + 2, ny + 2, nx + 2)
+    rng = np.random.default_rng(seed)
+
+    def street_point(z, used):
+        while True:
+            x, y = rng.uniform(5, nx - 5), rng.uniform(5, ny - 5)
+            c = (int(x), int(y), int(z))
+            ok = all(mask[c[2] + 1 + dz, c[1] + 1 + dy, c[0] + 1 + dx] == 0
+                     for dx in (-2, -1, 0, 1, 2) for dy in (-2, -1, 0, 1, 2) for dz in (-1, 0, 1))
+            if ok and c not in used:
+                used.add(c)
+                return x, y, z
+
+    used = set()
+    tx, ty, tz = street_point(3.6, used)
+    # trial position: displaced, with fractional parts away from the trilinear cell edges
+    px = np.floor(tx + 1.4) + 0.83
+    py = np.floor(ty - 0.9) + 0.29
+    pz = 4.12
+    probes = np.array([street_point(rng.uniform(1.5, 6.5), used) for _ in range(nprobe)])
+
+    def src(x, y, z):
+        return abi.reference_source(sx=x, sy=y, sz=z, ex=x + (40.0 if speed else 0.0), ey=y, ez=z, speed=speed,
+                                    amp=1e-3, freq=1.0 / 30.0, t0=30.0, waveform=abi.LBM_WAVE_RICKER,
+                                    injection=injection, radius=2, sigma_cells=1.0)
+
+    true_src, trial = src(tx, ty, tz), src(px, py, pz)
+    o = OracleSolver(cfg, [true_src], probes, triangles=tris)
+    o.step(steps)
+    observed = o.get_probes()
+    return dict(cfg=cfg, true=true_src, trial=trial, probes=probes, triangles=tris, steps=steps,
+                observed=observed)
+
+
+def source_copy(src, shift=(0.0, 0.0, 0.0), table=None):
+    """Copy of an lbm_source with its path shifted rigidly by `shift` and,
+    with `table`, the waveform replaced by that per-step signal (amp 1).
+    The table array must outlive the source: it is returned alongside."""
+    names = [f[0] for f in abi.LbmSource._fields_]
+    kw = {n: getattr(src, n) for n in names if n not in ("table", "table_len")}
+    for a, n in enumerate(("sx", "sy", "sz")):
+        kw[n] += shift[a]
+    for a, n in enumerate(("ex", "ey", "ez")):
+        kw[n] += shift[a]
+    keep = None
+    if table is not None:
+        keep = np.ascontiguousarray(table, dtype=np.float64)
+        kw.update(waveform=abi.LBM_WAVE_TABLE, amp=1.0, table=keep.ctypes.data_as(abi.c_double_p),
+                  table_len=len(keep))
+    return abi.reference_source(**kw), keep
+
+
+def source_signal(src, steps, dt):
+    """val(t_s) of a Ricker source at steps 0..steps-1 (the forward's waveform)."""
+    t = np.arange(steps) * dt
+    a = (np.pi * src.freq * (t - src.t0)) ** 2
+    return src.amp * (1.0 - 2.0 * a) * np.exp(-a)
+
+
+def misfit(pred, observed):
+    """1/2 sum (pred - observed)^2 over the probes inside the grid (FP64)."""
+    m = np.isfinite(pred[0])
+    return 0.5 * float(np.sum((pred[:, m] - observed[:, m]) ** 2))
+
+
 def build_pair(sc):
     """(CUDA solver, FP64 oracle) for one scenario."""
     from nlos_lbm import Solver
