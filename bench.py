@@ -212,7 +212,7 @@ def e2e_measure(solver, w, steps):
     return (t1 - t0) * 1e3, (h1 - h0) / steps, (d1 - d0) / steps
 
 
-def adjoint_measure(device, torch, reps=1, ckpt=(200, 20)):
+def adjoint_measure(device, torch, reps=1, ckpt=(200, 0)):
     """Gradients per second of lbm_adjoint_grad on the 256x256x128 patch
     (3000 steps, 64 receivers): observed series from a forward run of the
     true source, then the misfit gradient at the trial source, timed with CUDA
@@ -227,6 +227,7 @@ def adjoint_measure(device, torch, reps=1, ckpt=(200, 20)):
     observed = truth.get_probes()
     truth.close()
     s = nlos_lbm.Solver(w["cfg"], w["sources"], w["probes"], triangles=w["triangles"])
+    k_outer, k_inner, dev_bytes, fwd_steps = s.adjoint_plan(w["steps"], *ckpt)
     stream = torch.cuda.ExternalStream(s.stream)
     s.adjoint_grad(observed[:100], *ckpt)   # warm-up (allocations, first launches)
     times = []
@@ -243,7 +244,8 @@ def adjoint_measure(device, torch, reps=1, ckpt=(200, 20)):
     nx, ny, nz = workloads.cells(w["cfg"])
     ms = float(np.median(times))
     return {"workload": "adjoint256: " + w["description"], "grad_per_s": 1e3 / ms, "ms_per_grad": ms,
-            "steps": w["steps"], "cells": nx * ny * nz, "ckpt_outer_inner": list(ckpt), "loss": loss,
+            "steps": w["steps"], "cells": nx * ny * nz, "ckpt_outer_inner": [k_outer, k_inner],
+            "device_gb": dev_bytes / 1e9, "forward_steps": fwd_steps, "loss": loss,
             "grad_pos": [float(v) for v in gpos], "grad_signal_norm": float(np.linalg.norm(gsig)),
             "launches": launches, "fwd_equiv_glups": nx * ny * nz * w["steps"] / (ms / 1e3) / 1e9}
 

@@ -165,26 +165,24 @@ __global__ void __launch_bounds__(128) k_adj_ghost(AdjGhostArgs a)
     const long long lt = t - F.first;
     const int u = (int)(lt % F.nu), v = (int)(lt / F.nu);
     const Layout& L = a.L;
-    int ci, cj, ck, gi, gj, gk;
+    // ghost cell g (the forward ghost kernel's enumeration of the face)
+    int gi, gj, gk;
     if (F.axis == 0)
     {
-        cj = gj = 1 + u;
-        ck = gk = 1 + v;
-        ci = F.side ? L.nx : 1;
         gi = F.side ? L.nx + 1 : 0;
+        gj = 1 + u;
+        gk = 1 + v;
     }
     else if (F.axis == 1)
     {
-        ci = gi = 1 + u;
-        ck = gk = 1 + v;
-        cj = F.side ? L.ny : 1;
+        gi = 1 + u;
         gj = F.side ? L.ny + 1 : 0;
+        gk = 1 + v;
     }
     else
     {
-        ci = gi = 1 + u;
-        cj = gj = 1 + v;
-        ck = F.side ? L.nz : 1;
+        gi = 1 + u;
+        gj = 1 + v;
         gk = F.side ? L.nz + 1 : 0;
     }
     // lamHt at the ghost: what the interior cells y = g + e_q pulled from it
@@ -200,19 +198,8 @@ __global__ void __launch_bounds__(128) k_adj_ghost(AdjGhostArgs a)
         lh[q] = v;
     }
     // moments of the interior cell the ghost was built from
-    float rho = 0.f, jx = 0.f, jy = 0.f, jz = 0.f;
-#pragma unroll
-    for (int q = 0; q < Q; ++q)
-    {
-        const float g = a.fwd[L.elem(q, ci, cj, ck)];
-        rho += g;
-        if (ex(q) > 0) jx += g;
-        if (ex(q) < 0) jx -= g;
-        if (ey(q) > 0) jy += g;
-        if (ey(q) < 0) jy -= g;
-        if (ez(q) > 0) jz += g;
-        if (ez(q) < 0) jz -= g;
-    }
+    const float4 m = __ldg(a.face_mom + t);
+    const float rho = m.x, jx = m.y, jy = m.z, jz = m.w;
     D4 D[Q];
     nscbc_delta4(D4{rho, {1.f, 0.f, 0.f, 0.f}}, D4{jx, {0.f, 1.f, 0.f, 0.f}}, D4{jy, {0.f, 0.f, 1.f, 0.f}},
                  D4{jz, {0.f, 0.f, 0.f, 1.f}}, F.axis, F.side, D);
@@ -227,74 +214,318 @@ __global__ void __launch_bounds__(128) k_adj_ghost(AdjGhostArgs a)
         a.gadj[off + (long long)p * n + lt] = lh[p] + vk[0] + ex(p) * vk[1] + ey(p) * vk[2] + ez(p) * vk[3];
 }
 
-// lamF^{s-1} = J_C(F^{s-1})^T lamH^s.  With F the pulled populations,
+__device__ __forceinline__ uint32_t near_bits(const StepArgs& a, const Layout& L, int col, int j, int k)
+{
+    return a.near[((long long)k * (L.ny + 2) + j) * L.words_per_row + (col >> 5)] >> (col & 31);
+}
+
+__device__ __forceinline__ float2 ldg2(const float* p) { return __ldg(reinterpret_cast<const float2*>(p)); }
+
+// packed FP32x2 arithmetic (sm_100): both cells of a pair in one instruction
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, f2(-1.0f), a); }
+// c_q . (x, y, z) for a pair head q (components 0 or +-1)
+__device__ __forceinline__ float2 cdot(int q, float2 x, float2 y, float2 z)
+{
+    float2 r = f2(0.f);
+    bool any = false;
+    if (ex(q)) r = ex(q) > 0 ? x : mul2(x, f2(-1.f)), any = true;
+    if (ey(q)) r = any ? (ey(q) > 0 ? add2(r, y) : sub2(r, y)) : (ey(q) > 0 ? y : mul2(y, f2(-1.f))), any = true;
+    if (ez(q)) r = any ? (ez(q) > 0 ? add2(r, z) : sub2(r, z)) : (ez(q) > 0 ? z : mul2(z, f2(-1.f)));
+    return r;
+}
+
+// Pair (c0 + d, c0 + 1 + d), d = -1, 0, +1, of the row whose element of
+// column c0 is at `row` (block-interleaved layout, 32-cell blocks): one
+// aligned float2 per lane; the +-1 shift takes the neighbour element from the
+// adjacent lane and, at the warp edge, from the adjacent block (the same
+// scheme as the forward step).  Every lane of the warp must call it.
+template <int D>
+__device__ __forceinline__ float2 shifted_pair(const float* row, int lane)
+{
+    constexpr int BC = 32, BE = 19 * BC;
+    const float2 cur = ldg2(row);
+    if (D == 0) return cur;
+    if (D < 0)
+    {
+        float prev = __shfl_up_sync(kFull, cur.y, 1);
+        if (lane == 0) prev = ldg2(row - BE + (BC - 2)).y;
+        return make_float2(prev, cur.x);
+    }
+    float next = __shfl_down_sync(kFull, cur.x, 1);
+    if (lane == 31) next = ldg2(row + BE - (BC - 2)).x;
+    return make_float2(cur.y, next);
+}
+
+// Each block asks L2 for the lines that the same tile `dist` rows later will
+// read: the 19 lamF lines of each interleaved block from the neighbour rows,
+// and the moment lines of the row itself.  Prefetches hold no registers, so
+// they add loads in flight beyond what the register budget allows.
+template <int TILE>
+__device__ __forceinline__ void prefetch_ahead(const AdjStepArgs& a, int dist, int j, int k, int col0)
+{
+    constexpr int BC = 32, NBLK = TILE / BC, NMOM = TILE * 16 / 128;
+    const Layout& L = a.L;
+    const long long r = (long long)(k - 1) * L.ny + (j - 1) + dist;
+    if (r >= (long long)L.ny * L.nz) return;
+    const int jj = 1 + (int)(r % L.ny), kk = 1 + (int)(r / L.ny);
+    for (int t = threadIdx.x; t < 19 * NBLK + NMOM; t += blockDim.x)
+    {
+        const void* p;
+        if (t < 19 * NBLK)
+        {
+            const int q = t / NBLK, b = t - q * NBLK;
+            const int col = col0 + b * BC;
+            if (col >= L.nx) continue;
+            p = a.lam_in + L.elem(q, col + 1, jj + ey(q), kk + ez(q));
+        }
+        else
+        {
+            const int col = col0 + (t - 19 * NBLK) * 8;
+            if (col >= L.nx) continue;
+            p = a.mom_prev + (((long long)(kk - 1) * L.ny + (jj - 1)) * L.nx + col);
+        }
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+    }
+}
+
+// lamF^{s-1} = J_C(F^{s-1})^T lamH^s for two x-adjacent cells per thread.
+// With F the pulled populations (only their stored moments are read),
 // rho' = sum F, J = sum c F, r = 1 + rho':
 //   (J_C^T l)_p = a l_p + b (A + c_p . B)
 //   A = sum_q l_q w_q (1 - (4.5 (c_q.J)^2 - 1.5 J^2) / r^2)
 //   B = sum_q l_q w_q (3 c_q + (9 (c_q.J) c_q - 3 J) / r)
-// with a = (1 - sigma)(1 - omega), b = (1 - sigma) omega; SOLID cells copy.
-__global__ void __launch_bounds__(128) k_adj_step(AdjStepArgs a)
+// a = (1 - sigma)(1 - omega), b = (1 - sigma) omega; SOLID cells copy.
+// lamH (gather of lamF^s with the bounce-back terms) stays in registers for
+// the output.  J_C^T is linear in lamH, so the ghost-adjoint terms of the
+// open-face cells are applied afterwards by k_adj_face.
+template <int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) k_adj_step(AdjStepArgs a)
 {
+    constexpr int BC = 32;
     const Layout& L = a.L;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
-    if (i > L.nx) return;
+    const int lane = threadIdx.x & 31;
+    const int c0r = 2 * (blockIdx.x * BLOCK + threadIdx.x);
+    const bool active = c0r < L.nx;
+    const int c0 = active ? c0r : ((L.nx - 1) & ~1);   // inactive lanes shadow a valid pair
     const int j = blockIdx.y + 1, k = blockIdx.z + 1;
-    float lg[Q];
-    gather_lam(L, a.sa.links, a.lam_in, a.gadj, a.gadj_off, i, j, k, lg);
+    const long long e0 = L.elem(0, c0 + 1, j, k);
+    const long long rs = L.row_stride, ps = L.plane_stride;
+
+    if (a.prefetch_rows > 0) prefetch_ahead<2 * BLOCK>(a, a.prefetch_rows, j, k, 2 * BLOCK * blockIdx.x);
+
+    uint32_t lk0 = 0, lk1 = 0;
+    if (active)
+    {
+        const uint32_t b = near_bits(a.sa, L, c0, j, k) & 3u;
+        const long long cl = L.cell(c0 + 1, j, k);
+        if (b & 1u) lk0 = a.sa.links[cl];
+        if (b & 2u) lk1 = a.sa.links[cl + 1];
+    }
+    const bool any_link = __any_sync(kFull, (lk0 | lk1) != 0u);
+    const bool xlo = c0 == 0;                 // first cell at i = 1
+    const bool xhi0 = c0 == L.nx - 1;         // first cell at i = nx (nx odd)
+    const bool xhi1 = c0 + 1 == L.nx - 1;     // second cell at i = nx
+    const bool has1 = c0 + 1 < L.nx;
+
+    // ---- moments of F^{s-1}, stored by the forward recomputation
+    float2 rho, jx, jy, jz;
+    {
+        const long long mi = ((long long)(k - 1) * L.ny + (j - 1)) * L.nx + c0;
+        const float4 m0 = __ldg(a.mom_prev + mi);
+        const float4 m1 = has1 ? __ldg(a.mom_prev + mi + 1) : m0;
+        rho = make_float2(m0.x, m1.x);
+        jx = make_float2(m0.y, m1.y);
+        jy = make_float2(m0.z, m1.z);
+        jz = make_float2(m0.w, m1.w);
+    }
+
+    // ---- lamH^s of the pair: transposed pull of lamF^s.  Cell y + e_q pulled
+    // direction q from y; rows outside the interior pulled nothing, and there
+    // the adjoint buffers hold 0 (their halo rows are never written), so the
+    // loads need no row test.
+    const bool solid0 = (lk0 & kSolidSelfBit) != 0u, solid1 = (lk1 & kSolidSelfBit) != 0u;
+    float2 lg[Q];
+    {
+        const float* own = a.lam_in + e0;
+#pragma unroll
+        for (int q = 0; q < Q; ++q)
+        {
+            const float* row = own + (ey(q) * rs + ez(q) * ps) + q * BC;
+            if (ex(q) == 0) lg[q] = shifted_pair<0>(row, lane);
+            else if (ex(q) > 0) lg[q] = shifted_pair<1>(row, lane);
+            else lg[q] = shifted_pair<-1>(row, lane);
+        }
+        // columns outside the interior pulled nothing (and the neighbour block
+        // read there may belong to another row)
+        if (xlo | xhi0 | xhi1)
+        {
+#pragma unroll
+            for (int q = 0; q < Q; ++q)
+            {
+                if (ex(q) < 0 && xlo) lg[q].x = 0.f;
+                if (ex(q) > 0 && xhi0) lg[q].x = 0.f;
+                if (ex(q) > 0 && xhi1) lg[q].y = 0.f;
+            }
+        }
+        if (any_link)
+        {
+            // a SOLID cell is pulled from by nobody (its neighbours bounce back) ...
+#pragma unroll
+            for (int q = 0; q < Q; ++q)
+            {
+                if (solid0) lg[q].x = 0.f;
+                if (solid1) lg[q].y = 0.f;
+            }
+            // ... and y pulled direction inv(q) from itself when y + e_q is SOLID
+#pragma unroll
+            for (int q = 0; q < Q; ++q)
+            {
+                if (((lk0 | lk1) >> inv(q)) & 1u)
+                {
+                    const float2 o = ldg2(own + inv(q) * BC);
+                    if ((lk0 >> inv(q)) & 1u) lg[q].x += o.x;
+                    if ((lk1 >> inv(q)) & 1u) lg[q].y += o.y;
+                }
+            }
+        }
+    }
+    if (!active) return;
+
+    // ---- J_C^T, packed FP32x2 over the pair, directions taken with their
+    // opposites (c_qb = -c_q, so both share c.J)
+    const float syz = fmaxf(a.sa.sig_y[j - 1], a.sa.sig_z[k - 1]);
+    const float sg0 = fmaxf(a.sa.sig_x[c0], syz), sg1 = fmaxf(has1 ? a.sa.sig_x[c0 + 1] : 0.f, syz);
+    float2 ca = make_float2((1.0f - sg0) * (1.0f - a.sa.omega), (1.0f - sg1) * (1.0f - a.sa.omega));
+    float2 cb = make_float2((1.0f - sg0) * a.sa.omega, (1.0f - sg1) * a.sa.omega);
+    if (solid0) ca.x = 1.0f, cb.x = 0.0f;
+    if (solid1) ca.y = 1.0f, cb.y = 0.0f;
+    if (!has1) ca.y = 0.0f, cb.y = 0.0f;   // no second cell: keep the padding column at 0
+    float2 r = add2(rho, f2(1.0f));
+    if (r.x <= 0.f) r.x = 1e-12f;
+    if (r.y <= 0.f) r.y = 1e-12f;
+    const float2 ir = make_float2(1.0f / r.x, 1.0f / r.y);
+    const float2 ir2 = mul2(ir, ir);
+    const float2 j2 = fma2(jz, jz, fma2(jy, jy, mul2(jx, jx)));
+    // s0 = sum w l, s1 = sum w l (c.J)^2, v = sum w l c, u = sum w l (c.J) c
+    float2 s0 = mul2(f2(wf(0)), lg[0]), s1 = f2(0.f);
+    float2 vx = f2(0.f), vy = vx, vz = vx, ux = vx, uy = vx, uz = vx;
+#pragma unroll
+    for (int p = 0; p < 9; ++p)
+    {
+        const int q = pair_head(p), qb = inv(q);
+        const float2 cj = cdot(q, jx, jy, jz);
+        const float2 sp = mul2(f2(wf(q)), add2(lg[q], lg[qb]));
+        const float2 dm = mul2(f2(wf(q)), sub2(lg[q], lg[qb]));
+        const float2 t = mul2(sp, cj);
+        s0 = add2(s0, sp);
+        s1 = fma2(t, cj, s1);
+        if (ex(q)) vx = ex(q) > 0 ? add2(vx, dm) : sub2(vx, dm), ux = ex(q) > 0 ? add2(ux, t) : sub2(ux, t);
+        if (ey(q)) vy = ey(q) > 0 ? add2(vy, dm) : sub2(vy, dm), uy = ey(q) > 0 ? add2(uy, t) : sub2(uy, t);
+        if (ez(q)) vz = ez(q) > 0 ? add2(vz, dm) : sub2(vz, dm), uz = ez(q) > 0 ? add2(uz, t) : sub2(uz, t);
+    }
+    // A = s0 (1 + 1.5 J^2 / r^2) - 4.5 s1 / r^2;  B = 3 v + (9 u - 3 J s0) / r
+    const float2 A = sub2(mul2(s0, fma2(mul2(j2, ir2), f2(1.5f), f2(1.0f))), mul2(mul2(s1, ir2), f2(4.5f)));
+    const float2 Bx = fma2(vx, f2(3.0f), mul2(sub2(mul2(ux, f2(9.0f)), mul2(mul2(jx, s0), f2(3.0f))), ir));
+    const float2 By = fma2(vy, f2(3.0f), mul2(sub2(mul2(uy, f2(9.0f)), mul2(mul2(jy, s0), f2(3.0f))), ir));
+    const float2 Bz = fma2(vz, f2(3.0f), mul2(sub2(mul2(uz, f2(9.0f)), mul2(mul2(jz, s0), f2(3.0f))), ir));
+    float* out = a.lam_out + e0;
+    const float2 cbA = mul2(cb, A);
+    *reinterpret_cast<float2*>(out) = fma2(ca, lg[0], cbA);
+#pragma unroll
+    for (int p = 0; p < 9; ++p)
+    {
+        const int q = pair_head(p), qb = inv(q);
+        const float2 cB = mul2(cb, cdot(q, Bx, By, Bz));
+        *reinterpret_cast<float2*>(out + q * BC) = fma2(ca, lg[q], add2(cbA, cB));
+        *reinterpret_cast<float2*>(out + qb * BC) = fma2(ca, lg[qb], sub2(cbA, cB));
+    }
+}
+
+// Ghost-adjoint terms of step s at the open-face cells: J_C(F^{s-1})^T of
+// the summed ghost-adjoint contributions, added to lamF^{s-1} after
+// k_adj_step.  One thread per face cell; a cell on several open faces (an
+// edge) is handled by the thread of the first such face only, so every cell
+// is updated once and in a fixed order.
+__global__ void __launch_bounds__(128) k_adj_face(AdjStepArgs a, GhostArgs ga)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ga.total) return;
+    int fi = 0;
+    while (fi + 1 < ga.nfaces && t >= ga.face[fi + 1].first) ++fi;
+    const GhostFace F = ga.face[fi];
+    const long long lt = t - F.first;
+    const int u = (int)(lt % F.nu), v = (int)(lt / F.nu);
+    const Layout& L = a.L;
+    int i, j, k;
+    if (F.axis == 0)
+    {
+        i = F.side ? L.nx : 1;
+        j = 1 + u;
+        k = 1 + v;
+    }
+    else if (F.axis == 1)
+    {
+        i = 1 + u;
+        j = F.side ? L.ny : 1;
+        k = 1 + v;
+    }
+    else
+    {
+        i = 1 + u;
+        j = 1 + v;
+        k = F.side ? L.nz : 1;
+    }
+    const bool at[6] = {i == 1, i == L.nx, j == 1, j == L.ny, k == 1, k == L.nz};
+    int owner = -1;
+    for (int f = 0; f < 6 && owner < 0; ++f)
+        if (at[f] && a.gadj_off[f] >= 0) owner = f;
+    if (owner != F.axis * 2 + F.side) return;
+    float g[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) g[q] = 0.f;
+#pragma unroll
+    for (int f = 0; f < 6; ++f)
+    {
+        if (!at[f] || a.gadj_off[f] < 0) continue;
+        const int axis = f / 2;
+        const long long n = face_cells(L, axis), c = face_cell(L, axis, i, j, k);
+#pragma unroll
+        for (int q = 0; q < Q; ++q) g[q] += a.gadj[a.gadj_off[f] + (long long)q * n + c];
+    }
     const uint32_t lk = a.sa.links[L.cell(i, j, k)];
-    const long long e0 = L.elem(0, i, j, k);
+    float* out = a.lam_out + L.elem(0, i, j, k);
     if (lk & kSolidSelfBit)
     {
 #pragma unroll
-        for (int q = 0; q < Q; ++q) a.lam_out[e0 + q * L.bc] = lg[q];
+        for (int q = 0; q < Q; ++q) out[q * L.bc] += g[q];
         return;
     }
-    // F^{s-1}: pull from Ht^{s-1} with bounce-back and x-face ghosts
-    float F[Q];
-#pragma unroll
-    for (int q = 0; q < Q; ++q)
-    {
-        const int si = i - ex(q);
-        if ((lk >> q) & 1u) F[q] = a.fwd_prev[L.elem(inv(q), i, j, k)];
-        else if (si == 0) F[q] = a.xgh_prev[a.sa.xf.gh_index(0, q, j - ey(q), k - ez(q), L.ny, L.nz)];
-        else if (si == L.nx + 1) F[q] = a.xgh_prev[a.sa.xf.gh_index(1, q, j - ey(q), k - ez(q), L.ny, L.nz)];
-        else F[q] = a.fwd_prev[L.elem(q, si, j - ey(q), k - ez(q))];
-    }
-    float rho = 0.f, jx = 0.f, jy = 0.f, jz = 0.f;
-#pragma unroll
-    for (int q = 0; q < Q; ++q)
-    {
-        rho += F[q];
-        if (ex(q) > 0) jx += F[q];
-        if (ex(q) < 0) jx -= F[q];
-        if (ey(q) > 0) jy += F[q];
-        if (ey(q) < 0) jy -= F[q];
-        if (ez(q) > 0) jz += F[q];
-        if (ez(q) < 0) jz -= F[q];
-    }
-    float r = 1.0f + rho;
+    const float4 m = a.mom_prev[((long long)(k - 1) * L.ny + (j - 1)) * L.nx + (i - 1)];
+    float r = 1.0f + m.x;
     if (r <= 0.f) r = 1e-12f;
     const float ir = 1.0f / r;
-    const float j2 = jx * jx + jy * jy + jz * jz;
+    const float j2 = m.y * m.y + m.z * m.z + m.w * m.w;
     float A = 0.f, Bx = 0.f, By = 0.f, Bz = 0.f;
 #pragma unroll
     for (int q = 0; q < Q; ++q)
     {
-        const float cj = (float)ex(q) * jx + (float)ey(q) * jy + (float)ez(q) * jz;
-        const float wl = wf(q) * lg[q];
+        const float cj = (float)ex(q) * m.y + (float)ey(q) * m.z + (float)ez(q) * m.w;
+        const float wl = wf(q) * g[q];
         A += wl * (1.0f - (4.5f * cj * cj - 1.5f * j2) * ir * ir);
-        const float t = 3.0f + 9.0f * cj * ir;
-        Bx += wl * ((float)ex(q) * t - 3.0f * jx * ir);
-        By += wl * ((float)ey(q) * t - 3.0f * jy * ir);
-        Bz += wl * ((float)ez(q) * t - 3.0f * jz * ir);
+        const float tq = 3.0f + 9.0f * cj * ir;
+        Bx += wl * ((float)ex(q) * tq - 3.0f * m.y * ir);
+        By += wl * ((float)ey(q) * tq - 3.0f * m.z * ir);
+        Bz += wl * ((float)ez(q) * tq - 3.0f * m.w * ir);
     }
     const float sg = fmaxf(a.sa.sig_x[i - 1], fmaxf(a.sa.sig_y[j - 1], a.sa.sig_z[k - 1]));
-    const float keep = 1.0f - sg;
-    const float ca = keep * (1.0f - a.sa.omega), cb = keep * a.sa.omega;
+    const float ca = (1.0f - sg) * (1.0f - a.sa.omega), cb = (1.0f - sg) * a.sa.omega;
 #pragma unroll
     for (int p = 0; p < Q; ++p)
-        a.lam_out[e0 + p * L.bc] =
-            ca * lg[p] + cb * (A + (float)ex(p) * Bx + (float)ey(p) * By + (float)ez(p) * Bz);
+        out[p * L.bc] += ca * g[p] + cb * (A + (float)ex(p) * Bx + (float)ey(p) * By + (float)ez(p) * Bz);
 }
 
 // Residual of each probe enters the adjoint of every population it summed.
@@ -356,10 +587,20 @@ cudaError_t launch_adj_ghost(const AdjGhostArgs& a, cudaStream_t stream)
     return cudaGetLastError();
 }
 
-cudaError_t launch_adj_step(const AdjStepArgs& a, cudaStream_t stream)
+cudaError_t launch_adj_step(const AdjStepArgs& a, const GhostArgs& ga, int variant, cudaStream_t stream)
 {
-    const dim3 g((unsigned)((a.L.nx + 127) / 128), (unsigned)a.L.ny, (unsigned)a.L.nz);
-    k_adj_step<<<g, 128, 0, stream>>>(a);
+    if (a.L.bc != 32) return cudaErrorInvalidValue;   // FP32 layout only
+    constexpr int kBlock = 128;
+    const dim3 g((unsigned)((a.L.nx + 2 * kBlock - 1) / (2 * kBlock)), (unsigned)a.L.ny, (unsigned)a.L.nz);
+    switch (variant)
+    {
+    case 1: k_adj_step<kBlock, 5><<<g, kBlock, 0, stream>>>(a); break;
+    case 2: k_adj_step<kBlock, 6><<<g, kBlock, 0, stream>>>(a); break;
+    default: k_adj_step<kBlock, 1><<<g, kBlock, 0, stream>>>(a); break;
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess || ga.total <= 0) return e;
+    k_adj_face<<<(unsigned)((ga.total + 127) / 128), 128, 0, stream>>>(a, ga);
     return cudaGetLastError();
 }
 

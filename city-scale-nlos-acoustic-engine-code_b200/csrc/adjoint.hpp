@@ -11,7 +11,10 @@
 //   dL/dm_s       = sum_cells w_hat_c sum_q w_q lamH^s[q](c)                              (source, additive)
 //   lamF^{s-1}    = J_C(F^{s-1})^T lamH^s + probe residuals of step s-1
 // The pull transposed is a gather: cell y collects what the cells y + e_q
-// pulled from it, so no atomics are needed.
+// pulled from it, so no atomics are needed.  J_C(F) depends on F only through
+// its moments (rho', J), and the ghost Jacobian on the moments of the interior
+// face cell, so the forward recomputation stores those moments per step
+// (16 bytes per cell) instead of the populations (76 bytes per cell).
 #pragma once
 
 #include <cstdint>
@@ -26,10 +29,10 @@ struct AdjStepArgs
     StepArgs sa;            // links, sponge, omega of the forward step
     const float* lam_in;    // lamF^s, population layout
     float* lam_out;         // lamF^{s-1}
-    const float* fwd_prev;  // Ht^{s-1} populations (pull source of F^{s-1})
-    const float* xgh_prev;  // x-face ghosts of step s-1
+    const float4* mom_prev; // moments (rho', J) of F^{s-1}, dense cell order (launch_step_moments)
     const float* gadj;      // ghost-adjoint contributions of step s, per open face
     long long gadj_off[6];  // offset of face f in gadj, -1 = face not open
+    int prefetch_rows;      // > 0: each block prefetches into L2 the lines of the row this far ahead
 };
 
 struct AdjGhostArgs
@@ -38,7 +41,7 @@ struct AdjGhostArgs
     GhostArgs ga;           // open faces (same enumeration as the forward ghost kernel)
     const uint32_t* links;
     const float* lam_in;    // lamF^s
-    const float* fwd;       // Ht^s populations (interior face cells)
+    const float4* face_mom; // moments of H^s at each ghost's interior cell (GhostArgs::face_mom of step s)
     float* gadj;            // out: per open face [Q][nu * nv]
     long long gadj_off[6];
 };
@@ -74,7 +77,11 @@ struct AdjProbeArgs
 };
 
 cudaError_t launch_adj_ghost(const AdjGhostArgs& a, cudaStream_t stream);
-cudaError_t launch_adj_step(const AdjStepArgs& a, cudaStream_t stream);
+// J_C^T of the gathered lamF^s over every interior cell, then the
+// ghost-adjoint terms of the open faces `ga` (two launches).  variant:
+// register cap of the step kernel (0: none, 1: 5 blocks of 128 per SM, 2: 6
+// blocks); same work in all.
+cudaError_t launch_adj_step(const AdjStepArgs& a, const GhostArgs& ga, int variant, cudaStream_t stream);
 cudaError_t launch_adj_source(const AdjSourceArgs& a, cudaStream_t stream);
 cudaError_t launch_adj_probe(float* lam, const AdjProbeArgs& a, cudaStream_t stream);
 

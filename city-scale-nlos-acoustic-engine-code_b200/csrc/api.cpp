@@ -36,6 +36,9 @@ constexpr int kProbeRows = 4096;   // probe-series rows buffered on the device
 // cap plus line prefetches 96 rows ahead.
 constexpr int kDefaultStepVariant[2] = {0, 4};
 constexpr int kDefaultPrefetchRows[2] = {0, 96};
+// Register cap of the adjoint step kernel (launch_adj_step variant).
+constexpr int kDefaultAdjointVariant = 1;
+constexpr int kDefaultAdjointPrefetchRows = 0;
 
 struct SourceState
 {
@@ -1467,7 +1470,96 @@ void source_cells(const lbm_handle* h, const lbm_source& p, const SourceEntry& e
     }
 }
 
+// Checkpoint schedule of one adjoint evaluation: outer interval K1, inner
+// interval K2 and the device bytes it allocates.  ckpt_inner <= 0 picks the
+// largest K2 <= K1 whose buffers fit in 90 % of the free device memory.
+struct AdjPlan
+{
+    int K1 = 0, K2 = 0, M = 0, NI = 0, ncell = 0;
+    size_t pop = 0, ck_slot = 0, st_slot = 0;   // floats; st_slot: one step's stored moments
+    size_t mom_n = 0;                            // float4 of cell moments per stored step
+    long long gadj_n = 0;
+    size_t bytes = 0;
+    long long fwd_steps = 0;                     // forward steps run, recomputation included
+};
+
+size_t round64(size_t n) { return (n + 63) / 64 * 64; }
+
+AdjPlan adjoint_plan(const lbm_handle* h, int T, int ckpt_outer, int ckpt_inner)
+{
+    AdjPlan p;
+    const Layout& L = h->L;
+    const lbm_source& s = h->srcs[0].s;
+    p.ncell = s.injection == LBM_INJECT_TRILINEAR ? 8 : (2 * s.radius + 1) * (2 * s.radius + 1) * (2 * s.radius + 1);
+    p.pop = round64((size_t)L.total);
+    p.ck_slot = p.pop + round64((size_t)2 * Q * L.ny * L.nz);
+    // stored per step: moments of F^s for every cell, moments of H^s at every ghost's interior cell
+    p.mom_n = round64((size_t)L.nx * L.ny * L.nz);
+    p.st_slot = 4 * (p.mom_n + round64((size_t)std::max(h->ga.total, 1LL)));
+    for (int f = 0; f < h->ga.nfaces; ++f) p.gadj_n += (long long)Q * h->ga.face[f].nu * h->ga.face[f].nv;
+    p.K1 = std::min(ckpt_outer > 0 ? ckpt_outer : 200, T);
+    p.M = (T + p.K1 - 1) / p.K1;
+    const int np = h->nprobe();
+    const auto bytes = [&](int K2) {
+        const size_t ni = (size_t)((p.K1 + K2 - 1) / K2);
+        return ((p.M + ni) * p.ck_slot + (size_t)(K2 + 1) * p.st_slot + 2 * p.pop + (size_t)std::max(p.gadj_n, 1LL)) *
+                   sizeof(float) +
+               (size_t)T * ((size_t)2 * np * sizeof(double) + (size_t)p.ncell * sizeof(AdjSourceCell) + 4 * sizeof(double));
+    };
+    if (ckpt_inner > 0)
+    {
+        p.K2 = std::min(ckpt_inner, p.K1);
+    }
+    else
+    {
+        size_t fr = 0, tot = 0;
+        if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) fr = 0;
+        const double budget = 0.9 * (double)fr;
+        p.K2 = 1;
+        for (int K2 = p.K1; K2 >= 1; --K2)
+            if ((double)bytes(K2) <= budget)
+            {
+                p.K2 = K2;
+                break;
+            }
+    }
+    p.NI = (p.K1 + p.K2 - 1) / p.K2;
+    p.bytes = bytes(p.K2);
+    // forward steps (fused pull-collide launches): the first pass, the outer
+    // recompute to the inner checkpoints and the recompute of every inner
+    // segment (its last state needs only the source and ghost fill)
+    p.fwd_steps = T;
+    for (int m = 0; m < p.M; ++m)
+    {
+        const long long O = (long long)m * p.K1, E = std::min<long long>(O + p.K1, T);
+        const long long N = (E - O + p.K2 - 1) / p.K2;
+        p.fwd_steps += std::max(O + (N - 1) * p.K2 - 1, 0LL) - std::max(O - 1, 0LL);
+        for (long long n = 0; n < N; ++n)
+        {
+            const long long a0 = O + n * p.K2, a1 = std::min(a0 + p.K2, E);
+            p.fwd_steps += a1 - 1 - std::max(a0 - 1, 0LL);
+        }
+    }
+    return p;
+}
+
 }  // namespace
+
+extern "C" int lbm_adjoint_plan(lbm_handle* h, int nsteps, int ckpt_outer, int ckpt_inner, int* outer, int* inner,
+                                long long* device_bytes, long long* forward_steps)
+{
+    int st = check_ready(h);
+    if (st) return st;
+    if (h->srcs.size() != 1) return h->fail(LBM_ERR_UNSUPPORTED, "the adjoint needs exactly one source");
+    if (nsteps < 1) return h->fail(LBM_ERR_INVALID_ARGUMENT, "nsteps < 1");
+    CK(cudaSetDevice(h->device), "cudaSetDevice");
+    const AdjPlan p = adjoint_plan(h, nsteps, ckpt_outer, ckpt_inner);
+    if (outer) *outer = p.K1;
+    if (inner) *inner = p.K2;
+    if (device_bytes) *device_bytes = (long long)p.bytes;
+    if (forward_steps) *forward_steps = p.fwd_steps;
+    return LBM_OK;
+}
 
 extern "C" int lbm_adjoint_grad(lbm_handle* h, int nsteps, const double* observed, int ckpt_outer, int ckpt_inner,
                                 double* loss, double* grad_pos, double* grad_signal, double* predicted)
@@ -1484,18 +1576,12 @@ extern "C" int lbm_adjoint_grad(lbm_handle* h, int nsteps, const double* observe
     if (st) return st;
 
     const int T = nsteps;
-    const int K1 = std::min(ckpt_outer > 0 ? ckpt_outer : 200, T);
-    const int K2 = std::min(ckpt_inner > 0 ? ckpt_inner : 20, K1);
+    const AdjPlan plan = adjoint_plan(h, T, ckpt_outer, ckpt_inner);
+    const int K1 = plan.K1, K2 = plan.K2, M = plan.M, NI = plan.NI, ncell = plan.ncell;
     const Layout& L = h->L;
-    const int M = (T + K1 - 1) / K1;          // outer checkpoints
-    const int NI = (K1 + K2 - 1) / K2;        // inner checkpoints per outer segment
-    const size_t n_xexp = (size_t)2 * Q * L.ny * L.nz, n_xgh = (size_t)2 * Q * (L.ny + 2) * (L.nz + 2);
-    const auto r64 = [](size_t n) { return (n + 63) / 64 * 64; };
-    const size_t pop = r64((size_t)L.total);
+    const size_t n_xexp = (size_t)2 * Q * L.ny * L.nz;
+    const size_t pop = plan.pop;
     const SourceState& src = h->srcs[0];
-    const int ncell = src.s.injection == LBM_INJECT_TRILINEAR
-                          ? 8
-                          : (2 * src.s.radius + 1) * (2 * src.s.radius + 1) * (2 * src.s.radius + 1);
 
     // Source schedule and injection cells of every step (host, FP64).
     std::vector<SourceEntry> entries((size_t)T);
@@ -1518,9 +1604,11 @@ extern "C" int lbm_adjoint_grad(lbm_handle* h, int nsteps, const double* observe
 
     DevScratch mem;
     cudaError_t e = cudaSuccess;
-    StateSlots outer{mem.get<float>((size_t)M * (pop + r64(n_xexp)), e), pop, r64(n_xexp)};
-    StateSlots inner{mem.get<float>((size_t)NI * (pop + r64(n_xexp)), e), pop, r64(n_xexp)};
-    StateSlots store{mem.get<float>((size_t)(K2 + 1) * (pop + r64(n_xgh)), e), pop, r64(n_xgh)};
+    StateSlots outer{mem.get<float>((size_t)M * plan.ck_slot, e), pop, plan.ck_slot - pop};
+    StateSlots inner{mem.get<float>((size_t)NI * plan.ck_slot, e), pop, plan.ck_slot - pop};
+    float* store = mem.get<float>((size_t)(K2 + 1) * plan.st_slot, e);
+    const auto mom_of = [&](long long slot) { return (float4*)(store + (size_t)slot * plan.st_slot); };
+    const auto face_mom_of = [&](long long slot) { return mom_of(slot) + plan.mom_n; };
     float* lam[2] = {mem.get<float>(pop, e), mem.get<float>(pop, e)};
     float* gadj = mem.get<float>((size_t)gadj_n, e);
     double* d_pred = mem.get<double>((size_t)T * np, e);
@@ -1531,9 +1619,13 @@ extern "C" int lbm_adjoint_grad(lbm_handle* h, int nsteps, const double* observe
     CK(cudaMemcpyAsync(d_cells, cells.data(), cells.size() * sizeof(AdjSourceCell), cudaMemcpyHostToDevice, h->stream),
        "adjoint upload");
     CK(cudaMemsetAsync(d_out, 0, (size_t)T * 4 * sizeof(double), h->stream), "adjoint memset");
-
     const size_t pop_bytes = (size_t)L.total * sizeof(float);
     SourceArgs sargs = source_args(h, false);
+    int adj_variant = kDefaultAdjointVariant;
+    if (const char* v = std::getenv("NLOS_LBM_ADJ_VARIANT")) adj_variant = std::atoi(v);
+    if (adj_variant < 0 || adj_variant > 2) return h->fail(LBM_ERR_BAD_CONFIG, "NLOS_LBM_ADJ_VARIANT out of range");
+    int adj_prefetch = kDefaultAdjointPrefetchRows;
+    if (const char* v = std::getenv("NLOS_LBM_ADJ_PREFETCH_ROWS")) adj_prefetch = std::max(0, std::atoi(v));
     long kernels = 0;
     const auto save_g = [&](const StateSlots& sl, long long idx) {
         cudaError_t r = cudaMemcpyAsync(sl.pop_of(idx), h->f[h->cur], pop_bytes, cudaMemcpyDeviceToDevice, h->stream);
@@ -1547,14 +1639,6 @@ extern "C" int lbm_adjoint_grad(lbm_handle* h, int nsteps, const double* observe
         cudaError_t r = cudaMemcpyAsync(h->f[0], sl.pop_of(idx), pop_bytes, cudaMemcpyDeviceToDevice, h->stream);
         if (r == cudaSuccess)
             r = cudaMemcpyAsync(h->xf.xexp, sl.face_of(idx), n_xexp * sizeof(float), cudaMemcpyDeviceToDevice,
-                                h->stream);
-        return r;
-    };
-    const auto save_ht = [&](long long idx) {
-        cudaError_t r =
-            cudaMemcpyAsync(store.pop_of(idx), h->f[h->cur], pop_bytes, cudaMemcpyDeviceToDevice, h->stream);
-        if (r == cudaSuccess)
-            r = cudaMemcpyAsync(store.face_of(idx), h->xf.xgh, n_xgh * sizeof(float), cudaMemcpyDeviceToDevice,
                                 h->stream);
         return r;
     };
@@ -1582,6 +1666,29 @@ extern "C" int lbm_adjoint_grad(lbm_handle* h, int nsteps, const double* observe
             r = launch_probe(h->storage, h->f[h->cur], L, h->sa, pa, h->stream);
             kernels++;
         }
+        h->cur ^= 1;
+        return r;
+    };
+    // Recompute of step s for the reverse pass: source and ghost fill
+    // recording the moments of H^s at the ghosts' interior cells, then the
+    // fused step recording the moments of F^s, both into store slot `slot`.
+    const auto stored_source_ghost = [&](int s, long long slot) {
+        sargs.direct[0] = entries[s];
+        cudaError_t r = launch_source(h->storage, h->f[h->cur], L, h->sa, sargs, h->stream);
+        kernels++;
+        if (r == cudaSuccess && h->ga.total > 0)
+        {
+            GhostArgs g = h->ga;
+            g.face_mom = face_mom_of(slot);
+            r = launch_ghost(h->storage, h->f[h->cur], L, g, h->stream);
+            kernels++;
+        }
+        return r;
+    };
+    const auto stored_collide = [&](long long slot) {
+        kernels++;
+        const cudaError_t r =
+            launch_step_moments((const float*)h->f[h->cur], (float*)h->f[h->cur ^ 1], L, h->sa, mom_of(slot), h->stream);
         h->cur ^= 1;
         return r;
     };
@@ -1651,15 +1758,14 @@ extern "C" int lbm_adjoint_grad(lbm_handle* h, int nsteps, const double* observe
             CK(restore_g(inner, n), "restore");
             for (int s = cn; s < a1; ++s)
             {
-                CK(source_ghost(s), "recompute");
-                CK(save_ht(s - cn), "store");
-                if (s + 1 < a1) CK(collide(s, false), "recompute");
+                CK(stored_source_ghost(s, s - cn), "recompute");
+                if (s + 1 < a1) CK(stored_collide(s - cn), "recompute");
             }
             for (int s = a1 - 1; s >= a0; --s)
             {
                 if (h->ga.total > 0)
                 {
-                    AdjGhostArgs ga{L, h->ga, h->links, lam[la], store.pop_of(s - cn), gadj, {}};
+                    AdjGhostArgs ga{L, h->ga, h->links, lam[la], face_mom_of(s - cn), gadj, {}};
                     std::copy(gadj_off, gadj_off + 6, ga.gadj_off);
                     CK(launch_adj_ghost(ga, h->stream), "adjoint ghost");
                     kernels++;
@@ -1669,11 +1775,10 @@ extern "C" int lbm_adjoint_grad(lbm_handle* h, int nsteps, const double* observe
                 CK(launch_adj_source(sa, h->stream), "adjoint source");
                 kernels++;
                 if (s == 0) continue;
-                AdjStepArgs as{L, h->sa, lam[la], lam[la ^ 1], store.pop_of(s - 1 - cn), store.face_of(s - 1 - cn),
-                               gadj, {}};
+                AdjStepArgs as{L, h->sa, lam[la], lam[la ^ 1], mom_of(s - 1 - cn), gadj, {}, adj_prefetch};
                 std::copy(gadj_off, gadj_off + 6, as.gadj_off);
-                CK(launch_adj_step(as, h->stream), "adjoint step");
-                kernels++;
+                CK(launch_adj_step(as, h->ga, adj_variant, h->stream), "adjoint step");
+                kernels += h->ga.total > 0 ? 2 : 1;
                 la ^= 1;
                 pa.resid = d_resid + (size_t)(s - 1) * np;
                 CK(launch_adj_probe(lam[la], pa, h->stream), "adjoint probe");

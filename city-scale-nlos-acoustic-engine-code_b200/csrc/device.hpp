@@ -127,6 +127,7 @@ struct GhostArgs
     long long total;
     float scale;
     XFace xf;
+    float4* face_mom;          // non-null: moments (rho', J) of each ghost's interior cell, [total]
 };
 
 struct StepArgs
@@ -167,6 +168,12 @@ cudaError_t launch_ghost(int storage, void* f, const Layout& L, const GhostArgs&
 // variant 0 instead.
 cudaError_t launch_step(int storage, const void* fin, void* fout, const Layout& L, const StepArgs& a,
                         float scale, int variant, cudaStream_t stream);
+// Fused step (FP32 storage, the default implementation) that also writes the
+// moments (rho', jx, jy, jz) of every cell's pulled populations to `mom`,
+// dense cell order ((k-1) ny + (j-1)) nx + (i-1): the forward data of the
+// adjoint's BGK Jacobian.
+cudaError_t launch_step_moments(const float* fin, float* fout, const Layout& L, const StepArgs& a, float4* mom,
+                                cudaStream_t stream);
 cudaError_t launch_probe(int storage, const void* f, const Layout& L, const StepArgs& sa, const ProbeArgs& a,
                          cudaStream_t stream);
 // (float)(rho - 1) of every interior cell, pulled from the pre-step buffer `f`.

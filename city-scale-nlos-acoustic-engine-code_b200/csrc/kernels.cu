@@ -181,7 +181,7 @@ __device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b
 // A SOLID cell gets cA = 1, cB = 0, so its pulled values pass through
 // unchanged (06:933-938).
 __device__ __forceinline__ void collide2(float2 (&G)[Q], float inv_scale, float omega, float2 sigma, bool solid0,
-                                         bool solid1)
+                                         bool solid1, float4& mom0, float4& mom1)
 {
     // rho' and J in the family-B order (06:21-23)
     const float2 rho = add2(add2(add2(add2(G[0], G[1]), add2(G[2], G[3])), add2(add2(G[4], G[5]), add2(G[6], G[7]))),
@@ -193,6 +193,8 @@ __device__ __forceinline__ void collide2(float2 (&G)[Q], float inv_scale, float 
                            add2(add2(add2(G[4], G[8]), add2(G[10], G[17])), G[18]));
     const float2 jz = sub2(add2(add2(add2(G[5], G[11]), add2(G[13], G[15])), G[17]),
                            add2(add2(add2(G[6], G[12]), add2(G[14], G[16])), G[18]));
+    mom0 = make_float4(rho.x, jx.x, jy.x, jz.x);   // moments of the pulled populations
+    mom1 = make_float4(rho.y, jx.y, jy.y, jz.y);
     float2 r = fma2(rho, f2(inv_scale), f2(1.0f));
     if (r.x <= 0.f) r.x = 1e-12f;   // 06:948
     if (r.y <= 0.f) r.y = 1e-12f;
@@ -240,9 +242,12 @@ __device__ __forceinline__ void collide2(float2 (&G)[Q], float inv_scale, float 
 // (warp shuffle) and, at the warp edge, from one extra aligned load.  Cells
 // next to the x faces take their x-halo sources from the x-face ghosts and
 // export their results for the next ghost fill.
-template <typename S, int BLOCK, int MINB>
+// MOM: also write the moments (rho', J) of every cell's pulled populations to
+// `mom` (dense cell order, float4 per cell), the forward data the adjoint's
+// BGK Jacobian needs.
+template <typename S, int BLOCK, int MINB, bool MOM = false>
 __global__ void __launch_bounds__(BLOCK, MINB) k_step(const S* __restrict__ fin, S* __restrict__ fout, Layout L,
-                                                      StepArgs a, float inv_scale)
+                                                      StepArgs a, float inv_scale, float4* __restrict__ mom = nullptr)
 {
     using P = PairIo<S>;
     constexpr int BC = block_cells(sizeof(S));   // cells per interleaved block
@@ -328,7 +333,14 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step(const S* __restrict__ fin,
 
     const float syz = fmaxf(a.sig_y[j - 1], a.sig_z[k - 1]);
     const float2 sg = make_float2(fmaxf(a.sig_x[c0], syz), fmaxf(c0 + 1 < L.nx ? a.sig_x[c0 + 1] : 0.f, syz));
-    collide2(G, inv_scale, a.omega, sg, (lk0 & kSolidSelfBit) != 0u, (lk1 & kSolidSelfBit) != 0u);
+    float4 m0, m1;
+    collide2(G, inv_scale, a.omega, sg, (lk0 & kSolidSelfBit) != 0u, (lk1 & kSolidSelfBit) != 0u, m0, m1);
+    if constexpr (MOM)
+    {
+        const long long mi = ((long long)(k - 1) * L.ny + (j - 1)) * L.nx + c0;
+        mom[mi] = m0;
+        if (c0 + 1 < L.nx) mom[mi + 1] = m1;
+    }
 
     S* out = fout + e0;
 #pragma unroll
@@ -773,6 +785,13 @@ __device__ __forceinline__ void nscbc(float (&G)[Q], int axis, int side, float i
         G[q] += geq_dev(q, rhoB, rB, bx, by, bz, inv_scale) - geq_dev(q, rho, rI, ux, uy, uz, inv_scale);
 }
 
+__device__ __forceinline__ void store_moments(const float (&G)[Q], float4* out)
+{
+    float rho, jx, jy, jz;
+    moments(G, rho, jx, jy, jz);
+    *out = make_float4(rho, jx, jy, jz);
+}
+
 template <typename S>
 __global__ void __launch_bounds__(128) k_ghost(S* __restrict__ f, Layout L, GhostArgs a)
 {
@@ -791,6 +810,7 @@ __global__ void __launch_bounds__(128) k_ghost(S* __restrict__ f, Layout L, Ghos
         const int j = 1 + u, k = 1 + v;
 #pragma unroll
         for (int q = 0; q < Q; ++q) G[q] = a.xf.xexp[a.xf.exp_index(F.side, q, j, k, L.ny, L.nz)];
+        if (a.face_mom) store_moments(G, a.face_mom + t);
         nscbc(G, 0, F.side, inv_scale);
 #pragma unroll
         for (int q = 0; q < Q; ++q) a.xf.xgh[a.xf.gh_index(F.side, q, j, k, L.ny, L.nz)] = G[q];
@@ -816,6 +836,7 @@ __global__ void __launch_bounds__(128) k_ghost(S* __restrict__ f, Layout L, Ghos
     S* B = f + L.elem(0, ci, gj, gk);
 #pragma unroll
     for (int q = 0; q < Q; ++q) G[q] = Io<S>::ld(I + q * BC);
+    if (a.face_mom) store_moments(G, a.face_mom + t);
     nscbc(G, F.axis, F.side, inv_scale);
 #pragma unroll
     for (int q = 0; q < Q; ++q) Io<S>::st(B + q * BC, G[q]);
@@ -1008,6 +1029,13 @@ cudaError_t launch_step(int storage, const void* fin, void* fout, const Layout& 
 {
     if (storage == 0) return launch_step_t<float>((const float*)fin, (float*)fout, L, a, 1.0f, variant, stream);
     return launch_step_t<__half>((const __half*)fin, (__half*)fout, L, a, 1.0f / scale, variant, stream);
+}
+
+cudaError_t launch_step_moments(const float* fin, float* fout, const Layout& L, const StepArgs& a, float4* mom,
+                                cudaStream_t stream)
+{
+    k_step<float, 128, 0, true><<<pair_grid(L, 128), 128, 0, stream>>>(fin, fout, L, a, 1.0f, mom);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_source(int storage, void* f, const Layout& L, const StepArgs& sa, const SourceArgs& a,

@@ -188,6 +188,8 @@ def bind_product(lib):
         "lbm_get_transfer_bytes": (ctypes.c_int, [P, c_long_p, c_long_p]),
         "lbm_adjoint_grad": (ctypes.c_int, [P, ctypes.c_int, c_double_p, ctypes.c_int, ctypes.c_int, c_double_p,
                                             c_double_p, c_double_p, c_double_p]),
+        "lbm_adjoint_plan": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_int, ctypes.c_int, c_int_p, c_int_p,
+                                            ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]),
         "lbm_city_generate": (ctypes.c_int, [ctypes.POINTER(LbmCityParams), c_float_p, ctypes.c_int,
                                              c_int_p, c_double_p]),
         "lbm_stl_write": (ctypes.c_int, [ctypes.c_char_p, c_float_p, ctypes.c_int]),

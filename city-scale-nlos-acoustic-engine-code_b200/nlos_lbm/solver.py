@@ -214,6 +214,14 @@ class Solver:
                     "lbm_adjoint_grad")
         return loss.value, gpos, gsig, pred
 
+    def adjoint_plan(self, nsteps, ckpt_outer=0, ckpt_inner=0):
+        """(outer, inner, device_bytes, forward_steps) of lbm_adjoint_plan."""
+        o, i = ctypes.c_int(), ctypes.c_int()
+        b, f = ctypes.c_longlong(), ctypes.c_longlong()
+        self._check(self.lib.lbm_adjoint_plan(self.h, int(nsteps), int(ckpt_outer), int(ckpt_inner), ctypes.byref(o),
+                                              ctypes.byref(i), ctypes.byref(b), ctypes.byref(f)), "lbm_adjoint_plan")
+        return o.value, i.value, b.value, f.value
+
     def clear_sources(self):
         self._check(self.lib.lbm_clear_sources(self.h), "lbm_clear_sources")
 

@@ -257,10 +257,13 @@ int lbm_get_mask(lbm_handle* h, uint8_t* out, long capacity);
  * the forward model is exactly lbm_step's (same kernels, FP32 storage).
  * A reverse-time discrete adjoint of the fused step: the forward pass keeps a
  * checkpoint every ckpt_outer steps (<= 0: 200), each segment is recomputed
- * with inner checkpoints every ckpt_inner steps (<= 0: 20), and each inner
- * segment once more, storing its states, before it is run backwards.  Device
- * memory: about (nsteps/ckpt_outer + ckpt_outer/ckpt_inner + ckpt_inner + 3)
- * population buffers.  Requires FP32 storage, exactly one source and at least
+ * with inner checkpoints every ckpt_inner steps, and each inner segment once
+ * more, storing its states, before it is run backwards.  ckpt_inner <= 0
+ * picks the largest interval up to ckpt_outer whose buffers fit in 90 % of the
+ * free device memory (ckpt_inner = ckpt_outer stores whole outer segments and
+ * needs no second recompute).  Device memory: about (nsteps/ckpt_outer +
+ * ckpt_outer/ckpt_inner + ckpt_inner + 3) population buffers; lbm_adjoint_plan
+ * gives the exact figure.  Requires FP32 storage, exactly one source and at least
  * one probe.  Observed entries that are NaN, probes outside the grid and the
  * probe rows of SOLID cells (which read 0 whatever the state) contribute no
  * gradient.  Starts from and returns to the rest state (step 0, empty probe
@@ -268,6 +271,13 @@ int lbm_get_mask(lbm_handle* h, uint8_t* out, long capacity);
  * series.  grad_pos, grad_signal and predicted may be NULL. */
 int lbm_adjoint_grad(lbm_handle* h, int nsteps, const double* observed, int ckpt_outer, int ckpt_inner,
                      double* loss, double* grad_pos, double* grad_signal, double* predicted);
+/* The schedule lbm_adjoint_grad would run with these arguments (no
+ * counterpart in the reference): the effective outer and inner checkpoint
+ * intervals, the device bytes it allocates and the number of forward steps
+ * it runs, recomputation included (nsteps when nothing is recomputed).
+ * Every output may be NULL. */
+int lbm_adjoint_plan(lbm_handle* h, int nsteps, int ckpt_outer, int ckpt_inner, int* outer, int* inner,
+                     long long* device_bytes, long long* forward_steps);
 
 /* ---- measurement ---------------------------------------------------------- */
 

@@ -131,3 +131,14 @@ def test_adjoint_rejects_unsupported_set_ups(gpu):
     with pytest.raises(LBMError) as e:
         g.adjoint_grad(np.zeros((10, 0)))
     assert e.value.status == abi.LBM_ERR_STATE
+
+
+def test_adjoint_plan(gpu):
+    sc = scenarios.adjoint_scenario(nx=32, ny=24, nz=16, steps=45, nprobe=6)
+    g = Solver(sc["cfg"], [sc["trial"]], sc["probes"], triangles=sc["triangles"])
+    assert g.adjoint_plan(45, 7, 3)[:2] == (7, 3)
+    assert g.adjoint_plan(45, 100, 60)[:2] == (45, 45)            # intervals clamp to the run
+    o, i, nbytes, fwd = g.adjoint_plan(45, 0, 0)                   # small grid: whole segments fit
+    assert (o, i) == (45, 45) and nbytes > 0 and fwd == 2 * 45 - 1
+    assert g.adjoint_plan(45, 45, 45)[3] == 2 * 45 - 1              # one forward pass + one recompute
+    assert g.adjoint_plan(45, 9, 1)[3] > g.adjoint_plan(45, 9, 9)[3]
