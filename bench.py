@@ -212,15 +212,19 @@ def e2e_measure(solver, w, steps):
     return (t1 - t0) * 1e3, (h1 - h0) / steps, (d1 - d0) / steps
 
 
-def adjoint_measure(device, torch, reps=1, ckpt=(200, 0)):
+def adjoint_measure(device, torch, reps=2, ckpt=(200, 0), workload="adjoint256", steps=None):
     """Gradients per second of lbm_adjoint_grad on the 256x256x128 patch
     (3000 steps, 64 receivers): observed series from a forward run of the
     true source, then the misfit gradient at the trial source, timed with CUDA
-    events on the library's stream around whole lbm_adjoint_grad calls."""
+    events on the library's stream around whole lbm_adjoint_grad calls
+    (median of `reps`; the untimed warm-up call allocates the workspace the
+    handle keeps)."""
     import nlos_lbm
     from nlos_lbm import workloads
 
-    w = workloads.build("adjoint256")
+    w = workloads.build(workload)
+    if steps:
+        w["steps"] = int(steps)
     w["cfg"].device = device
     truth = nlos_lbm.Solver(w["cfg"], [w["true_source"]], w["probes"], triangles=w["triangles"])
     truth.step(w["steps"])
@@ -229,7 +233,7 @@ def adjoint_measure(device, torch, reps=1, ckpt=(200, 0)):
     s = nlos_lbm.Solver(w["cfg"], w["sources"], w["probes"], triangles=w["triangles"])
     k_outer, k_inner, dev_bytes, fwd_steps = s.adjoint_plan(w["steps"], *ckpt)
     stream = torch.cuda.ExternalStream(s.stream)
-    s.adjoint_grad(observed[:100], *ckpt)   # warm-up (allocations, first launches)
+    s.adjoint_grad(observed, *ckpt)   # warm-up: workspace allocation, first launches
     times = []
     for _ in range(reps):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -243,7 +247,7 @@ def adjoint_measure(device, torch, reps=1, ckpt=(200, 0)):
         launches = s.launch_count - l0
     nx, ny, nz = workloads.cells(w["cfg"])
     ms = float(np.median(times))
-    return {"workload": "adjoint256: " + w["description"], "grad_per_s": 1e3 / ms, "ms_per_grad": ms,
+    return {"workload": workload + ": " + w["description"], "grad_per_s": 1e3 / ms, "ms_per_grad": ms,
             "steps": w["steps"], "cells": nx * ny * nz, "ckpt_outer_inner": [k_outer, k_inner],
             "device_gb": dev_bytes / 1e9, "forward_steps": fwd_steps, "loss": loss,
             "grad_pos": [float(v) for v in gpos], "grad_signal_norm": float(np.linalg.norm(gsig)),
@@ -419,11 +423,22 @@ def main():
     ap.add_argument("--headline-only", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--adjoint-only", action="store_true",
+                    help="time lbm_adjoint_grad alone and print its JSON object (profiling runs)")
+    ap.add_argument("--adjoint-workload", default="adjoint256", choices=["adjoint256", "adjoint128"])
+    ap.add_argument("--adjoint-steps", type=int, default=None, help="override the adjoint run length")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.adjoint_only:
+        import torch
+
+        torch.cuda.set_device(0)
+        print(json.dumps(adjoint_measure(0, torch, workload=args.adjoint_workload, steps=args.adjoint_steps)),
+              flush=True)
+        return 0
     return run_our_arm(args)
 
 

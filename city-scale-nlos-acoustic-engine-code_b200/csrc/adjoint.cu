@@ -260,38 +260,6 @@ __device__ __forceinline__ float2 shifted_pair(const float* row, int lane)
     return make_float2(cur.y, next);
 }
 
-// Each block asks L2 for the lines that the same tile `dist` rows later will
-// read: the 19 lamF lines of each interleaved block from the neighbour rows,
-// and the moment lines of the row itself.  Prefetches hold no registers, so
-// they add loads in flight beyond what the register budget allows.
-template <int TILE>
-__device__ __forceinline__ void prefetch_ahead(const AdjStepArgs& a, int dist, int j, int k, int col0)
-{
-    constexpr int BC = 32, NBLK = TILE / BC, NMOM = TILE * 16 / 128;
-    const Layout& L = a.L;
-    const long long r = (long long)(k - 1) * L.ny + (j - 1) + dist;
-    if (r >= (long long)L.ny * L.nz) return;
-    const int jj = 1 + (int)(r % L.ny), kk = 1 + (int)(r / L.ny);
-    for (int t = threadIdx.x; t < 19 * NBLK + NMOM; t += blockDim.x)
-    {
-        const void* p;
-        if (t < 19 * NBLK)
-        {
-            const int q = t / NBLK, b = t - q * NBLK;
-            const int col = col0 + b * BC;
-            if (col >= L.nx) continue;
-            p = a.lam_in + L.elem(q, col + 1, jj + ey(q), kk + ez(q));
-        }
-        else
-        {
-            const int col = col0 + (t - 19 * NBLK) * 8;
-            if (col >= L.nx) continue;
-            p = a.mom_prev + (((long long)(kk - 1) * L.ny + (jj - 1)) * L.nx + col);
-        }
-        asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
-    }
-}
-
 // lamF^{s-1} = J_C(F^{s-1})^T lamH^s for two x-adjacent cells per thread.
 // With F the pulled populations (only their stored moments are read),
 // rho' = sum F, J = sum c F, r = 1 + rho':
@@ -314,8 +282,6 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_adj_step(AdjStepArgs a)
     const int j = blockIdx.y + 1, k = blockIdx.z + 1;
     const long long e0 = L.elem(0, c0 + 1, j, k);
     const long long rs = L.row_stride, ps = L.plane_stride;
-
-    if (a.prefetch_rows > 0) prefetch_ahead<2 * BLOCK>(a, a.prefetch_rows, j, k, 2 * BLOCK * blockIdx.x);
 
     uint32_t lk0 = 0, lk1 = 0;
     if (active)
@@ -484,7 +450,15 @@ __global__ void __launch_bounds__(128) k_adj_face(AdjStepArgs a, GhostArgs ga)
     for (int f = 0; f < 6 && owner < 0; ++f)
         if (at[f] && a.gadj_off[f] >= 0) owner = f;
     if (owner != F.axis * 2 + F.side) return;
-    float g[Q];
+    // every load first (one memory round trip): the cell's lamF^{s-1} (19
+    // lines apart for x-face cells), its links word and moments, the
+    // ghost-adjoint terms of each open face it lies on
+    float* out = a.lam_out + L.elem(0, i, j, k);
+    float lo[Q], g[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) lo[q] = out[q * L.bc];
+    const uint32_t lk = a.sa.links[L.cell(i, j, k)];
+    const float4 m = __ldg(a.mom_prev + ((long long)(k - 1) * L.ny + (j - 1)) * L.nx + (i - 1));
 #pragma unroll
     for (int q = 0; q < Q; ++q) g[q] = 0.f;
 #pragma unroll
@@ -494,17 +468,14 @@ __global__ void __launch_bounds__(128) k_adj_face(AdjStepArgs a, GhostArgs ga)
         const int axis = f / 2;
         const long long n = face_cells(L, axis), c = face_cell(L, axis, i, j, k);
 #pragma unroll
-        for (int q = 0; q < Q; ++q) g[q] += a.gadj[a.gadj_off[f] + (long long)q * n + c];
+        for (int q = 0; q < Q; ++q) g[q] += __ldg(a.gadj + a.gadj_off[f] + (long long)q * n + c);
     }
-    const uint32_t lk = a.sa.links[L.cell(i, j, k)];
-    float* out = a.lam_out + L.elem(0, i, j, k);
     if (lk & kSolidSelfBit)
     {
 #pragma unroll
-        for (int q = 0; q < Q; ++q) out[q * L.bc] += g[q];
+        for (int q = 0; q < Q; ++q) out[q * L.bc] = lo[q] + g[q];
         return;
     }
-    const float4 m = a.mom_prev[((long long)(k - 1) * L.ny + (j - 1)) * L.nx + (i - 1)];
     float r = 1.0f + m.x;
     if (r <= 0.f) r = 1e-12f;
     const float ir = 1.0f / r;
@@ -525,7 +496,7 @@ __global__ void __launch_bounds__(128) k_adj_face(AdjStepArgs a, GhostArgs ga)
     const float ca = (1.0f - sg) * (1.0f - a.sa.omega), cb = (1.0f - sg) * a.sa.omega;
 #pragma unroll
     for (int p = 0; p < Q; ++p)
-        out[p * L.bc] += ca * g[p] + cb * (A + (float)ex(p) * Bx + (float)ey(p) * By + (float)ez(p) * Bz);
+        out[p * L.bc] = lo[p] + ca * g[p] + cb * (A + (float)ex(p) * Bx + (float)ey(p) * By + (float)ez(p) * Bz);
 }
 
 // Residual of each probe enters the adjoint of every population it summed.
@@ -590,13 +561,26 @@ cudaError_t launch_adj_ghost(const AdjGhostArgs& a, cudaStream_t stream)
 cudaError_t launch_adj_step(const AdjStepArgs& a, const GhostArgs& ga, int variant, cudaStream_t stream)
 {
     if (a.L.bc != 32) return cudaErrorInvalidValue;   // FP32 layout only
-    constexpr int kBlock = 128;
-    const dim3 g((unsigned)((a.L.nx + 2 * kBlock - 1) / (2 * kBlock)), (unsigned)a.L.ny, (unsigned)a.L.nz);
-    switch (variant)
+    // rows of up to 128 columns take 64-thread blocks, so no warp idles
+    const int block = a.L.nx <= 128 ? 64 : 128;
+    const dim3 g((unsigned)((a.L.nx + 2 * block - 1) / (2 * block)), (unsigned)a.L.ny, (unsigned)a.L.nz);
+    if (block == 64)
     {
-    case 1: k_adj_step<kBlock, 5><<<g, kBlock, 0, stream>>>(a); break;
-    case 2: k_adj_step<kBlock, 6><<<g, kBlock, 0, stream>>>(a); break;
-    default: k_adj_step<kBlock, 1><<<g, kBlock, 0, stream>>>(a); break;
+        switch (variant)
+        {
+        case 1: k_adj_step<64, 10><<<g, 64, 0, stream>>>(a); break;
+        case 2: k_adj_step<64, 12><<<g, 64, 0, stream>>>(a); break;
+        default: k_adj_step<64, 1><<<g, 64, 0, stream>>>(a); break;
+        }
+    }
+    else
+    {
+        switch (variant)
+        {
+        case 1: k_adj_step<128, 5><<<g, 128, 0, stream>>>(a); break;
+        case 2: k_adj_step<128, 6><<<g, 128, 0, stream>>>(a); break;
+        default: k_adj_step<128, 1><<<g, 128, 0, stream>>>(a); break;
+        }
     }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess || ga.total <= 0) return e;

@@ -38,7 +38,6 @@ constexpr int kDefaultStepVariant[2] = {0, 4};
 constexpr int kDefaultPrefetchRows[2] = {0, 96};
 // Register cap of the adjoint step kernel (launch_adj_step variant).
 constexpr int kDefaultAdjointVariant = 1;
-constexpr int kDefaultAdjointPrefetchRows = 0;
 
 struct SourceState
 {
@@ -114,6 +113,11 @@ struct lbm_handle
     cudaGraphExec_t graph = nullptr;
     int graph_kernels = 0;
 
+    // adjoint workspace (checkpoints, stored moments, adjoint populations),
+    // kept between lbm_adjoint_grad calls; lbm_adjoint_release frees it
+    void* adj_ws = nullptr;
+    size_t adj_ws_bytes = 0;
+
     // kernel timing
     bool timing = false;
     std::vector<cudaEvent_t> ev;
@@ -160,6 +164,9 @@ struct lbm_handle
         if (h_table) cudaFreeHost(h_table);
         if (h_probe_out) cudaFreeHost(h_probe_out);
         ctl_host = nullptr; h_table = nullptr; h_probe_out = nullptr;
+        if (adj_ws) cudaFree(adj_ws);
+        adj_ws = nullptr;
+        adj_ws_bytes = 0;
         if (stream) cudaStreamDestroy(stream);
         stream = nullptr;
         inited = false;
@@ -1341,21 +1348,18 @@ extern "C" int lbm_voxelize(const lbm_config* cfg, const float* tris, int ntris,
 
 namespace {
 
-// Device memory of one adjoint evaluation, freed on every exit path.
-struct DevScratch
+// Sub-allocations of the adjoint workspace, 256-byte aligned.  With a null
+// base it only counts the bytes.
+struct Carve
 {
-    std::vector<void*> ptrs;
-    ~DevScratch()
-    {
-        for (void* p : ptrs) cudaFree(p);
-    }
+    char* base = nullptr;
+    size_t used = 0;
     template <typename T>
-    T* get(size_t n, cudaError_t& e)
+    T* get(size_t n)
     {
-        void* p = nullptr;
-        if (e == cudaSuccess) e = cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T));
-        if (e == cudaSuccess) ptrs.push_back(p);
-        return (T*)p;
+        T* p = base ? (T*)(base + used) : nullptr;
+        used += (std::max<size_t>(n, 1) * sizeof(T) + 255) / 256 * 256;
+        return p;
     }
 };
 
@@ -1502,9 +1506,18 @@ AdjPlan adjoint_plan(const lbm_handle* h, int T, int ckpt_outer, int ckpt_inner)
     const int np = h->nprobe();
     const auto bytes = [&](int K2) {
         const size_t ni = (size_t)((p.K1 + K2 - 1) / K2);
-        return ((p.M + ni) * p.ck_slot + (size_t)(K2 + 1) * p.st_slot + 2 * p.pop + (size_t)std::max(p.gadj_n, 1LL)) *
-                   sizeof(float) +
-               (size_t)T * ((size_t)2 * np * sizeof(double) + (size_t)p.ncell * sizeof(AdjSourceCell) + 4 * sizeof(double));
+        Carve c;
+        c.get<float>((size_t)p.M * p.ck_slot);
+        c.get<float>(ni * p.ck_slot);
+        c.get<float>((size_t)(K2 + 1) * p.st_slot);
+        c.get<float>(p.pop);
+        c.get<float>(p.pop);
+        c.get<float>((size_t)p.gadj_n);
+        c.get<double>((size_t)T * np);
+        c.get<double>((size_t)T * np);
+        c.get<AdjSourceCell>((size_t)T * p.ncell);
+        c.get<double>((size_t)T * 4);
+        return c.used;
     };
     if (ckpt_inner > 0)
     {
@@ -1514,7 +1527,7 @@ AdjPlan adjoint_plan(const lbm_handle* h, int T, int ckpt_outer, int ckpt_inner)
     {
         size_t fr = 0, tot = 0;
         if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) fr = 0;
-        const double budget = 0.9 * (double)fr;
+        const double budget = 0.9 * (double)(fr + h->adj_ws_bytes);   // the workspace is reused
         p.K2 = 1;
         for (int K2 = p.K1; K2 >= 1; --K2)
             if ((double)bytes(K2) <= budget)
@@ -1544,6 +1557,20 @@ AdjPlan adjoint_plan(const lbm_handle* h, int T, int ckpt_outer, int ckpt_inner)
 }
 
 }  // namespace
+
+extern "C" int lbm_adjoint_release(lbm_handle* h)
+{
+    if (!h) return LBM_ERR_INVALID_ARGUMENT;
+    if (h->adj_ws)
+    {
+        CK(cudaSetDevice(h->device), "cudaSetDevice");
+        CK(cudaStreamSynchronize(h->stream), "adjoint release");
+        cudaFree(h->adj_ws);
+    }
+    h->adj_ws = nullptr;
+    h->adj_ws_bytes = 0;
+    return LBM_OK;
+}
 
 extern "C" int lbm_adjoint_plan(lbm_handle* h, int nsteps, int ckpt_outer, int ckpt_inner, int* outer, int* inner,
                                 long long* device_bytes, long long* forward_steps)
@@ -1602,20 +1629,41 @@ extern "C" int lbm_adjoint_grad(lbm_handle* h, int nsteps, const double* observe
         gadj_n += (long long)Q * F.nu * F.nv;
     }
 
-    DevScratch mem;
-    cudaError_t e = cudaSuccess;
-    StateSlots outer{mem.get<float>((size_t)M * plan.ck_slot, e), pop, plan.ck_slot - pop};
-    StateSlots inner{mem.get<float>((size_t)NI * plan.ck_slot, e), pop, plan.ck_slot - pop};
-    float* store = mem.get<float>((size_t)(K2 + 1) * plan.st_slot, e);
+    // workspace: carved from one allocation kept in the handle between calls
+    StateSlots outer, inner;
+    float* store;
+    float* lam[2];
+    float* gadj;
+    double *d_pred, *d_resid, *d_out;
+    AdjSourceCell* d_cells;
+    const auto carve = [&](Carve& c) {
+        outer = StateSlots{c.get<float>((size_t)M * plan.ck_slot), pop, plan.ck_slot - pop};
+        inner = StateSlots{c.get<float>((size_t)NI * plan.ck_slot), pop, plan.ck_slot - pop};
+        store = c.get<float>((size_t)(K2 + 1) * plan.st_slot);
+        lam[0] = c.get<float>(pop);
+        lam[1] = c.get<float>(pop);
+        gadj = c.get<float>((size_t)gadj_n);
+        d_pred = c.get<double>((size_t)T * np);
+        d_resid = c.get<double>((size_t)T * np);
+        d_cells = c.get<AdjSourceCell>(cells.size());
+        d_out = c.get<double>((size_t)T * 4);
+    };
+    {
+        Carve count;
+        carve(count);
+        if (count.used > h->adj_ws_bytes)
+        {
+            if (h->adj_ws) cudaFree(h->adj_ws);
+            h->adj_ws = nullptr;
+            h->adj_ws_bytes = 0;
+            CK(cudaMalloc(&h->adj_ws, count.used), "adjoint workspace");
+            h->adj_ws_bytes = count.used;
+        }
+        Carve c{(char*)h->adj_ws, 0};
+        carve(c);
+    }
     const auto mom_of = [&](long long slot) { return (float4*)(store + (size_t)slot * plan.st_slot); };
     const auto face_mom_of = [&](long long slot) { return mom_of(slot) + plan.mom_n; };
-    float* lam[2] = {mem.get<float>(pop, e), mem.get<float>(pop, e)};
-    float* gadj = mem.get<float>((size_t)gadj_n, e);
-    double* d_pred = mem.get<double>((size_t)T * np, e);
-    double* d_resid = mem.get<double>((size_t)T * np, e);
-    AdjSourceCell* d_cells = mem.get<AdjSourceCell>(cells.size(), e);
-    double* d_out = mem.get<double>((size_t)T * 4, e);
-    if (e != cudaSuccess) return h->cuda_fail(e, "adjoint buffers");
     CK(cudaMemcpyAsync(d_cells, cells.data(), cells.size() * sizeof(AdjSourceCell), cudaMemcpyHostToDevice, h->stream),
        "adjoint upload");
     CK(cudaMemsetAsync(d_out, 0, (size_t)T * 4 * sizeof(double), h->stream), "adjoint memset");
@@ -1624,8 +1672,6 @@ extern "C" int lbm_adjoint_grad(lbm_handle* h, int nsteps, const double* observe
     int adj_variant = kDefaultAdjointVariant;
     if (const char* v = std::getenv("NLOS_LBM_ADJ_VARIANT")) adj_variant = std::atoi(v);
     if (adj_variant < 0 || adj_variant > 2) return h->fail(LBM_ERR_BAD_CONFIG, "NLOS_LBM_ADJ_VARIANT out of range");
-    int adj_prefetch = kDefaultAdjointPrefetchRows;
-    if (const char* v = std::getenv("NLOS_LBM_ADJ_PREFETCH_ROWS")) adj_prefetch = std::max(0, std::atoi(v));
     long kernels = 0;
     const auto save_g = [&](const StateSlots& sl, long long idx) {
         cudaError_t r = cudaMemcpyAsync(sl.pop_of(idx), h->f[h->cur], pop_bytes, cudaMemcpyDeviceToDevice, h->stream);
@@ -1775,7 +1821,7 @@ extern "C" int lbm_adjoint_grad(lbm_handle* h, int nsteps, const double* observe
                 CK(launch_adj_source(sa, h->stream), "adjoint source");
                 kernels++;
                 if (s == 0) continue;
-                AdjStepArgs as{L, h->sa, lam[la], lam[la ^ 1], mom_of(s - 1 - cn), gadj, {}, adj_prefetch};
+                AdjStepArgs as{L, h->sa, lam[la], lam[la ^ 1], mom_of(s - 1 - cn), gadj, {}};
                 std::copy(gadj_off, gadj_off + 6, as.gadj_off);
                 CK(launch_adj_step(as, h->ga, adj_variant, h->stream), "adjoint step");
                 kernels += h->ga.total > 0 ? 2 : 1;

@@ -190,6 +190,7 @@ def bind_product(lib):
                                             c_double_p, c_double_p, c_double_p]),
         "lbm_adjoint_plan": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_int, ctypes.c_int, c_int_p, c_int_p,
                                             ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]),
+        "lbm_adjoint_release": (ctypes.c_int, [P]),
         "lbm_city_generate": (ctypes.c_int, [ctypes.POINTER(LbmCityParams), c_float_p, ctypes.c_int,
                                              c_int_p, c_double_p]),
         "lbm_stl_write": (ctypes.c_int, [ctypes.c_char_p, c_float_p, ctypes.c_int]),

@@ -222,6 +222,10 @@ class Solver:
                                               ctypes.byref(i), ctypes.byref(b), ctypes.byref(f)), "lbm_adjoint_plan")
         return o.value, i.value, b.value, f.value
 
+    def adjoint_release(self):
+        """Frees the adjoint workspace kept by the handle (lbm_adjoint_release)."""
+        self._check(self.lib.lbm_adjoint_release(self.h), "lbm_adjoint_release")
+
     def clear_sources(self):
         self._check(self.lib.lbm_clear_sources(self.h), "lbm_clear_sources")
 

@@ -16,6 +16,8 @@ reference's heightmap ray cast.
              emitting a Ricker wavelet (period 30 steps), 64 street-level
              receivers, 3000 steps; the trial source (the unknown of the
              localisation) sits a few cells away
+  adjoint128 the same at 128x128x128 (profiler-sized: 160 MB per population
+             buffer, still larger than L2)
 """
 import numpy as np
 
@@ -117,10 +119,10 @@ def build(name, storage=None, seed=2024):
                                    freq=1 / 40.0, waveform=abi.LBM_WAVE_SINE, injection=abi.LBM_INJECT_TRILINEAR)
         return dict(cfg=cfg, sources=[src], probes=probes, triangles=tris, steps=4000, coverage=cov,
                     description="synthetic city 2048x2048x256, source flying at z=120 Mach 0.15, 512 probes")
-    if name == "adjoint256":
+    if name in ("adjoint256", "adjoint128"):
         from .solver import city_triangles
 
-        nx, ny, nz = 256, 256, 128
+        nx, ny, nz = (256, 256, 128) if name == "adjoint256" else (128, 128, 128)
         tris, cov = city_triangles(nx, ny, seed=seed, fp=(20, 60), height=(10, 80), coverage=0.40, street=8,
                                    margin=24)
         cfg = lattice_config(nx, ny, nz, 0.52, sponge_width=16.0, sponge_faces=FIVE_FACES,
@@ -135,7 +137,7 @@ def build(name, storage=None, seed=2024):
                                         injection=abi.LBM_INJECT_TRILINEAR)
         return dict(cfg=cfg, sources=[ricker(trial_xyz)], true_source=ricker(true_xyz), probes=pts[1:],
                     triangles=tris, steps=3000, coverage=cov,
-                    description="transient localisation 256x256x128 city patch, Ricker period 30, 64 receivers, "
+                    description=f"transient localisation {nx}x{ny}x{nz} city patch, Ricker period 30, 64 receivers, "
                                 "3000 steps")
     raise KeyError(name)
 

@@ -278,6 +278,11 @@ int lbm_adjoint_grad(lbm_handle* h, int nsteps, const double* observed, int ckpt
  * Every output may be NULL. */
 int lbm_adjoint_plan(lbm_handle* h, int nsteps, int ckpt_outer, int ckpt_inner, int* outer, int* inner,
                      long long* device_bytes, long long* forward_steps);
+/* lbm_adjoint_grad keeps its device workspace in the handle so repeated
+ * gradient evaluations (the iterations of a localisation) allocate nothing
+ * after the first; this frees it now instead of at lbm_destroy.  No
+ * counterpart in the reference. */
+int lbm_adjoint_release(lbm_handle* h);
 
 /* ---- measurement ---------------------------------------------------------- */
 

@@ -142,3 +142,16 @@ def test_adjoint_plan(gpu):
     assert (o, i) == (45, 45) and nbytes > 0 and fwd == 2 * 45 - 1
     assert g.adjoint_plan(45, 45, 45)[3] == 2 * 45 - 1              # one forward pass + one recompute
     assert g.adjoint_plan(45, 9, 1)[3] > g.adjoint_plan(45, 9, 9)[3]
+
+
+def test_workspace_is_kept_and_released(gpu):
+    sc = scenarios.adjoint_scenario(nx=32, ny=24, nz=16, steps=40, nprobe=6)
+    g = Solver(sc["cfg"], [sc["trial"]], sc["probes"], triangles=sc["triangles"])
+    r1 = g.adjoint_grad(sc["observed"], 9, 4)
+    r2 = g.adjoint_grad(sc["observed"][:20], 9, 4)    # smaller run in the kept workspace
+    r3 = g.adjoint_grad(sc["observed"], 9, 4)
+    g.adjoint_release()
+    r4 = g.adjoint_grad(sc["observed"], 9, 4)         # fresh workspace
+    for r in (r3, r4):
+        assert r[0] == r1[0] and np.array_equal(r[1], r1[1]) and np.array_equal(r[2], r1[2])
+    assert r2[2].shape == (20,)
