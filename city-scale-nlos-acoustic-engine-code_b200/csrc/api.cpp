@@ -113,6 +113,12 @@ struct lbm_handle
     cudaGraphExec_t graph = nullptr;
     int graph_kernels = 0;
 
+    // scheme A (family 01-04): omega and source-weight profiles, x-face arrays of both parities
+    SchemeAArgs aa{};
+    float* a_prof = nullptr;           // om_x | om_y | om_z | fld_x | fld_y | fld_z
+    float* xgh_par[2] = {nullptr, nullptr};
+    bool scheme_a() const { return cfg.scheme == LBM_SCHEME_A; }
+
     // adjoint workspace (checkpoints, stored moments, adjoint populations),
     // kept between lbm_adjoint_grad calls; lbm_adjoint_release frees it
     void* adj_ws = nullptr;
@@ -155,6 +161,8 @@ struct lbm_handle
         cudaFree(sig); sig = nullptr;
         cudaFree(xf.xexp); xf.xexp = nullptr;
         cudaFree(xf.xgh); xf.xgh = nullptr;
+        xgh_par[0] = xgh_par[1] = nullptr;
+        cudaFree(a_prof); a_prof = nullptr;
         cudaFree(ctl); ctl = nullptr;
         cudaFree(d_table); d_table = nullptr;
         cudaFree(d_probe_ijk); d_probe_ijk = nullptr;
@@ -242,8 +250,26 @@ int validate(const lbm_config& c, std::string& why)
     if (!(c.x_max > c.x_min && c.y_max > c.y_min && c.z_max > c.z_min))
         return why = "empty domain", LBM_ERR_BAD_CONFIG;
     for (int f = 0; f < 6; ++f)
-        if (c.face_bc[f] < LBM_BC_NSCBC || c.face_bc[f] > LBM_BC_WALL)
+        if (c.face_bc[f] < LBM_BC_NSCBC || c.face_bc[f] > LBM_BC_COPY)
             return why = "face_bc out of range", LBM_ERR_BAD_CONFIG;
+    if (c.scheme != LBM_SCHEME_B && c.scheme != LBM_SCHEME_A) return why = "unknown scheme", LBM_ERR_BAD_CONFIG;
+    if (!(c.dt >= 0)) return why = "dt must be >= 0 (0: cs*dx/c_phys)", LBM_ERR_BAD_CONFIG;
+    int ncopy = 0, nnscbc = 0;
+    for (int f = 0; f < 6; ++f)
+    {
+        ncopy += c.face_bc[f] == LBM_BC_COPY;
+        nnscbc += c.face_bc[f] == LBM_BC_NSCBC;
+    }
+    if (c.scheme == LBM_SCHEME_B && ncopy) return why = "LBM_BC_COPY needs scheme A", LBM_ERR_BAD_CONFIG;
+    if (c.scheme == LBM_SCHEME_A)
+    {
+        if (c.storage != LBM_STORE_F32) return why = "scheme A runs on FP32 storage", LBM_ERR_BAD_CONFIG;
+        if (nnscbc) return why = "scheme A has no characteristic (NSCBC) faces", LBM_ERR_BAD_CONFIG;
+        if (ncopy != 0 && ncopy != 6) return why = "zero-gradient (LBM_BC_COPY) halos on all six faces or none",
+                                      LBM_ERR_BAD_CONFIG;
+        if (c.tau_sponge_max > 0 && c.tau_sponge_max < c.tau)
+            return why = "tau_sponge_max must be >= tau", LBM_ERR_BAD_CONFIG;
+    }
     if (c.storage != LBM_STORE_F32 && c.storage != LBM_STORE_F16)
         return why = "storage must be LBM_STORE_F32 or LBM_STORE_F16", LBM_ERR_BAD_CONFIG;
     if (c.storage == LBM_STORE_F16 && !(c.f16_scale > 0)) return why = "f16_scale must be > 0", LBM_ERR_BAD_CONFIG;
@@ -347,6 +373,92 @@ void grid_size(const lbm_config& c, int& nx, int& ny, int& nz)
         cudaError_t e_ = (expr);                          \
         if (e_ != cudaSuccess) return h->cuda_fail(e_, where); \
     } while (0)
+
+// Scheme-A profiles on the device: omega of the tau ramp per axis (a cell's
+// omega is the minimum over its three axes, equal to 1 / tau(min distance)
+// since tau grows toward the faces; 02:164-179, 03:148-160), the field
+// source's weight factors per axis, halo-inclusive (02:181, 03:166-169), and
+// the background equilibrium feq(1, u0) the state is stored relative to
+// (03:162-163).
+int upload_scheme_a_profiles(lbm_handle* h)
+{
+    const lbm_config& c = h->cfg;
+    const Layout& L = h->L;
+    const int n[3] = {L.nx, L.ny, L.nz};
+    const unsigned sf = c.sponge_faces;
+    const int w = (int)c.sponge_width;
+    std::vector<float> prof;
+    prof.reserve((size_t)2 * (L.nx + L.ny + L.nz) + 6);
+    for (int a = 0; a < 3; ++a)
+        for (int g = 0; g < n[a]; ++g)
+        {
+            int d = 1 << 30;
+            if (sf & (1u << (2 * a))) d = std::min(d, g);
+            if (sf & (1u << (2 * a + 1))) d = std::min(d, n[a] - 1 - g);
+            double tau = c.tau;
+            if (c.tau_sponge_max > 0 && d >= 0 && d < w)
+            {
+                const double r = (double)(w - d) / w;
+                tau = c.tau + (c.tau_sponge_max - c.tau) * r * r;
+            }
+            prof.push_back((float)(1.0 / tau));
+        }
+    const lbm_source* fs = nullptr;
+    int fsi = -1;
+    for (size_t i = 0; i < h->srcs.size(); ++i)
+        if (h->srcs[i].s.injection == LBM_INJECT_FIELD)
+        {
+            fs = &h->srcs[i].s;
+            fsi = (int)i;
+        }
+    const double lo[3] = {c.x_min, c.y_min, c.z_min};
+    for (int a = 0; a < 3; ++a)
+        for (int g = 0; g <= n[a] + 1; ++g)
+        {
+            double v = 1.0;
+            if (fs)
+            {
+                const double sig = fs->sigma_cells * c.dx;
+                const double ctr[3] = {fs->sx, fs->sy, fs->sz};
+                const double x = lo[a] + ((g - 1) + 0.5) * c.dx - ctr[a];
+                v = std::exp(-x * x / (2.0 * sig * sig));
+            }
+            prof.push_back((float)v);
+        }
+    if (!h->a_prof) CK(cudaMalloc(&h->a_prof, prof.size() * sizeof(float)), "scheme A profiles");
+    CK(cudaMemcpyAsync(h->a_prof, prof.data(), prof.size() * sizeof(float), cudaMemcpyHostToDevice, h->stream),
+       "scheme A profiles");
+    CK(cudaStreamSynchronize(h->stream), "scheme A profiles");
+    h->h2d_bytes += (long)(prof.size() * sizeof(float));
+    SchemeAArgs& b = h->aa;
+    b.om_x = h->a_prof;
+    b.om_y = b.om_x + L.nx;
+    b.om_z = b.om_y + L.ny;
+    b.fld_x = b.om_z + L.nz;
+    b.fld_y = b.fld_x + L.nx + 2;
+    b.fld_z = b.fld_y + L.ny + 2;
+    b.om_bulk = (float)(1.0 / c.tau);
+    b.field_mode = fs ? fs->field_mode : -1;
+    b.src_index = fsi;
+    b.nsrc = (int)h->srcs.size();
+    double u2 = 0.0;
+    for (int a = 0; a < 3; ++a)
+    {
+        b.flow[a] = (float)c.flow[a];
+        u2 += c.flow[a] * c.flow[a];
+    }
+    for (int q = 0; q < Q; ++q)
+    {
+        const double cu = ex(q) * c.flow[0] + ey(q) * c.flow[1] + ez(q) * c.flow[2];
+        b.base[q] = (float)(wd(q) * (3.0 * cu + 4.5 * cu * cu - 1.5 * u2));
+        b.cu0[q] = (float)cu;
+    }
+    b.u0sq = (float)u2;
+    b.copy = c.face_bc[LBM_FACE_XLO] == LBM_BC_COPY ? 1 : 0;
+    b.table = h->d_table;
+    b.ctl = h->ctl;
+    return LBM_OK;
+}
 
 }  // namespace
 
@@ -489,8 +601,21 @@ extern "C" int lbm_add_source(lbm_handle* h, const lbm_source* s)
     if ((int)h->srcs.size() >= kMaxSources) return h->fail(LBM_ERR_UNSUPPORTED, "at most 8 sources");
     if (s->injection == LBM_INJECT_GAUSS && (s->radius < 0 || s->radius > 3 || !(s->sigma_cells > 0)))
         return h->fail(LBM_ERR_INVALID_ARGUMENT, "Gaussian stencil needs radius 0..3 and sigma_cells > 0");
-    if (s->injection != LBM_INJECT_GAUSS && s->injection != LBM_INJECT_TRILINEAR)
+    if (s->injection != LBM_INJECT_GAUSS && s->injection != LBM_INJECT_TRILINEAR && s->injection != LBM_INJECT_FIELD)
         return h->fail(LBM_ERR_INVALID_ARGUMENT, "unknown injection");
+    if (h->cfg.scheme == LBM_SCHEME_A)
+    {
+        if (s->injection != LBM_INJECT_FIELD)
+            return h->fail(LBM_ERR_UNSUPPORTED, "scheme A takes field sources (LBM_INJECT_FIELD) only");
+        if (!h->srcs.empty()) return h->fail(LBM_ERR_UNSUPPORTED, "scheme A takes one field source");
+        if (!(s->sigma_cells > 0)) return h->fail(LBM_ERR_INVALID_ARGUMENT, "field source needs sigma_cells > 0");
+        if (s->field_mode != LBM_FIELD_DST && s->field_mode != LBM_FIELD_FORCE)
+            return h->fail(LBM_ERR_INVALID_ARGUMENT, "unknown field_mode");
+    }
+    else if (s->injection == LBM_INJECT_FIELD)
+    {
+        return h->fail(LBM_ERR_UNSUPPORTED, "field sources need scheme A");
+    }
     if (s->waveform < LBM_WAVE_GAUSS || s->waveform > LBM_WAVE_TABLE)
         return h->fail(LBM_ERR_INVALID_ARGUMENT, "unknown waveform");
     if (s->waveform == LBM_WAVE_TABLE && (s->table_len < 0 || (s->table_len > 0 && !s->table)))
@@ -502,6 +627,7 @@ extern "C" int lbm_add_source(lbm_handle* h, const lbm_source* s)
     h->srcs.push_back(std::move(st));
     h->table_rows = 0;   // schedule must be rebuilt
     if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; }
+    if (h->inited && h->scheme_a()) return upload_scheme_a_profiles(h);
     return LBM_OK;
 }
 
@@ -511,6 +637,7 @@ extern "C" int lbm_clear_sources(lbm_handle* h)
     h->srcs.clear();
     h->table_rows = 0;
     if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; }
+    if (h->inited && h->scheme_a()) return upload_scheme_a_profiles(h);
     return LBM_OK;
 }
 
@@ -546,6 +673,7 @@ extern "C" int lbm_init(lbm_handle* h)
     // Grid (06:330-334, MPI size 1: one block, off = 0) and time step (06:200-203).
     grid_size(c, h->NXg, h->NYg, h->NZg);
     h->dt = (kCs * c.dx) / c.c_phys;
+    if (c.dt > 0) h->dt = c.dt;
     const int nx = h->NXg, ny = h->NYg, nz = h->NZg;
     if (nx < 1 || ny < 1 || nz < 1) return h->fail(LBM_ERR_BAD_CONFIG, "grid has no cells");
     const int nxt = nx + 2, nyt = ny + 2, nzt = nz + 2;
@@ -606,13 +734,16 @@ extern "C" int lbm_init(lbm_handle* h)
     h->sig = dalloc<float>((size_t)nx + ny + nz, e);
     const size_t n_xexp = (size_t)2 * Q * ny * nz, n_xgh = (size_t)2 * Q * nyt * nzt;
     h->xf.xexp = dalloc<float>(n_xexp, e);
-    h->xf.xgh = dalloc<float>(n_xgh, e);
+    const size_t n_xgh_all = n_xgh * (h->scheme_a() ? 2 : 1);   // scheme A: one array per step parity
+    h->xf.xgh = dalloc<float>(n_xgh_all, e);
     h->ctl = dalloc<Control>(1, e);
     if (e != cudaSuccess) return h->cuda_fail(e, "device allocation");
     CK(cudaMemsetAsync(h->links, 0, cells * sizeof(uint32_t), h->stream), "memset links");
     CK(cudaMemsetAsync(h->near, 0, near_words * sizeof(uint32_t), h->stream), "memset near");
     CK(cudaMemsetAsync(h->xf.xexp, 0, n_xexp * sizeof(float), h->stream), "memset x faces");
-    CK(cudaMemsetAsync(h->xf.xgh, 0, n_xgh * sizeof(float), h->stream), "memset x faces");
+    CK(cudaMemsetAsync(h->xf.xgh, 0, n_xgh_all * sizeof(float), h->stream), "memset x faces");
+    h->xgh_par[0] = h->xf.xgh;
+    h->xgh_par[1] = h->xf.xgh + (h->scheme_a() ? n_xgh : 0);
     CK(cudaMallocHost(&h->ctl_host, sizeof(Control)), "cudaMallocHost");
     CK(cudaMemcpyAsync(h->sig, sx.data(), sx.size() * 4, cudaMemcpyHostToDevice, h->stream), "upload sponge");
     CK(cudaMemcpyAsync(h->sig + nx, sy.data(), sy.size() * 4, cudaMemcpyHostToDevice, h->stream), "upload sponge");
@@ -624,6 +755,18 @@ extern "C" int lbm_init(lbm_handle* h)
         e = cudaMemcpyAsync(d_mask, h->mask.data(), nloc, cudaMemcpyHostToDevice, h->stream);
         // links[c] belongs to the cell with linear index c (interior cells only)
         if (e == cudaSuccess) e = launch_build_links(d_mask, h->links, h->near, L, h->stream);
+        if (e == cudaSuccess && h->scheme_a())
+        {
+            const int ps = upload_scheme_a_profiles(h);
+            if (ps != LBM_OK)
+            {
+                cudaFree(d_mask);
+                return ps;
+            }
+            e = launch_init_a((float*)h->f[0], (float*)h->f[1], h->xgh_par[0], h->xgh_par[1], d_mask, L, h->aa,
+                              h->stream);
+            h->launches += 1;
+        }
         cudaError_t e2 = cudaStreamSynchronize(h->stream);
         cudaFree(d_mask);
         if (e == cudaSuccess) e = e2;
@@ -705,9 +848,9 @@ extern "C" int lbm_init(lbm_handle* h)
     // Source schedule buffers (sized for the maximum source count so sources
     // may change after init).
     const size_t ns = kMaxSources;
-    h->d_table = dalloc<SourceEntry>(ns * kTableRows, e);
+    h->d_table = dalloc<SourceEntry>(ns * (kTableRows + 1), e);   // + 1: scheme-A forcing reads row s + 1
     if (e != cudaSuccess) return h->cuda_fail(e, "source table");
-    CK(cudaMallocHost(&h->h_table, ns * kTableRows * sizeof(SourceEntry)), "cudaMallocHost");
+    CK(cudaMallocHost(&h->h_table, ns * (kTableRows + 1) * sizeof(SourceEntry)), "cudaMallocHost");
     h->table_base = 0;
     h->table_rows = 0;
 
@@ -762,8 +905,39 @@ ProbeArgs probe_args(lbm_handle* h, bool batched, long long direct_row)
     return a;
 }
 
-cudaError_t timed_step_launch(lbm_handle* h, const void* fin, void* fout)
+// Arguments of the scheme-A kernels of step s, which reads buffer `parity`:
+// batched steps read the source schedule from the device table, direct
+// calls get the masses of steps s and s + 1 from the host.
+void scheme_a_args(lbm_handle* h, int parity, bool batched, long long s, StepArgs& sa, SchemeAArgs& b)
 {
+    sa = h->sa;
+    sa.xf.xgh = h->xgh_par[parity];
+    b = h->aa;
+    b.table = h->d_table;
+    b.ctl = batched ? h->ctl : nullptr;
+    b.xgh_out = h->xgh_par[parity ^ 1];
+    b.mass_direct[0] = b.mass_direct[1] = 0.f;
+    if (!batched && b.field_mode >= 0)
+    {
+        const SourceState& fs = h->srcs[(size_t)b.src_index];
+        b.mass_direct[0] = (float)source_entry(fs, (double)s * h->dt, h->dt).mass;
+        b.mass_direct[1] = (float)source_entry(fs, (double)(s + 1) * h->dt, h->dt).mass;
+    }
+}
+
+// The fused step of the handle's scheme from buffer `parity` into the other,
+// bracketed by timing events when kernel timing is on.
+cudaError_t timed_step_launch(lbm_handle* h, int parity, bool batched, long long s)
+{
+    const auto launch = [&]() {
+        if (!h->scheme_a())
+            return launch_step(h->storage, h->f[parity], h->f[parity ^ 1], h->L, h->sa, h->scale, h->step_variant,
+                               h->stream);
+        StepArgs sa;
+        SchemeAArgs b;
+        scheme_a_args(h, parity, batched, s, sa, b);
+        return launch_step_a((const float*)h->f[parity], (float*)h->f[parity ^ 1], h->L, sa, b, h->stream);
+    };
     cudaError_t e;
     if (h->timing)
     {
@@ -779,13 +953,13 @@ cudaError_t timed_step_launch(lbm_handle* h, const void* fin, void* fout)
         }
         e = cudaEventRecord(h->ev[h->ev_used], h->stream);
         if (e != cudaSuccess) return e;
-        e = launch_step(h->storage, fin, fout, h->L, h->sa, h->scale, h->step_variant, h->stream);
+        e = launch();
         if (e != cudaSuccess) return e;
         e = cudaEventRecord(h->ev[h->ev_used + 1], h->stream);
         h->ev_used += 2;
         return e;
     }
-    return launch_step(h->storage, fin, fout, h->L, h->sa, h->scale, h->step_variant, h->stream);
+    return launch();
 }
 
 // Collect the kernel times recorded since the last harvest (synchronises).
@@ -814,6 +988,25 @@ cudaError_t enqueue_batched_step(lbm_handle* h, int parity, int& kernels)
     void* fc = h->f[parity];
     void* fn = h->f[parity ^ 1];
     kernels = 0;
+    if (h->scheme_a())
+    {
+        // the field source acts inside the step; halo copies and probes read the same buffer
+        StepArgs sa;
+        SchemeAArgs b;
+        scheme_a_args(h, parity, true, 0, sa, b);
+        e = timed_step_launch(h, parity, true, 0);
+        if (e != cudaSuccess) return e;
+        kernels++;
+        if (b.copy)
+        {
+            e = launch_copy_a((const float*)fc, (float*)fn, h->L, sa, b, h->stream);
+            if (e != cudaSuccess) return e;
+            kernels++;
+        }
+        e = launch_probe_a((const float*)fc, h->L, sa, b, probe_args(h, true, 0), h->stream);
+        kernels++;
+        return e;
+    }
     if (!h->srcs.empty())
     {
         e = launch_source(h->storage, fc, h->L, h->sa, source_args(h, true), h->stream);
@@ -826,7 +1019,7 @@ cudaError_t enqueue_batched_step(lbm_handle* h, int parity, int& kernels)
         if (e != cudaSuccess) return e;
         kernels++;
     }
-    e = timed_step_launch(h, fc, fn);
+    e = timed_step_launch(h, parity, true, 0);
     if (e != cudaSuccess) return e;
     kernels++;
     e = launch_probe(h->storage, fc, h->L, h->sa, probe_args(h, true, 0), h->stream);
@@ -880,15 +1073,15 @@ int fill_table(lbm_handle* h, long long s0)
     const size_t ns = h->srcs.size();
     if (ns == 0) return LBM_OK;
     CK(cudaStreamSynchronize(h->stream), "table refill");   // staging buffer reuse
-    for (long long r = 0; r < kTableRows; ++r)
+    for (long long r = 0; r <= kTableRows; ++r)   // rows of steps s0 .. s0 + kTableRows
     {
         const double t = (double)(s0 + r) * h->dt;   // t = s * dt (06:1079)
         for (size_t s = 0; s < ns; ++s) h->h_table[r * ns + s] = source_entry(h->srcs[s], t, h->dt);
     }
-    CK(cudaMemcpyAsync(h->d_table, h->h_table, ns * kTableRows * sizeof(SourceEntry), cudaMemcpyHostToDevice,
+    CK(cudaMemcpyAsync(h->d_table, h->h_table, ns * (kTableRows + 1) * sizeof(SourceEntry), cudaMemcpyHostToDevice,
                        h->stream),
        "table upload");
-    h->h2d_bytes += (long)(ns * kTableRows * sizeof(SourceEntry));
+    h->h2d_bytes += (long)(ns * (kTableRows + 1) * sizeof(SourceEntry));
     h->table_base = s0;
     h->table_rows = kTableRows;
     return LBM_OK;
@@ -899,6 +1092,16 @@ int check_ready(lbm_handle* h)
     if (!h) return LBM_ERR_INVALID_ARGUMENT;
     if (!h->inited) return h->fail(LBM_ERR_STATE, "lbm_init has not run");
     return LBM_OK;
+}
+
+// (float)(rho - 1) of the last step into d (device, interior cells).
+cudaError_t field_rho_last_step(lbm_handle* h, float* d)
+{
+    if (!h->scheme_a()) return launch_field_rho(h->storage, h->f[h->cur ^ 1], d, h->L, h->sa, h->scale, h->stream);
+    StepArgs sa;
+    SchemeAArgs b;
+    scheme_a_args(h, h->cur ^ 1, false, h->step - 1, sa, b);
+    return launch_field_rho_a((const float*)h->f[h->cur ^ 1], d, h->L, sa, b, h->stream);
 }
 
 int reset_halos_if_dirty(lbm_handle* h)
@@ -950,6 +1153,7 @@ extern "C" int lbm_apply_source(lbm_handle* h, double t)
     int st = check_ready(h);
     if (st) return st;
     if (h->srcs.empty()) return LBM_OK;
+    if (h->scheme_a()) return LBM_OK;   // scheme A: the field source acts inside lbm_step_collision_bgk
     CK(cudaSetDevice(h->device), "cudaSetDevice");
     SourceArgs a = source_args(h, false);
     for (size_t s = 0; s < h->srcs.size(); ++s) a.direct[s] = source_entry(h->srcs[s], t, h->dt);
@@ -962,6 +1166,7 @@ extern "C" int lbm_exchange_halos(lbm_handle* h)
 {
     int st = check_ready(h);
     if (st) return st;
+    if (h->scheme_a()) return LBM_OK;   // scheme A: each step writes the next step's halo values
     CK(cudaSetDevice(h->device), "cudaSetDevice");
     st = reset_halos_if_dirty(h);
     if (st) return st;
@@ -978,8 +1183,16 @@ extern "C" int lbm_step_collision_bgk(lbm_handle* h)
     int st = check_ready(h);
     if (st) return st;
     CK(cudaSetDevice(h->device), "cudaSetDevice");
-    CK(timed_step_launch(h, h->f[h->cur], h->f[h->cur ^ 1]), "step kernel");
+    CK(timed_step_launch(h, h->cur, false, h->step), "step kernel");
     h->launches++;
+    if (h->scheme_a() && h->aa.copy)
+    {
+        StepArgs sa;
+        SchemeAArgs b;
+        scheme_a_args(h, h->cur, false, h->step, sa, b);
+        CK(launch_copy_a((const float*)h->f[h->cur], (float*)h->f[h->cur ^ 1], h->L, sa, b, h->stream), "halo copy");
+        h->launches++;
+    }
     h->cur ^= 1;
     h->step++;
     return harvest_timing(h);
@@ -998,8 +1211,21 @@ extern "C" int lbm_record_probes(lbm_handle* h)
         if (st) return st;
     }
     // the pre-step buffer of the last collision step is intact until the next one
-    CK(launch_probe(h->storage, h->f[h->cur ^ 1], h->L, h->sa, probe_args(h, false, h->probe_pending), h->stream),
-       "probe kernel");
+    if (h->scheme_a())
+    {
+        StepArgs sa;
+        SchemeAArgs b;
+        scheme_a_args(h, h->cur ^ 1, false, h->step - 1, sa, b);
+        CK(launch_probe_a((const float*)h->f[h->cur ^ 1], h->L, sa, b, probe_args(h, false, h->probe_pending),
+                          h->stream),
+           "probe kernel");
+    }
+    else
+    {
+        CK(launch_probe(h->storage, h->f[h->cur ^ 1], h->L, h->sa, probe_args(h, false, h->probe_pending),
+                        h->stream),
+           "probe kernel");
+    }
     h->launches++;
     h->probe_pending++;
     return LBM_OK;
@@ -1170,7 +1396,7 @@ extern "C" int lbm_get_rho(lbm_handle* h, float* out, long capacity)
     CK(cudaSetDevice(h->device), "cudaSetDevice");
     float* d = nullptr;
     CK(cudaMalloc(&d, n * sizeof(float)), "rho buffer");
-    cudaError_t e = launch_field_rho(h->storage, h->f[h->cur ^ 1], d, L, h->sa, h->scale, h->stream);
+    cudaError_t e = field_rho_last_step(h, d);
     if (e == cudaSuccess) e = cudaMemcpyAsync(out, d, n * sizeof(float), cudaMemcpyDeviceToHost, h->stream);
     h->d2h_bytes += (long)(n * sizeof(float));
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
@@ -1202,7 +1428,7 @@ extern "C" int lbm_get_rho_noalloc(lbm_handle* h, float* out, long capacity)
     float* d = nullptr;
     CK(field_scratch_address(h->device, &d), "static field array address");
     // every cell of the first n entries is written by the kernel: nothing to clear
-    CK(launch_field_rho(h->storage, h->f[h->cur ^ 1], d, L, h->sa, h->scale, h->stream), "field kernel");
+    CK(field_rho_last_step(h, d), "field kernel");
     CK(cudaMemcpyAsync(out, d, (size_t)n * sizeof(float), cudaMemcpyDeviceToHost, h->stream), "field download");
     CK(cudaStreamSynchronize(h->stream), "field download");
     h->launches++;
@@ -1216,6 +1442,7 @@ extern "C" int lbm_get_f(lbm_handle* h, double* out, long capacity)
     if (st) return st;
     const Layout& L = h->L;
     const size_t n = (size_t)(L.nx + 2) * (L.ny + 2) * (L.nz + 2) * Q;
+    if (h->scheme_a()) return h->fail(LBM_ERR_UNSUPPORTED, "scheme A stores post-collision populations; use lbm_get_rho");
     if (!out || (long)n > capacity) return h->fail(LBM_ERR_CAPACITY, "f buffer too small");
     CK(cudaSetDevice(h->device), "cudaSetDevice");
     double* d = nullptr;
@@ -1236,6 +1463,7 @@ extern "C" int lbm_set_f(lbm_handle* h, const double* in, long count)
     if (st) return st;
     const Layout& L = h->L;
     const size_t n = (size_t)(L.nx + 2) * (L.ny + 2) * (L.nz + 2) * Q;
+    if (h->scheme_a()) return h->fail(LBM_ERR_UNSUPPORTED, "scheme A state cannot be set from f");
     if (!in || count != (long)n) return h->fail(LBM_ERR_INVALID_ARGUMENT, "f size mismatch");
     CK(cudaSetDevice(h->device), "cudaSetDevice");
     double* d = nullptr;
@@ -1594,6 +1822,7 @@ extern "C" int lbm_adjoint_grad(lbm_handle* h, int nsteps, const double* observe
     int st = check_ready(h);
     if (st) return st;
     if (h->storage != LBM_STORE_F32) return h->fail(LBM_ERR_UNSUPPORTED, "the adjoint runs on FP32 storage");
+    if (h->scheme_a()) return h->fail(LBM_ERR_UNSUPPORTED, "the adjoint differentiates scheme B");
     if (h->srcs.size() != 1) return h->fail(LBM_ERR_UNSUPPORTED, "the adjoint needs exactly one source");
     const int np = h->nprobe();
     if (np < 1) return h->fail(LBM_ERR_STATE, "the adjoint needs probes");

@@ -153,6 +153,41 @@ struct ProbeArgs
     float scale;
 };
 
+// Scheme A (the reference's 01-04 family).  The stored state is the
+// post-collision populations P^s as deviations from the background
+// equilibrium feq(1, u0) (so a uniform flow is an exact fixed point and FP32
+// resolves the acoustic perturbation, not the flow); a step pulls P^s (pull = stream of the
+// source cells' post-collision values), adds the destination source,
+// collides with the cell's own omega and stores P^{s+1}.  A population that
+// arrives from a SOLID cell must be the destination's own pre-collision value
+// of the opposite direction: each fluid cell writes that value into the
+// SOLID neighbour's (otherwise unused) slot for the next step, so the next
+// pull reads it like any other.  Zero-gradient halos are collided copies of
+// the nearest interior cell, written for the next step by k_copy_a.  x-halo
+// values live in two x-face arrays that alternate with the step parity.
+struct SchemeAArgs
+{
+    const float* om_x;         // 1/tau per interior column i-1 (tau ramp), likewise om_y, om_z;
+    const float* om_y;         //   a cell's omega is the minimum of the three
+    const float* om_z;
+    float om_bulk;             // 1/tau of halo cells (they lie outside every ramp)
+    const float* fld_x;        // source weight factors, halo-inclusive index 0..n+1;
+    const float* fld_y;        //   weight(i,j,k) = fld_x[i] fld_y[j] fld_z[k]
+    const float* fld_z;
+    int field_mode;            // -1: no field source, 0: LBM_FIELD_DST, 1: LBM_FIELD_FORCE
+    int src_index;             // which source of the schedule is the field source
+    int nsrc;
+    float flow[3];             // background velocity u0 (lattice units)
+    float base[19];            // feq(1, u0) - w_q: stored values are deviations from feq(1, u0)
+    float cu0[19];             // c_q . u0
+    float u0sq;                // u0 . u0
+    const SourceEntry* table;  // schedule rows [row][nsrc] (row = step - ctl->table_base), as SourceArgs
+    const Control* ctl;        // nullptr: use mass_direct
+    float mass_direct[2];      // mass of step s and of step s + 1 (direct launches)
+    float* xgh_out;            // x-halo values written for the next step
+    int copy;                  // zero-gradient halos on every face
+};
+
 // ---- launchers (kernels.cu) ----------------------------------------------
 // storage: 0 = float, 1 = __half.  All launches go to `stream`.
 cudaError_t launch_build_links(const uint8_t* mask_ref, uint32_t* links, uint32_t* near, const Layout& L,
@@ -185,6 +220,19 @@ cudaError_t launch_export_f(int storage, const void* f, double* out, const Layou
                             cudaStream_t stream);
 cudaError_t launch_import_f(int storage, void* f, const double* in, const Layout& L, const XFace& xf, float scale,
                             cudaStream_t stream);
+
+// Scheme A: fused step (FP32 storage), the zero-gradient halo copies of the
+// next step, the initial state, and probes / field of a scheme-A state.
+cudaError_t launch_step_a(const float* fin, float* fout, const Layout& L, const StepArgs& a, const SchemeAArgs& b,
+                          cudaStream_t stream);
+cudaError_t launch_copy_a(const float* fin, float* fout, const Layout& L, const StepArgs& a, const SchemeAArgs& b,
+                          cudaStream_t stream);
+cudaError_t launch_init_a(float* f0, float* f1, float* xgh0, float* xgh1, const uint8_t* mask_ref, const Layout& L,
+                          const SchemeAArgs& b, cudaStream_t stream);
+cudaError_t launch_probe_a(const float* f, const Layout& L, const StepArgs& sa, const SchemeAArgs& b,
+                           const ProbeArgs& a, cudaStream_t stream);
+cudaError_t launch_field_rho_a(const float* f, float* out, const Layout& L, const StepArgs& sa, const SchemeAArgs& b,
+                               cudaStream_t stream);
 
 // Capacity (cells) of the statically reserved field array used by
 // lbm_get_rho_noalloc, and the device address of that array on `device`

@@ -1,0 +1,487 @@
+// Scheme A of the D3Q19 acoustic step: the update of the reference's family-A
+// programs (01-04), FP32 deviation storage.  See SchemeAArgs (device.hpp) for
+// the state and the SOLID-neighbour slots; the per-step formulas follow
+// 02:363-420 (destination source, SOLID cells skipped) and 03:402-441
+// (forcing at the collided cell, zero-gradient halos).
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "device.hpp"
+#include "lattice.cuh"
+
+namespace lbm {
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int BC = 32;        // FP32 cells per interleaved block
+constexpr int BE = 19 * BC;   // elements per block
+
+__device__ __forceinline__ float2 ldg2(const float* p) { return __ldg(reinterpret_cast<const float2*>(p)); }
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, f2(-1.0f), a); }
+
+__device__ __forceinline__ uint32_t near_bits(const StepArgs& a, const Layout& L, int col, int j, int k)
+{
+    return a.near[((long long)k * (L.ny + 2) + j) * L.words_per_row + (col >> 5)] >> (col & 31);
+}
+
+// mass (val(t) dt gain) of step s + ahead of the field source
+__device__ __forceinline__ float field_mass(const SchemeAArgs& b, int ahead)
+{
+    if (!b.ctl) return b.mass_direct[ahead];
+    const long long row = b.ctl->step - b.ctl->table_base + ahead;
+    return (float)b.table[row * b.nsrc + b.src_index].mass;
+}
+
+__device__ __forceinline__ float cell_omega(const SchemeAArgs& b, int i, int j, int k)
+{
+    return fminf(b.om_x[i - 1], fminf(b.om_y[j - 1], b.om_z[k - 1]));
+}
+
+__device__ __forceinline__ float field_weight(const SchemeAArgs& b, int i, int j, int k)
+{
+    return b.fld_x[i] * b.fld_y[j] * b.fld_z[k];
+}
+
+// BGK of one cell on deviations d = f - feq(1, u0): with rho' = sum d,
+// J' = sum c d (so rho = 1 + rho', J = u0 + J'), the equilibrium deviation is
+//   w_q (rho' + 3 c.J' + (4.5 E_q - 1.5 E) / rho),
+//   E_q = (c.J)^2 - rho (c.u0)^2 = 2 (c.u0)(c.J') + (c.J')^2 - rho' (c.u0)^2,
+//   E   = J^2 - rho u0^2       = 2 u0.J' + J'^2 - rho' u0^2,
+// written without the cancellation of feq(rho, u) - feq(1, u0); d' = d - om (d - geq).
+__device__ __forceinline__ void moments1(const float (&G)[Q], float& rho, float& jx, float& jy, float& jz)
+{
+    rho = jx = jy = jz = 0.f;
+#pragma unroll
+    for (int q = 0; q < Q; ++q)
+    {
+        rho += G[q];
+        jx += ex(q) * G[q];
+        jy += ey(q) * G[q];
+        jz += ez(q) * G[q];
+    }
+}
+
+__device__ __forceinline__ void collide1(float (&G)[Q], float om, const SchemeAArgs& b)
+{
+    float rho, jx, jy, jz;
+    moments1(G, rho, jx, jy, jz);
+    float r = 1.0f + rho;
+    if (r <= 0.f) r = 1e-12f;
+    const float ir = 1.0f / r;
+    const float uj = b.flow[0] * jx + b.flow[1] * jy + b.flow[2] * jz;
+    const float E = 2.0f * uj + jx * jx + jy * jy + jz * jz - rho * b.u0sq;
+    const float base = rho - 1.5f * E * ir;
+#pragma unroll
+    for (int q = 0; q < Q; ++q)
+    {
+        const float cj = ex(q) * jx + ey(q) * jy + ez(q) * jz;
+        const float Eq = (2.0f * b.cu0[q] + cj) * cj - rho * b.cu0[q] * b.cu0[q];
+        const float geq = wf(q) * (base + 3.0f * cj + 4.5f * Eq * ir);
+        G[q] = G[q] - om * (G[q] - geq);
+    }
+}
+
+// forcing term of the collided cell (03:74-78, 03:422-435)
+__device__ __forceinline__ float force_term(const SchemeAArgs& b, int q, float s_amp, float om)
+{
+    return wf(q) * s_amp * (1.0f + 3.0f * b.cu0[q]) * (1.0f - 0.5f * om);
+}
+
+// Populations arriving at interior cell (i, j, k) in the step that reads f:
+// the stored values of the source cells (x-halo sources from the x-face
+// array), plus the destination source for those that left a fluid cell.
+__device__ __forceinline__ void pull_a(const float* __restrict__ f, const Layout& L, const StepArgs& sa,
+                                       const SchemeAArgs& b, int i, int j, int k, float (&G)[Q], uint32_t& lk)
+{
+    lk = sa.links[L.cell(i, j, k)];
+#pragma unroll
+    for (int q = 0; q < Q; ++q)
+    {
+        const int si = i - ex(q);
+        if (si == 0) G[q] = sa.xf.xgh[sa.xf.gh_index(0, q, j - ey(q), k - ez(q), L.ny, L.nz)];
+        else if (si == L.nx + 1) G[q] = sa.xf.xgh[sa.xf.gh_index(1, q, j - ey(q), k - ez(q), L.ny, L.nz)];
+        else G[q] = __ldg(f + L.elem(q, si, j - ey(q), k - ez(q)));
+    }
+    if (b.field_mode == 0)
+    {
+        const float S = field_mass(b, 0) * field_weight(b, i, j, k);
+#pragma unroll
+        for (int q = 0; q < Q; ++q)
+            if (!((lk >> q) & 1u)) G[q] += wf(q) * S;
+    }
+}
+
+// ---------------------------------------------------------------- step
+// Two x-adjacent cells per thread, aligned float2 loads with warp shuffles
+// for the +-1 x shift (the same access scheme as the scheme-B step).
+template <int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) k_step_a(const float* __restrict__ fin, float* __restrict__ fout,
+                                                        Layout L, StepArgs a, SchemeAArgs b)
+{
+    const int lane = threadIdx.x & 31;
+    const int c0r = 2 * (blockIdx.x * BLOCK + threadIdx.x);
+    const bool active = c0r < L.nx;
+    const int c0 = active ? c0r : ((L.nx - 1) & ~1);   // inactive lanes shadow a valid pair
+    const int j = blockIdx.y + 1, k = blockIdx.z + 1;
+    const long long e0 = L.elem(0, c0 + 1, j, k);
+    const float* own = fin + e0;
+    const long long rs = L.row_stride, ps = L.plane_stride;
+
+    uint32_t lk0 = 0, lk1 = 0;
+    if (active)
+    {
+        const uint32_t nb = near_bits(a, L, c0, j, k) & 3u;
+        const long long cl = L.cell(c0 + 1, j, k);
+        if (nb & 1u) lk0 = a.links[cl];
+        if (nb & 2u) lk1 = a.links[cl + 1];
+    }
+    const bool any_link = __any_sync(kFull, (lk0 | lk1) != 0u);
+
+    float2 G[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q)
+    {
+        const float* row = own - (ey(q) * rs + ez(q) * ps) + q * BC;
+        const float2 cur = ldg2(row);
+        if (ex(q) == 0)
+        {
+            G[q] = cur;
+        }
+        else if (ex(q) > 0)
+        {
+            float prev = __shfl_up_sync(kFull, cur.y, 1);
+            if (lane == 0) prev = ldg2(row - BE + (BC - 2)).y;
+            G[q] = make_float2(prev, cur.x);
+        }
+        else
+        {
+            float next = __shfl_down_sync(kFull, cur.x, 1);
+            if (lane == 31) next = ldg2(row + BE - (BC - 2)).x;
+            G[q] = make_float2(cur.y, next);
+        }
+    }
+    const bool has1 = c0 + 1 < L.nx;
+    const bool xlo = active && c0 == 0, xhi0 = active && c0 == L.nx - 1, xhi1 = active && c0 + 1 == L.nx - 1;
+    if (xlo | xhi0 | xhi1)
+    {
+#pragma unroll
+        for (int q = 0; q < Q; ++q)
+        {
+            if (ex(q) == 0) continue;
+            const float g = a.xf.xgh[a.xf.gh_index(ex(q) > 0 ? 0 : 1, q, j - ey(q), k - ez(q), L.ny, L.nz)];
+            if (ex(q) > 0 && xlo) G[q].x = g;
+            if (ex(q) < 0 && xhi0) G[q].x = g;
+            if (ex(q) < 0 && xhi1) G[q].y = g;
+        }
+    }
+    if (!active) return;
+    const bool solid0 = (lk0 & kSolidSelfBit) != 0u;
+    const bool solid1 = !has1 || (lk1 & kSolidSelfBit) != 0u;
+    if (solid0 && solid1) return;   // SOLID cells are not updated (02:371)
+
+    // destination source, for populations that left a fluid cell (02:373, 02:405)
+    if (b.field_mode == 0)
+    {
+        const float m = field_mass(b, 0);
+        const float2 S = make_float2(m * field_weight(b, c0 + 1, j, k), has1 ? m * field_weight(b, c0 + 2, j, k) : 0.f);
+#pragma unroll
+        for (int q = 0; q < Q; ++q)
+        {
+            const float2 add = mul2(f2(wf(q)), S);
+            if (!((lk0 >> q) & 1u)) G[q].x += add.x;
+            if (!((lk1 >> q) & 1u)) G[q].y += add.y;
+        }
+    }
+    // pre-collision values for the SOLID neighbours' slots: the next step
+    // pulls direction q from the SOLID cell dst - e_q and must read this
+    // cell's own value of direction inv(q) (02:391-394)
+    if (any_link)
+    {
+#pragma unroll
+        for (int q = 0; q < Q; ++q)
+        {
+#pragma unroll
+            for (int c = 0; c < 2; ++c)
+            {
+                const uint32_t lkc = c ? lk1 : lk0;
+                const bool sol = c ? solid1 : solid0;
+                if (sol || !((lkc >> q) & 1u)) continue;
+                const int si = c0 + 1 + c - ex(q), sj = j - ey(q), sk = k - ez(q);
+                const float v = c ? G[inv(q)].y : G[inv(q)].x;
+                if (si == 0 || si == L.nx + 1) b.xgh_out[a.xf.gh_index(si == 0 ? 0 : 1, q, sj, sk, L.ny, L.nz)] = v;
+                else fout[L.elem(q, si, sj, sk)] = v;
+            }
+        }
+    }
+
+    // BGK with each cell's own omega, FP32x2
+    const float2 om = make_float2(cell_omega(b, c0 + 1, j, k), has1 ? cell_omega(b, c0 + 2, j, k) : 1.0f);
+    {
+        float2 rho = f2(0.f), jx = f2(0.f), jy = f2(0.f), jz = f2(0.f);
+#pragma unroll
+        for (int q = 0; q < Q; ++q)
+        {
+            rho = add2(rho, G[q]);
+            if (ex(q) > 0) jx = add2(jx, G[q]);
+            if (ex(q) < 0) jx = sub2(jx, G[q]);
+            if (ey(q) > 0) jy = add2(jy, G[q]);
+            if (ey(q) < 0) jy = sub2(jy, G[q]);
+            if (ez(q) > 0) jz = add2(jz, G[q]);
+            if (ez(q) < 0) jz = sub2(jz, G[q]);
+        }
+        float2 r = add2(rho, f2(1.0f));
+        if (r.x <= 0.f) r.x = 1e-12f;
+        if (r.y <= 0.f) r.y = 1e-12f;
+        const float2 ir = make_float2(1.0f / r.x, 1.0f / r.y);
+        // E = 2 u0.J' + J'^2 - rho' u0^2 (see collide1)
+        const float2 uj = fma2(f2(b.flow[2]), jz, fma2(f2(b.flow[1]), jy, mul2(f2(b.flow[0]), jx)));
+        const float2 E = fma2(rho, f2(-b.u0sq), fma2(uj, f2(2.0f), fma2(jz, jz, fma2(jy, jy, mul2(jx, jx)))));
+        const float2 base = fma2(mul2(ir, E), f2(-1.5f), rho);
+        const float2 k45 = mul2(ir, f2(4.5f));
+        const float2 keep = sub2(f2(1.0f), om);
+#pragma unroll
+        for (int q = 0; q < Q; ++q)
+        {
+            float2 cj = f2(0.f);
+            if (ex(q) > 0) cj = add2(cj, jx);
+            if (ex(q) < 0) cj = sub2(cj, jx);
+            if (ey(q) > 0) cj = add2(cj, jy);
+            if (ey(q) < 0) cj = sub2(cj, jy);
+            if (ez(q) > 0) cj = add2(cj, jz);
+            if (ez(q) < 0) cj = sub2(cj, jz);
+            const float c0 = b.cu0[q];
+            // E_q = (2 c.u0 + c.J') c.J' - rho' (c.u0)^2
+            const float2 Eq = fma2(rho, f2(-c0 * c0), mul2(add2(f2(2.0f * c0), cj), cj));
+            const float2 geq = mul2(f2(wf(q)), fma2(cj, f2(3.0f), fma2(k45, Eq, base)));
+            G[q] = fma2(keep, G[q], mul2(om, geq));
+        }
+    }
+    // forcing of this cell for the populations it sends next (03:424-435)
+    if (b.field_mode == 1)
+    {
+        const float m = field_mass(b, 1);
+        const float s0 = m * field_weight(b, c0 + 1, j, k), s1 = has1 ? m * field_weight(b, c0 + 2, j, k) : 0.f;
+#pragma unroll
+        for (int q = 0; q < Q; ++q)
+        {
+            G[q].x += force_term(b, q, s0, om.x);
+            G[q].y += force_term(b, q, s1, om.y);
+        }
+    }
+
+    float* out = fout + e0;
+    if (!(solid0 | solid1))
+    {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) *reinterpret_cast<float2*>(out + q * BC) = G[q];
+    }
+    else
+    {
+        // a SOLID cell's slots hold what its neighbours wrote for the next step
+#pragma unroll
+        for (int q = 0; q < Q; ++q)
+        {
+            if (!solid0) out[q * BC] = G[q].x;
+            if (!solid1) out[q * BC + 1] = G[q].y;
+        }
+    }
+}
+
+// ---------------------------------------------------------------- halo copies
+// Zero-gradient halos (03:175-237): every halo cell is a copy of the nearest
+// interior cell I taken before the step and then collided like any cell,
+// with the halo's own tau (outside every ramp) and source weight.  For the
+// step after this one, the halo's post-collision values are
+// C_bulk(f(I)) + force(halo), with f(I) the populations arriving at I in this
+// step.  One thread per halo cell: x-halo planes (edges and corners
+// included), then the y-halo rows, then the z-halo rows.
+__global__ void __launch_bounds__(128) k_copy_a(const float* __restrict__ fin, float* __restrict__ fout, Layout L,
+                                                 StepArgs a, SchemeAArgs b)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long nyt = L.ny + 2, nzt = L.nz + 2;
+    const long long nX = 2 * nyt * nzt, nY = 2LL * L.nx * nzt, nZ = 2LL * L.nx * L.ny;
+    int ih, jh, kh;
+    if (t < nX)
+    {
+        const long long r = t % (nyt * nzt);
+        ih = t < nyt * nzt ? 0 : L.nx + 1;
+        jh = (int)(r % nyt);
+        kh = (int)(r / nyt);
+    }
+    else if (t < nX + nY)
+    {
+        const long long u = t - nX, r = u % (L.nx * nzt);
+        jh = u < L.nx * nzt ? 0 : L.ny + 1;
+        ih = 1 + (int)(r % L.nx);
+        kh = (int)(r / L.nx);
+    }
+    else if (t < nX + nY + nZ)
+    {
+        const long long u = t - nX - nY, r = u % ((long long)L.nx * L.ny);
+        kh = u < (long long)L.nx * L.ny ? 0 : L.nz + 1;
+        ih = 1 + (int)(r % L.nx);
+        jh = 1 + (int)(r / L.nx);
+    }
+    else
+    {
+        return;
+    }
+    const int i = min(max(ih, 1), L.nx), j = min(max(jh, 1), L.ny), k = min(max(kh, 1), L.nz);
+    float G[Q];
+    uint32_t lk;
+    pull_a(fin, L, a, b, i, j, k, G, lk);
+    collide1(G, b.om_bulk, b);
+    if (b.field_mode == 1)
+    {
+        const float s = field_mass(b, 1) * field_weight(b, ih, jh, kh);
+#pragma unroll
+        for (int q = 0; q < Q; ++q) G[q] += force_term(b, q, s, b.om_bulk);
+    }
+    if (ih == 0 || ih == L.nx + 1)
+    {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) b.xgh_out[a.xf.gh_index(ih == 0 ? 0 : 1, q, jh, kh, L.ny, L.nz)] = G[q];
+    }
+    else
+    {
+        float* out = fout + L.elem(0, ih, jh, kh);
+#pragma unroll
+        for (int q = 0; q < Q; ++q) out[q * BC] = G[q];
+    }
+}
+
+// ---------------------------------------------------------------- set-up
+// Initial state of both population buffers and both x-face arrays, as
+// deviations from feq(1, u0): fluid cells 0; fluid halo cells 0 with
+// zero-gradient halos and rest w_q (-base) otherwise; a SOLID cell's slot q
+// holds the value its neighbour cell + e_q would put there, feq(1, u0) of
+// direction inv(q).
+// mask_ref: the reference's halo-inclusive mask, i fastest.
+__global__ void __launch_bounds__(128) k_init_a(float* __restrict__ f0, float* __restrict__ f1,
+                                                float* __restrict__ xgh0, float* __restrict__ xgh1,
+                                                const uint8_t* __restrict__ m, Layout L, SchemeAArgs b)
+{
+    const int i0 = blockIdx.x * blockDim.x + threadIdx.x;   // 0..nx+1
+    const int j = blockIdx.y, k = blockIdx.z;               // halo-inclusive
+    if (i0 > L.nx + 1) return;
+    const long long nxt = L.nx + 2, nyt = L.ny + 2;
+    const bool solid = m[(long long)i0 + j * nxt + k * nxt * nyt] != 0;
+    const bool halo = i0 == 0 || i0 == L.nx + 1 || j == 0 || j == L.ny + 1 || k == 0 || k == L.nz + 1;
+#pragma unroll
+    for (int q = 0; q < Q; ++q)
+    {
+        float v = 0.f;
+        if (solid) v = b.base[inv(q)] - b.base[q];
+        else if (halo && !b.copy) v = -b.base[q];
+        if (i0 == 0 || i0 == L.nx + 1)
+        {
+            const long long g = XFace{nullptr, nullptr}.gh_index(i0 == 0 ? 0 : 1, q, j, k, L.ny, L.nz);
+            xgh0[g] = v;
+            xgh1[g] = v;
+        }
+        else
+        {
+            const long long e = L.elem(q, i0, j, k);
+            f0[e] = v;
+            f1[e] = v;
+        }
+    }
+}
+
+// ---------------------------------------------------------------- probes, field
+// rho - 1 after the step that reads f (the reference records rho of the
+// arriving populations, 02:411, 03:438); SOLID cells read 0.
+__global__ void __launch_bounds__(256) k_probe_a(const float* __restrict__ f, Layout L, StepArgs sa, SchemeAArgs b,
+                                                 ProbeArgs a)
+{
+    const long long row = a.ctl ? a.ctl->step - a.ctl->probe_base : a.direct_row;
+    for (int p = threadIdx.x; p < a.n; p += blockDim.x)
+    {
+        const int i = a.ijk[3 * p], j = a.ijk[3 * p + 1], k = a.ijk[3 * p + 2];
+        double val;
+        if (i < 0)
+        {
+            val = __longlong_as_double(0x7ff8000000000000LL);
+        }
+        else
+        {
+            float G[Q];
+            uint32_t lk;
+            pull_a(f, L, sa, b, i, j, k, G, lk);
+            float rho = 0.f;
+#pragma unroll
+            for (int q = 0; q < Q; ++q) rho += G[q];
+            val = (lk & kSolidSelfBit) ? 0.0 : (double)rho;
+            a.energy[p] += val * val;
+        }
+        a.out[row * a.n + p] = val;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && a.ctl) a.ctl->step += 1;
+}
+
+__global__ void __launch_bounds__(128) k_field_rho_a(const float* __restrict__ f, float* __restrict__ out, Layout L,
+                                                     StepArgs sa, SchemeAArgs b)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    if (i > L.nx) return;
+    const int j = blockIdx.y + 1, k = blockIdx.z + 1;
+    float G[Q];
+    uint32_t lk;
+    pull_a(f, L, sa, b, i, j, k, G, lk);
+    float rho = 0.f;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) rho += G[q];
+    out[((long long)(k - 1) * L.ny + (j - 1)) * L.nx + (i - 1)] = (lk & kSolidSelfBit) ? 0.f : rho;
+}
+
+}  // namespace
+
+cudaError_t launch_step_a(const float* fin, float* fout, const Layout& L, const StepArgs& a, const SchemeAArgs& b,
+                          cudaStream_t stream)
+{
+    if (L.bc != BC) return cudaErrorInvalidValue;
+    constexpr int kBlock = 128;
+    const dim3 g((unsigned)((L.nx + 2 * kBlock - 1) / (2 * kBlock)), (unsigned)L.ny, (unsigned)L.nz);
+    k_step_a<kBlock, 0><<<g, kBlock, 0, stream>>>(fin, fout, L, a, b);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_copy_a(const float* fin, float* fout, const Layout& L, const StepArgs& a, const SchemeAArgs& b,
+                          cudaStream_t stream)
+{
+    const long long n = 2LL * (L.ny + 2) * (L.nz + 2) + 2LL * L.nx * (L.nz + 2) + 2LL * L.nx * L.ny;
+    k_copy_a<<<(unsigned)((n + 127) / 128), 128, 0, stream>>>(fin, fout, L, a, b);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_init_a(float* f0, float* f1, float* xgh0, float* xgh1, const uint8_t* mask_ref, const Layout& L,
+                          const SchemeAArgs& b, cudaStream_t stream)
+{
+    const dim3 g((unsigned)((L.nx + 2 + 127) / 128), (unsigned)(L.ny + 2), (unsigned)(L.nz + 2));
+    k_init_a<<<g, 128, 0, stream>>>(f0, f1, xgh0, xgh1, mask_ref, L, b);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_probe_a(const float* f, const Layout& L, const StepArgs& sa, const SchemeAArgs& b,
+                           const ProbeArgs& a, cudaStream_t stream)
+{
+    k_probe_a<<<1, 256, 0, stream>>>(f, L, sa, b, a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_field_rho_a(const float* f, float* out, const Layout& L, const StepArgs& sa, const SchemeAArgs& b,
+                               cudaStream_t stream)
+{
+    const dim3 g((unsigned)((L.nx + 127) / 128), (unsigned)L.ny, (unsigned)L.nz);
+    k_field_rho_a<<<g, 128, 0, stream>>>(f, out, L, sa, b);
+    return cudaGetLastError();
+}
+
+}  // namespace lbm

@@ -28,11 +28,13 @@ LBM_ERR_IO = -9
 LBM_ERR_UNSUPPORTED = -10
 LBM_NOALLOC_MAX_CELLS = 8388608
 
-LBM_BC_NSCBC, LBM_BC_REST, LBM_BC_WALL = 0, 1, 2
+LBM_BC_NSCBC, LBM_BC_REST, LBM_BC_WALL, LBM_BC_COPY = 0, 1, 2, 3
+LBM_SCHEME_B, LBM_SCHEME_A = 0, 1
+LBM_FIELD_DST, LBM_FIELD_FORCE = 0, 1
 FACE_XLO, FACE_XHI, FACE_YLO, FACE_YHI, FACE_ZLO, FACE_ZHI = range(6)
 LBM_STORE_F32, LBM_STORE_F16 = 0, 1
 LBM_WAVE_GAUSS, LBM_WAVE_SINE, LBM_WAVE_RICKER, LBM_WAVE_TABLE = 0, 1, 2, 3
-LBM_INJECT_GAUSS, LBM_INJECT_TRILINEAR = 0, 1
+LBM_INJECT_GAUSS, LBM_INJECT_TRILINEAR, LBM_INJECT_FIELD = 0, 1, 2
 
 # Family-B lattice (06:21-31)
 Q = 19
@@ -62,6 +64,10 @@ class LbmConfig(ctypes.Structure):
         ("device", ctypes.c_int),
         ("use_graphs", ctypes.c_int),
         ("verbose", ctypes.c_int),
+        ("scheme", ctypes.c_int),
+        ("tau_sponge_max", ctypes.c_double),
+        ("flow", ctypes.c_double * 3),
+        ("dt", ctypes.c_double),
     ]
 
 
@@ -80,6 +86,7 @@ class LbmSource(ctypes.Structure):
         ("radius", ctypes.c_int),
         ("table", c_double_p),
         ("table_len", ctypes.c_int),
+        ("field_mode", ctypes.c_int),
     ]
 
 
@@ -119,7 +126,14 @@ def reference_config(**kw):
     c.device = 0
     c.use_graphs = 1
     c.verbose = 0
+    c.scheme = LBM_SCHEME_B
+    c.tau_sponge_max = 0.0
+    c.dt = 0.0
     for k, v in kw.items():
+        if k == "flow":
+            for a in range(3):
+                c.flow[a] = v[a]
+            continue
         if k == "face_bc":
             for f in range(6):
                 c.face_bc[f] = v[f]

@@ -24,7 +24,7 @@ NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 CXX = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-CU_SOURCES = ["kernels.cu", "adjoint.cu"]
+CU_SOURCES = ["kernels.cu", "adjoint.cu", "scheme_a.cu"]
 CXX_SOURCES = ["api.cpp", "geometry.cpp"]
 HEADERS = ["adjoint.hpp", "device.hpp", "geometry.hpp", "lattice.cuh"]
 

@@ -53,8 +53,20 @@ enum
 {
     LBM_BC_NSCBC = 0,  /* characteristic open boundary, zero incoming wave (06:684-835) */
     LBM_BC_REST = 1,   /* halo held at rest equilibrium w_q (06:677-682 with use_nscbc=false) */
-    LBM_BC_WALL = 2    /* SOLID halo: halfway bounce-back (ground plane, 06:520-531) */
+    LBM_BC_WALL = 2,   /* SOLID halo: halfway bounce-back (ground plane, 06:520-531) */
+    LBM_BC_COPY = 3    /* zero-gradient halo, a copy of the nearest interior cell that then
+                          collides like any cell (fill_halo_copy 03:175-237); scheme A only,
+                          and then on all six faces */
 };
+
+/* Update scheme.  B is the family of 05-08 (06:906-972): pull, halfway
+ * bounce-back, BGK with one tau and a sponge blend toward rest.  A is the
+ * family of 01-04 (02:363-420, 03:402-441): every population arriving at a
+ * cell is the post-collision value of the cell it left, relaxed with that
+ * cell's own tau (a tau ramp is the sponge, 02:164-179, 03:148-160), while a
+ * population arriving from a SOLID cell is the destination's own
+ * pre-collision value of the opposite direction. */
+enum { LBM_SCHEME_B = 0, LBM_SCHEME_A = 1 };
 enum { LBM_FACE_XLO = 0, LBM_FACE_XHI, LBM_FACE_YLO, LBM_FACE_YHI, LBM_FACE_ZLO, LBM_FACE_ZHI };
 
 enum { LBM_STORE_F32 = 0, LBM_STORE_F16 = 1 };
@@ -71,7 +83,17 @@ enum
 enum
 {
     LBM_INJECT_GAUSS = 0,     /* (2R+1)^3 Gaussian, fluid-normalised          (06:587-666) */
-    LBM_INJECT_TRILINEAR = 1  /* 8 cells, trilinear weights, fluid-normalised */
+    LBM_INJECT_TRILINEAR = 1, /* 8 cells, trilinear weights, fluid-normalised */
+    LBM_INJECT_FIELD = 2      /* scheme A: every cell, weight exp(-|x - s|^2 / (2 sigma^2)),
+                                 sigma = sigma_cells * dx, not normalised (02:181, 03:166-169) */
+};
+/* How a LBM_INJECT_FIELD source enters a scheme-A step. */
+enum
+{
+    LBM_FIELD_DST = 0,   /* w_q * weight(dst) * val(t) * dt added to every population streamed
+                            from a fluid cell, after the collision (02:373, 02:405) */
+    LBM_FIELD_FORCE = 1  /* forcing at the cell being collided: w_q * weight * val(t) * dt
+                            * (1 + 3 c_q.flow) * (1 - 1/(2 tau)) (03:74-78, 03:424-435) */
 };
 
 /* Solver configuration: the member fields of LBMSolver (06:244-268), the
@@ -94,6 +116,15 @@ typedef struct lbm_config
     int device;                                      /* CUDA device ordinal */
     int use_graphs;                                  /* replay multi-step runs as CUDA graphs */
     int verbose;                                     /* print the reference's progress lines */
+    /* scheme A (01-04 family); ignored by scheme B */
+    int scheme;                                      /* LBM_SCHEME_B (default) or LBM_SCHEME_A */
+    double tau_sponge_max;                           /* tau at the sponge faces: tau + (max - tau) r^2,
+                                                        r = (width - d)/width, d = cells to the nearest
+                                                        sponge face (02:164-179, 03:148-160); <= 0: none */
+    double flow[3];                                  /* uniform background velocity, lattice units
+                                                        (03:121 uz = Ma cs); initial state feq(1, flow) */
+    double dt;                                       /* > 0: time step in seconds instead of cs*dx/c_phys
+                                                        (02:36 uses the constant 0.577350269) */
 } lbm_config;
 
 /* One sound source: DroneSource (06:211-239) plus its time function. */
@@ -112,6 +143,7 @@ typedef struct lbm_source
     int radius;             /* Gaussian stencil radius in cells (06:587: 2), 0..3 */
     const double* table;    /* LBM_WAVE_TABLE samples (copied at lbm_add_source) */
     int table_len;
+    int field_mode;         /* LBM_FIELD_* for LBM_INJECT_FIELD */
 } lbm_source;
 
 /* Seeded synthetic city: axis-aligned box buildings written as triangles. */

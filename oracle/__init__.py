@@ -70,6 +70,7 @@ def _load():
             "orc_get_ground_height": (None, [P, _dp]),
             "orc_get_probes": (ctypes.c_long, [P, _dp, ctypes.c_long]),
             "orc_adjoint_grad": (ctypes.c_int, [P, ctypes.c_int, _dp, ctypes.c_int, _dp, _dp, _dp, _dp]),
+            "orc_get_tau_a": (None, [P, _dp]),
         }
         for n, (r, a) in sig.items():
             fn = getattr(lib, n)
@@ -197,6 +198,12 @@ class OracleSolver:
         self.lib.orc_get_ground_height(self.h, _ptr(out))
         return out
 
+    def get_tau_a(self):
+        """Per-cell tau of a scheme-A run (the ramp sponge)."""
+        out = np.empty(self.ncell_halo)
+        self.lib.orc_get_tau_a(self.h, _ptr(out))
+        return out
+
     def adjoint_grad(self, observed, K=0):
         """FP64 discrete adjoint (orc_adjoint_grad): (loss, grad_pos[3],
         grad_signal[nsteps], predicted[nsteps, nprobe]); needs the state right
@@ -219,6 +226,75 @@ class OracleSolver:
             if n >= 0:
                 return out[: n * self.nprobe].reshape(n, self.nprobe)
             cap = cap * 4 + 1024 * max(self.nprobe, 1)
+
+
+class RefAParams(ctypes.Structure):
+    _fields_ = ([(n, ctypes.c_double) for n in "x_min x_max y_min y_max z_min z_max dx amp b_param omega Ma "
+                 "tau_bulk tau_sponge_max".split()] + [("sponge_width", ctypes.c_int), ("omega_lb", ctypes.c_double)])
+
+
+def refa_available(which):
+    return os.path.exists(os.path.join(HERE, "_ref", "libref%s.so" % which))
+
+
+class RefASolver:
+    """An unmodified family-A reference program (02 Lloyd's mirror or 03
+    Doppler) through oracle/ref_harness_a.cpp: set-up, then steps of
+    exchange_halos() + step(); fields in the reference's own layout."""
+
+    def __init__(self, which, **params):
+        lib = ctypes.CDLL(os.path.join(HERE, "_ref", "libref%s.so" % which))
+        P = ctypes.c_void_p
+        for n, (r, a) in {"refa_create": (P, [ctypes.POINTER(RefAParams)]), "refa_destroy": (None, [P]),
+                          "refa_dims": (None, [P, abi.c_int_p]), "refa_dt": (ctypes.c_double, [P]),
+                          "refa_step": (None, [P, ctypes.c_int]), "refa_get_rho": (None, [P, _dp]),
+                          "refa_get_f": (None, [P, _dp]), "refa_get_tau": (None, [P, _dp]),
+                          "refa_get_source": (None, [P, _dp]), "refa_get_mask": (None, [P, abi.c_uint8_p]),
+                          "refa_set_threads": (None, [ctypes.c_int])}.items():
+            fn = getattr(lib, n)
+            fn.restype, fn.argtypes = r, a
+        self.lib = lib
+        p = RefAParams()
+        for k, v in params.items():
+            setattr(p, k, v)
+        self.h = lib.refa_create(ctypes.byref(p))
+        n3 = (ctypes.c_int * 3)()
+        lib.refa_dims(self.h, n3)
+        self.dims_halo = tuple(n3)
+        self.dt = lib.refa_dt(self.h)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.refa_destroy(self.h)
+            self.h = None
+
+    @property
+    def ncell_halo(self):
+        nx, ny, nz = self.dims_halo
+        return nx * ny * nz
+
+    def step(self, n=1):
+        self.lib.refa_step(self.h, int(n))
+
+    def _get(self, fn, n, dtype=np.float64, t=_dp):
+        out = np.empty(n, dtype=dtype)
+        fn(self.h, _ptr(out, t))
+        return out
+
+    def get_rho(self):
+        return self._get(self.lib.refa_get_rho, self.ncell_halo)
+
+    def get_f(self):
+        return self._get(self.lib.refa_get_f, self.ncell_halo * 19)
+
+    def get_tau(self):
+        return self._get(self.lib.refa_get_tau, self.ncell_halo)
+
+    def get_source(self):
+        return self._get(self.lib.refa_get_source, self.ncell_halo)
+
+    def get_mask(self):
+        return self._get(self.lib.refa_get_mask, self.ncell_halo, np.uint8, abi.c_uint8_p)
 
 
 class RefParams(ctypes.Structure):

@@ -55,6 +55,7 @@ struct orc_handle
     size_t Nloc;
     double dt;
     double *f_curr, *f_next, *rho, *sponge, *gH;
+    double *tau_a, *field_a;   /* scheme A: per-cell tau (ramp sponge) and source weight */
     unsigned char* mask;
     int mask_override;
     /* geometry (GeometryEngine 06:60-193) */
@@ -116,6 +117,7 @@ void orc_destroy(orc_handle* h)
 {
     if (!h) return;
     free(h->f_curr); free(h->f_next); free(h->rho); free(h->sponge); free(h->gH); free(h->mask);
+    free(h->tau_a); free(h->field_a);
     free(h->tris); free(h->bin_start); free(h->bin_items);
     for (int i = 0; i < h->nsrc; ++i) free(h->srcs[i].table);
     free(h->srcs); free(h->probe_xyz); free(h->probe_idx); free(h->series);
@@ -380,6 +382,179 @@ static void init_domain(orc_handle* h)
         }
 }
 
+static double source_value(const orc_handle* h, const src_t* s, double t);
+
+/* ---------------------------------------------------------------- scheme A
+ * The reference's family-A update (01-04): every population arriving at a
+ * fluid cell is the post-collision value of the cell it left, relaxed with
+ * that cell's tau; a population arriving from a SOLID cell is the
+ * destination's own pre-collision value of the opposite direction; SOLID
+ * cells are not updated (02:363-420, 03:402-441).  Family-A direction order
+ * (02:15-19, 03:15-17). */
+static const int EXA[Q] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0};
+static const int EYA[Q] = {0, 0, 0, 1, -1, 0, 0, 1, -1, -1, 1, 0, 0, 0, 0, 1, -1, 1, -1};
+static const int EZA[Q] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, -1, -1, 1};
+static const int INVA[Q] = {0, 2, 1, 4, 3, 6, 5, 8, 7, 10, 9, 12, 11, 14, 13, 16, 15, 18, 17};
+
+static inline double feq_a(int q, double r, double ux, double uy, double uz)
+{
+    double cu = EXA[q] * ux + EYA[q] * uy + EZA[q] * uz;
+    double u2 = ux * ux + uy * uy + uz * uz;
+    return W[q] * r * (1.0 + 3.0 * cu + 4.5 * cu * cu - 1.5 * u2);
+}
+
+/* tau ramp (02:164-179, 03:148-160): d = whole cells to the nearest sponge
+ * face (halo cells have d < 0), tau = tau + (max - tau) ((w - d) / w)^2 for
+ * 0 <= d < w; source weights exp(-|x - s|^2 / (2 sigma^2)) at every cell
+ * centre (02:181, 03:166-169); initial state feq(1, flow) (03:162-163). */
+static void init_scheme_a(orc_handle* h)
+{
+    const lbm_config* c = &h->cfg;
+    const unsigned sf = c->sponge_faces;
+    const int w = (int)c->sponge_width;
+    h->tau_a = (double*)malloc(h->Nloc * sizeof(double));
+    h->field_a = (double*)calloc(h->Nloc, sizeof(double));
+    const src_t* fs = NULL;
+    for (int i = 0; i < h->nsrc; ++i)
+        if (h->srcs[i].s.injection == LBM_INJECT_FIELD) fs = &h->srcs[i];
+    const double sig = fs ? fs->s.sigma_cells * c->dx : 1.0;
+    #pragma omp parallel for collapse(2)
+    for (int k = 0; k < h->nz_t; ++k)
+        for (int j = 0; j < h->ny_t; ++j)
+            for (int i = 0; i < h->nx_t; ++i)
+            {
+                const size_t idx = loc(h, i, j, k);
+                const int gx = i - 1, gy = j - 1, gz = k - 1;
+                int d = 1 << 30;
+                if (sf & (1u << LBM_FACE_XLO)) d = gx < d ? gx : d;
+                if (sf & (1u << LBM_FACE_XHI)) d = h->NXg - 1 - gx < d ? h->NXg - 1 - gx : d;
+                if (sf & (1u << LBM_FACE_YLO)) d = gy < d ? gy : d;
+                if (sf & (1u << LBM_FACE_YHI)) d = h->NYg - 1 - gy < d ? h->NYg - 1 - gy : d;
+                if (sf & (1u << LBM_FACE_ZLO)) d = gz < d ? gz : d;
+                if (sf & (1u << LBM_FACE_ZHI)) d = h->NZg - 1 - gz < d ? h->NZg - 1 - gz : d;
+                double tau = c->tau;
+                if (c->tau_sponge_max > 0 && d >= 0 && d < w)
+                {
+                    const double r = (double)(w - d) / w;
+                    tau = c->tau + (c->tau_sponge_max - c->tau) * r * r;
+                }
+                h->tau_a[idx] = tau;
+                if (fs)
+                {
+                    const double x = c->x_min + (gx + 0.5) * c->dx - fs->s.sx;
+                    const double y = c->y_min + (gy + 0.5) * c->dx - fs->s.sy;
+                    const double z = c->z_min + (gz + 0.5) * c->dx - fs->s.sz;
+                    h->field_a[idx] = exp(-(x * x + y * y + z * z) / (2.0 * sig * sig));
+                }
+                for (int q = 0; q < Q; ++q) h->f_curr[idx * Q + q] = feq_a(q, 1.0, c->flow[0], c->flow[1], c->flow[2]);
+            }
+}
+
+/* Halo fill of a scheme-A step: REST faces hold feq(1, 0) (02:227-360 at
+ * MPI size 1), COPY faces take the nearest interior cell (03:175-237, x
+ * faces first, then y, then z, each over the whole halo plane). */
+static void halos_a(orc_handle* h)
+{
+    const lbm_config* c = &h->cfg;
+    if (c->face_bc[0] == LBM_BC_COPY)
+    {
+        const int nxt = h->nx_t, nyt = h->ny_t, nzt = h->nz_t;
+        for (int k = 0; k < nzt; ++k)
+            for (int j = 0; j < nyt; ++j)
+            {
+                memcpy(&h->f_curr[loc(h, 0, j, k) * Q], &h->f_curr[loc(h, 1, j, k) * Q], Q * sizeof(double));
+                memcpy(&h->f_curr[loc(h, h->nx + 1, j, k) * Q], &h->f_curr[loc(h, h->nx, j, k) * Q], Q * sizeof(double));
+            }
+        for (int k = 0; k < nzt; ++k)
+            for (int i = 0; i < nxt; ++i)
+            {
+                memcpy(&h->f_curr[loc(h, i, 0, k) * Q], &h->f_curr[loc(h, i, 1, k) * Q], Q * sizeof(double));
+                memcpy(&h->f_curr[loc(h, i, h->ny + 1, k) * Q], &h->f_curr[loc(h, i, h->ny, k) * Q], Q * sizeof(double));
+            }
+        for (int j = 0; j < nyt; ++j)
+            for (int i = 0; i < nxt; ++i)
+            {
+                memcpy(&h->f_curr[loc(h, i, j, 0) * Q], &h->f_curr[loc(h, i, j, 1) * Q], Q * sizeof(double));
+                memcpy(&h->f_curr[loc(h, i, j, h->nz + 1) * Q], &h->f_curr[loc(h, i, j, h->nz) * Q], Q * sizeof(double));
+            }
+        return;
+    }
+    orc_exchange_halos(h);   /* REST faces: feq(1,0); WALL halos are SOLID and never read */
+}
+
+/* One scheme-A step at step index s (time t = s dt). */
+void orc_exchange_halos(orc_handle* h);
+
+static void step_a(orc_handle* h, long s)
+{
+    const lbm_config* c = &h->cfg;
+    const double t = s * h->dt;
+    const src_t* fs = NULL;
+    for (int i = 0; i < h->nsrc; ++i)
+        if (h->srcs[i].s.injection == LBM_INJECT_FIELD) fs = &h->srcs[i];
+    const double mass = fs ? source_value(h, fs, t) * h->dt * fs->s.gain : 0.0;
+    const int force = fs && fs->s.field_mode == LBM_FIELD_FORCE;
+    const double fx = c->flow[0], fy = c->flow[1], fz = c->flow[2];
+    halos_a(h);
+    const int nx = h->nx, ny = h->ny, nz = h->nz;
+    #pragma omp parallel for collapse(2)
+    for (int k = 1; k <= nz; ++k)
+        for (int j = 1; j <= ny; ++j)
+            for (int i = 1; i <= nx; ++i)
+            {
+                const size_t dst = loc(h, i, j, k);
+                if (h->mask[dst] == SOLID) continue;
+                double rho_new = 0.0;
+                for (int q = 0; q < Q; ++q)
+                {
+                    const size_t src = loc(h, i - EXA[q], j - EYA[q], k - EZA[q]);
+                    double fn;
+                    if (h->mask[src] == SOLID)
+                    {
+                        fn = h->f_curr[dst * Q + INVA[q]];
+                    }
+                    else
+                    {
+                        double r = 0, ux = 0, uy = 0, uz = 0;
+                        for (int p = 0; p < Q; ++p)
+                        {
+                            const double v = h->f_curr[src * Q + p];
+                            r += v;
+                            ux += v * EXA[p];
+                            uy += v * EYA[p];
+                            uz += v * EZA[p];
+                        }
+                        if (r > 1e-12)
+                        {
+                            ux /= r; uy /= r; uz /= r;
+                        }
+                        else
+                        {
+                            r = 1.0; ux = fx; uy = fy; uz = fz;
+                        }
+                        const double tau_s = h->tau_a[src];
+                        const double fo = h->f_curr[src * Q + q];
+                        fn = fo - (fo - feq_a(q, r, ux, uy, uz)) / tau_s;
+                        if (force)
+                        {
+                            const double cu = EXA[q] * fx + EYA[q] * fy + EZA[q] * fz;
+                            fn += W[q] * (h->field_a[src] * mass) * (1.0 + 3.0 * cu) * (1.0 - 0.5 / tau_s);
+                        }
+                        else if (fs)
+                        {
+                            fn += W[q] * (h->field_a[dst] * mass);
+                        }
+                    }
+                    h->f_next[dst * Q + q] = fn;
+                    rho_new += fn;
+                }
+                h->rho[dst] = rho_new;
+            }
+    double* tmp = h->f_curr;
+    h->f_curr = h->f_next;
+    h->f_next = tmp;
+}
+
 int orc_init(orc_handle* h)
 {
     const lbm_config* c = &h->cfg;
@@ -391,6 +566,7 @@ int orc_init(orc_handle* h)
     h->nx_t = h->nx + 2; h->ny_t = h->ny + 2; h->nz_t = h->nz + 2;
     h->Nloc = (size_t)h->nx_t * h->ny_t * h->nz_t;
     h->dt = (CS * c->dx) / c->c_phys;   /* UnitConverter::get_dt_phys 06:200-203 */
+    if (c->dt > 0) h->dt = c->dt;
 
     int had_mask = h->mask != NULL && h->mask_override;
     unsigned char* keep = NULL;
@@ -412,6 +588,7 @@ int orc_init(orc_handle* h)
         for (int q = 0; q < Q; ++q) h->f_curr[(size_t)i * Q + q] = feq0[q];
 
     init_domain(h);
+    if (c->scheme == LBM_SCHEME_A) init_scheme_a(h);
 
     int status = LBM_OK;
     free(h->probe_idx);
@@ -489,6 +666,7 @@ static int cell_in_grid(const orc_handle* h, int gi, int gj, int gk)
 /* LBMSolver::apply_source (06:576-667; 08:540-628 for the sine), one source. */
 static void apply_one_source(orc_handle* h, src_t* s, double t)
 {
+    if (s->s.injection == LBM_INJECT_FIELD) return;   /* scheme A: applied inside step_a */
     const lbm_config* c = &h->cfg;
     const double dt = h->dt;
     const double DX = c->dx;
@@ -768,10 +946,17 @@ void orc_step(orc_handle* h, int nsteps)
 {
     for (int n = 0; n < nsteps; ++n)
     {
-        const double t = h->step * h->dt;
-        orc_apply_source(h, t);
-        orc_exchange_halos(h);
-        orc_step_collision_bgk(h);
+        if (h->cfg.scheme == LBM_SCHEME_A)
+        {
+            step_a(h, h->step);   /* the field source acts inside the step */
+        }
+        else
+        {
+            const double t = h->step * h->dt;
+            orc_apply_source(h, t);
+            orc_exchange_halos(h);
+            orc_step_collision_bgk(h);
+        }
         orc_record_probes(h);
         h->step++;
     }
@@ -790,6 +975,10 @@ void orc_set_f(orc_handle* h, const double* in) { memcpy(h->f_curr, in, h->Nloc 
 void orc_get_mask(orc_handle* h, unsigned char* out) { memcpy(out, h->mask, h->Nloc); }
 void orc_get_rho(orc_handle* h, double* out) { memcpy(out, h->rho, h->Nloc * sizeof(double)); }
 void orc_get_sponge(orc_handle* h, double* out) { memcpy(out, h->sponge, h->Nloc * sizeof(double)); }
+void orc_get_tau_a(orc_handle* h, double* out)
+{
+    for (size_t i = 0; i < h->Nloc; ++i) out[i] = h->tau_a ? h->tau_a[i] : h->cfg.tau;
+}
 void orc_get_ground_height(orc_handle* h, double* out)
 {
     memcpy(out, h->gH, (size_t)h->nx_t * h->ny_t * sizeof(double));

@@ -56,6 +56,7 @@ void orc_set_f(orc_handle* h, const double* in);
 void orc_get_mask(orc_handle* h, unsigned char* out);
 void orc_get_rho(orc_handle* h, double* out);
 void orc_get_sponge(orc_handle* h, double* out);
+void orc_get_tau_a(orc_handle* h, double* out);
 void orc_get_ground_height(orc_handle* h, double* out);
 long orc_get_probes(orc_handle* h, double* out, long capacity);
 

@@ -8,7 +8,10 @@ Each fixture runs one reference-native scenario of tests/scenarios.py through
 oracle/_ref/libref06.so or libref08.so (the reference's own apply_source /
 exchange_halos / step_collision_bgk, 06:1077-1092) and stores the probe
 series, the voxelised mask, a window of the final populations and two FP64
-checksums of the whole population array.  The fixtures pin the oracle (and,
+checksums of the whole population array.  The family-A fixtures (lloyd_a,
+doppler_a) run 02_lloyds_mirror.cpp / 03_doppler_effect.cpp through
+oracle/_ref/libref02.so / libref03.so (exchange_halos + step, 02:543-546,
+03:540-541) and store the final density field.  The fixtures pin the oracle (and,
 within tolerance, the CUDA solver) to the reference on machines where the
 reference itself is absent.
 """
@@ -72,10 +75,34 @@ def reference_run(name):
                 f_checksums=checksums(f), dims_halo=np.array(ref.dims_halo), steps=np.array(sc["steps"]))
 
 
+FAMILY_A = ("lloyd_a", "doppler_a")
+
+
+def reference_run_a(name):
+    """A family-A program (02 or 03) on its reduced scenario: rho - 1 of every
+    interior cell after the scenario's steps (SOLID cells as 0), its tau and
+    source-weight fields and the mask."""
+    sc = scenarios.family_a(name)
+    ref = oracle.RefASolver(sc["ref"], **sc["ref_params"])
+    ref.step(sc["steps"])
+    nx, ny, nz = ref.dims_halo
+    inner = (slice(1, -1), slice(1, -1), slice(1, -1))
+    rho = ref.get_rho().reshape(nz, ny, nx)[inner] - 1.0
+    mask = ref.get_mask().reshape(nz, ny, nx)
+    rho[mask[inner] == 1] = 0.0
+    return dict(rho_minus_1=rho, mask_bits=np.packbits(mask), dims_halo=np.array(ref.dims_halo),
+                steps=np.array(sc["steps"]), dt=np.array(ref.dt))
+
+
 def main():
     oracle.build(ref=True)
     for name in CASES:
         out = reference_run(name)
+        path = os.path.join(HERE, name + ".npz")
+        np.savez_compressed(path, **out)
+        print(path, {k: v.shape for k, v in out.items()})
+    for name in FAMILY_A:
+        out = reference_run_a(name)
         path = os.path.join(HERE, name + ".npz")
         np.savez_compressed(path, **out)
         print(path, {k: v.shape for k, v in out.items()})

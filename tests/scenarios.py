@@ -170,6 +170,58 @@ def misfit(pred, observed):
     return 0.5 * float(np.sum((pred[:, m] - observed[:, m]) ** 2))
 
 
+def family_a(name, n=40, steps=60):
+    """Reduced versions of the family-A programs for the scheme-A path.
+
+    lloyd_a: 02_lloyds_mirror.cpp (Lloyd's mirror): x, y in [-4, 4], z in
+    [-0.8, 4] at dx = 0.2 (02's cell size), the first layer above z_min SOLID
+    (02:153-158), rest halos, tau 0.51 ramping to 1 over 15 cells from x-,
+    x+, y-, y+, z+ (02:164-179), time-harmonic Gaussian source
+    0.5 exp(-ln2 r^2 / 2) sin(pi t / 15) at the origin added at the
+    destination (02:181, 02:373); dt = 0.577350269 dx / c (02:36).
+    doppler_a: 03_doppler_effect.cpp (uniform flow): an n^3 grid at
+    dx = 0.25, Mach 0.2 flow along z, zero-gradient halos, tau 0.51 ramping to
+    0.9 over 10 cells from every face, Gaussian forcing 0.01 exp(-r^2 /
+    (2 dx^2)) sin(2 pi s / 30) at the grid centre (03:121, 03:135-169).
+
+    Returns dict(cfg, sources, probes, mask, steps, ref, ref_params)."""
+    if name == "lloyd_a":
+        dx = 0.2
+        cfg = abi.reference_config(x_min=-4.0, x_max=4.0, y_min=-4.0, y_max=4.0, z_min=-0.8, z_max=4.0, dx=dx,
+                                   c_phys=1.0, tau=0.51, use_geometry=0, face_bc=(abi.LBM_BC_REST,) * 6,
+                                   sponge_faces=ALL_FACES & ~(1 << abi.FACE_ZLO), sponge_width=15.0, sky_z=1e30,
+                                   scheme=abi.LBM_SCHEME_A, tau_sponge_max=1.0, dt=0.577350269 * dx / 1.0)
+        nx, ny, nz = 40, 40, 24
+        mask = np.zeros((nz + 2, ny + 2, nx + 2), np.uint8)
+        mask[1] = 1                                  # gz == 0 is SOLID; halos stay FLUID
+        sig_cells = np.sqrt(2.0 / (2.0 * np.log(2.0))) / dx   # exp(-ln2 r^2 / b), b = 2
+        src = abi.reference_source(sx=0.0, sy=0.0, sz=0.0, ex=0.0, ey=0.0, ez=0.0, amp=0.5, freq=1.0 / 30.0,
+                                   waveform=abi.LBM_WAVE_SINE, injection=abi.LBM_INJECT_FIELD,
+                                   sigma_cells=sig_cells, field_mode=abi.LBM_FIELD_DST)
+        tz = -0.8 + (int((0.0 + 0.8) / dx + 0.5) + 0.5) * dx
+        probes = np.stack([np.full(8, 0.1), np.linspace(-3.5, 3.5, 8), np.full(8, tz)], 1)
+        ref_params = dict(x_min=-4.0, x_max=4.0, y_min=-4.0, y_max=4.0, z_min=-0.8, z_max=4.0, dx=dx, amp=0.5,
+                          b_param=2.0)
+        return dict(cfg=cfg, sources=[src], probes=probes, mask=mask.ravel(), steps=steps, ref="02",
+                    ref_params=ref_params)
+    if name == "doppler_a":
+        dx, Ma, cs = 0.25, 0.2, 0.5773502691896257
+        dt = cs * dx / 1.0
+        cfg = abi.reference_config(x_min=0.0, x_max=n * dx, y_min=0.0, y_max=n * dx, z_min=0.0, z_max=n * dx, dx=dx,
+                                   c_phys=1.0, tau=0.51, use_geometry=0, face_bc=(abi.LBM_BC_COPY,) * 6,
+                                   sponge_faces=ALL_FACES, sponge_width=10.0, sky_z=1e30, scheme=abi.LBM_SCHEME_A,
+                                   tau_sponge_max=0.9, flow=(0.0, 0.0, Ma * cs), dt=dt)
+        c = (n / 2.0 + 0.5) * dx                      # (g - n/2) dx about cell centres (03:135-168)
+        src = abi.reference_source(sx=c, sy=c, sz=c, ex=c, ey=c, ez=c, amp=0.01,
+                                   freq=(2.0 * np.pi / 30.0) / (2.0 * np.pi * dt), waveform=abi.LBM_WAVE_SINE,
+                                   injection=abi.LBM_INJECT_FIELD, sigma_cells=1.0, field_mode=abi.LBM_FIELD_FORCE)
+        probes = np.stack([np.full(8, c), np.full(8, c), np.linspace(1.1, n * dx - 1.1, 8)], 1)
+        ref_params = dict(x_min=0.0, x_max=n * dx, y_min=0.0, y_max=n * dx, z_min=0.0, z_max=n * dx, dx=dx,
+                          amp=0.01, Ma=Ma, tau_bulk=0.51, tau_sponge_max=0.9, sponge_width=10)
+        return dict(cfg=cfg, sources=[src], probes=probes, mask=None, steps=steps, ref="03", ref_params=ref_params)
+    raise KeyError(name)
+
+
 def build_pair(sc):
     """(CUDA solver, FP64 oracle) for one scenario."""
     from nlos_lbm import Solver

@@ -1,0 +1,120 @@
+"""Scheme A (the reference's family-A programs 01-04) on the GPU, through the
+C-ABI, against the FP64 oracle's family-A restatement (itself checked
+against the unmodified 02/03 programs in tests/test_oracle_family_a.py and
+the fixtures in tests/golden/).
+
+Tolerances: FP32 deviation storage against FP64, probe (density) series
+relative L2 <= 1e-5 and field max error <= 1e-5 of the field's largest
+deviation, the FP32 bars of the scheme-B parity tests.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import scenarios
+from nlos_lbm import LBMError, Solver, abi
+from oracle import OracleSolver
+from scenarios import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+PROBE_TOL = 1e-5
+FIELD_TOL = 1e-5
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def _solver(sc, **kw):
+    return Solver(sc["cfg"], sc["sources"], sc["probes"], mask=sc["mask"], **kw)
+
+
+@pytest.mark.parametrize("name", ["lloyd_a", "doppler_a"])
+def test_scheme_a_matches_oracle(name, gpu):
+    sc = scenarios.family_a(name)
+    g = _solver(sc)
+    o = OracleSolver(sc["cfg"], sc["sources"], sc["probes"], mask=sc["mask"])
+    g.step(sc["steps"])
+    o.step(sc["steps"])
+    pg, po = g.get_probes(), o.get_probes()
+    assert pg.shape == po.shape == (sc["steps"], len(sc["probes"]))
+    assert np.max(np.abs(po)) > 0
+    assert rel_l2(pg, po) <= PROBE_TOL, rel_l2(pg, po)
+    nx, ny, nz = g.dims
+    fo = (o.get_rho().reshape(nz + 2, ny + 2, nx + 2)[1:-1, 1:-1, 1:-1] - 1.0)
+    mask = o.get_mask().reshape(nz + 2, ny + 2, nx + 2)[1:-1, 1:-1, 1:-1]
+    fo[mask == 1] = 0.0
+    fg = g.get_rho().astype(np.float64)
+    assert np.max(np.abs(fg - fo)) <= FIELD_TOL * np.max(np.abs(fo))
+
+
+@pytest.mark.parametrize("name", ["lloyd_a", "doppler_a"])
+def test_scheme_a_matches_reference_fixture(name, gpu):
+    path = os.path.join(GOLDEN, name + ".npz")
+    gold = np.load(path)
+    sc = scenarios.family_a(name, steps=int(gold["steps"]))
+    g = _solver(sc)
+    g.step(sc["steps"])
+    nx, ny, nz = g.dims
+    fg = g.get_rho().astype(np.float64).reshape(nz, ny, nx)
+    ref = gold["rho_minus_1"]                       # reference's rho - 1 on interior cells, SOLID as 0
+    assert np.max(np.abs(fg - ref)) <= FIELD_TOL * np.max(np.abs(ref))
+
+
+def test_scheme_a_direct_calls_equal_batched_steps(gpu):
+    sc = scenarios.family_a("doppler_a", steps=12)
+    a = _solver(sc)
+    a.step(sc["steps"])
+    b = _solver(sc)
+    for s in range(sc["steps"]):
+        b.apply_source(s * b.dt)          # no-op for field sources: they act inside the step
+        b.exchange_halos()                # no-op: each step writes the next step's halos
+        b.step_collision_bgk()
+        b.record_probes()
+    assert np.array_equal(a.get_probes(), b.get_probes())
+    assert np.array_equal(a.get_rho(), b.get_rho())
+
+
+def test_scheme_a_solid_wall_direct_equals_batched(gpu):
+    sc = scenarios.family_a("lloyd_a", steps=9)
+    a = _solver(sc)
+    a.step(sc["steps"])
+    b = _solver(sc)
+    for s in range(sc["steps"]):
+        b.step_collision_bgk()
+        b.record_probes()
+    assert np.array_equal(a.get_probes(), b.get_probes())
+
+
+def test_uniform_flow_is_steady(gpu):
+    sc = scenarios.family_a("doppler_a", steps=40)
+    g = Solver(sc["cfg"], [], sc["probes"])     # no source: feq(1, flow) everywhere is a fixed point
+    g.step(sc["steps"])
+    assert np.max(np.abs(g.get_probes())) <= 1e-6
+    assert np.max(np.abs(g.get_rho())) <= 1e-6
+
+
+def test_scheme_a_rejects_unsupported_set_ups(gpu):
+    sc = scenarios.family_a("doppler_a")
+    cfg = sc["cfg"]
+    for bad in (dict(storage=abi.LBM_STORE_F16, f16_scale=100.0), dict(face_bc=(abi.LBM_BC_NSCBC,) * 6),
+                dict(face_bc=(abi.LBM_BC_COPY,) * 5 + (abi.LBM_BC_REST,)), dict(tau_sponge_max=0.505)):
+        c = abi.reference_config(**{f[0]: getattr(cfg, f[0]) for f in abi.LbmConfig._fields_
+                                    if f[0] not in ("face_bc", "flow")},
+                                 face_bc=tuple(cfg.face_bc), flow=tuple(cfg.flow))
+        for k, v in bad.items():
+            if k == "face_bc":
+                for f in range(6):
+                    c.face_bc[f] = v[f]
+            else:
+                setattr(c, k, v)
+        with pytest.raises(LBMError) as e:
+            Solver(c, [], None)
+        assert e.value.status == abi.LBM_ERR_BAD_CONFIG
+    g = Solver(cfg, [], None)
+    point = abi.reference_source(sx=5.0, sy=5.0, sz=5.0, ex=5.0, ey=5.0, ez=5.0)
+    with pytest.raises(LBMError) as e:
+        g.add_source(point)
+    assert e.value.status == abi.LBM_ERR_UNSUPPORTED
+    with pytest.raises(LBMError) as e:
+        g.get_f()
+    assert e.value.status == abi.LBM_ERR_UNSUPPORTED
