@@ -139,7 +139,7 @@ def make_solver(name, storage, device):
     w = workloads.build(name, storage=storage)
     w["cfg"].device = device
     t0 = time.time()
-    s = nlos_lbm.Solver(w["cfg"], w["sources"], w["probes"], triangles=w["triangles"])
+    s = nlos_lbm.Solver(w["cfg"], w["sources"], w["probes"], triangles=w["triangles"], mask=w.get("mask"))
     return s, w, time.time() - t0
 
 
@@ -254,6 +254,34 @@ def adjoint_measure(device, torch, reps=2, ckpt=(200, 0), workload="adjoint256",
             "launches": launches, "fwd_equiv_glups": nx * ny * nz * w["steps"] / (ms / 1e3) / 1e9}
 
 
+def family_a_cpu(name, seconds=5.0):
+    """The unmodified family-A reference program (02 or 03 through
+    oracle/_ref, FP64, OpenMP on all host threads) on a sub-domain of its own
+    set-up, in GLUPS; None where the harness was not built."""
+    import oracle
+
+    which = {"lloyd_a": "02", "doppler_a": "03"}[name]
+    if not oracle.refa_available(which):
+        return None
+    if which == "02":
+        p = dict(x_min=-10.0, x_max=10.0, y_min=-10.0, y_max=10.0, z_min=-2.0, z_max=10.0, dx=0.2, amp=0.5,
+                 b_param=2.0)
+    else:
+        p = dict(x_min=0.0, x_max=25.0, y_min=0.0, y_max=25.0, z_min=0.0, z_max=37.5, dx=0.25, amp=0.01, Ma=0.2,
+                 tau_bulk=0.51, tau_sponge_max=0.9, sponge_width=20)
+    ref = oracle.RefASolver(which, **p)
+    nx, ny, nz = (d - 2 for d in ref.dims_halo)
+    ref.step(1)
+    n, t = 0, 0.0
+    while t < seconds:
+        t0 = time.perf_counter()
+        ref.step(2)
+        t += time.perf_counter() - t0
+        n += 2
+    return {"value": nx * ny * nz * n / t / 1e9, "unit": "GLUPS", "cores": os.cpu_count(), "kind": "reference",
+            "sample": f"{nx}x{ny}x{nz} sub-domain, {n} steps of exchange_halos+step, FP64"}
+
+
 def cpu_baseline(steps_hint=None):
     """Reference CPU step on a bounded sub-domain of the city (rank 0, N=1)."""
     import oracle
@@ -361,6 +389,20 @@ def run_our_arm(args):
             del s2
             gc.collect()
 
+    family_a = {}
+    if world == 1 and not args.headline_only:
+        # the reference's family-A programs at their own sizes on scheme A (FP32)
+        for nm in ("lloyd_a", "doppler_a"):
+            s2, _, r = measure(nm, None, args.steps, args.warmup, local, torch, barrier, reduce_max)
+            family_a[nm] = {k: r[k] for k in ("glups_rank", "ms", "kernel_ms_avg", "dims", "bytes_per_cell",
+                                               "description")}
+            family_a[nm]["hbm_frac_kernel"] = (r["cells"] * r["bytes_per_cell"] / (r["kernel_ms_avg"] / 1e3) / 1e9
+                                               / hbm_peak)
+            if not args.no_cpu:
+                family_a[nm]["cpu_reference"] = family_a_cpu(nm)
+            del s2
+            gc.collect()
+
     adjoint = None
     if world == 1 and not args.headline_only and not args.no_adjoint:
         adjoint = adjoint_measure(local, torch)
@@ -398,6 +440,8 @@ def run_our_arm(args):
     }
     if adjoint is not None:
         line["adjoint"] = adjoint
+    if family_a:
+        line["family_a"] = family_a
     if secondary.get("city1024_fp32") and secondary.get("city1024_fp16"):
         line["fp16_over_fp32"] = secondary["city1024_fp16"]["glups_rank"] / secondary["city1024_fp32"]["glups_rank"]
     if world == 1 and rank == 0 and not args.no_cpu:
@@ -417,7 +461,9 @@ def main():
     ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="city2048", choices=["city2048", "city1024", "city512", "lloyd", "scatter"])
+    ap.add_argument("--workload", default="city2048",
+                    choices=["city2048", "city1024", "city512", "lloyd", "scatter", "lloyd_a", "lloyd_a_small",
+                             "doppler_a"])
     ap.add_argument("--storage", default=None, choices=["fp32", "fp16"],
                     help="population storage of the headline workload (default: the workload's own)")
     ap.add_argument("--headline-only", action="store_true")

@@ -449,7 +449,7 @@ cudaError_t launch_step_a(const float* fin, float* fout, const Layout& L, const 
     if (L.bc != BC) return cudaErrorInvalidValue;
     constexpr int kBlock = 128;
     const dim3 g((unsigned)((L.nx + 2 * kBlock - 1) / (2 * kBlock)), (unsigned)L.ny, (unsigned)L.nz);
-    k_step_a<kBlock, 0><<<g, kBlock, 0, stream>>>(fin, fout, L, a, b);
+    k_step_a<kBlock, 7><<<g, kBlock, 0, stream>>>(fin, fout, L, a, b);
     return cudaGetLastError();
 }
 

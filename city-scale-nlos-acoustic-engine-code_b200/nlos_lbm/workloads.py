@@ -18,6 +18,12 @@ reference's heightmap ray cast.
              localisation) sits a few cells away
   adjoint128 the same at 128x128x128 (profiler-sized: 160 MB per population
              buffer, still larger than L2)
+  lloyd_a    02_lloyds_mirror.cpp at its own size (scheme A): 500x500x300 at
+             dx 0.2, ground layer SOLID, tau ramp 0.51 -> 1, time-harmonic
+             Gaussian source at the origin, 391 steps (to T = 45 s)
+  doppler_a  03_doppler_effect.cpp at its own size (scheme A): 400x400x600 at
+             dx 0.25, Mach 0.2 flow along z, zero-gradient halos, tau ramp
+             0.51 -> 0.9 over 20 cells, 762 steps (to T = 110 s)
 """
 import numpy as np
 
@@ -139,6 +145,38 @@ def build(name, storage=None, seed=2024):
                     triangles=tris, steps=3000, coverage=cov,
                     description=f"transient localisation {nx}x{ny}x{nz} city patch, Ricker period 30, 64 receivers, "
                                 "3000 steps")
+    if name in ("lloyd_a", "lloyd_a_small"):
+        # 02:53-56 domain, 02:32 dx, 02:126 omega, 02:138-181 physics; the
+        # small one (profiler-sized) at dx 0.4: 250x250x150
+        dx = 0.2 if name == "lloyd_a" else 0.4
+        nx, nz = int(100.0 / dx + 0.5), int(60.0 / dx + 0.5)
+        cfg = lattice_config(nx, nx, nz, 0.51, x_min=-50.0, x_max=50.0, y_min=-50.0, y_max=50.0, z_min=-10.0,
+                             z_max=50.0, dx=dx, c_phys=1.0, face_bc=(abi.LBM_BC_REST,) * 6,
+                             sponge_faces=ALL_FACES & ~(1 << abi.FACE_ZLO), sponge_width=15.0,
+                             scheme=abi.LBM_SCHEME_A, tau_sponge_max=1.0, dt=0.577350269 * dx)
+        mask = np.zeros((nz + 2, nx + 2, nx + 2), np.uint8)
+        mask[1] = 1                                   # gz == 0 is SOLID (02:153-158)
+        src = abi.reference_source(sx=0.0, sy=0.0, sz=0.0, ex=0.0, ey=0.0, ez=0.0, amp=0.5, freq=1.0 / 30.0,
+                                   waveform=abi.LBM_WAVE_SINE, injection=abi.LBM_INJECT_FIELD,
+                                   sigma_cells=np.sqrt(2.0 / (2.0 * np.log(2.0))) / dx,
+                                   field_mode=abi.LBM_FIELD_DST)
+        probes = np.stack([np.full(64, 0.1), np.linspace(-49.9, 49.9, 64), np.full(64, 0.1)], 1)
+        return dict(cfg=cfg, sources=[src], probes=probes, triangles=None, mask=mask.ravel(), steps=391,
+                    description=f"Lloyd's mirror (02) {nx}x{nx}x{nz}, scheme A, ground layer, tau ramp")
+    if name == "doppler_a":
+        # 03:32, 03:51, 03:55-63, 03:121, 03:135-169
+        dx, Ma, cs = 0.25, 0.2, 0.5773502691896257
+        n = (400, 400, 600)
+        cfg = lattice_config(*n, 0.51, x_max=n[0] * dx, y_max=n[1] * dx, z_max=n[2] * dx, dx=dx, c_phys=1.0,
+                             face_bc=(abi.LBM_BC_COPY,) * 6, sponge_faces=ALL_FACES, sponge_width=20.0,
+                             scheme=abi.LBM_SCHEME_A, tau_sponge_max=0.9, flow=(0.0, 0.0, Ma * cs), dt=cs * dx)
+        ctr = [(m / 2.0 + 0.5) * dx for m in n]
+        src = abi.reference_source(sx=ctr[0], sy=ctr[1], sz=ctr[2], ex=ctr[0], ey=ctr[1], ez=ctr[2], amp=0.01,
+                                   freq=1.0 / (30.0 * cs * dx), waveform=abi.LBM_WAVE_SINE,
+                                   injection=abi.LBM_INJECT_FIELD, sigma_cells=1.0, field_mode=abi.LBM_FIELD_FORCE)
+        probes = np.stack([np.full(64, ctr[0]), np.full(64, ctr[1]), np.linspace(1.0, n[2] * dx - 1.0, 64)], 1)
+        return dict(cfg=cfg, sources=[src], probes=probes, triangles=None, mask=None, steps=762,
+                    description="Doppler (03) 400x400x600, scheme A, Mach 0.2 flow, zero-gradient halos")
     raise KeyError(name)
 
 
