@@ -308,13 +308,19 @@ void sponge_axis(const lbm_config& c, int axis, int n, std::vector<float>& out)
 // The voxelised mask of init_domain (06:460-531) in the reference's
 // halo-inclusive layout: SOLID below the ground height of the column unless
 // above sky_z, then the halo rules x faces, y faces, z faces in that order
-// (a WALL face is SOLID, every other face FLUID).
-void build_mask(const lbm_config& c, const HeightField& geo, int nx, int ny, int nz, uint8_t* m)
+// (a WALL face is SOLID, every other face FLUID).  gH_given: ground heights
+// of every column already cast (on the GPU, bit-identical), else cast here.
+void build_mask(const lbm_config& c, const HeightField& geo, int nx, int ny, int nz, uint8_t* m,
+                const double* gH_given = nullptr)
 {
     const int nxt = nx + 2, nyt = ny + 2, nzt = nz + 2;
     std::vector<double> gH((size_t)nxt * nyt, -1e30);
     const bool geom = c.use_geometry != 0;
-    if (geom)
+    if (geom && gH_given)
+    {
+        std::copy(gH_given, gH_given + gH.size(), gH.begin());
+    }
+    else if (geom)
     {
 #pragma omp parallel for collapse(2) schedule(dynamic, 16)
         for (int j = 0; j < nyt; ++j)
@@ -708,7 +714,17 @@ extern "C" int lbm_init(lbm_handle* h)
         {
             return h->fail(LBM_ERR_OUT_OF_MEMORY, "host mask");
         }
-        build_mask(c, h->geo, nx, ny, nz, h->mask.data());
+        // the ray cast of every column runs on the GPU (voxel.cu) when there is geometry
+        std::vector<double> gH;
+        if (c.use_geometry && h->geo.triangle_count() > 0)
+        {
+            gH.assign((size_t)nxt * nyt, 0.0);
+            CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+            const int ve = ground_height_device(h->geo, c.x_min, c.y_min, c.dx, nxt, nyt, gH.data(), h->stream);
+            if (ve != 0) return h->cuda_fail((cudaError_t)ve, "ground heights");
+            h->launches += 1;
+        }
+        build_mask(c, h->geo, nx, ny, nz, h->mask.data(), gH.empty() ? nullptr : gH.data());
     }
 
     // Sponge profiles.
@@ -718,7 +734,7 @@ extern "C" int lbm_init(lbm_handle* h)
     sponge_axis(c, 2, nz, sz);
 
     // Device buffers.
-    CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    if (!h->stream) CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "cudaStreamCreate");
     const size_t esz = h->storage == LBM_STORE_F16 ? 2 : 4;
     const size_t pop_bytes = (size_t)L.total * esz;
     cudaError_t e = cudaSuccess;

@@ -142,6 +142,30 @@ double HeightField::ground_height(double x, double y) const
     return max_z;
 }
 
+void HeightField::export_flat(std::vector<double>& tri15, std::vector<int>& bin_start, std::vector<int>& bin_items,
+                              double gmin[3], double gmax[3], double& cell_w, double& cell_h) const
+{
+    tri15.resize(tris_.size() * 15);
+    for (size_t i = 0; i < tris_.size(); ++i)
+        for (int d = 0; d < 3; ++d)
+        {
+            tri15[15 * i + d] = tris_[i].v1[d];
+            tri15[15 * i + 3 + d] = tris_[i].v2[d];
+            tri15[15 * i + 6 + d] = tris_[i].v3[d];
+            tri15[15 * i + 9 + d] = tris_[i].mn[d];
+            tri15[15 * i + 12 + d] = tris_[i].mx[d];
+        }
+    bin_start = bin_start_;
+    bin_items = bin_items_;
+    for (int d = 0; d < 3; ++d)
+    {
+        gmin[d] = gmin_[d];
+        gmax[d] = gmax_[d];
+    }
+    cell_w = cell_w_;
+    cell_h = cell_h_;
+}
+
 // ---------------------------------------------------------------- city
 
 namespace {

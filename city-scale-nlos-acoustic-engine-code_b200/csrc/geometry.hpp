@@ -25,6 +25,10 @@ public:
     // from z = 10000 straight down, -1e30 when there is none.
     double ground_height(double x, double y) const;
     size_t triangle_count() const { return tris_.size(); }
+    // The bin grid and triangles as flat arrays for the device ray cast
+    // (voxel.cu): tri15 = per triangle v1, v2, v3, min, max (15 doubles).
+    void export_flat(std::vector<double>& tri15, std::vector<int>& bin_start, std::vector<int>& bin_items,
+                     double gmin[3], double gmax[3], double& cell_w, double& cell_h) const;
 
 private:
     struct Tri
@@ -45,5 +49,11 @@ private:
 // per box, vertices on multiples of dx.  Returns the plan coverage reached.
 double city_generate(const lbm_city_params& p, std::vector<float>& tris);
 bool stl_write(const char* path, const float* tris, int ntris);
+
+// HeightField::ground_height of every column of the halo-inclusive grid on
+// the GPU, bit-identical to the host: gH[j * nxt + i] for the cell centre
+// x = x_min + (i - 0.5) dx, y = y_min + (j - 0.5) dx (voxel.cu).
+int ground_height_device(const HeightField& geo, double x_min, double y_min, double dx, int nxt, int nyt,
+                         double* gH, void* stream);
 
 }  // namespace lbm

@@ -24,7 +24,9 @@ NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 CXX = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-CU_SOURCES = ["kernels.cu", "adjoint.cu", "scheme_a.cu"]
+CU_SOURCES = ["kernels.cu", "adjoint.cu", "scheme_a.cu", "voxel.cu"]
+# voxel.cu must round every FP64 expression as the host does (no FMA contraction)
+CU_FLAGS = {"voxel.cu": ["-fmad=false"]}
 CXX_SOURCES = ["api.cpp", "geometry.cpp"]
 HEADERS = ["adjoint.hpp", "device.hpp", "geometry.hpp", "lattice.cuh"]
 
@@ -59,7 +61,7 @@ def build(verbose=False, force=False, ptxas_verbose=False):
         objs.append(o)
         if force or _newer(o, [s] + headers):
             cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-ccbin", CXX, "-Xcompiler", "-fPIC",
-                   "-I" + INCLUDE, "-I" + CSRC, "-c", s, "-o", o]
+                   "-I" + INCLUDE, "-I" + CSRC, *CU_FLAGS.get(src, []), "-c", s, "-o", o]
             if ptxas_verbose:
                 cmd.insert(1, "-Xptxas=-v")
             log += _run(cmd, verbose)
