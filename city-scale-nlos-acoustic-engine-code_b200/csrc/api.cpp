@@ -29,6 +29,7 @@ using namespace lbm;
 namespace {
 
 constexpr int kTableRows = 4096;   // source-schedule rows resident on the device
+constexpr int kBcCut = 100;        // face of a z-slab that borders the next slab (internal face type)
 constexpr int kProbeRows = 4096;   // probe-series rows buffered on the device
 // Fused-step implementation and L2 prefetch distance per storage type, from
 // launch-shape sweeps on the 1024x1024x256 city (B200): FP32 is fastest with
@@ -58,6 +59,9 @@ T* dalloc(size_t n, cudaError_t& err)
 struct lbm_handle
 {
     lbm_config cfg{};
+    lbm_config lcfg{};                 // the grid this handle holds: cfg, or its z-slab (lbm_init)
+    bool slab = false;
+    int nz_global = 0;
     std::string err;
     int storage = LBM_STORE_F32;
     float scale = 1.0f;
@@ -239,6 +243,7 @@ SourceEntry source_entry(const SourceState& st, double t, double dt)
     const double val = source_value(st, t, dt);
     drone_position(st.s, t, e.cx, e.cy, e.cz);
     e.mass = val * dt * st.s.gain;   // numerator of A (06:631)
+    e.wsum = 0.0;
     return e;
 }
 
@@ -261,6 +266,13 @@ int validate(const lbm_config& c, std::string& why)
         nnscbc += c.face_bc[f] == LBM_BC_NSCBC;
     }
     if (c.scheme == LBM_SCHEME_B && ncopy) return why = "LBM_BC_COPY needs scheme A", LBM_ERR_BAD_CONFIG;
+    if (c.slab_k0 < 0 || c.slab_nz < 0) return why = "slab_k0 and slab_nz must be >= 0", LBM_ERR_BAD_CONFIG;
+    if (c.slab_nz > 0)
+    {
+        const int nzg = (int)((c.z_max - c.z_min) / c.dx + 0.5);
+        if (c.slab_k0 + c.slab_nz > nzg) return why = "the z-slab reaches past the grid", LBM_ERR_BAD_CONFIG;
+        if (c.scheme != LBM_SCHEME_B) return why = "z-slabs run scheme B", LBM_ERR_BAD_CONFIG;
+    }
     if (c.scheme == LBM_SCHEME_A)
     {
         if (c.storage != LBM_STORE_F32) return why = "scheme A runs on FP32 storage", LBM_ERR_BAD_CONFIG;
@@ -360,8 +372,10 @@ void build_mask(const lbm_config& c, const HeightField& geo, int nx, int ny, int
     for (int j = 0; j < nyt; ++j)
         for (int i = 0; i < nxt; ++i)
         {
-            m[(size_t)i + (size_t)j * nxt] = wall(LBM_FACE_ZLO);
-            m[(size_t)i + (size_t)j * nxt + (size_t)(nz + 1) * nxt * nyt] = wall(LBM_FACE_ZHI);
+            // a cut of a z-slab keeps the geometry of the neighbour slab's layer
+            if (c.face_bc[LBM_FACE_ZLO] != kBcCut) m[(size_t)i + (size_t)j * nxt] = wall(LBM_FACE_ZLO);
+            if (c.face_bc[LBM_FACE_ZHI] != kBcCut)
+                m[(size_t)i + (size_t)j * nxt + (size_t)(nz + 1) * nxt * nyt] = wall(LBM_FACE_ZHI);
         }
 }
 
@@ -672,9 +686,27 @@ extern "C" int lbm_probe_info(lbm_handle* h, int* owned, int* in_solid)
 extern "C" int lbm_init(lbm_handle* h)
 {
     if (!h) return LBM_ERR_INVALID_ARGUMENT;
-    const lbm_config& c = h->cfg;
     h->release();
     CK(cudaSetDevice(h->device), "cudaSetDevice");
+
+    // The grid this handle holds: the whole configured grid, or its z-slab
+    // (layers slab_k0 .. slab_k0 + slab_nz - 1) with the cut faces marked.
+    {
+        int gx, gy, gz;
+        grid_size(h->cfg, gx, gy, gz);
+        h->nz_global = gz;
+        h->lcfg = h->cfg;
+        h->slab = h->cfg.slab_nz > 0;
+        if (h->slab)
+        {
+            lbm_config& l = h->lcfg;
+            l.z_min = h->cfg.z_min + h->cfg.slab_k0 * h->cfg.dx;
+            l.z_max = l.z_min + h->cfg.slab_nz * h->cfg.dx;
+            if (h->cfg.slab_k0 > 0) l.face_bc[LBM_FACE_ZLO] = kBcCut;
+            if (h->cfg.slab_k0 + h->cfg.slab_nz < gz) l.face_bc[LBM_FACE_ZHI] = kBcCut;
+        }
+    }
+    const lbm_config& c = h->lcfg;
 
     // Grid (06:330-334, MPI size 1: one block, off = 0) and time step (06:200-203).
     grid_size(c, h->NXg, h->NYg, h->NZg);
@@ -731,7 +763,17 @@ extern "C" int lbm_init(lbm_handle* h)
     std::vector<float> sx, sy, sz;
     sponge_axis(c, 0, nx, sx);
     sponge_axis(c, 1, ny, sy);
-    sponge_axis(c, 2, nz, sz);
+    if (!h->slab)
+    {
+        sponge_axis(c, 2, nz, sz);
+    }
+    else
+    {
+        // distances to the faces of the whole grid, sliced to this slab
+        std::vector<float> szg;
+        sponge_axis(h->cfg, 2, h->nz_global, szg);
+        sz.assign(szg.begin() + h->cfg.slab_k0, szg.begin() + h->cfg.slab_k0 + nz);
+    }
 
     // Device buffers.
     if (!h->stream) CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "cudaStreamCreate");
@@ -902,7 +944,8 @@ SourceArgs source_args(lbm_handle* h, bool batched)
     a.ctl = batched ? h->ctl : nullptr;
     a.x_min = h->cfg.x_min;
     a.y_min = h->cfg.y_min;
-    a.z_min = h->cfg.z_min;
+    a.z_min = h->cfg.z_min;    // the whole grid's origin: weights as in an undivided run
+    a.k_off = h->slab ? h->cfg.slab_k0 : 0;
     a.dx = h->cfg.dx;
     a.scale = h->scale;
     return a;
@@ -1083,6 +1126,77 @@ int drain_probes(lbm_handle* h)
     return LBM_OK;
 }
 
+// Source entry of step time t for this handle.  A z-slab whose source
+// stencil reaches past its own layers gets the fluid-weight sum of the whole
+// stencil (k_source divides by it), from the geometry: the mask of any cell
+// of the whole grid follows from the ground heights (06:469-489); with a
+// caller's mask (lbm_set_mask) cells beyond the slab's halo count as fluid.
+SourceEntry entry_for(const lbm_handle* h, const SourceState& st, double t)
+{
+    SourceEntry e = source_entry(st, t, h->dt);
+    if (!h->slab || e.mass == 0.0) return e;
+    const lbm_config& c = h->cfg;
+    const lbm_source& p = st.s;
+    const int k0 = c.slab_k0, k1 = c.slab_k0 + c.slab_nz, nzg = h->nz_global;
+    const int nx = h->NXg, ny = h->NYg;
+    const auto fluid = [&](int gi, int gj, int gk) {
+        if (gi < 0 || gi >= nx || gj < 0 || gj >= ny || gk < 0 || gk >= nzg) return false;
+        if (!h->mask_override.empty())
+        {
+            if (gk < k0 - 1 || gk > k1) return true;
+            const size_t nxt = nx + 2, nyt = ny + 2;
+            return h->mask[(size_t)(gi + 1) + (size_t)(gj + 1) * nxt + (size_t)(gk - k0 + 1) * nxt * nyt] == 0;
+        }
+        if (!c.use_geometry) return true;
+        const double x = c.x_min + (gi + 0.5) * c.dx, y = c.y_min + (gj + 0.5) * c.dx, z = c.z_min + (gk + 0.5) * c.dx;
+        if (z > c.sky_z) return true;
+        return !(z < h->geo.ground_height(x, y));
+    };
+    std::vector<int> cells;   // gi, gj, gk
+    std::vector<double> w;
+    if (p.injection == LBM_INJECT_TRILINEAR)
+    {
+        const double fx = (e.cx - c.x_min) / c.dx - 0.5, fy = (e.cy - c.y_min) / c.dx - 0.5,
+                     fz = (e.cz - c.z_min) / c.dx - 0.5;
+        const int i0 = (int)std::floor(fx), j0 = (int)std::floor(fy), kk0 = (int)std::floor(fz);
+        const double tx = fx - i0, ty = fy - j0, tz = fz - kk0;
+        for (int b = 0; b < 8; ++b)
+        {
+            cells.insert(cells.end(), {i0 + (b & 1), j0 + ((b >> 1) & 1), kk0 + (b >> 2)});
+            w.push_back(((b & 1) ? tx : 1.0 - tx) * (((b >> 1) & 1) ? ty : 1.0 - ty) * ((b >> 2) ? tz : 1.0 - tz));
+        }
+    }
+    else
+    {
+        const int R = p.radius, n = 2 * R + 1;
+        const double sigma2 = (p.sigma_cells * c.dx) * (p.sigma_cells * c.dx);
+        const int ic = (int)std::floor((e.cx - c.x_min) / c.dx), jc = (int)std::floor((e.cy - c.y_min) / c.dx),
+                  kc = (int)std::floor((e.cz - c.z_min) / c.dx);
+        for (int t3 = 0; t3 < n * n * n; ++t3)
+        {
+            const int gi = ic + t3 % n - R, gj = jc + (t3 / n) % n - R, gk = kc + t3 / (n * n) - R;
+            const double ddx = c.x_min + (gi + 0.5) * c.dx - e.cx, ddy = c.y_min + (gj + 0.5) * c.dx - e.cy,
+                         ddz = c.z_min + (gk + 0.5) * c.dx - e.cz;
+            cells.insert(cells.end(), {gi, gj, gk});
+            w.push_back(std::exp(-0.5 * (ddx * ddx + ddy * ddy + ddz * ddz) / sigma2));
+        }
+    }
+    bool outside = false, inside = false;
+    for (size_t b = 0; b < w.size(); ++b)
+    {
+        const int gk = cells[3 * b + 2];
+        if (gk < 0 || gk >= nzg) continue;
+        (gk < k0 || gk >= k1 ? outside : inside) = true;
+    }
+    if (!outside || !inside) return e;   // the slab's own cells are the whole stencil, or none of it
+    double S = 0.0;
+    for (size_t b = 0; b < w.size(); ++b)
+        if (fluid(cells[3 * b], cells[3 * b + 1], cells[3 * b + 2])) S += w[b];
+    if (S < 1e-30) e.mass = 0.0;   // nothing to inject into (06:627)
+    else e.wsum = S;
+    return e;
+}
+
 // Fills the device source schedule with rows for steps [s0, s0 + rows).
 int fill_table(lbm_handle* h, long long s0)
 {
@@ -1092,7 +1206,7 @@ int fill_table(lbm_handle* h, long long s0)
     for (long long r = 0; r <= kTableRows; ++r)   // rows of steps s0 .. s0 + kTableRows
     {
         const double t = (double)(s0 + r) * h->dt;   // t = s * dt (06:1079)
-        for (size_t s = 0; s < ns; ++s) h->h_table[r * ns + s] = source_entry(h->srcs[s], t, h->dt);
+        for (size_t s = 0; s < ns; ++s) h->h_table[r * ns + s] = entry_for(h, h->srcs[s], t);
     }
     CK(cudaMemcpyAsync(h->d_table, h->h_table, ns * (kTableRows + 1) * sizeof(SourceEntry), cudaMemcpyHostToDevice,
                        h->stream),
@@ -1172,7 +1286,7 @@ extern "C" int lbm_apply_source(lbm_handle* h, double t)
     if (h->scheme_a()) return LBM_OK;   // scheme A: the field source acts inside lbm_step_collision_bgk
     CK(cudaSetDevice(h->device), "cudaSetDevice");
     SourceArgs a = source_args(h, false);
-    for (size_t s = 0; s < h->srcs.size(); ++s) a.direct[s] = source_entry(h->srcs[s], t, h->dt);
+    for (size_t s = 0; s < h->srcs.size(); ++s) a.direct[s] = entry_for(h, h->srcs[s], t);
     CK(launch_source(h->storage, h->f[h->cur], h->L, h->sa, a, h->stream), "source kernel");
     h->launches++;
     return LBM_OK;
@@ -1839,6 +1953,7 @@ extern "C" int lbm_adjoint_grad(lbm_handle* h, int nsteps, const double* observe
     if (st) return st;
     if (h->storage != LBM_STORE_F32) return h->fail(LBM_ERR_UNSUPPORTED, "the adjoint runs on FP32 storage");
     if (h->scheme_a()) return h->fail(LBM_ERR_UNSUPPORTED, "the adjoint differentiates scheme B");
+    if (h->slab) return h->fail(LBM_ERR_UNSUPPORTED, "the adjoint runs on a whole grid, not a z-slab");
     if (h->srcs.size() != 1) return h->fail(LBM_ERR_UNSUPPORTED, "the adjoint needs exactly one source");
     const int np = h->nprobe();
     if (np < 1) return h->fail(LBM_ERR_STATE, "the adjoint needs probes");
@@ -2096,4 +2211,80 @@ extern "C" int lbm_adjoint_grad(lbm_handle* h, int nsteps, const double* observe
     if (predicted) std::copy(pred.begin(), pred.end(), predicted);
     *loss = Lsum;
     return rest_state(h);
+}
+
+// ---------------------------------------------------------------- z-slabs
+
+extern "C" int lbm_slab_exchange(lbm_handle* lo, lbm_handle* hi)
+{
+    if (!lo || !hi || lo == hi) return LBM_ERR_INVALID_ARGUMENT;
+    int st = check_ready(lo);
+    if (st) return st;
+    st = check_ready(hi);
+    if (st) return st;
+    if (!lo->slab || !hi->slab) return lo->fail(LBM_ERR_STATE, "lbm_slab_exchange needs two z-slab handles");
+    if (lo->cfg.slab_k0 + lo->cfg.slab_nz != hi->cfg.slab_k0)
+        return lo->fail(LBM_ERR_INVALID_ARGUMENT, "the upper slab does not start where the lower one ends");
+    if (lo->L.nx != hi->L.nx || lo->L.ny != hi->L.ny || lo->storage != hi->storage)
+        return lo->fail(LBM_ERR_INVALID_ARGUMENT, "slabs of different grids");
+    const Layout &A = lo->L, &B = hi->L;
+    const size_t esz = lo->storage == LBM_STORE_F16 ? 2 : 4;
+    const size_t plane = (size_t)A.plane_stride * esz;   // one z-plane, all rows (y-ghost rows included)
+    char* a = (char*)lo->f[lo->cur];
+    char* b = (char*)hi->f[hi->cur];
+    const auto plane_at = [&](char* f, int k) { return f + ((size_t)kFrontElems + (size_t)k * A.plane_stride) * esz; };
+    // x-face ghost rows of one plane: 38 rows of ny + 2 floats, (nz + 2)(ny + 2) floats apart
+    const size_t row = (size_t)(A.ny + 2) * sizeof(float);
+    const size_t pitch_a = (size_t)(A.nz + 2) * row, pitch_b = (size_t)(B.nz + 2) * row;
+    const auto gh_row = [&](const lbm_handle* h, int k) { return (char*)(h->xf.xgh + (size_t)k * (h->L.ny + 2)); };
+    const auto copy_into = [&](lbm_handle* to, char* dst_plane, char* dst_gh, size_t dst_pitch, const lbm_handle* from,
+                               const char* src_plane, const char* src_gh, size_t src_pitch) {
+        cudaError_t e;
+        if (to->device == from->device)
+        {
+            e = cudaMemcpyAsync(dst_plane, src_plane, plane, cudaMemcpyDeviceToDevice, to->stream);
+            if (e == cudaSuccess)
+                e = cudaMemcpy2DAsync(dst_gh, dst_pitch, src_gh, src_pitch, row, 2 * Q, cudaMemcpyDeviceToDevice,
+                                      to->stream);
+            return e;
+        }
+        e = cudaMemcpyPeerAsync(dst_plane, to->device, src_plane, from->device, plane, to->stream);
+        for (int r = 0; r < 2 * Q && e == cudaSuccess; ++r)
+            e = cudaMemcpyPeerAsync(dst_gh + r * dst_pitch, to->device, src_gh + r * src_pitch, from->device, row,
+                                    to->stream);
+        return e;
+    };
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaError_t e = cudaSuccess;
+    for (int n = 0; n < 4 && e == cudaSuccess; ++n)
+    {
+        e = cudaSetDevice(n % 2 ? hi->device : lo->device);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev[n], cudaEventDisableTiming);
+    }
+    // ev0: lower's halo fill done; ev1: upper's; ev2: copies into upper done; ev3: into lower
+    if (e == cudaSuccess) e = cudaSetDevice(lo->device);
+    if (e == cudaSuccess) e = cudaEventRecord(ev[0], lo->stream);
+    if (e == cudaSuccess) e = cudaSetDevice(hi->device);
+    if (e == cudaSuccess) e = cudaEventRecord(ev[1], hi->stream);
+    // upper's halo plane 0 <- lower's plane nz; the lower's plane must have its halo fill
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(hi->stream, ev[0], 0);
+    if (e == cudaSuccess)
+        e = copy_into(hi, plane_at(b, 0), gh_row(hi, 0), pitch_b, lo, plane_at(a, A.nz), gh_row(lo, A.nz), pitch_a);
+    if (e == cudaSuccess) e = cudaEventRecord(ev[2], hi->stream);
+    // lower's halo plane nz + 1 <- upper's plane 1
+    if (e == cudaSuccess) e = cudaSetDevice(lo->device);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(lo->stream, ev[1], 0);
+    if (e == cudaSuccess)
+        e = copy_into(lo, plane_at(a, A.nz + 1), gh_row(lo, A.nz + 1), pitch_a, hi, plane_at(b, 1), gh_row(hi, 1),
+                      pitch_b);
+    if (e == cudaSuccess) e = cudaEventRecord(ev[3], lo->stream);
+    // neither slab overwrites the buffer the other one reads before that copy is done
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(lo->stream, ev[2], 0);
+    if (e == cudaSuccess) e = cudaSetDevice(hi->device);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(hi->stream, ev[3], 0);
+    for (int n = 0; n < 4; ++n)
+        if (ev[n]) cudaEventDestroy(ev[n]);   // released once the streams pass them
+    cudaSetDevice(lo->device);
+    if (e != cudaSuccess) return lo->cuda_fail(e, "slab exchange");
+    return LBM_OK;
 }

@@ -79,6 +79,8 @@ struct SourceEntry
 {
     double cx, cy, cz;     // position at this step (DroneSource::update, 06:221-238)
     double mass;           // val(t) * dt * gain: total mass injected this step (06:631)
+    double wsum;           // > 0: fluid weight sum of the whole stencil, given by the host when the
+                           // stencil reaches past this z-slab (0: the kernel sums its own cells)
 };
 
 struct SourceArgs
@@ -88,8 +90,9 @@ struct SourceArgs
     SourceEntry direct[kMaxSources];   // used when table == nullptr
     const SourceEntry* table;          // [row][nsrc], row = step - ctl->table_base
     const Control* ctl;                // nullptr: use `direct`
-    double x_min, y_min, z_min, dx;
+    double x_min, y_min, z_min, dx;   // origin of the whole grid
     float scale;
+    int k_off;                         // first z-layer of this handle's slab (0: the whole grid)
 };
 
 struct GhostFace

@@ -687,7 +687,9 @@ __global__ void __launch_bounds__(512) k_source(S* __restrict__ f, Layout L, Ste
             const int ic = (int)floor((e.cx - a.x_min) / a.dx);
             const int jc = (int)floor((e.cy - a.y_min) / a.dx);
             const int kc = (int)floor((e.cz - a.z_min) / a.dx);
-            if (ic < -R || ic >= L.nx + R || jc < -R || jc >= L.ny + R || kc < -R || kc >= L.nz + R) continue;
+            if (ic < -R || ic >= L.nx + R || jc < -R || jc >= L.ny + R || kc - a.k_off < -R ||
+                kc - a.k_off >= L.nz + R)
+                continue;
             if (tid < n * n * n)
             {
                 gi = ic + tid % n - R;
@@ -702,10 +704,13 @@ __global__ void __launch_bounds__(512) k_source(S* __restrict__ f, Layout L, Ste
                 in = true;
             }
         }
+        // weights in the coordinates of the whole grid; a z-slab holds layers k_off..
+        gk -= a.k_off;
         bool fluid = false;
         if (in && gi >= 0 && gi < L.nx && gj >= 0 && gj < L.ny && gk >= 0 && gk < L.nz)
             fluid = (sa.links[L.cell(gi + 1, gj + 1, gk + 1)] & kSolidSelfBit) == 0u;
-        const double sum = block_sum(fluid ? ww : 0.0, red);
+        const double bsum = block_sum(fluid ? ww : 0.0, red);
+        const double sum = e.wsum > 0.0 ? e.wsum : bsum;   // a stencil across a z-slab cut
         if (sum < 1e-30) continue;
         const double A = e.mass / sum;
         if (fluid)

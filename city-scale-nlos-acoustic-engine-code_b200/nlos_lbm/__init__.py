@@ -5,5 +5,5 @@ Python side of the C-ABI in include/nlos_lbm.h.  ``abi`` describes the ABI
 LBMSolver interface; ``build`` compiles liblbm_b200.so in-tree.
 """
 from . import abi  # noqa: F401
-from .solver import (DroneSource, LBMError, LBMSolver, Probe, Solver, city_triangles,  # noqa: F401
+from .solver import (DroneSource, LBMError, LBMSolver, Probe, SlabGroup, Solver, city_triangles,  # noqa: F401
                      library, stl_write, voxelize)

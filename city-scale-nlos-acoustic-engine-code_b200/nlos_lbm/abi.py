@@ -68,6 +68,8 @@ class LbmConfig(ctypes.Structure):
         ("tau_sponge_max", ctypes.c_double),
         ("flow", ctypes.c_double * 3),
         ("dt", ctypes.c_double),
+        ("slab_k0", ctypes.c_int),
+        ("slab_nz", ctypes.c_int),
     ]
 
 
@@ -205,6 +207,7 @@ def bind_product(lib):
         "lbm_adjoint_plan": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_int, ctypes.c_int, c_int_p, c_int_p,
                                             ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]),
         "lbm_adjoint_release": (ctypes.c_int, [P]),
+        "lbm_slab_exchange": (ctypes.c_int, [P, P]),
         "lbm_city_generate": (ctypes.c_int, [ctypes.POINTER(LbmCityParams), c_float_p, ctypes.c_int,
                                              c_int_p, c_double_p]),
         "lbm_stl_write": (ctypes.c_int, [ctypes.c_char_p, c_float_p, ctypes.c_int]),

@@ -125,6 +125,12 @@ typedef struct lbm_config
                                                         (03:121 uz = Ma cs); initial state feq(1, flow) */
     double dt;                                       /* > 0: time step in seconds instead of cs*dx/c_phys
                                                         (02:36 uses the constant 0.577350269) */
+    /* z-slab of a decomposed domain (scheme B): the handle holds interior
+     * z-layers slab_k0 .. slab_k0 + slab_nz - 1 of the grid above; slab_nz = 0:
+     * the whole grid.  Cuts between slabs have no boundary treatment: their
+     * halo planes come from the neighbour slab (lbm_slab_exchange). */
+    int slab_k0;
+    int slab_nz;
 } lbm_config;
 
 /* One sound source: DroneSource (06:211-239) plus its time function. */
@@ -315,6 +321,20 @@ int lbm_adjoint_plan(lbm_handle* h, int nsteps, int ckpt_outer, int ckpt_inner, 
  * after the first; this frees it now instead of at lbm_destroy.  No
  * counterpart in the reference. */
 int lbm_adjoint_release(lbm_handle* h);
+
+/* ---- z-slab decomposition --------------------------------------------------- */
+
+/* Halo exchange between two z-slab handles of one domain (no counterpart in
+ * this form; the reference's MPI decomposition exchanges every face through
+ * exchange_halos, 06:837-903).  `lower` holds the layers just below
+ * `upper`.  Call it once per time step, after lbm_apply_source and
+ * lbm_exchange_halos of both handles and before their
+ * lbm_step_collision_bgk: the boundary interior plane of each slab (its
+ * y-ghost rows included) and the x-face ghost rows of that plane are copied
+ * into the other slab's halo.  The copies run on the receiving handle's
+ * stream, ordered against both streams with events, so the handles may live
+ * on different GPUs (peer copies) or on the same one. */
+int lbm_slab_exchange(lbm_handle* lower, lbm_handle* upper);
 
 /* ---- measurement ---------------------------------------------------------- */
 
