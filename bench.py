@@ -32,8 +32,9 @@ sys.path.insert(0, REPO)
 
 METRIC = "D3Q19 GLUPS, %HBM peak: FP16-store vs FP32 @<=1e-3 probe L2; adjoint grad/s"
 # bytes of DRAM traffic per cell update of the fused step kernel, from ncu
-# captures (2.563e9 B and 5.132e9 B for 33.55e6 cells)
-NCU_TRAFFIC_PER_CELL = {"fp16": 2.563e9 / 33554432, "fp32": 5.132e9 / 33554432}
+# captures of the default kernels on the 512x512x128 city (k_step_hw:
+# 2.644e9 B, k_step<float>: 5.132e9 B for 33.55e6 cells)
+NCU_TRAFFIC_PER_CELL = {"fp16": 2.644e9 / 33554432, "fp32": 5.132e9 / 33554432}
 UNIT = "GLUPS"
 
 

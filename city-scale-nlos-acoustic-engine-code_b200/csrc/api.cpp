@@ -33,9 +33,10 @@ constexpr int kBcCut = 100;        // face of a z-slab that borders the next sla
 constexpr int kProbeRows = 4096;   // probe-series rows buffered on the device
 // Fused-step implementation and L2 prefetch distance per storage type, from
 // launch-shape sweeps on the 1024x1024x256 city (B200): FP32 is fastest with
-// the plain pair kernel; FP16 with the packed pair kernel at a 64-register
-// cap plus line prefetches 96 rows ahead.
-constexpr int kDefaultStepVariant[2] = {0, 4};
+// the plain pair kernel; FP16 with the warp pipelines of cp.async copies,
+// two blocks in flight per warp and 20 warps per SM (the prefetch distance
+// applies to the register-held FP16 variants 4-7 only).
+constexpr int kDefaultStepVariant[2] = {0, 10};
 constexpr int kDefaultPrefetchRows[2] = {0, 96};
 // Register cap of the adjoint step kernel (launch_adj_step variant).
 constexpr int kDefaultAdjointVariant = 1;
@@ -842,7 +843,11 @@ extern "C" int lbm_init(lbm_handle* h)
     const int si = h->storage == LBM_STORE_F16 ? 1 : 0;
     h->step_variant = kDefaultStepVariant[si];
     if (const char* v = std::getenv("NLOS_LBM_STEP_VARIANT")) h->step_variant = std::atoi(v);
-    if (h->step_variant < 0 || h->step_variant > 7) return h->fail(LBM_ERR_BAD_CONFIG, "NLOS_LBM_STEP_VARIANT out of range");
+    if (h->step_variant < 0 || h->step_variant > 13) return h->fail(LBM_ERR_BAD_CONFIG, "NLOS_LBM_STEP_VARIANT out of range");
+    {
+        const cudaError_t e = prepare_step(h->storage == LBM_STORE_F16 ? 1 : 0, h->step_variant);
+        if (e != cudaSuccess) return h->cuda_fail(e, "step set-up");
+    }
     h->sa.prefetch_rows = kDefaultPrefetchRows[si];
     if (const char* v = std::getenv("NLOS_LBM_PREFETCH_ROWS")) h->sa.prefetch_rows = std::max(0, std::atoi(v));
 

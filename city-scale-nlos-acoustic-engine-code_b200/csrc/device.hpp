@@ -202,10 +202,16 @@ cudaError_t launch_ghost(int storage, void* f, const Layout& L, const GhostArgs&
 // cells per thread (0: 128 threads, 1: 128 threads with at most 64
 // registers, 2: 256 threads, 3: 64 threads); 4-7: FP16 storage only, kept
 // packed as half2 through the update (cells per thread / register cap:
-// 4: 2/64, 5: 4/85, 6: 2/51, 7: 4/102, 128 threads); FP32 storage runs
-// variant 0 instead.
+// 4: 2/64, 5: 4/85, 6: 2/51, 7: 4/102, 128 threads); 8-12: FP16 storage,
+// warp pipelines of cp.async copies into shared memory (blocks in flight per
+// warp / warps per CTA: 8: 4/4, 9: 3/4, 10: 2/4, 11: 6/2, 12: 4/8), whose
+// collision takes fewer operations in another rounding order; 13: as 10 with
+// the collision of 4-7; FP32 storage runs variant 0 instead of 4-13.
 cudaError_t launch_step(int storage, const void* fin, void* fout, const Layout& L, const StepArgs& a,
                         float scale, int variant, cudaStream_t stream);
+// One-time set-up of a step variant on the current device (shared-memory
+// attribute, occupancy); call before the first launch or capture.
+cudaError_t prepare_step(int storage, int variant);
 // Fused step (FP32 storage, the default implementation) that also writes the
 // moments (rho', jx, jy, jz) of every cell's pulled populations to `mom`,
 // dense cell order ((k-1) ny + (j-1)) nx + (i-1): the forward data of the

@@ -435,6 +435,66 @@ __device__ __forceinline__ void collide2_packed(unsigned (&w)[Q], float inv_scal
     }
 }
 
+// collide2_packed() in fewer operations, for kernels with registers to
+// spare: each word is converted to FP32 once; the moments share partial sums
+// (rho = g0 + rest + S(x+) + S(x-), jx = S(x+) - S(x-)); each direction of a
+// pair (q, inv q) is two FMAs from the pair's equilibrium term
+//   e = (cB w k45) (c.J)^2 + cB w base,   G'_q = cA G_q + e +- 3 cB w (c.J).
+// Same formulas as collide2(); the rounding order differs.
+__device__ __forceinline__ void collide2_grouped(unsigned (&w)[Q], float inv_scale, float omega, float2 sigma,
+                                                 bool solid0, bool solid1)
+{
+    float2 g[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) g[q] = h2f(w[q]);
+    const float2 sxp = add2(add2(add2(g[1], g[7]), add2(g[8], g[11])), g[12]);
+    const float2 sxn = add2(add2(add2(g[2], g[9]), add2(g[10], g[13])), g[14]);
+    const float2 rest = add2(add2(add2(g[3], g[4]), add2(g[5], g[6])), add2(add2(g[15], g[16]), add2(g[17], g[18])));
+    const float2 rho = add2(add2(g[0], rest), add2(sxp, sxn));
+    const float2 jx = sub2(sxp, sxn);
+    const float2 jy = sub2(add2(add2(add2(g[3], g[7]), add2(g[9], g[15])), g[16]),
+                           add2(add2(add2(g[4], g[8]), add2(g[10], g[17])), g[18]));
+    const float2 jz = sub2(add2(add2(add2(g[5], g[11]), add2(g[13], g[15])), g[17]),
+                           add2(add2(add2(g[6], g[12]), add2(g[14], g[16])), g[18]));
+    float2 r = fma2(rho, f2(inv_scale), f2(1.0f));
+    if (r.x <= 0.f) r.x = 1e-12f;   // 06:948
+    if (r.y <= 0.f) r.y = 1e-12f;
+    const float2 irs = make_float2(__fdividef(inv_scale, r.x), __fdividef(inv_scale, r.y));
+    const float2 j2 = fma2(jz, jz, fma2(jy, jy, mul2(jx, jx)));
+    const float2 base = fma2(mul2(irs, j2), f2(-1.5f), rho);
+    const float2 k45 = mul2(irs, f2(4.5f));
+    const float2 keep = sub2(f2(1.0f), sigma);
+    float2 cA = mul2(keep, f2(1.0f - omega));
+    float2 cB = mul2(keep, f2(omega));
+    if (solid0) cA.x = 1.0f, cB.x = 0.0f;
+    if (solid1) cA.y = 1.0f, cB.y = 0.0f;
+    const float2 cBw1 = mul2(cB, f2(wf(1))), cBw2 = mul2(cB, f2(wf(7)));
+    const float2 K1 = mul2(cBw1, k45), K2 = mul2(cBw2, k45);
+    const float2 B1 = mul2(cBw1, base), B2 = mul2(cBw2, base);
+    const float2 T1 = mul2(cB, f2(3.0f * wf(1))), T2 = mul2(cB, f2(3.0f * wf(7)));
+    const float2 N1 = mul2(cB, f2(-3.0f * wf(1))), N2 = mul2(cB, f2(-3.0f * wf(7)));
+    w[0] = f2h(fma2(cA, g[0], mul2(mul2(cB, f2(wf(0))), base)));
+#pragma unroll
+    for (int p = 0; p < 9; ++p)
+    {
+        const int q = pair_head(p);
+        const int qb = inv(q);
+        float2 cj;
+        if (p == 0) cj = jx;
+        else if (p == 1) cj = jy;
+        else if (p == 2) cj = jz;
+        else if (p == 3) cj = add2(jx, jy);
+        else if (p == 4) cj = sub2(jx, jy);
+        else if (p == 5) cj = add2(jx, jz);
+        else if (p == 6) cj = sub2(jx, jz);
+        else if (p == 7) cj = add2(jy, jz);
+        else cj = sub2(jy, jz);
+        const float2 e = fma2(q < 7 ? K1 : K2, mul2(cj, cj), q < 7 ? B1 : B2);
+        w[q] = f2h(fma2(q < 7 ? T1 : T2, cj, fma2(cA, g[q], e)));
+        w[qb] = f2h(fma2(q < 7 ? N1 : N2, cj, fma2(cA, g[qb], e)));
+    }
+}
+
 // FP16 fused step, CELLS = 2 or 4 x-adjacent cells per thread (one aligned
 // 4- or 8-byte vector per direction).  Same pull / bounce-back / x-face /
 // collision semantics as k_step.
@@ -591,6 +651,281 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step_h(const __half* __restrict
             }
         }
     }
+}
+
+// ---------------------------------------------------------------- FP16 step, warp pipelines
+// Each warp walks whole rows one interleaved block (64 cells, two per lane)
+// at a time and keeps the source lines of its next P blocks in flight as
+// cp.async copies into its own ring of shared-memory slots: the bytes in
+// flight no longer depend on registers or on resident warps, and no barrier
+// couples the warps of a CTA.  A block's 19 source lines (direction q from
+// row (j - ey, k - ez)) are 152 16-byte pieces, five copy instructions per
+// lane.  The x neighbour of the block's first / last cell is the last /
+// first element of the previous / next block of the same row, which the ring
+// still / already holds (at the row ends the x-face ghosts replace it).  The
+// near-solid words of a block are loaded one block ahead of its copies and
+// its links words travel with the copies when any bit is set.
+namespace wp {
+constexpr int kPopBytes = 19 * 128;           // one block's 19 source lines
+constexpr int kLinkOff = kPopBytes;           // 64 links words
+constexpr int kNearOff = kPopBytes + 256;     // the block's 2 near-solid words
+constexpr int kGhostOff = kNearOff + 16;      // x-face ghosts of a row-end block: 5 per side
+constexpr int kSlotBytes = kGhostOff + 48;
+// Directions with ex > 0 (ghosts of the low x face) and ex < 0 (high face).
+__device__ __forceinline__ int ghost_dir(int i) { return i < 5 ? (i < 1 ? 1 : i < 3 ? i + 6 : i + 8) : (i < 6 ? 2 : i < 8 ? i + 3 : i + 5); }
+}  // namespace wp
+
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async8(uint32_t dst, const void* src)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async4(uint32_t dst, const void* src)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait()
+{
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// Position of direction q (ex != 0) in a slot's x-face ghosts (inverse of wp::ghost_dir).
+__host__ __device__ constexpr int ghost_slot(int q)
+{
+    constexpr int t[Q] = {-1, 0, 5, -1, -1, -1, -1, 1, 2, 6, 7, 3, 4, 8, 9, -1, -1, -1, -1};
+    return t[q];
+}
+
+template <int P, int WARPS, int MINB, bool GROUPED = true>
+__global__ void __launch_bounds__(32 * WARPS, MINB) k_step_hw(const __half* __restrict__ fin,
+                                                               __half* __restrict__ fout, Layout L, StepArgs a,
+                                                               float inv_scale)
+{
+    constexpr int S = P + 2;   // ring slots: blocks t - 1 .. t + P
+    constexpr uint32_t kDirBits = (1u << Q) - 1u;
+    extern __shared__ __align__(128) unsigned char wp_smem[];
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    unsigned char* ring = wp_smem + warp * (S * wp::kSlotBytes);
+    const uint32_t ring_s = (uint32_t)__cvta_generic_to_shared(ring);
+    const int nrows = L.ny * L.nz;
+    const int all_warps = gridDim.x * WARPS;
+    const int r0 = blockIdx.x * WARPS + warp;   // rows r0, r0 + all_warps, ...; r = (k-1) ny + (j-1)
+    if (r0 >= nrows) return;
+
+    // element offsets of this lane's five 16-byte pieces from the destination block
+    int poff[5];
+#pragma unroll
+    for (int i = 0; i < 5; ++i)
+    {
+        const int p = i * 32 + lane;
+        const int q = min(p >> 3, 18);
+        poff[i] = -(c_ey[q] * (int)L.row_stride + c_ez[q] * (int)L.plane_stride) + q * 64 + (p & 7) * 8;
+    }
+
+    // lanes 0-4 copy the low-face ghosts of a row-start block, lanes 5-9 the
+    // high-face ghosts of a row-end block: ghost of direction q for row
+    // (j, k) is xgh[gh_index(side, q, j - ey, k - ez)] = row (k (ny+2) + j) + goff
+    const int gq = wp::ghost_dir(lane < 10 ? lane : 0);
+    const int goff = (lane < 5 ? 0 : 19) * (L.nz + 2) * (L.ny + 2) + gq * (L.nz + 2) * (L.ny + 2) -
+                     c_ez[gq] * (L.ny + 2) - c_ey[gq];
+
+    // ---- copy cursor: the next block whose lines are copied
+    int ci_r = r0, ci_b = 0;
+    const __half* ci_src = nullptr;     // the block's own position (lines are offset by poff)
+    const uint32_t* ci_near = nullptr;  // the block's two near-solid words
+    const uint32_t* ci_link = nullptr;  // links words of this lane's two cells
+    const float* ci_gh = nullptr;       // this lane's x-face ghost of the row
+    const auto ci_row = [&]() {
+        const int k = 1 + ci_r / L.ny, j = 1 + ci_r - (k - 1) * L.ny;
+        ci_src = fin + L.elem(0, 1, j, k);
+        ci_near = a.near + ((long long)k * (L.ny + 2) + j) * L.words_per_row;
+        ci_link = a.links + L.cell(1, j, k) + 2 * lane;
+        ci_gh = a.xf.xgh + ((long long)k * (L.ny + 2) + j) + goff;
+    };
+    const auto ci_next = [&]() {
+        ci_src += 19 * 64;
+        ci_near += 2;
+        ci_link += 64;
+        if (++ci_b == L.nb)
+        {
+            ci_b = 0;
+            ci_r += all_warps;
+            if (ci_r < nrows) ci_row();
+        }
+    };
+    uint32_t n0 = 0u, n1 = 0u;   // near words of the copy cursor's block, loaded one block ahead
+    const auto load_near = [&]() {
+        n0 = __ldg(ci_near);
+        n1 = ci_b * 64 + 32 < L.nx ? __ldg(ci_near + 1) : 0u;
+    };
+    const auto issue = [&](int slot) {
+        const uint32_t dst = ring_s + slot * wp::kSlotBytes;
+#pragma unroll
+        for (int i = 0; i < 5; ++i)
+            if (i < 4 || lane < 24) cp_async16(dst + (i * 32 + lane) * 16, ci_src + poff[i]);
+        if (lane < 2) reinterpret_cast<uint32_t*>(ring + slot * wp::kSlotBytes + wp::kNearOff)[lane] = lane ? n1 : n0;
+        if ((n0 | n1) != 0u && ci_b * 64 + 2 * lane < L.nx) cp_async8(dst + wp::kLinkOff + lane * 8, ci_link);
+        if ((ci_b == 0 && lane < 5) || (ci_b == L.nb - 1 && lane >= 5 && lane < 10))
+            cp_async4(dst + wp::kGhostOff + lane * 4, ci_gh);
+    };
+
+    // ---- update cursor: the block being updated
+    int cc_r = r0, cc_b = 0, cc_j = 0, cc_k = 0, c0 = 0;
+    const unsigned* own = nullptr;   // this lane's word of line 0 of the block (line q: own[32 q])
+    unsigned* outp = nullptr;
+    float syz = 0.f;
+    const auto cc_row = [&]() {
+        cc_k = 1 + cc_r / L.ny;
+        cc_j = 1 + cc_r - (cc_k - 1) * L.ny;
+        const long long e = L.elem(0, 1, cc_j, cc_k);
+        own = reinterpret_cast<const unsigned*>(fin + e) + lane;
+        outp = reinterpret_cast<unsigned*>(fout + e) + lane;
+        c0 = 2 * lane;
+        syz = fmaxf(__ldg(a.sig_y + cc_j - 1), __ldg(a.sig_z + cc_k - 1));
+    };
+    const auto cc_next = [&]() {
+        own += 19 * 32;
+        outp += 19 * 32;
+        c0 += 64;
+        if (++cc_b == L.nb)
+        {
+            cc_b = 0;
+            cc_r += all_warps;
+            if (cc_r < nrows) cc_row();
+        }
+    };
+
+    ci_row();
+    cc_row();
+#pragma unroll 1
+    for (int p = 0; p < P; ++p)
+    {
+        if (ci_r < nrows)
+        {
+            load_near();
+            issue(p);
+            ci_next();
+        }
+        cp_async_commit();
+    }
+    if (ci_r < nrows) load_near();
+
+    int st = 0;   // slot of block t
+#pragma unroll 1
+    while (cc_r < nrows)
+    {
+        const int sp = st == 0 ? S - 1 : st - 1;
+        const int sn = st == S - 1 ? 0 : st + 1;
+        int si = st + P;
+        if (si >= S) si -= S;
+        if (ci_r < nrows)
+        {
+            issue(si);
+            ci_next();
+            if (ci_r < nrows) load_near();
+        }
+        cp_async_commit();
+        cp_async_wait<P - 1>();   // blocks up to t + 1 have landed
+        __syncwarp();
+
+        const int j = cc_j, k = cc_k;
+        const bool active = c0 < L.nx;
+        const int last = L.nx - 1 - c0;
+        const bool xlo = c0 == 0;
+        const bool xhi = last >= 0 && last < 2;
+        const bool edge = cc_b == 0 || cc_b == L.nb - 1;
+        const unsigned char* slot = ring + st * wp::kSlotBytes;
+
+        // links words of block t (they came with its lines, when a near-solid bit is set)
+        // sponge strengths of the two cells, first so that the loads are in flight early
+        const float sx0 = active ? __ldg(a.sig_x + c0) : 0.f;
+        const float sx1 = c0 + 1 < L.nx ? __ldg(a.sig_x + c0 + 1) : 0.f;
+        const uint2 nw = *reinterpret_cast<const uint2*>(slot + wp::kNearOff);
+        uint32_t lk0 = 0u, lk1 = 0u;
+        bool any_link = false;
+        if ((nw.x | nw.y) != 0u)
+        {
+            const uint32_t bits = active ? ((lane < 16 ? nw.x : nw.y) >> ((2 * lane) & 31)) & 3u : 0u;
+            const uint32_t* lw = reinterpret_cast<const uint32_t*>(slot + wp::kLinkOff) + 2 * lane;
+            lk0 = (bits & 1u) ? lw[0] : 0u;
+            lk1 = (bits & 2u) ? lw[1] : 0u;
+            any_link = __any_sync(kFull, ((lk0 | lk1) & kDirBits) != 0u);
+        }
+        const uint32_t lka = (lk0 | lk1) & kDirBits;
+
+        // pulled words: line q of the slot, shifted by ex(q) across lanes / blocks
+        const unsigned* cur = reinterpret_cast<const unsigned*>(slot) + lane;   // line q: cur[32 q]
+        const unsigned* prv = lane > 0 ? cur - 1
+                                       : (cc_b > 0 ? reinterpret_cast<const unsigned*>(ring + sp * wp::kSlotBytes) + 31
+                                                   : cur);
+        const unsigned* nxt =
+            lane < 31 ? cur + 1
+                      : (cc_b + 1 < L.nb ? reinterpret_cast<const unsigned*>(ring + sn * wp::kSlotBytes) : cur);
+        unsigned w[Q];
+#pragma unroll
+        for (int q = 0; q < Q; ++q)
+        {
+            const unsigned v = cur[32 * q];
+            if (ex(q) == 0) w[q] = v;
+            else if (ex(q) > 0) w[q] = __byte_perm(prv[32 * q], v, 0x5432);
+            else w[q] = __byte_perm(v, nxt[32 * q], 0x5432);
+        }
+        if (any_link)
+        {
+            // halfway bounce-back: the own cell's word of the opposite direction
+#pragma unroll
+            for (int q = 0; q < Q; ++q)
+            {
+                const unsigned o = ((lka >> q) & 1u) ? __ldg(own + inv(q) * 32) : 0u;
+                const unsigned m = ((0u - ((lk0 >> q) & 1u)) & 0x0000ffffu) | ((0u - ((lk1 >> q) & 1u)) & 0xffff0000u);
+                w[q] = (w[q] & ~m) | (o & m);
+            }
+        }
+        if (edge)
+        {
+            // x-face ghosts of the row ends (they came with the block's lines)
+            const float* gs = reinterpret_cast<const float*>(slot + wp::kGhostOff);
+#pragma unroll
+            for (int q = 0; q < Q; ++q)
+            {
+                if (ex(q) == 0) continue;
+                const float g = gs[ghost_slot(q)];
+                if (ex(q) > 0 && xlo && !((lk0 >> q) & 1u)) w[q] = set_lo(w[q], g);
+                if (ex(q) < 0 && xhi && last == 0 && !((lk0 >> q) & 1u)) w[q] = set_lo(w[q], g);
+                if (ex(q) < 0 && xhi && last == 1 && !((lk1 >> q) & 1u)) w[q] = set_hi(w[q], g);
+            }
+        }
+        if (active)
+        {
+            const float2 sg = make_float2(fmaxf(sx0, syz), fmaxf(sx1, syz));
+            if constexpr (GROUPED)
+                collide2_grouped(w, inv_scale, a.omega, sg, (lk0 & kSolidSelfBit) != 0u, (lk1 & kSolidSelfBit) != 0u);
+            else
+                collide2_packed(w, inv_scale, a.omega, sg, (lk0 & kSolidSelfBit) != 0u, (lk1 & kSolidSelfBit) != 0u);
+#pragma unroll
+            for (int q = 0; q < Q; ++q) outp[32 * q] = w[q];
+            if (edge && (xlo | xhi))
+            {
+#pragma unroll
+                for (int q = 0; q < Q; ++q)
+                {
+                    if (xlo) a.xf.xexp[a.xf.exp_index(0, q, j, k, L.ny, L.nz)] = h2f(w[q]).x;
+                    if (xhi && last == 0) a.xf.xexp[a.xf.exp_index(1, q, j, k, L.ny, L.nz)] = h2f(w[q]).x;
+                    if (xhi && last == 1) a.xf.xexp[a.xf.exp_index(1, q, j, k, L.ny, L.nz)] = h2f(w[q]).y;
+                }
+            }
+        }
+        __syncwarp();   // every lane is done with slot t - 1 before the next copy lands there
+        cc_next();
+        st = sn;
+    }
+    cp_async_wait<0>();
 }
 
 // ---------------------------------------------------------------- links
@@ -975,6 +1310,50 @@ dim3 grid_n(const Layout& L, int cells, int block)
     return dim3((unsigned)(((L.nx + cells - 1) / cells + block - 1) / block), (unsigned)L.ny, (unsigned)L.nz);
 }
 
+// Warp-pipelined FP16 step: dynamic shared memory (one ring per warp) and a
+// grid of as many CTAs as the GPU holds at once (every warp then walks rows
+// all_warps apart).  The attribute and the occupancy are set up once per device.
+template <int P, int WARPS, int MINB, bool GROUPED = true>
+cudaError_t hw_ctas(int* out)
+{
+    constexpr int smem = WARPS * (P + 2) * wp::kSlotBytes;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+    static std::mutex mu;
+    static int ctas[kMaxDevices] = {};
+    std::lock_guard<std::mutex> lock(mu);
+    if (!ctas[dev])
+    {
+        e = cudaFuncSetAttribute(k_step_hw<P, WARPS, MINB, GROUPED>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        int per_sm = 0, sms = 0;
+        if (e == cudaSuccess)
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_hw<P, WARPS, MINB, GROUPED>, 32 * WARPS, smem);
+        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (e != cudaSuccess) return e;
+        if (per_sm < 1) return cudaErrorInvalidConfiguration;
+        ctas[dev] = per_sm * sms;
+    }
+    *out = ctas[dev];
+    return cudaSuccess;
+}
+
+template <int P, int WARPS, int MINB, bool GROUPED = true>
+cudaError_t launch_hw(const __half* fin, __half* fout, const Layout& L, const StepArgs& a, float inv_scale,
+                      cudaStream_t stream)
+{
+    // the per-lane source offsets are 32-bit
+    if (L.plane_stride + L.row_stride + 19 * 64 > 0x7fffffffLL) return cudaErrorInvalidValue;
+    int ctas = 0;
+    const cudaError_t e = hw_ctas<P, WARPS, MINB, GROUPED>(&ctas);
+    if (e != cudaSuccess) return e;
+    const long long need = ((long long)L.ny * L.nz + WARPS - 1) / WARPS;
+    const int grid = (int)(need < ctas ? need : ctas);
+    k_step_hw<P, WARPS, MINB, GROUPED><<<grid, 32 * WARPS, WARPS * (P + 2) * wp::kSlotBytes, stream>>>(fin, fout, L, a, inv_scale);
+    return cudaGetLastError();
+}
+
 template <typename S>
 cudaError_t launch_step_t(const S* fin, S* fout, const Layout& L, const StepArgs& a, float inv_scale, int variant,
                           cudaStream_t stream)
@@ -983,6 +1362,12 @@ cudaError_t launch_step_t(const S* fin, S* fout, const Layout& L, const StepArgs
     {
         switch (variant)
         {
+        case 8: return launch_hw<4, 4, 3>(fin, fout, L, a, inv_scale, stream);
+        case 9: return launch_hw<3, 4, 4>(fin, fout, L, a, inv_scale, stream);
+        case 10: return launch_hw<2, 4, 5>(fin, fout, L, a, inv_scale, stream);
+        case 11: return launch_hw<6, 2, 4>(fin, fout, L, a, inv_scale, stream);
+        case 12: return launch_hw<4, 8, 1>(fin, fout, L, a, inv_scale, stream);
+        case 13: return launch_hw<2, 4, 5, false>(fin, fout, L, a, inv_scale, stream);
         case 4: k_step_h<2, 128, 8><<<grid_n(L, 2, 128), 128, 0, stream>>>(fin, fout, L, a, inv_scale); return cudaGetLastError();
         case 5: k_step_h<4, 128, 6><<<grid_n(L, 4, 128), 128, 0, stream>>>(fin, fout, L, a, inv_scale); return cudaGetLastError();
         case 6: k_step_h<2, 128, 10><<<grid_n(L, 2, 128), 128, 0, stream>>>(fin, fout, L, a, inv_scale); return cudaGetLastError();
@@ -1027,6 +1412,22 @@ cudaError_t launch_build_links(const uint8_t* mask_ref, uint32_t* links, uint32_
 {
     k_build_links<<<row_grid(L), 128, 0, stream>>>(mask_ref, links, near, L);
     return cudaGetLastError();
+}
+
+cudaError_t prepare_step(int storage, int variant)
+{
+    if (storage == 0) return cudaSuccess;
+    int ctas = 0;
+    switch (variant)
+    {
+    case 8: return hw_ctas<4, 4, 3>(&ctas);
+    case 9: return hw_ctas<3, 4, 4>(&ctas);
+    case 10: return hw_ctas<2, 4, 5>(&ctas);
+    case 11: return hw_ctas<6, 2, 4>(&ctas);
+    case 12: return hw_ctas<4, 8, 1>(&ctas);
+    case 13: return hw_ctas<2, 4, 5, false>(&ctas);
+    default: return cudaSuccess;
+    }
 }
 
 cudaError_t launch_step(int storage, const void* fin, void* fout, const Layout& L, const StepArgs& a,

@@ -1,0 +1,89 @@
+"""The implementations of the fused FP16 step (NLOS_LBM_STEP_VARIANT 4-13:
+register-held pairs and quads, and the warp pipelines of cp.async copies)
+pull the same values; those that sum the moments in the same order give
+bit-identical results.  The cases cover one partial block per row (nx < 64), exactly
+one block, several blocks with a partial last one, open x faces (NSCBC ghosts
+at both row ends), buildings (links and bounce-back) and more rows than
+resident warps.
+"""
+import numpy as np
+import pytest
+
+import nlos_lbm
+import oracle
+import scenarios
+from nlos_lbm import abi
+from scenarios import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+# FP16 deviation storage with scale 1/amplitude: the 1e-3 probe target
+FP16_PROBE_TOL = 1e-3
+
+# families of implementations with the same arithmetic: (reference variant, others)
+FAMILIES = [(4, [5, 6, 7, 13]),       # the collision with the moments as one chain of sums
+            (10, [8, 9, 11, 12])]     # shared partial sums and fused updates
+
+
+def wide_box(nx=200, ny=24, nz=20, steps=100):
+    """Open box (NSCBC on every face) four blocks wide with a partial last
+    block, a rigid box crossing a block boundary, a Gaussian pulse; the
+    probes sit where the pulse is well above the FP16 resolution."""
+    cfg = scenarios.lattice_config(nx, ny, nz, 0.55, face_bc=(abi.LBM_BC_NSCBC,) * 6, sponge_faces=(1 << 6) - 1,
+                                   sponge_width=6.0, sponge_strength=0.5, storage=abi.LBM_STORE_F16,
+                                   f16_scale=1000.0)
+    tris = scenarios.boxes_to_triangles([(56, 6, 5, 74, 16, 14), (150, 10, 0, 170, 20, 9)])
+    src = abi.reference_source(sx=100.3, sy=12.2, sz=10.1, ex=100.3, ey=12.2, ez=10.1, amp=1e-3, t0=12.0,
+                               sigma_t=3.0)
+    probes = np.array([[110.5, 12.5, 10.5], [90.5, 8.5, 6.5], [128.5, 12.5, 10.5], [64.5, 20.5, 3.5],
+                       [150.5, 5.5, 12.5], [60.5, 12.5, 10.5]])
+    return dict(cfg=cfg, sources=[src], probes=probes, triangles=tris, steps=steps)
+
+
+def fp16_case(name):
+    if name == "wide_box":
+        return wide_box()
+    amp = {"scatter_small": 1e-3, "lloyd_small": 5e-4, "city_small": 1e-3}[name]
+    sc = scenarios.scenario(name, storage=abi.LBM_STORE_F16, f16_scale=1.0 / amp)
+    sc["steps"] = min(sc["steps"], 120)
+    return sc
+
+
+def run(sc, variant, monkeypatch):
+    monkeypatch.setenv("NLOS_LBM_STEP_VARIANT", str(variant))
+    g = nlos_lbm.Solver(sc["cfg"], sc["sources"], sc["probes"], triangles=sc["triangles"])
+    monkeypatch.delenv("NLOS_LBM_STEP_VARIANT")
+    g.step(sc["steps"])
+    out = g.get_probes(), g.get_rho(), g.get_f()
+    g.close()
+    return out
+
+
+@pytest.mark.parametrize("name", ["scatter_small", "lloyd_small", "city_small", "wide_box"])
+def test_fp16_step_variants_bit_identical(name, gpu, monkeypatch):
+    sc = fp16_case(name)
+    for ref, others in FAMILIES:
+        base = run(sc, ref, monkeypatch)
+        assert np.max(np.abs(base[0])) > 0
+        for v in others:
+            got = run(sc, v, monkeypatch)
+            for a, b in zip(base, got):
+                assert np.array_equal(a, b), (name, v)
+
+
+@pytest.mark.parametrize("variant", [ref for ref, _ in FAMILIES])
+@pytest.mark.parametrize("name", ["scatter_small", "lloyd_small", "city_small", "wide_box"])
+def test_fp16_step_families_match_oracle(name, variant, gpu, monkeypatch):
+    sc = fp16_case(name)
+    probes, _, _ = run(sc, variant, monkeypatch)
+    o = oracle.OracleSolver(sc["cfg"], sc["sources"], sc["probes"], triangles=sc["triangles"])
+    o.step(sc["steps"])
+    assert rel_l2(probes, o.get_probes()) <= FP16_PROBE_TOL, rel_l2(probes, o.get_probes())
+
+
+def test_step_variant_out_of_range_is_rejected(gpu, monkeypatch):
+    sc = fp16_case("lloyd_small")
+    monkeypatch.setenv("NLOS_LBM_STEP_VARIANT", "14")
+    with pytest.raises(nlos_lbm.LBMError) as e:
+        nlos_lbm.Solver(sc["cfg"], sc["sources"], sc["probes"])
+    assert e.value.status == abi.LBM_ERR_BAD_CONFIG
