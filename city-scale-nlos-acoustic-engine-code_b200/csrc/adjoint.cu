@@ -267,9 +267,8 @@ __device__ __forceinline__ float2 shifted_pair(const float* row, int lane)
 //   A = sum_q l_q w_q (1 - (4.5 (c_q.J)^2 - 1.5 J^2) / r^2)
 //   B = sum_q l_q w_q (3 c_q + (9 (c_q.J) c_q - 3 J) / r)
 // a = (1 - sigma)(1 - omega), b = (1 - sigma) omega; SOLID cells copy.
-// lamH (gather of lamF^s with the bounce-back terms) stays in registers for
-// the output.  J_C^T is linear in lamH, so the ghost-adjoint terms of the
-// open-face cells are applied afterwards by k_adj_face.
+// lamH (gather of lamF^s with the bounce-back terms and, at the open faces,
+// the ghost-adjoint terms) stays in registers for the output.
 template <int BLOCK, int MINB>
 __global__ void __launch_bounds__(BLOCK, MINB) k_adj_step(AdjStepArgs a)
 {
@@ -361,6 +360,52 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_adj_step(AdjStepArgs a)
     }
     if (!active) return;
 
+    // ---- ghost-adjoint terms of the open faces the pair borders: lamH of a
+    // face cell also holds what the ghost fill took from it (k_adj_ghost),
+    // and J_C^T is applied to the sum.  y and z faces are whole rows (the
+    // branch is uniform across the CTA); the x faces touch the row ends.
+    {
+        const bool yz = (j == 1 && a.gadj_off[2] >= 0) || (j == L.ny && a.gadj_off[3] >= 0) ||
+                        (k == 1 && a.gadj_off[4] >= 0) || (k == L.nz && a.gadj_off[5] >= 0);
+        if (yz)
+        {
+#pragma unroll
+            for (int f = 2; f < 6; ++f)
+            {
+                const bool on = f == 2 ? j == 1 : f == 3 ? j == L.ny : f == 4 ? k == 1 : k == L.nz;
+                if (!on || a.gadj_off[f] < 0) continue;
+                const int axis = f / 2;
+                const long long n = face_cells(L, axis);
+                const float* g = a.gadj + a.gadj_off[f] + face_cell(L, axis, c0 + 1, j, k);
+#pragma unroll
+                for (int q = 0; q < Q; ++q)
+                {
+                    lg[q].x += __ldg(g + q * n);
+                    if (has1) lg[q].y += __ldg(g + q * n + 1);
+                }
+            }
+        }
+        if (xlo | xhi0 | xhi1)
+        {
+            const long long n = face_cells(L, 0), c = face_cell(L, 0, 1, j, k);
+#pragma unroll
+            for (int f = 0; f < 2; ++f)
+            {
+                if (a.gadj_off[f] < 0) continue;
+                const bool to0 = f == 0 ? xlo : xhi0, to1 = f == 1 && xhi1;
+                if (!(to0 | to1)) continue;
+                const float* g = a.gadj + a.gadj_off[f] + c;
+#pragma unroll
+                for (int q = 0; q < Q; ++q)
+                {
+                    const float v = __ldg(g + q * n);
+                    if (to0) lg[q].x += v;
+                    if (to1) lg[q].y += v;
+                }
+            }
+        }
+    }
+
     // ---- J_C^T, packed FP32x2 over the pair, directions taken with their
     // opposites (c_qb = -c_q, so both share c.J)
     const float syz = fmaxf(a.sa.sig_y[j - 1], a.sa.sig_z[k - 1]);
@@ -409,94 +454,6 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_adj_step(AdjStepArgs a)
         *reinterpret_cast<float2*>(out + q * BC) = fma2(ca, lg[q], add2(cbA, cB));
         *reinterpret_cast<float2*>(out + qb * BC) = fma2(ca, lg[qb], sub2(cbA, cB));
     }
-}
-
-// Ghost-adjoint terms of step s at the open-face cells: J_C(F^{s-1})^T of
-// the summed ghost-adjoint contributions, added to lamF^{s-1} after
-// k_adj_step.  One thread per face cell; a cell on several open faces (an
-// edge) is handled by the thread of the first such face only, so every cell
-// is updated once and in a fixed order.
-__global__ void __launch_bounds__(128) k_adj_face(AdjStepArgs a, GhostArgs ga)
-{
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= ga.total) return;
-    int fi = 0;
-    while (fi + 1 < ga.nfaces && t >= ga.face[fi + 1].first) ++fi;
-    const GhostFace F = ga.face[fi];
-    const long long lt = t - F.first;
-    const int u = (int)(lt % F.nu), v = (int)(lt / F.nu);
-    const Layout& L = a.L;
-    int i, j, k;
-    if (F.axis == 0)
-    {
-        i = F.side ? L.nx : 1;
-        j = 1 + u;
-        k = 1 + v;
-    }
-    else if (F.axis == 1)
-    {
-        i = 1 + u;
-        j = F.side ? L.ny : 1;
-        k = 1 + v;
-    }
-    else
-    {
-        i = 1 + u;
-        j = 1 + v;
-        k = F.side ? L.nz : 1;
-    }
-    const bool at[6] = {i == 1, i == L.nx, j == 1, j == L.ny, k == 1, k == L.nz};
-    int owner = -1;
-    for (int f = 0; f < 6 && owner < 0; ++f)
-        if (at[f] && a.gadj_off[f] >= 0) owner = f;
-    if (owner != F.axis * 2 + F.side) return;
-    // every load first (one memory round trip): the cell's lamF^{s-1} (19
-    // lines apart for x-face cells), its links word and moments, the
-    // ghost-adjoint terms of each open face it lies on
-    float* out = a.lam_out + L.elem(0, i, j, k);
-    float lo[Q], g[Q];
-#pragma unroll
-    for (int q = 0; q < Q; ++q) lo[q] = out[q * L.bc];
-    const uint32_t lk = a.sa.links[L.cell(i, j, k)];
-    const float4 m = __ldg(a.mom_prev + ((long long)(k - 1) * L.ny + (j - 1)) * L.nx + (i - 1));
-#pragma unroll
-    for (int q = 0; q < Q; ++q) g[q] = 0.f;
-#pragma unroll
-    for (int f = 0; f < 6; ++f)
-    {
-        if (!at[f] || a.gadj_off[f] < 0) continue;
-        const int axis = f / 2;
-        const long long n = face_cells(L, axis), c = face_cell(L, axis, i, j, k);
-#pragma unroll
-        for (int q = 0; q < Q; ++q) g[q] += __ldg(a.gadj + a.gadj_off[f] + (long long)q * n + c);
-    }
-    if (lk & kSolidSelfBit)
-    {
-#pragma unroll
-        for (int q = 0; q < Q; ++q) out[q * L.bc] = lo[q] + g[q];
-        return;
-    }
-    float r = 1.0f + m.x;
-    if (r <= 0.f) r = 1e-12f;
-    const float ir = 1.0f / r;
-    const float j2 = m.y * m.y + m.z * m.z + m.w * m.w;
-    float A = 0.f, Bx = 0.f, By = 0.f, Bz = 0.f;
-#pragma unroll
-    for (int q = 0; q < Q; ++q)
-    {
-        const float cj = (float)ex(q) * m.y + (float)ey(q) * m.z + (float)ez(q) * m.w;
-        const float wl = wf(q) * g[q];
-        A += wl * (1.0f - (4.5f * cj * cj - 1.5f * j2) * ir * ir);
-        const float tq = 3.0f + 9.0f * cj * ir;
-        Bx += wl * ((float)ex(q) * tq - 3.0f * m.y * ir);
-        By += wl * ((float)ey(q) * tq - 3.0f * m.z * ir);
-        Bz += wl * ((float)ez(q) * tq - 3.0f * m.w * ir);
-    }
-    const float sg = fmaxf(a.sa.sig_x[i - 1], fmaxf(a.sa.sig_y[j - 1], a.sa.sig_z[k - 1]));
-    const float ca = (1.0f - sg) * (1.0f - a.sa.omega), cb = (1.0f - sg) * a.sa.omega;
-#pragma unroll
-    for (int p = 0; p < Q; ++p)
-        out[p * L.bc] = lo[p] + ca * g[p] + cb * (A + (float)ex(p) * Bx + (float)ey(p) * By + (float)ez(p) * Bz);
 }
 
 // Residual of each probe enters the adjoint of every population it summed.
@@ -558,7 +515,7 @@ cudaError_t launch_adj_ghost(const AdjGhostArgs& a, cudaStream_t stream)
     return cudaGetLastError();
 }
 
-cudaError_t launch_adj_step(const AdjStepArgs& a, const GhostArgs& ga, int variant, cudaStream_t stream)
+cudaError_t launch_adj_step(const AdjStepArgs& a, int variant, cudaStream_t stream)
 {
     if (a.L.bc != 32) return cudaErrorInvalidValue;   // FP32 layout only
     // rows of up to 128 columns take 64-thread blocks, so no warp idles
@@ -582,9 +539,6 @@ cudaError_t launch_adj_step(const AdjStepArgs& a, const GhostArgs& ga, int varia
         default: k_adj_step<128, 1><<<g, 128, 0, stream>>>(a); break;
         }
     }
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess || ga.total <= 0) return e;
-    k_adj_face<<<(unsigned)((ga.total + 127) / 128), 128, 0, stream>>>(a, ga);
     return cudaGetLastError();
 }
 

@@ -2188,8 +2188,8 @@ extern "C" int lbm_adjoint_grad(lbm_handle* h, int nsteps, const double* observe
                 if (s == 0) continue;
                 AdjStepArgs as{L, h->sa, lam[la], lam[la ^ 1], mom_of(s - 1 - cn), gadj, {}};
                 std::copy(gadj_off, gadj_off + 6, as.gadj_off);
-                CK(launch_adj_step(as, h->ga, adj_variant, h->stream), "adjoint step");
-                kernels += h->ga.total > 0 ? 2 : 1;
+                CK(launch_adj_step(as, adj_variant, h->stream), "adjoint step");
+                kernels++;
                 la ^= 1;
                 pa.resid = d_resid + (size_t)(s - 1) * np;
                 CK(launch_adj_probe(lam[la], pa, h->stream), "adjoint probe");
