@@ -1839,10 +1839,15 @@ void source_cells(const lbm_handle* h, const lbm_source& p, const SourceEntry& e
 
 // Checkpoint schedule of one adjoint evaluation: outer interval K1, inner
 // interval K2 and the device bytes it allocates.  ckpt_inner <= 0 picks the
-// largest K2 <= K1 whose buffers fit in 90 % of the free device memory.
+// largest K2 <= K1 whose buffers fit in 90 % of the free device memory and
+// then, within the same budget, the longest tail of whole outer segments
+// [Tt, T) whose forward data the first pass stores (those segments are
+// reversed without a recompute).
 struct AdjPlan
 {
     int K1 = 0, K2 = 0, M = 0, NI = 0, ncell = 0;
+    int Tt = 0;                                  // tail start (T: no tail), a multiple of K1
+    int C = 0;                                   // store slots (steps of forward data)
     size_t pop = 0, ck_slot = 0, st_slot = 0;   // floats; st_slot: one step's stored moments
     size_t mom_n = 0;                            // float4 of cell moments per stored step
     long long gadj_n = 0;
@@ -1867,12 +1872,12 @@ AdjPlan adjoint_plan(const lbm_handle* h, int T, int ckpt_outer, int ckpt_inner)
     p.K1 = std::min(ckpt_outer > 0 ? ckpt_outer : 200, T);
     p.M = (T + p.K1 - 1) / p.K1;
     const int np = h->nprobe();
-    const auto bytes = [&](int K2) {
+    const auto bytes = [&](int K2, int C) {
         const size_t ni = (size_t)((p.K1 + K2 - 1) / K2);
         Carve c;
         c.get<float>((size_t)p.M * p.ck_slot);
         c.get<float>(ni * p.ck_slot);
-        c.get<float>((size_t)(K2 + 1) * p.st_slot);
+        c.get<float>((size_t)std::max(C, K2 + 1) * p.st_slot);
         c.get<float>(p.pop);
         c.get<float>(p.pop);
         c.get<float>((size_t)p.gadj_n);
@@ -1882,6 +1887,7 @@ AdjPlan adjoint_plan(const lbm_handle* h, int T, int ckpt_outer, int ckpt_inner)
         c.get<double>((size_t)T * 4);
         return c.used;
     };
+    p.Tt = T;
     if (ckpt_inner > 0)
     {
         p.K2 = std::min(ckpt_inner, p.K1);
@@ -1890,22 +1896,36 @@ AdjPlan adjoint_plan(const lbm_handle* h, int T, int ckpt_outer, int ckpt_inner)
     {
         size_t fr = 0, tot = 0;
         if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) fr = 0;
-        const double budget = 0.9 * (double)(fr + h->adj_ws_bytes);   // the workspace is reused
+        double budget = 0.9 * (double)(fr + h->adj_ws_bytes);   // the workspace is reused
+        // NLOS_LBM_ADJ_BUDGET: a smaller cap in bytes (e.g. for a GPU shared with other work)
+        if (const char* v = std::getenv("NLOS_LBM_ADJ_BUDGET")) budget = std::min(budget, std::atof(v));
         p.K2 = 1;
         for (int K2 = p.K1; K2 >= 1; --K2)
-            if ((double)bytes(K2) <= budget)
+            if ((double)bytes(K2, K2 + 1) <= budget)
             {
                 p.K2 = K2;
                 break;
             }
+        // the tail: steps max(Tt - 1, 0) .. T - 1 keep their forward data
+        for (int m = 0; m < p.M; ++m)
+        {
+            const int Tt = m * p.K1, need = T - std::max(Tt - 1, 0);
+            if ((double)bytes(p.K2, need) <= budget)
+            {
+                p.Tt = Tt;
+                break;
+            }
+        }
     }
+    p.C = std::max(p.K2 + 1, T - std::max(p.Tt - 1, 0));
+    if (p.Tt == T) p.C = p.K2 + 1;
     p.NI = (p.K1 + p.K2 - 1) / p.K2;
-    p.bytes = bytes(p.K2);
+    p.bytes = bytes(p.K2, p.C);
     // forward steps (fused pull-collide launches): the first pass, the outer
     // recompute to the inner checkpoints and the recompute of every inner
-    // segment (its last state needs only the source and ghost fill)
+    // segment before the tail (its last state needs only the source and ghost fill)
     p.fwd_steps = T;
-    for (int m = 0; m < p.M; ++m)
+    for (int m = 0; m < p.M && m * p.K1 < p.Tt; ++m)
     {
         const long long O = (long long)m * p.K1, E = std::min<long long>(O + p.K1, T);
         const long long N = (E - O + p.K2 - 1) / p.K2;
@@ -1970,6 +1990,8 @@ extern "C" int lbm_adjoint_grad(lbm_handle* h, int nsteps, const double* observe
     const int T = nsteps;
     const AdjPlan plan = adjoint_plan(h, T, ckpt_outer, ckpt_inner);
     const int K1 = plan.K1, K2 = plan.K2, M = plan.M, NI = plan.NI, ncell = plan.ncell;
+    const int Tt = plan.Tt;                        // steps Tt .. T-1 are reversed from the first pass's data
+    const int Mr = (Tt + K1 - 1) / K1;             // outer segments reversed with a recompute
     const Layout& L = h->L;
     const size_t n_xexp = (size_t)2 * Q * L.ny * L.nz;
     const size_t pop = plan.pop;
@@ -2004,7 +2026,7 @@ extern "C" int lbm_adjoint_grad(lbm_handle* h, int nsteps, const double* observe
     const auto carve = [&](Carve& c) {
         outer = StateSlots{c.get<float>((size_t)M * plan.ck_slot), pop, plan.ck_slot - pop};
         inner = StateSlots{c.get<float>((size_t)NI * plan.ck_slot), pop, plan.ck_slot - pop};
-        store = c.get<float>((size_t)(K2 + 1) * plan.st_slot);
+        store = c.get<float>((size_t)plan.C * plan.st_slot);
         lam[0] = c.get<float>(pop);
         lam[1] = c.get<float>(pop);
         gadj = c.get<float>((size_t)gadj_n);
@@ -2096,27 +2118,45 @@ extern "C" int lbm_adjoint_grad(lbm_handle* h, int nsteps, const double* observe
         }
         return r;
     };
-    const auto stored_collide = [&](long long slot) {
+    // probe_step >= 0: also the probe record of that step (first pass)
+    const auto stored_collide = [&](long long slot, int probe_step = -1) {
         kernels++;
-        const cudaError_t r =
+        cudaError_t r =
             launch_step_moments((const float*)h->f[h->cur], (float*)h->f[h->cur ^ 1], L, h->sa, mom_of(slot), h->stream);
+        if (r == cudaSuccess && probe_step >= 0)
+        {
+            ProbeArgs pa = probe_args(h, false, probe_step);
+            pa.out = d_pred;
+            r = launch_probe(h->storage, h->f[h->cur], L, h->sa, pa, h->stream);
+            kernels++;
+        }
         h->cur ^= 1;
         return r;
     };
     const auto ckpt_pos = [&](long long boundary) { return std::max(boundary - 1, 0LL); };
+    const long long cnT = ckpt_pos(Tt);   // first step whose forward data the first pass stores
 
-    // ---- forward pass: probe predictions and outer checkpoints G^{max(mK1-1,0)}
+    // ---- forward pass: probe predictions, outer checkpoints G^{max(mK1-1,0)}
+    // of the segments before the tail, and the tail's forward data
     {
         int m = 0;
         for (int s = 0; s < T; ++s)
         {
-            while (m < M && ckpt_pos((long long)m * K1) == s)
+            while (m < Mr && ckpt_pos((long long)m * K1) == s)
             {
                 CK(save_g(outer, m), "checkpoint");
                 ++m;
             }
-            CK(source_ghost(s), "adjoint forward");
-            CK(collide(s, true), "adjoint forward");
+            if (Tt < T && s >= cnT)
+            {
+                CK(stored_source_ghost(s, s - cnT), "adjoint forward");
+                CK(stored_collide(s - cnT, s), "adjoint forward");
+            }
+            else
+            {
+                CK(source_ghost(s), "adjoint forward");
+                CK(collide(s, true), "adjoint forward");
+            }
         }
     }
 
@@ -2146,9 +2186,41 @@ extern "C" int lbm_adjoint_grad(lbm_handle* h, int nsteps, const double* observe
     pa.resid = d_resid + (size_t)(T - 1) * np;
     CK(launch_adj_probe(lam[la], pa, h->stream), "adjoint probe");
     kernels++;
-    for (int m = M - 1; m >= 0; --m)
+    // adjoint steps a1-1 .. a0 with the forward data of step s in store slot s - cn
+    const auto reverse_segment = [&](int a0, int a1, int cn) -> int {
+        for (int s = a1 - 1; s >= a0; --s)
+        {
+            if (h->ga.total > 0)
+            {
+                AdjGhostArgs ga{L, h->ga, h->links, lam[la], face_mom_of(s - cn), gadj, {}};
+                std::copy(gadj_off, gadj_off + 6, ga.gadj_off);
+                CK(launch_adj_ghost(ga, h->stream), "adjoint ghost");
+                kernels++;
+            }
+            AdjSourceArgs sa{L, h->links, lam[la], gadj, {}, d_cells, ncell, s, d_out};
+            std::copy(gadj_off, gadj_off + 6, sa.gadj_off);
+            CK(launch_adj_source(sa, h->stream), "adjoint source");
+            kernels++;
+            if (s == 0) continue;
+            AdjStepArgs as{L, h->sa, lam[la], lam[la ^ 1], mom_of(s - 1 - cn), gadj, {}};
+            std::copy(gadj_off, gadj_off + 6, as.gadj_off);
+            CK(launch_adj_step(as, adj_variant, h->stream), "adjoint step");
+            kernels++;
+            la ^= 1;
+            pa.resid = d_resid + (size_t)(s - 1) * np;
+            CK(launch_adj_probe(lam[la], pa, h->stream), "adjoint probe");
+            kernels++;
+        }
+        return LBM_OK;
+    };
+    if (Tt < T)
     {
-        const int O = m * K1, E = std::min(O + K1, T);
+        st = reverse_segment(Tt, T, (int)cnT);
+        if (st) return st;
+    }
+    for (int m = Mr - 1; m >= 0; --m)
+    {
+        const int O = m * K1, E = std::min(O + K1, Tt);
         const int N = (E - O + K2 - 1) / K2;
         CK(restore_g(outer, m), "restore");
         long long at = ckpt_pos(O);   // the current buffer holds G^at
@@ -2172,29 +2244,8 @@ extern "C" int lbm_adjoint_grad(lbm_handle* h, int nsteps, const double* observe
                 CK(stored_source_ghost(s, s - cn), "recompute");
                 if (s + 1 < a1) CK(stored_collide(s - cn), "recompute");
             }
-            for (int s = a1 - 1; s >= a0; --s)
-            {
-                if (h->ga.total > 0)
-                {
-                    AdjGhostArgs ga{L, h->ga, h->links, lam[la], face_mom_of(s - cn), gadj, {}};
-                    std::copy(gadj_off, gadj_off + 6, ga.gadj_off);
-                    CK(launch_adj_ghost(ga, h->stream), "adjoint ghost");
-                    kernels++;
-                }
-                AdjSourceArgs sa{L, h->links, lam[la], gadj, {}, d_cells, ncell, s, d_out};
-                std::copy(gadj_off, gadj_off + 6, sa.gadj_off);
-                CK(launch_adj_source(sa, h->stream), "adjoint source");
-                kernels++;
-                if (s == 0) continue;
-                AdjStepArgs as{L, h->sa, lam[la], lam[la ^ 1], mom_of(s - 1 - cn), gadj, {}};
-                std::copy(gadj_off, gadj_off + 6, as.gadj_off);
-                CK(launch_adj_step(as, adj_variant, h->stream), "adjoint step");
-                kernels++;
-                la ^= 1;
-                pa.resid = d_resid + (size_t)(s - 1) * np;
-                CK(launch_adj_probe(lam[la], pa, h->stream), "adjoint probe");
-                kernels++;
-            }
+            st = reverse_segment(a0, a1, cn);
+            if (st) return st;
         }
     }
 

@@ -83,7 +83,8 @@ def test_adjoint_matches_central_fd_of_gpu_forward(case, gpu):
 def test_checkpoint_schedules_are_bit_identical(gpu):
     sc = scenarios.adjoint_scenario(nx=32, ny=24, nz=16, steps=45, nprobe=6)
     g = Solver(sc["cfg"], [sc["trial"]], sc["probes"], triangles=sc["triangles"])
-    runs = [g.adjoint_grad(sc["observed"], a, b) for a, b in ((0, 0), (45, 45), (7, 3), (1, 1), (10, 10))]
+    # (0, 0) and (10, 0): the whole run's forward data kept from the first pass
+    runs = [g.adjoint_grad(sc["observed"], a, b) for a, b in ((0, 0), (45, 45), (7, 3), (1, 1), (10, 10), (10, 0))]
     for r in runs[1:]:
         assert r[0] == runs[0][0]
         assert np.array_equal(r[1], runs[0][1])
@@ -138,10 +139,32 @@ def test_adjoint_plan(gpu):
     g = Solver(sc["cfg"], [sc["trial"]], sc["probes"], triangles=sc["triangles"])
     assert g.adjoint_plan(45, 7, 3)[:2] == (7, 3)
     assert g.adjoint_plan(45, 100, 60)[:2] == (45, 45)            # intervals clamp to the run
-    o, i, nbytes, fwd = g.adjoint_plan(45, 0, 0)                   # small grid: whole segments fit
-    assert (o, i) == (45, 45) and nbytes > 0 and fwd == 2 * 45 - 1
+    o, i, nbytes, fwd = g.adjoint_plan(45, 0, 0)                   # small grid: the whole run's forward
+    assert (o, i) == (45, 45) and nbytes > 0 and fwd == 45          # data fits, no recompute
+    o, i, nbytes, fwd = g.adjoint_plan(45, 10, 0)
+    assert (o, i) == (10, 10) and fwd == 45
     assert g.adjoint_plan(45, 45, 45)[3] == 2 * 45 - 1              # one forward pass + one recompute
     assert g.adjoint_plan(45, 9, 1)[3] > g.adjoint_plan(45, 9, 9)[3]
+
+
+def test_partial_stored_tail(gpu, monkeypatch):
+    """A memory cap that holds the forward data of the last two 10-step
+    segments: those are reversed from the first pass's data, the first three
+    with a recompute; the result is bit-identical to recomputing every segment."""
+    sc = scenarios.adjoint_scenario(nx=32, ny=24, nz=16, steps=45, nprobe=6)
+    g = Solver(sc["cfg"], [sc["trial"]], sc["probes"], triangles=sc["triangles"])
+    none = g.adjoint_plan(45, 10, 10)          # explicit inner interval: 11 store slots, no tail
+    full = g.adjoint_plan(45, 10, 0)           # everything fits: 45 store slots
+    slot = (full[2] - none[2]) / (45 - 11)
+    monkeypatch.setenv("NLOS_LBM_ADJ_BUDGET", str(none[2] + 5.5 * slot))   # 16 slots: steps 29..44
+    o, i, nbytes, fwd = g.adjoint_plan(45, 10, 0)
+    assert (o, i) == (10, 10) and fwd == 45 + 9 + 10 + 10
+    part = g.adjoint_grad(sc["observed"], 10, 0)
+    monkeypatch.delenv("NLOS_LBM_ADJ_BUDGET")
+    ref = g.adjoint_grad(sc["observed"], 10, 10)
+    assert part[0] == ref[0]
+    for a, b in zip(part[1:], ref[1:]):
+        assert np.array_equal(a, b)
 
 
 def test_workspace_is_kept_and_released(gpu):
