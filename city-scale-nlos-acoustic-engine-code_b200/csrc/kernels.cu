@@ -1051,14 +1051,19 @@ __global__ void __launch_bounds__(512) k_source(S* __restrict__ f, Layout L, Ste
         if (fluid)
         {
             const double add = A * ww * (double)a.scale;
+            // the 19 directions of one cell are 19 distinct elements: every load
+            // first (one round trip), then the stores
+            S* p = f + L.elem(0, gi + 1, gj + 1, gk + 1);   // direction q at p + q * bc
+            float v[Q];
+#pragma unroll
+            for (int q = 0; q < Q; ++q) v[q] = Io<S>::ldw(p + q * L.bc);
 #pragma unroll
             for (int q = 0; q < Q; ++q)
             {
-                S* p = f + L.elem(q, gi + 1, gj + 1, gk + 1);
-                Io<S>::st(p, Io<S>::ldw(p) + (float)(wd(q) * add));
+                Io<S>::st(p + q * L.bc, v[q] + (float)(wd(q) * add));
                 if (gi == 0 || gi == L.nx - 1)
                 {
-                    const float gs = Io<S>::ldw(p);   // the stored value, as the step would export it
+                    const float gs = Io<S>::ldw(p + q * L.bc);   // the stored value, as the step would export it
                     if (gi == 0) sa.xf.xexp[sa.xf.exp_index(0, q, gj + 1, gk + 1, L.ny, L.nz)] = gs;
                     if (gi == L.nx - 1) sa.xf.xexp[sa.xf.exp_index(1, q, gj + 1, gk + 1, L.ny, L.nz)] = gs;
                 }
