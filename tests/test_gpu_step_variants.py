@@ -87,3 +87,40 @@ def test_step_variant_out_of_range_is_rejected(gpu, monkeypatch):
     with pytest.raises(nlos_lbm.LBMError) as e:
         nlos_lbm.Solver(sc["cfg"], sc["sources"], sc["probes"])
     assert e.value.status == abi.LBM_ERR_BAD_CONFIG
+
+
+def odd_box(n3, storage, steps=30):
+    """Open box (NSCBC on every face) of an odd shape: rows shorter than, equal
+    to, or just longer than a 64-cell block, single-row planes."""
+    nx, ny, nz = n3
+    cfg = scenarios.lattice_config(nx, ny, nz, 0.55, face_bc=(abi.LBM_BC_NSCBC,) * 6, sponge_faces=0,
+                                   storage=storage, f16_scale=1000.0)
+    c = (nx / 2 + 0.1, ny / 2 + 0.2, nz / 2 + 0.3)
+    src = abi.reference_source(sx=c[0], sy=c[1], sz=c[2], ex=c[0], ey=c[1], ez=c[2], amp=1e-3, t0=6.0,
+                               sigma_t=2.0)
+    probes = np.array([[0.5, 0.5, 0.5], [nx - 0.5, ny - 0.5, nz - 0.5], [min(c[0] + 1.0, nx - 0.5), c[1], c[2]],
+                       [min(nx - 0.5, 63.5), 0.5, nz - 0.5]])
+    return dict(cfg=cfg, sources=[src], probes=probes, triangles=None, steps=steps)
+
+
+ODD_SHAPES = [(1, 5, 4), (3, 2, 3), (63, 2, 2), (65, 3, 2), (130, 1, 3)]
+
+
+@pytest.mark.parametrize("n3", ODD_SHAPES)
+def test_odd_shapes_match_oracle(n3, gpu, monkeypatch):
+    sc32 = odd_box(n3, abi.LBM_STORE_F32)
+    o = oracle.OracleSolver(sc32["cfg"], sc32["sources"], sc32["probes"])
+    o.step(sc32["steps"])
+    ref = o.get_probes()
+    assert np.max(np.abs(ref)) > 0
+    g = nlos_lbm.Solver(sc32["cfg"], sc32["sources"], sc32["probes"])
+    g.step(sc32["steps"])
+    assert rel_l2(g.get_probes(), ref) <= 1e-5, rel_l2(g.get_probes(), ref)
+    sc16 = odd_box(n3, abi.LBM_STORE_F16)
+    for base, others in FAMILIES:
+        first = run(sc16, base, monkeypatch)
+        assert rel_l2(first[0], ref) <= FP16_PROBE_TOL, (n3, base, rel_l2(first[0], ref))
+        for v in others:
+            got = run(sc16, v, monkeypatch)
+            for a, b in zip(first, got):
+                assert np.array_equal(a, b), (n3, v)
