@@ -7,6 +7,7 @@
 // -ffp-contract=off so the FP64 host arithmetic keeps the reference's
 // rounding.
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <cmath>
@@ -388,6 +389,16 @@ void grid_size(const lbm_config& c, int& nx, int& ny, int& nz)
     nz = (int)((c.z_max - c.z_min) / c.dx + 0.5);
 }
 
+// NVTX range around an entry point or a phase, for profilers (ncu --nvtx,
+// Nsight Systems); without an attached tool it costs a pointer test.
+struct NvtxRange
+{
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
+
 #define CK(expr, where)                                   \
     do                                                    \
     {                                                     \
@@ -686,6 +697,7 @@ extern "C" int lbm_probe_info(lbm_handle* h, int* owned, int* in_solid)
 
 extern "C" int lbm_init(lbm_handle* h)
 {
+    NvtxRange range("lbm_init");
     if (!h) return LBM_ERR_INVALID_ARGUMENT;
     h->release();
     CK(cudaSetDevice(h->device), "cudaSetDevice");
@@ -1368,6 +1380,7 @@ extern "C" int lbm_record_probes(lbm_handle* h)
 
 extern "C" int lbm_step(lbm_handle* h, int nsteps)
 {
+    NvtxRange range("lbm_step");
     int st = check_ready(h);
     if (st) return st;
     if (nsteps < 0) return LBM_ERR_INVALID_ARGUMENT;
@@ -1438,6 +1451,7 @@ extern "C" int lbm_step(lbm_handle* h, int nsteps)
 
 extern "C" int lbm_run(lbm_handle* h, double T_total, int frames)
 {
+    NvtxRange range("lbm_run");
     int st = check_ready(h);
     if (st) return st;
     // 06:1066-1068; steps s = 0..total_steps inclusive (06:1077).
@@ -1974,6 +1988,7 @@ extern "C" int lbm_adjoint_plan(lbm_handle* h, int nsteps, int ckpt_outer, int c
 extern "C" int lbm_adjoint_grad(lbm_handle* h, int nsteps, const double* observed, int ckpt_outer, int ckpt_inner,
                                 double* loss, double* grad_pos, double* grad_signal, double* predicted)
 {
+    NvtxRange range("lbm_adjoint_grad");
     int st = check_ready(h);
     if (st) return st;
     if (h->storage != LBM_STORE_F32) return h->fail(LBM_ERR_UNSUPPORTED, "the adjoint runs on FP32 storage");
@@ -2139,6 +2154,7 @@ extern "C" int lbm_adjoint_grad(lbm_handle* h, int nsteps, const double* observe
     // ---- forward pass: probe predictions, outer checkpoints G^{max(mK1-1,0)}
     // of the segments before the tail, and the tail's forward data
     {
+        NvtxRange phase("adjoint forward pass");
         int m = 0;
         for (int s = 0; s < T; ++s)
         {
@@ -2180,6 +2196,7 @@ extern "C" int lbm_adjoint_grad(lbm_handle* h, int nsteps, const double* observe
        "residual upload");
 
     // ---- reverse pass
+    NvtxRange reverse_phase("adjoint reverse pass");
     for (int b = 0; b < 2; ++b) CK(cudaMemsetAsync(lam[b], 0, pop * sizeof(float), h->stream), "adjoint memset");
     int la = 0;
     AdjProbeArgs pa{np, h->d_probe_ijk, nullptr, L};
@@ -2273,6 +2290,7 @@ extern "C" int lbm_adjoint_grad(lbm_handle* h, int nsteps, const double* observe
 
 extern "C" int lbm_slab_exchange(lbm_handle* lo, lbm_handle* hi)
 {
+    NvtxRange range("lbm_slab_exchange");
     if (!lo || !hi || lo == hi) return LBM_ERR_INVALID_ARGUMENT;
     int st = check_ready(lo);
     if (st) return st;
