@@ -8,6 +8,7 @@
 #include <cstdint>
 
 #include "adjoint.hpp"
+#include "check.cuh"
 #include "lattice.cuh"
 
 namespace lbm {
@@ -243,20 +244,26 @@ __device__ __forceinline__ float2 cdot(int q, float2 x, float2 y, float2 z)
 // aligned float2 per lane; the +-1 shift takes the neighbour element from the
 // adjacent lane and, at the warp edge, from the adjacent block (the same
 // scheme as the forward step).  Every lane of the warp must call it.
+// pair load of buffer `base` (total elements); the bounds-checked build tests the index first
+__device__ __forceinline__ float2 ldg2c(const float* p, const float* base, long long total)
+{
+    return LBM_IN(kChkAdjLoad, p - base, total - 1) ? ldg2(p) : make_float2(0.f, 0.f);
+}
+
 template <int D>
-__device__ __forceinline__ float2 shifted_pair(const float* row, int lane)
+__device__ __forceinline__ float2 shifted_pair(const float* row, int lane, const float* base, long long total)
 {
     constexpr int BC = 32, BE = 19 * BC;
-    const float2 cur = ldg2(row);
+    const float2 cur = ldg2c(row, base, total);
     if (D == 0) return cur;
     if (D < 0)
     {
         float prev = __shfl_up_sync(kFull, cur.y, 1);
-        if (lane == 0) prev = ldg2(row - BE + (BC - 2)).y;
+        if (lane == 0) prev = ldg2c(row - BE + (BC - 2), base, total).y;
         return make_float2(prev, cur.x);
     }
     float next = __shfl_down_sync(kFull, cur.x, 1);
-    if (lane == 31) next = ldg2(row + BE - (BC - 2)).x;
+    if (lane == 31) next = ldg2c(row + BE - (BC - 2), base, total).x;
     return make_float2(cur.y, next);
 }
 
@@ -300,8 +307,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_adj_step(AdjStepArgs a)
     float2 rho, jx, jy, jz;
     {
         const long long mi = ((long long)(k - 1) * L.ny + (j - 1)) * L.nx + c0;
-        const float4 m0 = __ldg(a.mom_prev + mi);
-        const float4 m1 = has1 ? __ldg(a.mom_prev + mi + 1) : m0;
+        const long long ncell = (long long)L.nx * L.ny * L.nz;
+        const float4 m0 = LBM_IN(kChkAdjLoad, mi, ncell) ? __ldg(a.mom_prev + mi) : make_float4(0.f, 0.f, 0.f, 0.f);
+        const float4 m1 = has1 && LBM_IN(kChkAdjLoad, mi + 1, ncell) ? __ldg(a.mom_prev + mi + 1) : m0;
         rho = make_float2(m0.x, m1.x);
         jx = make_float2(m0.y, m1.y);
         jy = make_float2(m0.z, m1.z);
@@ -320,9 +328,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_adj_step(AdjStepArgs a)
         for (int q = 0; q < Q; ++q)
         {
             const float* row = own + (ey(q) * rs + ez(q) * ps) + q * BC;
-            if (ex(q) == 0) lg[q] = shifted_pair<0>(row, lane);
-            else if (ex(q) > 0) lg[q] = shifted_pair<1>(row, lane);
-            else lg[q] = shifted_pair<-1>(row, lane);
+            if (ex(q) == 0) lg[q] = shifted_pair<0>(row, lane, a.lam_in, L.total);
+            else if (ex(q) > 0) lg[q] = shifted_pair<1>(row, lane, a.lam_in, L.total);
+            else lg[q] = shifted_pair<-1>(row, lane, a.lam_in, L.total);
         }
         // columns outside the interior pulled nothing (and the neighbour block
         // read there may belong to another row)
@@ -351,7 +359,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_adj_step(AdjStepArgs a)
             {
                 if (((lk0 | lk1) >> inv(q)) & 1u)
                 {
-                    const float2 o = ldg2(own + inv(q) * BC);
+                    const float2 o = ldg2c(own + inv(q) * BC, a.lam_in, L.total);
                     if ((lk0 >> inv(q)) & 1u) lg[q].x += o.x;
                     if ((lk1 >> inv(q)) & 1u) lg[q].y += o.y;
                 }
@@ -444,6 +452,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_adj_step(AdjStepArgs a)
     const float2 By = fma2(vy, f2(3.0f), mul2(sub2(mul2(uy, f2(9.0f)), mul2(mul2(jy, s0), f2(3.0f))), ir));
     const float2 Bz = fma2(vz, f2(3.0f), mul2(sub2(mul2(uz, f2(9.0f)), mul2(mul2(jz, s0), f2(3.0f))), ir));
     float* out = a.lam_out + e0;
+    if (!LBM_IN(kChkAdjStore, e0 + 18 * BC + 1, L.total)) return;
     const float2 cbA = mul2(cb, A);
     *reinterpret_cast<float2*>(out) = fma2(ca, lg[0], cbA);
 #pragma unroll
@@ -554,5 +563,7 @@ cudaError_t launch_adj_probe(float* lam, const AdjProbeArgs& a, cudaStream_t str
     k_adj_probe<<<(a.n + 127) / 128, 128, 0, stream>>>(lam, a);
     return cudaGetLastError();
 }
+
+cudaError_t check_read_adjoint(check::Status* out) { return check::read_and_clear(out); }
 
 }  // namespace lbm

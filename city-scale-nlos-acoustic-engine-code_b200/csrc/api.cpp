@@ -1670,6 +1670,43 @@ extern "C" int lbm_get_transfer_bytes(lbm_handle* h, long* h2d, long* d2h)
     return LBM_OK;
 }
 
+extern "C" int lbm_check_status(lbm_handle* h, long long* site, long long* index)
+{
+    if (!h || !site || !index) return LBM_ERR_INVALID_ARGUMENT;
+#ifndef LBM_CHECK
+    return h->fail(LBM_ERR_UNSUPPORTED, "bounds checks are compiled only into liblbm_b200_check.so");
+#else
+    CK(cudaSetDevice(h->device), "cudaSetDevice");
+    if (h->stream) CK(cudaStreamSynchronize(h->stream), "check status");
+    *site = 0;
+    *index = 0;
+    check::Status st[3];
+    CK(check_read_kernels(&st[0]), "check status");
+    CK(check_read_adjoint(&st[1]), "check status");
+    CK(check_read_scheme_a(&st[2]), "check status");
+    for (const check::Status& c : st)
+        if (c.site != 0 && *site == 0)
+        {
+            *site = c.site;
+            *index = c.index;
+        }
+    return LBM_OK;
+#endif
+}
+
+extern "C" int lbm_check_selftest(lbm_handle* h)
+{
+    if (!h) return LBM_ERR_INVALID_ARGUMENT;
+#ifndef LBM_CHECK
+    return h->fail(LBM_ERR_UNSUPPORTED, "bounds checks are compiled only into liblbm_b200_check.so");
+#else
+    CK(cudaSetDevice(h->device), "cudaSetDevice");
+    CK(launch_check_selftest(h->stream), "check self-test");
+    CK(cudaStreamSynchronize(h->stream), "check self-test");
+    return LBM_OK;
+#endif
+}
+
 extern "C" int lbm_bytes_per_cell(lbm_handle* h)
 {
     if (!h) return 0;

@@ -26,6 +26,8 @@
 
 #include <cuda_runtime.h>
 
+#include "check.cuh"
+
 namespace lbm {
 
 constexpr int kMaxSources = 8;
@@ -242,6 +244,14 @@ cudaError_t launch_probe_a(const float* f, const Layout& L, const StepArgs& sa, 
                            const ProbeArgs& a, cudaStream_t stream);
 cudaError_t launch_field_rho_a(const float* f, float* out, const Layout& L, const StepArgs& sa, const SchemeAArgs& b,
                                cudaStream_t stream);
+
+// Bounds-checked builds (-DLBM_CHECK): read and clear the first failed check
+// of each kernel file (site 0: none; always 0 in the product build), and a
+// kernel that fails one check on purpose (site 99) without touching memory.
+cudaError_t check_read_kernels(check::Status* out);
+cudaError_t check_read_adjoint(check::Status* out);
+cudaError_t check_read_scheme_a(check::Status* out);
+cudaError_t launch_check_selftest(cudaStream_t stream);
 
 // Capacity (cells) of the statically reserved field array used by
 // lbm_get_rho_noalloc, and the device address of that array on `device`

@@ -10,6 +10,7 @@
 #include <mutex>
 #include <type_traits>
 
+#include "check.cuh"
 #include "device.hpp"
 #include "lattice.cuh"
 
@@ -17,6 +18,15 @@ namespace lbm {
 namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
+
+// Extents of the side arrays (elements), for the bounds-checked build.
+__device__ __forceinline__ long long links_extent(const Layout& L) { return L.plane * (L.nz + 2); }
+__device__ __forceinline__ long long near_extent(const Layout& L)
+{
+    return (long long)L.words_per_row * (L.ny + 2) * (L.nz + 2);
+}
+__device__ __forceinline__ long long xgh_extent(const Layout& L) { return 2LL * 19 * (L.nz + 2) * (L.ny + 2); }
+__device__ __forceinline__ long long xexp_extent(const Layout& L) { return 2LL * 19 * L.nz * L.ny; }
 
 // Scalar access.  ld: read-only path (arrays the kernel does not write);
 // ldw: coherent load for arrays the same kernel also writes.
@@ -130,10 +140,13 @@ __device__ __forceinline__ void pull_cell(const S* __restrict__ f, const Layout&
     for (int q = 0; q < Q; ++q)
     {
         const int si = i - ex(q);
-        if ((lk >> q) & 1u) G[q] = Io<S>::ld(f + L.elem(inv(q), i, j, k));
+        long long e = -1;
+        G[q] = 0.f;
+        if ((lk >> q) & 1u) e = L.elem(inv(q), i, j, k);
         else if (si == 0) G[q] = sa.xf.xgh[sa.xf.gh_index(0, q, j - ey(q), k - ez(q), L.ny, L.nz)];
         else if (si == L.nx + 1) G[q] = sa.xf.xgh[sa.xf.gh_index(1, q, j - ey(q), k - ez(q), L.ny, L.nz)];
-        else G[q] = Io<S>::ld(f + L.elem(q, si, j - ey(q), k - ez(q)));
+        else e = L.elem(q, si, j - ey(q), k - ez(q));
+        if (e >= 0 && LBM_IN(kChkProbe, e, L.total)) G[q] = Io<S>::ld(f + e);
     }
 }
 
@@ -263,6 +276,12 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step(const S* __restrict__ fin,
     const long long rs = L.row_stride, ps = L.plane_stride;
     if (a.prefetch_rows > 0) prefetch_rows_ahead<S, 2 * BLOCK>(fin, L, a.prefetch_rows, j, k, 2 * BLOCK * blockIdx.x);
 
+    // pair load (the bounds-checked build tests the index first)
+    const auto ldp = [&](const S* p) -> typename P::V {
+        if (LBM_IN(kChkStepLoad, p - fin, L.total - 1)) return P::ld(p);
+        return typename P::V{};
+    };
+
     uint32_t lk0 = 0, lk1 = 0;
     if (active)
     {
@@ -278,7 +297,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step(const S* __restrict__ fin,
     for (int q = 0; q < Q; ++q)
     {
         const S* row = own - (ey(q) * rs + ez(q) * ps);
-        const typename P::V cur = P::ld(row + q * BC);
+        const typename P::V cur = ldp(row + q * BC);
         if (ex(q) == 0)
         {
             G[q] = P::cvt(cur);
@@ -288,7 +307,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step(const S* __restrict__ fin,
             // lane 0 sits at the start of a block: its left neighbour pair is
             // the last pair of the previous block
             auto prev = __shfl_up_sync(kFull, P::hi_of(cur), 1);
-            if (lane == 0) prev = P::hi_of(P::ld(row + q * BC - BE + (BC - 2)));
+            if (lane == 0) prev = P::hi_of(ldp(row + q * BC - BE + (BC - 2)));
             G[q] = P::left(prev, cur);
         }
         else
@@ -296,7 +315,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step(const S* __restrict__ fin,
             // lane 31 sits at the last pair of a block: its right neighbour
             // pair is the first pair of the next block
             auto next = __shfl_down_sync(kFull, P::lo_of(cur), 1);
-            if (lane == 31) next = P::lo_of(P::ld(row + q * BC + BE - (BC - 2)));
+            if (lane == 31) next = P::lo_of(ldp(row + q * BC + BE - (BC - 2)));
             G[q] = P::right(cur, next);
         }
     }
@@ -307,7 +326,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step(const S* __restrict__ fin,
         {
             if (((lk0 | lk1) >> q) & 1u)
             {
-                const float2 o = P::cvt(P::ld(own + inv(q) * BC));
+                const float2 o = P::cvt(ldp(own + inv(q) * BC));
                 if ((lk0 >> q) & 1u) G[q].x = o.x;
                 if ((lk1 >> q) & 1u) G[q].y = o.y;
             }
@@ -344,7 +363,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step(const S* __restrict__ fin,
 
     S* out = fout + e0;
 #pragma unroll
-    for (int q = 0; q < Q; ++q) P::st(out + q * BC, G[q]);
+    for (int q = 0; q < Q; ++q)
+        if (LBM_IN(kChkStepStore, e0 + q * BC, L.total - 1)) P::st(out + q * BC, G[q]);
 
     if (xlo | xhi0 | xhi1)
     {
@@ -761,17 +781,22 @@ __global__ void __launch_bounds__(32 * WARPS, MINB) k_step_hw(const __half* __re
     };
     uint32_t n0 = 0u, n1 = 0u;   // near words of the copy cursor's block, loaded one block ahead
     const auto load_near = [&]() {
-        n0 = __ldg(ci_near);
-        n1 = ci_b * 64 + 32 < L.nx ? __ldg(ci_near + 1) : 0u;
+        n0 = LBM_IN(kChkHwNear, ci_near - a.near, near_extent(L)) ? __ldg(ci_near) : 0u;
+        n1 = ci_b * 64 + 32 < L.nx && LBM_IN(kChkHwNear, ci_near + 1 - a.near, near_extent(L)) ? __ldg(ci_near + 1)
+                                                                                                   : 0u;
     };
     const auto issue = [&](int slot) {
         const uint32_t dst = ring_s + slot * wp::kSlotBytes;
 #pragma unroll
         for (int i = 0; i < 5; ++i)
-            if (i < 4 || lane < 24) cp_async16(dst + (i * 32 + lane) * 16, ci_src + poff[i]);
+            if ((i < 4 || lane < 24) && LBM_IN(kChkHwLine, (ci_src - fin) + poff[i], L.total - 7))
+                cp_async16(dst + (i * 32 + lane) * 16, ci_src + poff[i]);
         if (lane < 2) reinterpret_cast<uint32_t*>(ring + slot * wp::kSlotBytes + wp::kNearOff)[lane] = lane ? n1 : n0;
-        if ((n0 | n1) != 0u && ci_b * 64 + 2 * lane < L.nx) cp_async8(dst + wp::kLinkOff + lane * 8, ci_link);
-        if ((ci_b == 0 && lane < 5) || (ci_b == L.nb - 1 && lane >= 5 && lane < 10))
+        if ((n0 | n1) != 0u && ci_b * 64 + 2 * lane < L.nx &&
+            LBM_IN(kChkHwLinks, ci_link - a.links, links_extent(L) - 1))
+            cp_async8(dst + wp::kLinkOff + lane * 8, ci_link);
+        if (((ci_b == 0 && lane < 5) || (ci_b == L.nb - 1 && lane >= 5 && lane < 10)) &&
+            LBM_IN(kChkHwGhost, ci_gh - a.xf.xgh, xgh_extent(L)))
             cp_async4(dst + wp::kGhostOff + lane * 4, ci_gh);
     };
 
@@ -882,7 +907,12 @@ __global__ void __launch_bounds__(32 * WARPS, MINB) k_step_hw(const __half* __re
 #pragma unroll
             for (int q = 0; q < Q; ++q)
             {
-                const unsigned o = ((lka >> q) & 1u) ? __ldg(own + inv(q) * 32) : 0u;
+                const unsigned o =
+                    ((lka >> q) & 1u) &&
+                            LBM_IN(kChkHwBounce, 2 * (own - reinterpret_cast<const unsigned*>(fin)) + inv(q) * 64,
+                                   L.total - 1)
+                        ? __ldg(own + inv(q) * 32)
+                        : 0u;
                 const unsigned m = ((0u - ((lk0 >> q) & 1u)) & 0x0000ffffu) | ((0u - ((lk1 >> q) & 1u)) & 0xffff0000u);
                 w[q] = (w[q] & ~m) | (o & m);
             }
@@ -909,12 +939,16 @@ __global__ void __launch_bounds__(32 * WARPS, MINB) k_step_hw(const __half* __re
             else
                 collide2_packed(w, inv_scale, a.omega, sg, (lk0 & kSolidSelfBit) != 0u, (lk1 & kSolidSelfBit) != 0u);
 #pragma unroll
-            for (int q = 0; q < Q; ++q) outp[32 * q] = w[q];
+            for (int q = 0; q < Q; ++q)
+                if (LBM_IN(kChkHwStore, 2 * (outp - reinterpret_cast<unsigned*>(fout)) + 64 * q, L.total - 1))
+                    outp[32 * q] = w[q];
             if (edge && (xlo | xhi))
             {
 #pragma unroll
                 for (int q = 0; q < Q; ++q)
                 {
+                    if (!LBM_IN(kChkHwExport, a.xf.exp_index(xlo ? 0 : 1, q, j, k, L.ny, L.nz), xexp_extent(L)))
+                        continue;
                     if (xlo) a.xf.xexp[a.xf.exp_index(0, q, j, k, L.ny, L.nz)] = h2f(w[q]).x;
                     if (xhi && last == 0) a.xf.xexp[a.xf.exp_index(1, q, j, k, L.ny, L.nz)] = h2f(w[q]).x;
                     if (xhi && last == 1) a.xf.xexp[a.xf.exp_index(1, q, j, k, L.ny, L.nz)] = h2f(w[q]).y;
@@ -1048,7 +1082,9 @@ __global__ void __launch_bounds__(512) k_source(S* __restrict__ f, Layout L, Ste
         const double sum = e.wsum > 0.0 ? e.wsum : bsum;   // a stencil across a z-slab cut
         if (sum < 1e-30) continue;
         const double A = e.mass / sum;
-        if (fluid)
+        // (the bounds-checked build skips a cell whose 19 directions leave the buffer; no
+        // thread leaves the loop early, every thread reaches the barrier below)
+        if (fluid && LBM_IN(kChkSource, L.elem(18, gi + 1, gj + 1, gk + 1), L.total))
         {
             const double add = A * ww * (double)a.scale;
             // the 19 directions of one cell are 19 distinct elements: every load
@@ -1153,6 +1189,9 @@ __global__ void __launch_bounds__(128) k_ghost(S* __restrict__ f, Layout L, Ghos
     {
         // x faces: compact export -> compact ghost, both coalesced along j
         const int j = 1 + u, k = 1 + v;
+        if (!LBM_IN(kChkGhost, a.xf.exp_index(F.side, 18, j, k, L.ny, L.nz), xexp_extent(L)) ||
+            !LBM_IN(kChkGhost, a.xf.gh_index(F.side, 18, j, k, L.ny, L.nz), xgh_extent(L)))
+            return;
 #pragma unroll
         for (int q = 0; q < Q; ++q) G[q] = a.xf.xexp[a.xf.exp_index(F.side, q, j, k, L.ny, L.nz)];
         if (a.face_mom) store_moments(G, a.face_mom + t);
@@ -1177,6 +1216,9 @@ __global__ void __launch_bounds__(128) k_ghost(S* __restrict__ f, Layout L, Ghos
         gk = F.side ? L.nz + 1 : 0;
     }
     constexpr int BC = block_cells(sizeof(S));
+    if (!LBM_IN(kChkGhost, L.elem(18, ci, cj, ck), L.total) || !LBM_IN(kChkGhost, L.elem(18, ci, gj, gk), L.total) ||
+        !LBM_IN(kChkGhost, L.elem(0, ci, gj, gk), L.total))
+        return;
     const S* I = f + L.elem(0, ci, cj, ck);
     S* B = f + L.elem(0, ci, gj, gk);
 #pragma unroll
@@ -1299,6 +1341,14 @@ __global__ void k_import_f(S* __restrict__ f, const double* __restrict__ in, Lay
     }
 }
 
+// Self-test of the bounds-checked build: lane 5 tests an index one past its
+// extent (nothing is accessed), which must be recorded as site kChkSelfTest.
+__global__ void k_check_selftest()
+{
+    const int lane = threadIdx.x & 31;
+    if (lane == 5 && !LBM_IN(kChkSelfTest, 32 + lane, 37)) return;
+}
+
 // Statically reserved device array for lbm_get_rho_noalloc: the field of
 // (rho - 1) passes through it instead of a temporary cudaMalloc buffer.  It
 // exists on every GPU that loads this library, for the life of the process.
@@ -1410,6 +1460,14 @@ cudaError_t field_scratch_address(int device, float** ptr)
     }
     *ptr = cached[device];
     return cudaSuccess;
+}
+
+cudaError_t check_read_kernels(check::Status* out) { return check::read_and_clear(out); }
+
+cudaError_t launch_check_selftest(cudaStream_t stream)
+{
+    k_check_selftest<<<1, 32, 0, stream>>>();
+    return cudaGetLastError();
 }
 
 cudaError_t launch_build_links(const uint8_t* mask_ref, uint32_t* links, uint32_t* near, const Layout& L,

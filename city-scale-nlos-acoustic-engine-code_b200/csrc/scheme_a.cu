@@ -7,6 +7,7 @@
 
 #include <cstdint>
 
+#include "check.cuh"
 #include "device.hpp"
 #include "lattice.cuh"
 
@@ -142,12 +143,16 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step_a(const float* __restrict_
     }
     const bool any_link = __any_sync(kFull, (lk0 | lk1) != 0u);
 
+    // pair load (the bounds-checked build tests the index first)
+    const auto ldc = [&](const float* p) {
+        return LBM_IN(kChkALoad, p - fin, L.total - 1) ? ldg2(p) : make_float2(0.f, 0.f);
+    };
     float2 G[Q];
 #pragma unroll
     for (int q = 0; q < Q; ++q)
     {
         const float* row = own - (ey(q) * rs + ez(q) * ps) + q * BC;
-        const float2 cur = ldg2(row);
+        const float2 cur = ldc(row);
         if (ex(q) == 0)
         {
             G[q] = cur;
@@ -155,13 +160,13 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step_a(const float* __restrict_
         else if (ex(q) > 0)
         {
             float prev = __shfl_up_sync(kFull, cur.y, 1);
-            if (lane == 0) prev = ldg2(row - BE + (BC - 2)).y;
+            if (lane == 0) prev = ldc(row - BE + (BC - 2)).y;
             G[q] = make_float2(prev, cur.x);
         }
         else
         {
             float next = __shfl_down_sync(kFull, cur.x, 1);
-            if (lane == 31) next = ldg2(row + BE - (BC - 2)).x;
+            if (lane == 31) next = ldc(row + BE - (BC - 2)).x;
             G[q] = make_float2(cur.y, next);
         }
     }
@@ -214,7 +219,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step_a(const float* __restrict_
                 const int si = c0 + 1 + c - ex(q), sj = j - ey(q), sk = k - ez(q);
                 const float v = c ? G[inv(q)].y : G[inv(q)].x;
                 if (si == 0 || si == L.nx + 1) b.xgh_out[a.xf.gh_index(si == 0 ? 0 : 1, q, sj, sk, L.ny, L.nz)] = v;
-                else fout[L.elem(q, si, sj, sk)] = v;
+                else if (LBM_IN(kChkAStore, L.elem(q, si, sj, sk), L.total)) fout[L.elem(q, si, sj, sk)] = v;
             }
         }
     }
@@ -275,6 +280,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step_a(const float* __restrict_
     }
 
     float* out = fout + e0;
+    if (!LBM_IN(kChkAStore, e0 + 18 * BC + 1, L.total)) return;
     if (!(solid0 | solid1))
     {
 #pragma unroll
@@ -483,5 +489,7 @@ cudaError_t launch_field_rho_a(const float* f, float* out, const Layout& L, cons
     k_field_rho_a<<<g, 128, 0, stream>>>(f, out, L, sa, b);
     return cudaGetLastError();
 }
+
+cudaError_t check_read_scheme_a(check::Status* out) { return check::read_and_clear(out); }
 
 }  // namespace lbm

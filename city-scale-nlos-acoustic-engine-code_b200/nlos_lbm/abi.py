@@ -202,6 +202,8 @@ def bind_product(lib):
         "lbm_bytes_per_cell": (ctypes.c_int, [P]),
         "lbm_get_stream": (ctypes.c_void_p, [P]),
         "lbm_get_transfer_bytes": (ctypes.c_int, [P, c_long_p, c_long_p]),
+        "lbm_check_status": (ctypes.c_int, [P, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]),
+        "lbm_check_selftest": (ctypes.c_int, [P]),
         "lbm_adjoint_grad": (ctypes.c_int, [P, ctypes.c_int, c_double_p, ctypes.c_int, ctypes.c_int, c_double_p,
                                             c_double_p, c_double_p, c_double_p]),
         "lbm_adjoint_plan": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_int, ctypes.c_int, c_int_p, c_int_p,
@@ -222,4 +224,6 @@ def bind_product(lib):
 
 
 PACKAGE_DIR = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(PACKAGE_DIR, "liblbm_b200.so")
+# NLOS_LBM_CHECK=1 loads the bounds-checked build instead of the product
+CHECKED = os.environ.get("NLOS_LBM_CHECK", "0") not in ("", "0")
+LIB_PATH = os.path.join(PACKAGE_DIR, "liblbm_b200_check.so" if CHECKED else "liblbm_b200.so")

@@ -226,6 +226,17 @@ class Solver:
         """Frees the adjoint workspace kept by the handle (lbm_adjoint_release)."""
         self._check(self.lib.lbm_adjoint_release(self.h), "lbm_adjoint_release")
 
+    def check_status(self):
+        """(site, index) of the first failed bounds check since the last call
+        (site 0: none); bounds-checked library only (NLOS_LBM_CHECK=1)."""
+        site, index = ctypes.c_longlong(), ctypes.c_longlong()
+        self._check(self.lib.lbm_check_status(self.h, ctypes.byref(site), ctypes.byref(index)), "lbm_check_status")
+        return site.value, index.value
+
+    def check_selftest(self):
+        """Fails one bounds check on purpose (bounds-checked library only)."""
+        self._check(self.lib.lbm_check_selftest(self.h), "lbm_check_selftest")
+
     def clear_sources(self):
         self._check(self.lib.lbm_clear_sources(self.h), "lbm_clear_sources")
 

@@ -355,6 +355,19 @@ void* lbm_get_stream(lbm_handle* h);
  * schedules, control blocks and uploads in; probe series and results out). */
 int lbm_get_transfer_bytes(lbm_handle* h, long* h2d, long* d2h);
 
+/* ---- bounds-checked build (liblbm_b200_check.so, compiled with -DLBM_CHECK) --
+ * (no counterpart in the reference).  In that build every device access of
+ * the step, source, ghost, probe, adjoint-step and scheme-A kernels that
+ * could leave its array is tested first; a failing test records where (a
+ * site code, csrc/check.cuh) and the offending index, and the access is
+ * skipped, so the GPU never faults.  lbm_check_status synchronises the
+ * handle's stream, returns the first recorded failure on the handle's device
+ * (site 0: none) and clears it; the product build returns
+ * LBM_ERR_UNSUPPORTED.  lbm_check_selftest launches a kernel that fails one
+ * test on purpose (site 99, no memory access), to show the mechanism works. */
+int lbm_check_status(lbm_handle* h, long long* site, long long* index);
+int lbm_check_selftest(lbm_handle* h);
+
 /* ---- synthetic geometry -------------------------------------------------- */
 
 /* Fills tris (capacity triangles, 9 floats each) with the city's boxes

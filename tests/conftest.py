@@ -16,11 +16,12 @@ def pytest_configure(config):
 
 @pytest.fixture(scope="session", autouse=True)
 def _built():
-    """The product library and the oracle are built in-tree before any test."""
+    """The product library, its bounds-checked twin and the oracle are built in-tree before any test."""
     from nlos_lbm import build as product_build
     import oracle
 
     product_build.build()
+    product_build.build(check=True)
     oracle.build(ref=False)
     yield
 

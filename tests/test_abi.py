@@ -26,6 +26,13 @@ def test_library_exports_every_declared_symbol():
     assert not missing, missing
 
 
+def test_checked_library_exports_the_same_symbols():
+    """liblbm_b200_check.so (-DLBM_CHECK) is a drop-in twin of the product library."""
+    lib = ctypes.CDLL(os.path.join(abi.PACKAGE_DIR, "liblbm_b200_check.so"))
+    missing = [n for n in declared_functions() if not hasattr(lib, n)]
+    assert not missing, missing
+
+
 def test_python_binding_covers_header():
     bound = set()
 
