@@ -36,6 +36,9 @@ METRIC = "D3Q19 GLUPS, %HBM peak: FP16-store vs FP32 @<=1e-3 probe L2; adjoint g
 # 2.644e9 B, k_step<float>: 5.132e9 B for 33.55e6 cells)
 NCU_TRAFFIC_PER_CELL = {"fp16": 2.644e9 / 33554432, "fp32": 5.132e9 / 33554432}
 UNIT = "GLUPS"
+# steps of the FP16-vs-FP32 probe comparison on the 1024x1024x256 city (the
+# Ricker sources' first periods reach the nearer street-level probes)
+ERR_STEPS = 400
 
 
 def measured_peaks():
@@ -380,6 +383,7 @@ def run_our_arm(args):
     gc.collect()
 
     secondary = {}
+    series = {}
     if world == 1 and not args.headline_only:
         for nm, st in (("city1024", 0), ("city1024", 1)):
             s2, _, r = measure(nm, st, args.steps, args.warmup, local, torch, barrier, reduce_max)
@@ -387,8 +391,16 @@ def run_our_arm(args):
                                                                     "bytes_per_cell")}
             secondary[f"{nm}_{r['storage']}"]["hbm_frac_kernel"] = (
                 r["cells"] * r["bytes_per_cell"] / (r["kernel_ms_avg"] / 1e3) / 1e9 / hbm_peak)
+            # the probe error of the metric: both storages run on to the same
+            # step, then the FP16 series is compared with the FP32 one (FP32 is
+            # within a few 1e-6 of the FP64 oracle in the parity tests)
+            s2.step(max(0, ERR_STEPS - s2.step_count))
+            series[r["storage"]] = s2.get_probes()[:ERR_STEPS]
             del s2
             gc.collect()
+        a, b = series["fp16"], series["fp32"]
+        secondary["fp16_probe_rel_l2_vs_fp32"] = float(np.linalg.norm(a - b) / np.linalg.norm(b))
+        secondary["fp16_probe_error_steps"] = ERR_STEPS
 
     family_a = {}
     if world == 1 and not args.headline_only:
@@ -445,6 +457,7 @@ def run_our_arm(args):
         line["family_a"] = family_a
     if secondary.get("city1024_fp32") and secondary.get("city1024_fp16"):
         line["fp16_over_fp32"] = secondary["city1024_fp16"]["glups_rank"] / secondary["city1024_fp32"]["glups_rank"]
+        line["fp16_probe_rel_l2"] = secondary["fp16_probe_rel_l2_vs_fp32"]
     if world == 1 and rank == 0 and not args.no_cpu:
         line["cpu_baseline"] = {k: v for k, v in cpu_baseline().items() if k in ("value", "unit", "cores", "kind",
                                                                                   "sample")}
