@@ -188,16 +188,21 @@ __global__ void __launch_bounds__(128) k_adj_ghost(AdjGhostArgs a)
     }
     // lamHt at the ghost: what the interior cells y = g + e_q pulled from it
     // (none when y bounced back, i.e. when the ghost cell is SOLID)
+    // (the links word and the adjoint value are loaded independently and
+    // combined afterwards: one memory round trip instead of two)
     float lh[Q];
+    uint32_t lk[Q];
 #pragma unroll
     for (int q = 0; q < Q; ++q)
     {
         const int di = gi + ex(q), dj = gj + ey(q), dk = gk + ez(q);
-        float v = 0.f;
-        if (interior(L, di, dj, dk) && !((a.links[L.cell(di, dj, dk)] >> q) & 1u))
-            v = a.lam_in[L.elem(q, di, dj, dk)];
-        lh[q] = v;
+        const bool in = interior(L, di, dj, dk);
+        lk[q] = in ? __ldg(a.links + L.cell(di, dj, dk)) : 1u << q;
+        lh[q] = in ? __ldg(a.lam_in + L.elem(q, di, dj, dk)) : 0.f;
     }
+#pragma unroll
+    for (int q = 0; q < Q; ++q)
+        if ((lk[q] >> q) & 1u) lh[q] = 0.f;
     // moments of the interior cell the ghost was built from
     const float4 m = __ldg(a.face_mom + t);
     const float rho = m.x, jx = m.y, jy = m.z, jz = m.w;
