@@ -19,6 +19,7 @@ namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
 
+#ifdef LBM_CHECK
 // Extents of the side arrays (elements), for the bounds-checked build.
 __device__ __forceinline__ long long links_extent(const Layout& L) { return L.plane * (L.nz + 2); }
 __device__ __forceinline__ long long near_extent(const Layout& L)
@@ -27,6 +28,7 @@ __device__ __forceinline__ long long near_extent(const Layout& L)
 }
 __device__ __forceinline__ long long xgh_extent(const Layout& L) { return 2LL * 19 * (L.nz + 2) * (L.ny + 2); }
 __device__ __forceinline__ long long xexp_extent(const Layout& L) { return 2LL * 19 * L.nz * L.ny; }
+#endif
 
 // Scalar access.  ld: read-only path (arrays the kernel does not write);
 // ldw: coherent load for arrays the same kernel also writes.
