@@ -2,6 +2,7 @@
 // See adjoint.hpp for the recursion.  Every kernel is a gather: the transposed
 // pull-stream reads the adjoint populations of the neighbours that pulled
 // from a cell, mirroring the forward pull.
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -227,6 +228,14 @@ __device__ __forceinline__ uint32_t near_bits(const StepArgs& a, const Layout& L
 
 __device__ __forceinline__ float2 ldg2(const float* p) { return __ldg(reinterpret_cast<const float2*>(p)); }
 
+// (rho', jx, jy, jz) from the two FP16 pairs of PackedMoments
+__device__ __forceinline__ float4 unpack_moments(uint2 u)
+{
+    const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&u.x));
+    const float2 b = __half22float2(*reinterpret_cast<const __half2*>(&u.y));
+    return make_float4(a.x, a.y, b.x, b.y);
+}
+
 // packed FP32x2 arithmetic (sm_100): both cells of a pair in one instruction
 __device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
 __device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
@@ -312,9 +321,11 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_adj_step(AdjStepArgs a)
     float2 rho, jx, jy, jz;
     {
         const long long mi = ((long long)(k - 1) * L.ny + (j - 1)) * L.nx + c0;
-        const long long ncell = (long long)L.nx * L.ny * L.nz;
-        const float4 m0 = LBM_IN(kChkAdjLoad, mi, ncell) ? __ldg(a.mom_prev + mi) : make_float4(0.f, 0.f, 0.f, 0.f);
-        const float4 m1 = has1 && LBM_IN(kChkAdjLoad, mi + 1, ncell) ? __ldg(a.mom_prev + mi + 1) : m0;
+        [[maybe_unused]] const long long ncell = (long long)L.nx * L.ny * L.nz;
+        const uint2* mp = reinterpret_cast<const uint2*>(a.mom_prev);
+        const uint2 p0 = LBM_IN(kChkAdjLoad, mi, ncell) ? __ldg(mp + mi) : make_uint2(0u, 0u);
+        const uint2 p1 = has1 && LBM_IN(kChkAdjLoad, mi + 1, ncell) ? __ldg(mp + mi + 1) : p0;
+        const float4 m0 = unpack_moments(p0), m1 = unpack_moments(p1);
         rho = make_float2(m0.x, m1.x);
         jx = make_float2(m0.y, m1.y);
         jy = make_float2(m0.z, m1.z);

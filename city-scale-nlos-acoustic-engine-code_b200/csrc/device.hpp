@@ -216,10 +216,16 @@ cudaError_t launch_step(int storage, const void* fin, void* fout, const Layout& 
 cudaError_t prepare_step(int storage, int variant);
 // Fused step (FP32 storage, the default implementation) that also writes the
 // moments (rho', jx, jy, jz) of every cell's pulled populations to `mom`,
-// dense cell order ((k-1) ny + (j-1)) nx + (i-1): the forward data of the
-// adjoint's BGK Jacobian.
-cudaError_t launch_step_moments(const float* fin, float* fout, const Layout& L, const StepArgs& a, float4* mom,
-                                cudaStream_t stream);
+// dense cell order ((k-1) ny + (j-1)) nx + (i-1), as two FP16 pairs per cell
+// ((rho', jx), (jy, jz); PackedMoments): the forward data of the adjoint's
+// BGK Jacobian, where they enter only through terms of the wave's amplitude
+// (J^2, J / r), so half precision moves the gradient by ~1e-7 relative.
+struct PackedMoments
+{
+    unsigned rho_jx, jy_jz;   // __half2 bit patterns
+};
+cudaError_t launch_step_moments(const float* fin, float* fout, const Layout& L, const StepArgs& a,
+                                PackedMoments* mom, cudaStream_t stream);
 cudaError_t launch_probe(int storage, const void* f, const Layout& L, const StepArgs& sa, const ProbeArgs& a,
                          cudaStream_t stream);
 // (float)(rho - 1) of every interior cell, pulled from the pre-step buffer `f`.

@@ -260,9 +260,16 @@ __device__ __forceinline__ void collide2(float2 (&G)[Q], float inv_scale, float 
 // MOM: also write the moments (rho', J) of every cell's pulled populations to
 // `mom` (dense cell order, float4 per cell), the forward data the adjoint's
 // BGK Jacobian needs.
+__device__ __forceinline__ PackedMoments pack_moments(float4 m)
+{
+    const __half2 a = __floats2half2_rn(m.x, m.y), b = __floats2half2_rn(m.z, m.w);
+    return PackedMoments{*reinterpret_cast<const unsigned*>(&a), *reinterpret_cast<const unsigned*>(&b)};
+}
+
 template <typename S, int BLOCK, int MINB, bool MOM = false>
 __global__ void __launch_bounds__(BLOCK, MINB) k_step(const S* __restrict__ fin, S* __restrict__ fout, Layout L,
-                                                      StepArgs a, float inv_scale, float4* __restrict__ mom = nullptr)
+                                                      StepArgs a, float inv_scale,
+                                                      PackedMoments* __restrict__ mom = nullptr)
 {
     using P = PairIo<S>;
     constexpr int BC = block_cells(sizeof(S));   // cells per interleaved block
@@ -359,8 +366,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step(const S* __restrict__ fin,
     if constexpr (MOM)
     {
         const long long mi = ((long long)(k - 1) * L.ny + (j - 1)) * L.nx + c0;
-        mom[mi] = m0;
-        if (c0 + 1 < L.nx) mom[mi + 1] = m1;
+        mom[mi] = pack_moments(m0);
+        if (c0 + 1 < L.nx) mom[mi + 1] = pack_moments(m1);
     }
 
     S* out = fout + e0;
@@ -1502,8 +1509,8 @@ cudaError_t launch_step(int storage, const void* fin, void* fout, const Layout& 
     return launch_step_t<__half>((const __half*)fin, (__half*)fout, L, a, 1.0f / scale, variant, stream);
 }
 
-cudaError_t launch_step_moments(const float* fin, float* fout, const Layout& L, const StepArgs& a, float4* mom,
-                                cudaStream_t stream)
+cudaError_t launch_step_moments(const float* fin, float* fout, const Layout& L, const StepArgs& a,
+                                PackedMoments* mom, cudaStream_t stream)
 {
     k_step<float, 128, 0, true><<<pair_grid(L, 128), 128, 0, stream>>>(fin, fout, L, a, 1.0f, mom);
     return cudaGetLastError();
