@@ -257,7 +257,7 @@ int validate(const lbm_config& c, std::string& why)
     if (!(c.x_max > c.x_min && c.y_max > c.y_min && c.z_max > c.z_min))
         return why = "empty domain", LBM_ERR_BAD_CONFIG;
     for (int f = 0; f < 6; ++f)
-        if (c.face_bc[f] < LBM_BC_NSCBC || c.face_bc[f] > LBM_BC_COPY)
+        if (c.face_bc[f] < LBM_BC_NSCBC || c.face_bc[f] > LBM_BC_PERIODIC)
             return why = "face_bc out of range", LBM_ERR_BAD_CONFIG;
     if (c.scheme != LBM_SCHEME_B && c.scheme != LBM_SCHEME_A) return why = "unknown scheme", LBM_ERR_BAD_CONFIG;
     if (!(c.dt >= 0)) return why = "dt must be >= 0 (0: cs*dx/c_phys)", LBM_ERR_BAD_CONFIG;
@@ -268,6 +268,15 @@ int validate(const lbm_config& c, std::string& why)
         nnscbc += c.face_bc[f] == LBM_BC_NSCBC;
     }
     if (c.scheme == LBM_SCHEME_B && ncopy) return why = "LBM_BC_COPY needs scheme A", LBM_ERR_BAD_CONFIG;
+    int nper = 0;
+    for (int f = 0; f < 6; ++f) nper += c.face_bc[f] == LBM_BC_PERIODIC;
+    if (nper && (c.scheme != LBM_SCHEME_A || nper != 2 || c.face_bc[LBM_FACE_ZLO] != LBM_BC_PERIODIC ||
+                 c.face_bc[LBM_FACE_ZHI] != LBM_BC_PERIODIC))
+        return why = "LBM_BC_PERIODIC is scheme A on both z faces", LBM_ERR_BAD_CONFIG;
+    if (c.sponge_blend != 0 && c.sponge_blend != 1) return why = "sponge_blend must be 0 or 1", LBM_ERR_BAD_CONFIG;
+    if (c.sponge_blend && c.scheme != LBM_SCHEME_A) return why = "sponge_blend needs scheme A", LBM_ERR_BAD_CONFIG;
+    if (c.sponge_blend && c.tau_sponge_max > 0)
+        return why = "sponge_blend replaces the tau ramp (tau_sponge_max <= 0)", LBM_ERR_BAD_CONFIG;
     if (c.slab_k0 < 0 || c.slab_nz < 0) return why = "slab_k0 and slab_nz must be >= 0", LBM_ERR_BAD_CONFIG;
     if (c.slab_nz > 0)
     {
@@ -317,6 +326,16 @@ void sponge_axis(const lbm_config& c, int axis, int n, std::vector<float>& out)
         }
         out[(size_t)i - 1] = s > 1e-12 ? (float)s : 0.0f;
     }
+}
+
+// Periodic z (01:105-107): halo planes 0 and nz + 1 repeat planes nz and 1,
+// for a built mask and for a caller's (lbm_set_mask).
+void periodic_z_mask(const lbm_config& c, int nx, int ny, int nz, uint8_t* m)
+{
+    if (c.face_bc[LBM_FACE_ZLO] != LBM_BC_PERIODIC) return;
+    const size_t plane = (size_t)(nx + 2) * (ny + 2);
+    std::copy(m + (size_t)nz * plane, m + (size_t)(nz + 1) * plane, m);
+    std::copy(m + plane, m + 2 * plane, m + (size_t)(nz + 1) * plane);
 }
 
 // The voxelised mask of init_domain (06:460-531) in the reference's
@@ -379,6 +398,7 @@ void build_mask(const lbm_config& c, const HeightField& geo, int nx, int ny, int
             if (c.face_bc[LBM_FACE_ZHI] != kBcCut)
                 m[(size_t)i + (size_t)j * nxt + (size_t)(nz + 1) * nxt * nyt] = wall(LBM_FACE_ZHI);
         }
+    periodic_z_mask(c, nx, ny, nz, m);
 }
 
 void grid_size(const lbm_config& c, int& nx, int& ny, int& nz)
@@ -420,7 +440,7 @@ int upload_scheme_a_profiles(lbm_handle* h)
     const unsigned sf = c.sponge_faces;
     const int w = (int)c.sponge_width;
     std::vector<float> prof;
-    prof.reserve((size_t)2 * (L.nx + L.ny + L.nz) + 6);
+    prof.reserve((size_t)3 * (L.nx + L.ny + L.nz) + 6);
     for (int a = 0; a < 3; ++a)
         for (int g = 0; g < n[a]; ++g)
         {
@@ -457,6 +477,30 @@ int upload_scheme_a_profiles(lbm_handle* h)
             }
             prof.push_back((float)v);
         }
+    // 01's blend strength per axis (01:207-225): depth th - dist into the
+    // layer of thickness th = sponge_width dx, strength (depth / th)^2; the
+    // cell's value (01's largest depth over the axes) is the largest of the
+    // three, and values <= 1e-6 are 01's "not in the sponge" (01:302).
+    const double hi[3] = {c.x_max, c.y_max, c.z_max};
+    const double th = c.sponge_width * c.dx;
+    for (int a = 0; a < 3; ++a)
+        for (int g = 0; g < n[a]; ++g)
+        {
+            double sgv = 0.0;
+            if (c.sponge_blend)
+            {
+                const double x = lo[a] + (g + 0.5) * c.dx;
+                double dist = 0.0;
+                if ((sf & (1u << (2 * a))) && x < lo[a] + th) dist = (lo[a] + th) - x;
+                else if ((sf & (1u << (2 * a + 1))) && x > hi[a] - th) dist = x - (hi[a] - th);
+                if (dist > 0.0)
+                {
+                    const double r = dist / th;
+                    sgv = c.sponge_strength * r * r;
+                }
+            }
+            prof.push_back(sgv > 1e-6 ? (float)sgv : 0.0f);
+        }
     if (!h->a_prof) CK(cudaMalloc(&h->a_prof, prof.size() * sizeof(float)), "scheme A profiles");
     CK(cudaMemcpyAsync(h->a_prof, prof.data(), prof.size() * sizeof(float), cudaMemcpyHostToDevice, h->stream),
        "scheme A profiles");
@@ -469,6 +513,11 @@ int upload_scheme_a_profiles(lbm_handle* h)
     b.fld_x = b.om_z + L.nz;
     b.fld_y = b.fld_x + L.nx + 2;
     b.fld_z = b.fld_y + L.ny + 2;
+    b.sg_x = b.fld_z + L.nz + 2;
+    b.sg_y = b.sg_x + L.nx;
+    b.sg_z = b.sg_y + L.ny;
+    b.blend = c.sponge_blend ? 1 : 0;
+    b.zper = c.face_bc[LBM_FACE_ZLO] == LBM_BC_PERIODIC ? 1 : 0;
     b.om_bulk = (float)(1.0 / c.tau);
     b.field_mode = fs ? fs->field_mode : -1;
     b.src_index = fsi;
@@ -748,6 +797,7 @@ extern "C" int lbm_init(lbm_handle* h)
         if (h->mo_dims[0] != nxt || h->mo_dims[1] != nyt || h->mo_dims[2] != nzt)
             return h->fail(LBM_ERR_INVALID_ARGUMENT, "lbm_set_mask dimensions do not match the grid");
         h->mask = h->mask_override;
+        periodic_z_mask(c, nx, ny, nz, h->mask.data());
     }
     else
     {
@@ -837,6 +887,13 @@ extern "C" int lbm_init(lbm_handle* h)
             e = launch_init_a((float*)h->f[0], (float*)h->f[1], h->xgh_par[0], h->xgh_par[1], d_mask, L, h->aa,
                               h->stream);
             h->launches += 1;
+            if (e == cudaSuccess && h->aa.zper)
+            {
+                StepArgs sa = h->sa;
+                sa.links = h->links;
+                for (int p = 0; p < 2 && e == cudaSuccess; ++p) e = launch_zper_a((float*)h->f[p], L, sa, h->stream);
+                h->launches += 2;
+            }
         }
         cudaError_t e2 = cudaStreamSynchronize(h->stream);
         cudaFree(d_mask);
@@ -1625,6 +1682,37 @@ extern "C" int lbm_set_f(lbm_handle* h, const double* in, long count)
     if (e != cudaSuccess) return h->cuda_fail(e, "set_f");
     h->launches++;
     h->halo_dirty = true;
+    return LBM_OK;
+}
+
+extern "C" int lbm_set_density(lbm_handle* h, const double* rho_minus_1, long count)
+{
+    int st = check_ready(h);
+    if (st) return st;
+    const Layout& L = h->L;
+    const size_t n = (size_t)L.nx * L.ny * L.nz;
+    if (!h->scheme_a()) return h->fail(LBM_ERR_UNSUPPORTED, "lbm_set_density sets the scheme-A state");
+    if (h->step != 0) return h->fail(LBM_ERR_STATE, "lbm_set_density before the first step");
+    if (!rho_minus_1 || count != (long)n) return h->fail(LBM_ERR_INVALID_ARGUMENT, "density size mismatch");
+    std::vector<float> rp(n);
+    for (size_t i = 0; i < n; ++i) rp[i] = (float)rho_minus_1[i];
+    CK(cudaSetDevice(h->device), "cudaSetDevice");
+    float* d_rp = nullptr;
+    uint8_t* d_mask = nullptr;
+    cudaError_t e = cudaMalloc(&d_rp, n * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&d_mask, h->mask.size());
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_rp, rp.data(), n * sizeof(float), cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d_mask, h->mask.data(), h->mask.size(), cudaMemcpyHostToDevice, h->stream);
+    h->h2d_bytes += (long)(n * sizeof(float) + h->mask.size());
+    if (e == cudaSuccess)
+        e = launch_set_density_a((float*)h->f[h->cur], h->xgh_par[h->cur], d_rp, d_mask, L, h->aa, h->stream);
+    if (e == cudaSuccess && h->aa.zper) e = launch_zper_a((float*)h->f[h->cur], L, h->sa, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    cudaFree(d_rp);
+    cudaFree(d_mask);
+    if (e != cudaSuccess) return h->cuda_fail(e, "set_density");
+    h->launches += h->aa.zper ? 2 : 1;
     return LBM_OK;
 }
 

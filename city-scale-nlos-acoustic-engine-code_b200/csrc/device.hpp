@@ -191,6 +191,11 @@ struct SchemeAArgs
     float mass_direct[2];      // mass of step s and of step s + 1 (direct launches)
     float* xgh_out;            // x-halo values written for the next step
     int copy;                  // zero-gradient halos on every face
+    const float* sg_x;         // destination blend toward rest (01:207-225, 01:343-347): strength per
+    const float* sg_y;         //   interior column i-1, likewise sg_y, sg_z; a cell's is the maximum
+    const float* sg_z;         //   of the three, 0 outside the layer
+    int blend;                 // 1: populations that left a fluid cell are blended, (1-s) f + s w_q
+    int zper;                  // 1: periodic z, halo planes 0 / nz+1 repeat planes nz / 1
 };
 
 // ---- launchers (kernels.cu) ----------------------------------------------
@@ -250,6 +255,15 @@ cudaError_t launch_probe_a(const float* f, const Layout& L, const StepArgs& sa, 
                            const ProbeArgs& a, cudaStream_t stream);
 cudaError_t launch_field_rho_a(const float* f, float* out, const Layout& L, const StepArgs& sa, const SchemeAArgs& b,
                                cudaStream_t stream);
+// Periodic z: copy the stored values of the FLUID cells of planes nz and 1
+// into halo planes 0 and nz + 1 (a SOLID cell's slots are its mailbox), for
+// the initial state; the step kernel stores those planes twice itself.
+cudaError_t launch_zper_a(float* f, const Layout& L, const StepArgs& sa, cudaStream_t stream);
+// Initial state at rest with density 1 + rho_prime (interior cells, x
+// fastest) over the state lbm_init left: FLUID interior cells and the slots
+// of SOLID cells next to them.  mask_ref: the halo-inclusive mask.
+cudaError_t launch_set_density_a(float* f, float* xgh, const float* rho_prime, const uint8_t* mask_ref,
+                                 const Layout& L, const SchemeAArgs& b, cudaStream_t stream);
 
 // Bounds-checked builds (-DLBM_CHECK): read and clear the first failed check
 // of each kernel file (site 0: none; always 0 in the product build), and a

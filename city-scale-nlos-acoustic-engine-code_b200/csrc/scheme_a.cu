@@ -48,6 +48,12 @@ __device__ __forceinline__ float field_weight(const SchemeAArgs& b, int i, int j
     return b.fld_x[i] * b.fld_y[j] * b.fld_z[k];
 }
 
+// strength of the destination blend at interior cell (i, j, k) (01:207-225)
+__device__ __forceinline__ float cell_blend(const SchemeAArgs& b, int i, int j, int k)
+{
+    return fmaxf(b.sg_x[i - 1], fmaxf(b.sg_y[j - 1], b.sg_z[k - 1]));
+}
+
 // BGK of one cell on deviations d = f - feq(1, u0): with rho' = sum d,
 // J' = sum c d (so rho = 1 + rho', J = u0 + J'), the equilibrium deviation is
 //   w_q (rho' + 3 c.J' + (4.5 E_q - 1.5 E) / rho),
@@ -114,6 +120,14 @@ __device__ __forceinline__ void pull_a(const float* __restrict__ f, const Layout
 #pragma unroll
         for (int q = 0; q < Q; ++q)
             if (!((lk >> q) & 1u)) G[q] += wf(q) * S;
+    }
+    // (1 - s) f + s w_q on deviations from feq(1, u0): (1 - s) d - s base_q (01:343-347)
+    if (b.blend)
+    {
+        const float sg = cell_blend(b, i, j, k), keep = 1.0f - sg;
+#pragma unroll
+        for (int q = 0; q < Q; ++q)
+            if (!((lk >> q) & 1u)) G[q] = fmaf(keep, G[q], -sg * b.base[q]);
     }
 }
 
@@ -202,6 +216,19 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step_a(const float* __restrict_
             if (!((lk1 >> q) & 1u)) G[q].y += add.y;
         }
     }
+    // destination blend toward rest, same populations (01:343-347)
+    if (b.blend)
+    {
+        const float2 sg = make_float2(cell_blend(b, c0 + 1, j, k), has1 ? cell_blend(b, c0 + 2, j, k) : 0.f);
+        const float2 keep = sub2(f2(1.0f), sg);
+#pragma unroll
+        for (int q = 0; q < Q; ++q)
+        {
+            const float2 v = fma2(keep, G[q], mul2(sg, f2(-b.base[q])));
+            if (!((lk0 >> q) & 1u)) G[q].x = v.x;
+            if (!((lk1 >> q) & 1u)) G[q].y = v.y;
+        }
+    }
     // pre-collision values for the SOLID neighbours' slots: the next step
     // pulls direction q from the SOLID cell dst - e_q and must read this
     // cell's own value of direction inv(q) (02:391-394)
@@ -279,22 +306,32 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step_a(const float* __restrict_
         }
     }
 
-    float* out = fout + e0;
-    if (!LBM_IN(kChkAStore, e0 + 18 * BC + 1, L.total)) return;
-    if (!(solid0 | solid1))
-    {
-#pragma unroll
-        for (int q = 0; q < Q; ++q) *reinterpret_cast<float2*>(out + q * BC) = G[q];
-    }
-    else
-    {
-        // a SOLID cell's slots hold what its neighbours wrote for the next step
-#pragma unroll
-        for (int q = 0; q < Q; ++q)
+    const auto store = [&](long long ep) {
+        float* out = fout + ep;
+        if (!LBM_IN(kChkAStore, ep + 18 * BC + 1, L.total)) return;
+        if (!(solid0 | solid1))
         {
-            if (!solid0) out[q * BC] = G[q].x;
-            if (!solid1) out[q * BC + 1] = G[q].y;
+#pragma unroll
+            for (int q = 0; q < Q; ++q) *reinterpret_cast<float2*>(out + q * BC) = G[q];
         }
+        else
+        {
+            // a SOLID cell's slots hold what its neighbours wrote for the next step
+#pragma unroll
+            for (int q = 0; q < Q; ++q)
+            {
+                if (!solid0) out[q * BC] = G[q].x;
+                if (!solid1) out[q * BC + 1] = G[q].y;
+            }
+        }
+    };
+    store(e0);
+    // periodic z (01:286-299): planes nz and 1 are also the next step's halo
+    // planes 0 and nz + 1, stored twice here instead of copied afterwards
+    if (b.zper)
+    {
+        if (k == L.nz) store(e0 - (long long)L.nz * ps);
+        if (k == 1) store(e0 + (long long)L.nz * ps);
     }
 }
 
@@ -400,6 +437,78 @@ __global__ void __launch_bounds__(128) k_init_a(float* __restrict__ f0, float* _
     }
 }
 
+// ---------------------------------------------------------------- periodic z
+// 01 exchanges whole z planes with itself at one rank (01:286-299) after the
+// x and y halos are set, so halo plane 0 holds plane nz and halo plane nz + 1
+// plane 1, at every (i, j).  The stored values are post-collision and a
+// halo cell collides like the cell it repeats, so copying the stored values
+// of the FLUID interior columns is the exchange; the x- and y-halo cells of
+// those planes are rest (REST or WALL faces) and stay as lbm_init left them.
+// SOLID cells are not copied: their slots are the mailboxes that the
+// interior cells next to them write.  One thread per column and side.
+__global__ void __launch_bounds__(128) k_zper_a(float* __restrict__ f, Layout L, StepArgs sa)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long ncol = (long long)L.nx * L.ny;
+    if (t >= 2 * ncol) return;
+    const int side = t >= ncol;
+    const long long r = side ? t - ncol : t;
+    const int i = 1 + (int)(r % L.nx), j = 1 + (int)(r / L.nx);
+    const int ks = side ? 1 : L.nz, kd = side ? L.nz + 1 : 0;
+    if (sa.links[L.cell(i, j, ks)] & kSolidSelfBit) return;   // the halo cell is SOLID too
+    const long long es = L.elem(0, i, j, ks), ed = L.elem(0, i, j, kd);
+    if (!LBM_IN(kChkAStore, ed + 18 * BC, L.total) || !LBM_IN(kChkALoad, es + 18 * BC, L.total)) return;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) f[ed + q * BC] = f[es + q * BC];
+}
+
+// ---------------------------------------------------------------- initial density
+// 01's pulse (01:187-205): every FLUID cell starts at f = feq(1 + rho', u0)
+// = (1 + rho') (w_q + base_q), an equilibrium, which the collision keeps, so
+// the stored post-collision deviation is rho' (w_q + base_q).  A SOLID
+// cell's slot q holds the value its neighbour D = cell + e_q bounces back in
+// the first step, f(D) of direction inv(q): base_inv(q) - base_q +
+// rho'(D) (w_q + base_inv(q)) for FLUID interior D (w_inv(q) = w_q).  Other
+// cells keep the state lbm_init wrote.  One thread per halo-inclusive cell.
+__global__ void __launch_bounds__(128) k_set_density_a(float* __restrict__ f, float* __restrict__ xgh,
+                                                       const float* __restrict__ rp, const uint8_t* __restrict__ m,
+                                                       Layout L, SchemeAArgs b)
+{
+    const int i0 = blockIdx.x * blockDim.x + threadIdx.x;   // 0..nx+1
+    const int j = blockIdx.y, k = blockIdx.z;               // halo-inclusive
+    if (i0 > L.nx + 1) return;
+    const long long nxt = L.nx + 2, nyt = L.ny + 2;
+    const auto mref = [&](int ii, int jj, int kk) { return m[(long long)ii + jj * nxt + kk * nxt * nyt]; };
+    const auto rho_at = [&](int ii, int jj, int kk) {
+        return rp[((long long)(kk - 1) * L.ny + (jj - 1)) * L.nx + (ii - 1)];
+    };
+    const auto interior = [&](int ii, int jj, int kk) {
+        return ii >= 1 && ii <= L.nx && jj >= 1 && jj <= L.ny && kk >= 1 && kk <= L.nz;
+    };
+    const bool solid = mref(i0, j, k) != 0;
+    if (!solid)
+    {
+        if (!interior(i0, j, k)) return;
+        const float r = rho_at(i0, j, k);
+#pragma unroll
+        for (int q = 0; q < Q; ++q)
+        {
+            const long long e = L.elem(q, i0, j, k);
+            if (LBM_IN(kChkAStore, e, L.total)) f[e] = r * (wf(q) + b.base[q]);
+        }
+        return;
+    }
+#pragma unroll
+    for (int q = 0; q < Q; ++q)
+    {
+        const int di = i0 + ex(q), dj = j + ey(q), dk = k + ez(q);
+        if (!interior(di, dj, dk) || mref(di, dj, dk) != 0) continue;
+        const float v = b.base[inv(q)] - b.base[q] + rho_at(di, dj, dk) * (wf(q) + b.base[inv(q)]);
+        if (i0 == 0 || i0 == L.nx + 1) xgh[XFace{nullptr, nullptr}.gh_index(i0 == 0 ? 0 : 1, q, j, k, L.ny, L.nz)] = v;
+        else if (LBM_IN(kChkAStore, L.elem(q, i0, j, k), L.total)) f[L.elem(q, i0, j, k)] = v;
+    }
+}
+
 // ---------------------------------------------------------------- probes, field
 // rho - 1 after the step that reads f (the reference records rho of the
 // arriving populations, 02:411, 03:438); SOLID cells read 0.
@@ -487,6 +596,21 @@ cudaError_t launch_field_rho_a(const float* f, float* out, const Layout& L, cons
 {
     const dim3 g((unsigned)((L.nx + 127) / 128), (unsigned)L.ny, (unsigned)L.nz);
     k_field_rho_a<<<g, 128, 0, stream>>>(f, out, L, sa, b);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_zper_a(float* f, const Layout& L, const StepArgs& sa, cudaStream_t stream)
+{
+    const long long n = 2LL * L.nx * L.ny;
+    k_zper_a<<<(unsigned)((n + 127) / 128), 128, 0, stream>>>(f, L, sa);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_set_density_a(float* f, float* xgh, const float* rho_prime, const uint8_t* mask_ref,
+                                 const Layout& L, const SchemeAArgs& b, cudaStream_t stream)
+{
+    const dim3 g((unsigned)((L.nx + 2 + 127) / 128), (unsigned)(L.ny + 2), (unsigned)(L.nz + 2));
+    k_set_density_a<<<g, 128, 0, stream>>>(f, xgh, rho_prime, mask_ref, L, b);
     return cudaGetLastError();
 }
 

@@ -28,7 +28,7 @@ LBM_ERR_IO = -9
 LBM_ERR_UNSUPPORTED = -10
 LBM_NOALLOC_MAX_CELLS = 8388608
 
-LBM_BC_NSCBC, LBM_BC_REST, LBM_BC_WALL, LBM_BC_COPY = 0, 1, 2, 3
+LBM_BC_NSCBC, LBM_BC_REST, LBM_BC_WALL, LBM_BC_COPY, LBM_BC_PERIODIC = 0, 1, 2, 3, 4
 LBM_SCHEME_B, LBM_SCHEME_A = 0, 1
 LBM_FIELD_DST, LBM_FIELD_FORCE = 0, 1
 FACE_XLO, FACE_XHI, FACE_YLO, FACE_YHI, FACE_ZLO, FACE_ZHI = range(6)
@@ -70,6 +70,7 @@ class LbmConfig(ctypes.Structure):
         ("dt", ctypes.c_double),
         ("slab_k0", ctypes.c_int),
         ("slab_nz", ctypes.c_int),
+        ("sponge_blend", ctypes.c_int),
     ]
 
 
@@ -195,6 +196,7 @@ def bind_product(lib):
         "lbm_get_rho_noalloc": (ctypes.c_int, [P, c_float_p, ctypes.c_long]),
         "lbm_get_f": (ctypes.c_int, [P, c_double_p, ctypes.c_long]),
         "lbm_set_f": (ctypes.c_int, [P, c_double_p, ctypes.c_long]),
+        "lbm_set_density": (ctypes.c_int, [P, c_double_p, ctypes.c_long]),
         "lbm_get_mask": (ctypes.c_int, [P, c_uint8_p, ctypes.c_long]),
         "lbm_set_kernel_timing": (ctypes.c_int, [P, ctypes.c_int]),
         "lbm_get_kernel_time": (ctypes.c_int, [P, c_double_p, c_long_p]),

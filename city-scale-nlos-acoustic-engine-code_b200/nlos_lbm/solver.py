@@ -157,6 +157,12 @@ class Solver:
         f = np.ascontiguousarray(f, dtype=np.float64)
         self._check(self.lib.lbm_set_f(self.h, _ptr(f), f.size), "lbm_set_f")
 
+    def set_density(self, rho_prime):
+        """Scheme A: start at rest with density 1 + rho' at every interior
+        fluid cell (nx*ny*nz values, x fastest), before the first step."""
+        r = np.ascontiguousarray(rho_prime, dtype=np.float64).ravel()
+        self._check(self.lib.lbm_set_density(self.h, _ptr(r), r.size), "lbm_set_density")
+
     def get_rho(self):
         nx, ny, nz = self.dims
         out = np.empty(nx * ny * nz, dtype=np.float32)

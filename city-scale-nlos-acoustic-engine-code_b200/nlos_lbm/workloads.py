@@ -24,6 +24,10 @@ reference's heightmap ray cast.
   doppler_a  03_doppler_effect.cpp at its own size (scheme A): 400x400x600 at
              dx 0.25, Mach 0.2 flow along z, zero-gradient halos, tau ramp
              0.51 -> 0.9 over 20 cells, 762 steps (to T = 110 s)
+  scattering_a  01_acoustic_scattering.cpp at its own size (scheme A):
+             320x320x8 at dx 0.05, cylinder of radius 0.5, initial pulse,
+             destination blend sponge 0.5 deep, periodic z, 402 steps (to
+             T = 11 s plus 01's 20 extra steps)
 """
 import numpy as np
 
@@ -177,6 +181,31 @@ def build(name, storage=None, seed=2024):
         probes = np.stack([np.full(64, ctr[0]), np.full(64, ctr[1]), np.linspace(1.0, n[2] * dx - 1.0, 64)], 1)
         return dict(cfg=cfg, sources=[src], probes=probes, triangles=None, mask=None, steps=762,
                     description="Doppler (03) 400x400x600, scheme A, Mach 0.2 flow, zero-gradient halos")
+    if name == "scattering_a":
+        # 01:54-56 domain, 01:65 dx, 01:67 pulse amplitude, 01:157-225 set-up, 01:486-488 steps
+        dx, lo, hi = 0.05, -8.0, 8.0
+        n = int((hi - lo) / dx + 0.5)
+        nz = max(int(0.4 / dx + 0.5), 3)
+        faces = (1 << abi.FACE_XLO) | (1 << abi.FACE_XHI) | (1 << abi.FACE_YLO) | (1 << abi.FACE_YHI)
+        cfg = lattice_config(n, n, nz, 0.505, x_min=lo, x_max=hi, y_min=lo, y_max=hi, z_min=-0.2, z_max=0.2, dx=dx,
+                             c_phys=1.0, face_bc=(abi.LBM_BC_REST,) * 4 + (abi.LBM_BC_PERIODIC,) * 2,
+                             sponge_faces=faces, sponge_width=0.5 / dx, sponge_strength=1.0, sponge_blend=1,
+                             scheme=abi.LBM_SCHEME_A, dt=np.sqrt(1.0 / 3.0) * dx)
+        c = lo + (np.arange(-1, n + 1) + 0.5) * dx
+        solid = (c[None, :] ** 2 + c[:, None] ** 2) < 0.25
+        mask = np.broadcast_to(solid, (nz + 2,) + solid.shape).astype(np.uint8)
+        pulse = 0.01 * np.exp(-np.log(2.0) * ((c[None, :] - 4.0) ** 2 + c[:, None] ** 2))
+        pulse[solid] = 0.0
+        rho0 = np.broadcast_to(pulse[1:-1, 1:-1], (nz, n, n))
+        cell = lambda v: lo + (np.floor((v - lo) / dx) + 0.5) * dx
+        r135 = np.deg2rad(135.0)
+        probes = np.array([(cell(x), cell(y), -0.2 + (nz // 2 + 0.5) * dx)
+                           for x, y in ((0.0, 1.0), (np.cos(r135), np.sin(r135)), (-1.0, 0.0))])
+        max_steps = int(11.0 / (np.sqrt(1.0 / 3.0) * dx)) + 20
+        return dict(cfg=cfg, sources=[], probes=probes, triangles=None, mask=np.ascontiguousarray(mask).ravel(),
+                    rho0=np.ascontiguousarray(rho0).ravel(), steps=max_steps + 1,
+                    description=f"acoustic scattering (01) {n}x{n}x{nz}, scheme A, cylinder, blend sponge, "
+                                "periodic z")
     raise KeyError(name)
 
 

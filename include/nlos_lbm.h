@@ -54,9 +54,12 @@ enum
     LBM_BC_NSCBC = 0,  /* characteristic open boundary, zero incoming wave (06:684-835) */
     LBM_BC_REST = 1,   /* halo held at rest equilibrium w_q (06:677-682 with use_nscbc=false) */
     LBM_BC_WALL = 2,   /* SOLID halo: halfway bounce-back (ground plane, 06:520-531) */
-    LBM_BC_COPY = 3    /* zero-gradient halo, a copy of the nearest interior cell that then
+    LBM_BC_COPY = 3,   /* zero-gradient halo, a copy of the nearest interior cell that then
                           collides like any cell (fill_halo_copy 03:175-237); scheme A only,
                           and then on all six faces */
+    LBM_BC_PERIODIC = 4 /* periodic: the halo plane is the opposite interior plane (01:105-107,
+                           exchanged with itself at one rank, 01:288-299); scheme A, both z
+                           faces only */
 };
 
 /* Update scheme.  B is the family of 05-08 (06:906-972): pull, halfway
@@ -131,6 +134,12 @@ typedef struct lbm_config
      * halo planes come from the neighbour slab (lbm_slab_exchange). */
     int slab_k0;
     int slab_nz;
+    /* scheme A: 1 = the sponge is 01's blend at the destination (01:207-225,
+     * 01:343-347): every population arriving from a fluid cell becomes
+     * (1 - s) f + s w_q with s = sponge_strength ((w - d) / w)^2, d the
+     * distance of the cell centre to the nearest sponge face and w =
+     * sponge_width cells, where s > 1e-6; needs tau_sponge_max <= 0. */
+    int sponge_blend;
 } lbm_config;
 
 /* One sound source: DroneSource (06:211-239) plus its time function. */
@@ -280,6 +289,11 @@ int lbm_get_rho_noalloc(lbm_handle* h, float* out, long capacity);
  * halo-inclusive layout f[idx*19+q] (06:366, 06:206-209). */
 int lbm_get_f(lbm_handle* h, double* out, long capacity);
 int lbm_set_f(lbm_handle* h, const double* in, long count);
+/* Scheme A: initial state at rest with density 1 + rho_minus_1 at every
+ * interior fluid cell (count = nx*ny*nz, x fastest), i.e. f = feq(1 + rho',
+ * flow) (the pulse initial condition of 01:183-205); SOLID cells are
+ * unchanged.  After lbm_init, before the first step. */
+int lbm_set_density(lbm_handle* h, const double* rho_minus_1, long count);
 /* Voxelised mask, halo-inclusive, 0 FLUID / 1 SOLID (06:469-531). */
 int lbm_get_mask(lbm_handle* h, uint8_t* out, long capacity);
 

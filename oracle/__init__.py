@@ -64,6 +64,7 @@ def _load():
             "orc_get_dt": (ctypes.c_double, [P]),
             "orc_get_f": (None, [P, _dp]),
             "orc_set_f": (None, [P, _dp]),
+            "orc_set_density": (None, [P, _dp]),
             "orc_get_mask": (None, [P, abi.c_uint8_p]),
             "orc_get_rho": (None, [P, _dp]),
             "orc_get_sponge": (None, [P, _dp]),
@@ -177,6 +178,11 @@ class OracleSolver:
         f = np.ascontiguousarray(f, dtype=np.float64)
         self.lib.orc_set_f(self.h, _ptr(f))
 
+    def set_density(self, rho_prime):
+        """Scheme A: rest state with density 1 + rho' at interior fluid cells (x fastest)."""
+        r = np.ascontiguousarray(rho_prime, dtype=np.float64).ravel()
+        self.lib.orc_set_density(self.h, _ptr(r))
+
     def get_mask(self):
         out = np.empty(self.ncell_halo, dtype=np.uint8)
         self.lib.orc_get_mask(self.h, _ptr(out, abi.c_uint8_p))
@@ -238,8 +244,8 @@ def refa_available(which):
 
 
 class RefASolver:
-    """An unmodified family-A reference program (02 Lloyd's mirror or 03
-    Doppler) through oracle/ref_harness_a.cpp: set-up, then steps of
+    """An unmodified family-A reference program (01 acoustic scattering, 02
+    Lloyd's mirror or 03 Doppler) through oracle/ref_harness_a.cpp: set-up, then steps of
     exchange_halos() + step(); fields in the reference's own layout."""
 
     def __init__(self, which, **params):
@@ -250,6 +256,7 @@ class RefASolver:
                           "refa_step": (None, [P, ctypes.c_int]), "refa_get_rho": (None, [P, _dp]),
                           "refa_get_f": (None, [P, _dp]), "refa_get_tau": (None, [P, _dp]),
                           "refa_get_source": (None, [P, _dp]), "refa_get_mask": (None, [P, abi.c_uint8_p]),
+                          "refa_get_sponge": (None, [P, _dp]),
                           "refa_set_threads": (None, [ctypes.c_int])}.items():
             fn = getattr(lib, n)
             fn.restype, fn.argtypes = r, a
@@ -295,6 +302,10 @@ class RefASolver:
 
     def get_mask(self):
         return self._get(self.lib.refa_get_mask, self.ncell_halo, np.uint8, abi.c_uint8_p)
+
+    def get_sponge(self):
+        """01's destination-blend sponge strengths (zeros for 02 and 03)."""
+        return self._get(self.lib.refa_get_sponge, self.ncell_halo)
 
 
 class RefParams(ctypes.Structure):

@@ -300,6 +300,8 @@ int orc_set_probes(orc_handle* h, const double* xyz, int n)
 
 /* ---------------------------------------------------------------- init */
 
+static void halo_rules(orc_handle* h);
+
 static void init_domain(orc_handle* h)
 {
     const lbm_config* c = &h->cfg;
@@ -354,8 +356,22 @@ static void init_domain(orc_handle* h)
                 }
             }
 
-    if (h->mask_override) return;
-    /* Halo rules (06:509-531): x faces, then y faces, then z faces. */
+    if (!h->mask_override) halo_rules(h);
+    /* periodic z (01:105-107): the halo planes are the opposite planes, also
+       for a caller's mask */
+    if (c->face_bc[LBM_FACE_ZLO] == LBM_BC_PERIODIC)
+        for (int j = 0; j <= h->ny + 1; ++j)
+            for (int i = 0; i <= h->nx + 1; ++i)
+            {
+                h->mask[loc(h, i, j, 0)] = h->mask[loc(h, i, j, h->nz)];
+                h->mask[loc(h, i, j, h->nz + 1)] = h->mask[loc(h, i, j, 1)];
+            }
+}
+
+/* Halo rules (06:509-531): x faces, then y faces, then z faces. */
+static void halo_rules(orc_handle* h)
+{
+    const lbm_config* c = &h->cfg;
     const unsigned char mx0 = c->face_bc[LBM_FACE_XLO] == LBM_BC_WALL ? SOLID : FLUID;
     const unsigned char mx1 = c->face_bc[LBM_FACE_XHI] == LBM_BC_WALL ? SOLID : FLUID;
     const unsigned char my0 = c->face_bc[LBM_FACE_YLO] == LBM_BC_WALL ? SOLID : FLUID;
@@ -447,6 +463,31 @@ static void init_scheme_a(orc_handle* h)
                     h->field_a[idx] = exp(-(x * x + y * y + z * z) / (2.0 * sig * sig));
                 }
                 for (int q = 0; q < Q; ++q) h->f_curr[idx * Q + q] = feq_a(q, 1.0, c->flow[0], c->flow[1], c->flow[2]);
+                if (c->sponge_blend)
+                {
+                    /* 01's sponge (01:207-225): distance into the layer per axis, the
+                       largest of them, strength (dist / thickness)^2 */
+                    const double th = c->sponge_width * c->dx;
+                    const double x = c->x_min + (gx + 0.5) * c->dx;
+                    const double y = c->y_min + (gy + 0.5) * c->dx;
+                    const double z = c->z_min + (gz + 0.5) * c->dx;
+                    double dist_x = 0.0, dist_y = 0.0, dist_z = 0.0;
+                    if ((sf & (1u << LBM_FACE_XLO)) && x < c->x_min + th) dist_x = (c->x_min + th) - x;
+                    else if ((sf & (1u << LBM_FACE_XHI)) && x > c->x_max - th) dist_x = x - (c->x_max - th);
+                    if ((sf & (1u << LBM_FACE_YLO)) && y < c->y_min + th) dist_y = (c->y_min + th) - y;
+                    else if ((sf & (1u << LBM_FACE_YHI)) && y > c->y_max - th) dist_y = y - (c->y_max - th);
+                    if ((sf & (1u << LBM_FACE_ZLO)) && z < c->z_min + th) dist_z = (c->z_min + th) - z;
+                    else if ((sf & (1u << LBM_FACE_ZHI)) && z > c->z_max - th) dist_z = z - (c->z_max - th);
+                    double dist_max = dist_x > dist_y ? dist_x : dist_y;
+                    dist_max = dist_z > dist_max ? dist_z : dist_max;
+                    double sig = 0.0;
+                    if (dist_max > 0.0)
+                    {
+                        const double r_ratio = dist_max / th;
+                        sig = c->sponge_strength * r_ratio * r_ratio;
+                    }
+                    h->sponge[idx] = sig;
+                }
             }
 }
 
@@ -480,6 +521,13 @@ static void halos_a(orc_handle* h)
         return;
     }
     orc_exchange_halos(h);   /* REST faces: feq(1,0); WALL halos are SOLID and never read */
+    if (c->face_bc[LBM_FACE_ZLO] == LBM_BC_PERIODIC)
+    {
+        /* 01:286-299 at one rank: the rank is its own z neighbour, whole planes */
+        const size_t plane = (size_t)h->nx_t * h->ny_t * Q;
+        memcpy(&h->f_curr[loc(h, 0, 0, 0) * Q], &h->f_curr[loc(h, 0, 0, h->nz) * Q], plane * sizeof(double));
+        memcpy(&h->f_curr[loc(h, 0, 0, h->nz + 1) * Q], &h->f_curr[loc(h, 0, 0, 1) * Q], plane * sizeof(double));
+    }
 }
 
 /* One scheme-A step at step index s (time t = s dt). */
@@ -543,6 +591,12 @@ static void step_a(orc_handle* h, long s)
                         else if (fs)
                         {
                             fn += W[q] * (h->field_a[dst] * mass);
+                        }
+                        if (c->sponge_blend && h->sponge[dst] > 1e-6)
+                        {
+                            /* 01:343-347 */
+                            const double sigma = h->sponge[dst];
+                            fn = (1.0 - sigma) * fn + sigma * feq_a(q, 1.0, 0.0, 0.0, 0.0);
                         }
                     }
                     h->f_next[dst * Q + q] = fn;
@@ -972,6 +1026,22 @@ void orc_get_dims(orc_handle* h, int* n3, int* n3_halo)
 double orc_get_dt(orc_handle* h) { return h->dt; }
 void orc_get_f(orc_handle* h, double* out) { memcpy(out, h->f_curr, h->Nloc * Q * sizeof(double)); }
 void orc_set_f(orc_handle* h, const double* in) { memcpy(h->f_curr, in, h->Nloc * Q * sizeof(double)); }
+/* Scheme A initial state at rest with density 1 + rho' at interior fluid
+ * cells (01:183-205); rho_prime: nx*ny*nz values, x fastest. */
+void orc_set_density(orc_handle* h, const double* rho_prime)
+{
+    const lbm_config* c = &h->cfg;
+    for (int k = 1; k <= h->nz; ++k)
+        for (int j = 1; j <= h->ny; ++j)
+            for (int i = 1; i <= h->nx; ++i)
+            {
+                const size_t idx = loc(h, i, j, k);
+                if (h->mask[idx] == SOLID) continue;
+                const double r = 1.0 + rho_prime[((size_t)(k - 1) * h->ny + (j - 1)) * h->nx + (i - 1)];
+                h->rho[idx] = r;
+                for (int q = 0; q < Q; ++q) h->f_curr[idx * Q + q] = feq_a(q, r, c->flow[0], c->flow[1], c->flow[2]);
+            }
+}
 void orc_get_mask(orc_handle* h, unsigned char* out) { memcpy(out, h->mask, h->Nloc); }
 void orc_get_rho(orc_handle* h, double* out) { memcpy(out, h->rho, h->Nloc * sizeof(double)); }
 void orc_get_sponge(orc_handle* h, double* out) { memcpy(out, h->sponge, h->Nloc * sizeof(double)); }

@@ -53,6 +53,7 @@ void orc_get_dims(orc_handle* h, int* n3, int* n3_halo);
 double orc_get_dt(orc_handle* h);
 void orc_get_f(orc_handle* h, double* out);
 void orc_set_f(orc_handle* h, const double* in);
+void orc_set_density(orc_handle* h, const double* rho_prime);
 void orc_get_mask(orc_handle* h, unsigned char* out);
 void orc_get_rho(orc_handle* h, double* out);
 void orc_get_sponge(orc_handle* h, double* out);

@@ -219,7 +219,45 @@ def family_a(name, n=40, steps=60):
         ref_params = dict(x_min=0.0, x_max=n * dx, y_min=0.0, y_max=n * dx, z_min=0.0, z_max=n * dx, dx=dx,
                           amp=0.01, Ma=Ma, tau_bulk=0.51, tau_sponge_max=0.9, sponge_width=10)
         return dict(cfg=cfg, sources=[src], probes=probes, mask=None, steps=steps, ref="03", ref_params=ref_params)
+    if name == "scattering_a":
+        return scattering_a(steps=steps)
     raise KeyError(name)
+
+
+def scattering_a(steps=60, dx=0.1, x=(-3.0, 6.0), y=(-3.0, 3.0), z=(-0.2, 0.2), amp=0.01):
+    """01_acoustic_scattering.cpp (pulse scattered by a cylinder) on a reduced
+    domain: a cylinder of radius 0.5 at the origin along z (SOLID where
+    x^2 + y^2 < 0.25 at cell centres, halos included, 01:167-185), an initial
+    density pulse 1 + amp exp(-ln2 ((x-4)^2 + y^2)) at fluid cells
+    (01:187-205), tau 0.505 everywhere (01:305), rest halos on x and y and
+    periodic z (01:105-107), the destination blend sponge 0.5 deep on x and y
+    with strength 1 (01:170-171, 01:207-225); dt = sqrt(1/3) dx / c (01:33-38).
+    Probes sit at cell centres next to 01's A, B, C (01:157-162)."""
+    nxg = int((x[1] - x[0]) / dx + 0.5)
+    nyg = int((y[1] - y[0]) / dx + 0.5)
+    nzg = max(int((z[1] - z[0]) / dx + 0.5), 3)
+    faces = (1 << abi.FACE_XLO) | (1 << abi.FACE_XHI) | (1 << abi.FACE_YLO) | (1 << abi.FACE_YHI)
+    cfg = abi.reference_config(x_min=x[0], x_max=x[1], y_min=y[0], y_max=y[1], z_min=z[0], z_max=z[1], dx=dx,
+                               c_phys=1.0, tau=0.505, use_geometry=0,
+                               face_bc=(abi.LBM_BC_REST,) * 4 + (abi.LBM_BC_PERIODIC,) * 2,
+                               sponge_faces=faces, sponge_width=0.5 / dx, sponge_strength=1.0, sponge_blend=1,
+                               sky_z=1e30, scheme=abi.LBM_SCHEME_A, tau_sponge_max=0.0,
+                               dt=np.sqrt(1.0 / 3.0) * dx / 1.0)
+    xc = x[0] + (np.arange(-1, nxg + 1) + 0.5) * dx
+    yc = y[0] + (np.arange(-1, nyg + 1) + 0.5) * dx
+    solid2 = (xc[None, :] ** 2 + yc[:, None] ** 2) < 0.25
+    mask = np.broadcast_to(solid2, (nzg + 2,) + solid2.shape).astype(np.uint8)
+    pulse2 = amp * np.exp(-np.log(2.0) * ((xc[None, :] - 4.0) ** 2 + yc[:, None] ** 2))
+    pulse2[solid2] = 0.0
+    rho0 = np.broadcast_to(pulse2[1:-1, 1:-1], (nzg, nyg, nxg)).copy()
+    cell = lambda v, lo: lo + (np.floor((v - lo) / dx) + 0.5) * dx
+    r135 = np.deg2rad(135.0)
+    pts = [(0.0, 1.0), (np.cos(r135), np.sin(r135)), (-1.0, 0.0), (2.0, 0.0), (4.0, 0.0)]
+    zc = z[0] + (nzg // 2 + 0.5) * dx
+    probes = np.array([(cell(px, x[0]), cell(py, y[0]), zc) for px, py in pts])
+    ref_params = dict(x_min=x[0], x_max=x[1], y_min=y[0], y_max=y[1], z_min=z[0], z_max=z[1], dx=dx, amp=amp)
+    return dict(cfg=cfg, sources=[], probes=probes, mask=np.ascontiguousarray(mask).ravel(), rho0=rho0.ravel(),
+                steps=steps, ref="01", ref_params=ref_params)
 
 
 def build_pair(sc):

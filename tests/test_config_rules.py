@@ -1,5 +1,6 @@
 """Configuration rules lbm_create enforces before any device work (runs
-without a GPU): scheme A limits and z-slab bounds."""
+without a GPU): scheme A limits (periodic z, the destination blend sponge)
+and z-slab bounds."""
 import ctypes
 
 import pytest
@@ -33,6 +34,13 @@ def _cfg(**kw):
     dict(slab_k0=10, slab_nz=8),                                                 # past the 16 layers
     dict(slab_k0=-1, slab_nz=4),
     dict(slab_k0=0, slab_nz=8, scheme=abi.LBM_SCHEME_A, face_bc=(abi.LBM_BC_REST,) * 6),
+    dict(face_bc=(abi.LBM_BC_REST,) * 4 + (abi.LBM_BC_PERIODIC,) * 2),          # periodic needs scheme A
+    dict(scheme=abi.LBM_SCHEME_A, face_bc=(abi.LBM_BC_PERIODIC,) * 2 + (abi.LBM_BC_REST,) * 4),   # z only
+    dict(scheme=abi.LBM_SCHEME_A, face_bc=(abi.LBM_BC_REST,) * 5 + (abi.LBM_BC_PERIODIC,)),      # both z faces
+    dict(scheme=abi.LBM_SCHEME_A, face_bc=(abi.LBM_BC_REST,) * 6, sponge_blend=1, tau_sponge_max=1.0),
+    dict(face_bc=(abi.LBM_BC_REST,) * 6, sponge_blend=1),                        # blend needs scheme A
+    dict(scheme=abi.LBM_SCHEME_A, face_bc=(abi.LBM_BC_REST,) * 6, sponge_blend=2),
+    dict(face_bc=(5,) * 6),
 ])
 def test_rejected_configs(kw):
     assert _create(_cfg(**kw)) == abi.LBM_ERR_BAD_CONFIG
@@ -42,6 +50,7 @@ def test_rejected_configs(kw):
     dict(scheme=abi.LBM_SCHEME_A, face_bc=(abi.LBM_BC_REST,) * 6, tau_sponge_max=1.0),
     dict(scheme=abi.LBM_SCHEME_A, face_bc=(abi.LBM_BC_COPY,) * 6, flow=(0.0, 0.0, 0.1)),
     dict(slab_k0=8, slab_nz=8),
+    dict(scheme=abi.LBM_SCHEME_A, face_bc=(abi.LBM_BC_REST,) * 4 + (abi.LBM_BC_PERIODIC,) * 2, sponge_blend=1),
 ])
 def test_accepted_configs(kw):
     # without a GPU the device check comes after validation

@@ -1,7 +1,7 @@
 """Scheme A (the reference's family-A programs 01-04) on the GPU, through the
 C-ABI, against the FP64 oracle's family-A restatement (itself checked
-against the unmodified 02/03 programs in tests/test_oracle_family_a.py and
-the fixtures in tests/golden/).
+against the unmodified 01/02/03 programs in tests/test_oracle_family_a.py
+and the fixtures in tests/golden/).
 
 Tolerances: FP32 deviation storage against FP64, probe (density) series
 relative L2 <= 1e-5 and field max error <= 1e-5 of the field's largest
@@ -25,14 +25,24 @@ GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
 
 def _solver(sc, **kw):
-    return Solver(sc["cfg"], sc["sources"], sc["probes"], mask=sc["mask"], **kw)
+    g = Solver(sc["cfg"], sc["sources"], sc["probes"], mask=sc["mask"], **kw)
+    if sc.get("rho0") is not None:
+        g.set_density(sc["rho0"])
+    return g
 
 
-@pytest.mark.parametrize("name", ["lloyd_a", "doppler_a"])
+def _oracle(sc):
+    o = OracleSolver(sc["cfg"], sc["sources"], sc["probes"], mask=sc["mask"])
+    if sc.get("rho0") is not None:
+        o.set_density(sc["rho0"])
+    return o
+
+
+@pytest.mark.parametrize("name", ["lloyd_a", "doppler_a", "scattering_a"])
 def test_scheme_a_matches_oracle(name, gpu):
     sc = scenarios.family_a(name)
     g = _solver(sc)
-    o = OracleSolver(sc["cfg"], sc["sources"], sc["probes"], mask=sc["mask"])
+    o = _oracle(sc)
     g.step(sc["steps"])
     o.step(sc["steps"])
     pg, po = g.get_probes(), o.get_probes()
@@ -47,7 +57,7 @@ def test_scheme_a_matches_oracle(name, gpu):
     assert np.max(np.abs(fg - fo)) <= FIELD_TOL * np.max(np.abs(fo))
 
 
-@pytest.mark.parametrize("name", ["lloyd_a", "doppler_a"])
+@pytest.mark.parametrize("name", ["lloyd_a", "doppler_a", "scattering_a"])
 def test_scheme_a_matches_reference_fixture(name, gpu):
     path = os.path.join(GOLDEN, name + ".npz")
     gold = np.load(path)
@@ -83,6 +93,60 @@ def test_scheme_a_solid_wall_direct_equals_batched(gpu):
         b.step_collision_bgk()
         b.record_probes()
     assert np.array_equal(a.get_probes(), b.get_probes())
+
+
+def _scattering_3d(steps, **kw):
+    """01's set-up with a pulse that varies along the periodic z axis, so
+    the halo planes carry something the interior planes do not already hold."""
+    sc = scenarios.scattering_a(steps=steps, z=(-0.4, 0.4), **kw)
+    nx, ny, nz = 90, 60, 8
+    zc = -0.4 + (np.arange(nz) + 0.5) * 0.1
+    rho0 = sc["rho0"].reshape(nz, ny, nx) * (1.0 + 0.5 * np.cos(2.0 * np.pi * (zc - 0.13) / 0.8))[:, None, None]
+    sc["rho0"] = rho0.ravel()
+    return sc
+
+
+def test_periodic_z_pulse_matches_oracle(gpu):
+    sc = _scattering_3d(50)
+    g, o = _solver(sc), _oracle(sc)
+    g.step(sc["steps"])
+    o.step(sc["steps"])
+    assert rel_l2(g.get_probes(), o.get_probes()) <= PROBE_TOL
+    nx, ny, nz = g.dims
+    fo = o.get_rho().reshape(nz + 2, ny + 2, nx + 2)[1:-1, 1:-1, 1:-1] - 1.0
+    fo[o.get_mask().reshape(nz + 2, ny + 2, nx + 2)[1:-1, 1:-1, 1:-1] == 1] = 0.0
+    assert np.ptp(fo[:, 30, 70]) > 1e-4                  # the field still varies along z
+    assert np.max(np.abs(g.get_rho().astype(np.float64) - fo)) <= FIELD_TOL * np.max(np.abs(fo))
+
+
+def test_periodic_z_direct_calls_equal_batched_steps(gpu):
+    sc = _scattering_3d(10)
+    a = _solver(sc)
+    a.step(sc["steps"])
+    b = _solver(sc)
+    for s in range(sc["steps"]):
+        b.step_collision_bgk()
+        b.record_probes()
+    assert np.array_equal(a.get_probes(), b.get_probes())
+    assert np.array_equal(a.get_rho(), b.get_rho())
+
+
+def test_set_density_rules(gpu):
+    sc = scenarios.scattering_a(steps=2)
+    g = _solver(sc)
+    with pytest.raises(LBMError) as e:
+        g.set_density(sc["rho0"][:-1])
+    assert e.value.status == abi.LBM_ERR_INVALID_ARGUMENT
+    g.step(1)
+    with pytest.raises(LBMError) as e:
+        g.set_density(sc["rho0"])
+    assert e.value.status == abi.LBM_ERR_STATE
+    b = Solver(scenarios.family_a("doppler_a")["cfg"], [], None)
+    b.set_density(np.zeros(b.dims[0] * b.dims[1] * b.dims[2]))    # any scheme-A set-up
+    lat = Solver(scenarios.lattice_config(16, 16, 8, 0.52, use_geometry=0), [], None)
+    with pytest.raises(LBMError) as e:
+        lat.set_density(np.zeros(16 * 16 * 8))
+    assert e.value.status == abi.LBM_ERR_UNSUPPORTED
 
 
 def test_uniform_flow_is_steady(gpu):
