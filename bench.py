@@ -36,6 +36,7 @@ METRIC = "D3Q19 GLUPS, %HBM peak: FP16-store vs FP32 @<=1e-3 probe L2; adjoint g
 # 2.644e9 B, k_step<float>: 5.132e9 B for 33.55e6 cells)
 NCU_TRAFFIC_PER_CELL = {"fp16": 2.644e9 / 33554432, "fp32": 5.132e9 / 33554432}
 UNIT = "GLUPS"
+L2_BYTES = 126e6   # B200 L2
 # steps of the FP16-vs-FP32 probe comparison on the 1024x1024x256 city (the
 # Ricker sources' first periods reach the nearer street-level probes)
 ERR_STEPS = 400
@@ -195,9 +196,22 @@ def measure(name, storage, steps, warmup, device, torch, barrier, reduce_max, ke
 def e2e_measure(solver, w, steps):
     """Through the C-ABI with host buffers: the source amplitude series goes
     host->device (lbm_add_source with a table waveform, uploaded inside
-    lbm_step) and the probe series device->host (lbm_get_probes)."""
+    lbm_step) and the probe series device->host (lbm_get_probes).  A workload
+    without a source (01's initial pulse) has only the probe series."""
+    import ctypes
+
     from nlos_lbm import abi
 
+    if not w["sources"]:
+        solver.get_probes()
+        h0, d0 = solver.transfer_bytes()
+        t0 = time.perf_counter()
+        solver.step(steps)
+        series = solver.get_probes()
+        t1 = time.perf_counter()
+        h1, d1 = solver.transfer_bytes()
+        assert series.shape[0] >= steps
+        return (t1 - t0) * 1e3, (h1 - h0) / steps, (d1 - d0) / steps
     base = w["sources"][0]
     s0 = solver.step_count
     table = np.zeros(s0 + steps)
@@ -207,9 +221,9 @@ def e2e_measure(solver, w, steps):
     h0, d0 = solver.transfer_bytes()
     t0 = time.perf_counter()
     solver.clear_sources()
-    src = abi.reference_source(sx=base.sx, sy=base.sy, sz=base.sz, ex=base.ex, ey=base.ey, ez=base.ez,
-                               speed=base.speed, amp=base.amp, waveform=abi.LBM_WAVE_TABLE,
-                               injection=base.injection)
+    src = abi.LbmSource()
+    ctypes.pointer(src)[0] = base   # every field of the workload's source, then a table waveform
+    src.waveform = abi.LBM_WAVE_TABLE
     src.table = table.ctypes.data_as(abi.c_double_p)
     src.table_len = len(table)
     solver.add_source(src)
@@ -450,7 +464,9 @@ def run_our_arm(args):
                    "storage": head["storage"], "plan_coverage": head["coverage"],
                    "fluid_fraction": head["fluid_fraction"],
                    "parallelism": f"replicas x{n}" if n > 1 else "single GPU",
-                   "l2": "inputs larger than L2 (populations %.1f GB per step)" % (cells * head["bytes_per_cell"] / 1e9)},
+                   "l2": ("inputs larger than L2 (populations %.1f GB per step)" if cells * head["bytes_per_cell"] > 2 * L2_BYTES
+                          else "inputs about the size of L2 (populations %.2f GB per step)")
+                   % (cells * head["bytes_per_cell"] / 1e9)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                      "frac": achieved / hbm_peak, "traffic": traffic, "peak_kind": peak_kind,
                      "kernel": "k_step (fused pull-stream + bounce-back + BGK + sponge)",

@@ -102,30 +102,28 @@ __device__ __forceinline__ D4 operator/(D4 a, D4 b)
                (a.d[2] * b.v - a.v * b.d[2]) * iv2, (a.d[3] * b.v - a.v * b.d[3]) * iv2}};
 }
 
-__device__ __forceinline__ D4 dot_c4(int q, D4 x, D4 y, D4 z)
-{
-    D4 r = dc(0.f);
-    if (ex(q) > 0) r = r + x;
-    if (ex(q) < 0) r = r - x;
-    if (ey(q) > 0) r = r + y;
-    if (ey(q) < 0) r = r - y;
-    if (ez(q) > 0) r = r + z;
-    if (ez(q) < 0) r = r - z;
-    return r;
-}
-
-// geq(rho', r, u) - w_q rho-free part, in deviation units with scale 1:
-//   w_q (rho' + r (3 c.u + 4.5 (c.u)^2 - 1.5 u^2))
-__device__ __forceinline__ D4 geq4(int q, D4 rho, D4 r, D4 ux, D4 uy, D4 uz)
-{
-    const D4 cu = dot_c4(q, ux, uy, uz);
-    const D4 u2 = ux * ux + uy * uy + uz * uz;
-    return wf(q) * (rho + r * (3.0f * cu + 4.5f * (cu * cu) - 1.5f * u2));
-}
-
 // Ghost delta D_q(m) = geq(rho_B, u_B) - geq(rho_I, u_I) of the open boundary
-// (06:684-835), as a function of the interior moments m = (rho', J).
-__device__ __forceinline__ void nscbc_delta4(D4 rho, D4 jx, D4 jy, D4 jz, int axis, int side, D4 (&D)[Q])
+// (06:684-835) as a function of the interior moments m = (rho', J), with
+// geq(q; rho', r, u) = w_q (rho' + r (3 c.u + 4.5 (c.u)^2 - 1.5 u^2)) in
+// deviation units with scale 1.  The adjoint needs only sum_q lam_q D_q(m)
+// and its gradient in m, which go through the weighted moments of lam:
+//   A0 = sum w lam, A1 = sum w lam c, A2 = sum w lam c c^T (xx yy zz xy xz yz),
+//   A0 rho' + r (3 A1.u + 4.5 u^T A2 u - 1.5 u^2 A0).
+struct LamMoments
+{
+    float a0, a1[3], a2[6];
+};
+__device__ __forceinline__ D4 lam_geq4(const LamMoments& A, D4 rho, D4 r, D4 ux, D4 uy, D4 uz)
+{
+    const D4 cu = A.a1[0] * ux + A.a1[1] * uy + A.a1[2] * uz;
+    const D4 xx = ux * ux, yy = uy * uy, zz = uz * uz;
+    const D4 quad = A.a2[0] * xx + A.a2[1] * yy + A.a2[2] * zz +
+                    2.0f * (A.a2[3] * (ux * uy) + A.a2[4] * (ux * uz) + A.a2[5] * (uy * uz));
+    return A.a0 * rho + r * (3.0f * cu + 4.5f * quad - 1.5f * (A.a0 * (xx + yy + zz)));
+}
+
+// sum_q lam_q D_q(m), one scalar whose four derivatives are J_ghost^T lam.
+__device__ __forceinline__ D4 nscbc_lam4(const LamMoments& A, D4 rho, D4 jx, D4 jy, D4 jz, int axis, int side)
 {
     const D4 rI = dc(1.0f) + rho;
     const D4 ux = jx / rI, uy = jy / rI, uz = jz / rI;
@@ -148,8 +146,7 @@ __device__ __forceinline__ void nscbc_delta4(D4 rho, D4 jx, D4 jy, D4 jz, int ax
     const D4 rhoB = (1.0f / cs2) * pB;
     const D4 rB = dc(1.0f) + rhoB;
     const D4 bx = axis == 0 ? unB : ux, by = axis == 1 ? unB : uy, bz = axis == 2 ? unB : uz;
-#pragma unroll
-    for (int q = 0; q < Q; ++q) D[q] = geq4(q, rhoB, rB, bx, by, bz) - geq4(q, rho, rI, ux, uy, uz);
+    return lam_geq4(A, rhoB, rB, bx, by, bz) - lam_geq4(A, rho, rI, ux, uy, uz);
 }
 
 // ---------------------------------------------------------------- kernels
@@ -164,8 +161,8 @@ __global__ void __launch_bounds__(128) k_adj_ghost(AdjGhostArgs a)
     int fi = 0;
     while (fi + 1 < a.ga.nfaces && t >= a.ga.face[fi + 1].first) ++fi;
     const GhostFace F = a.ga.face[fi];
-    const long long lt = t - F.first;
-    const int u = (int)(lt % F.nu), v = (int)(lt / F.nu);
+    const int lt = (int)(t - F.first);
+    const int u = lt % F.nu, v = lt / F.nu;
     const Layout& L = a.L;
     // ghost cell g (the forward ghost kernel's enumeration of the face)
     int gi, gj, gk;
@@ -187,34 +184,49 @@ __global__ void __launch_bounds__(128) k_adj_ghost(AdjGhostArgs a)
         gj = 1 + v;
         gk = F.side ? L.nz + 1 : 0;
     }
-    // lamHt at the ghost: what the interior cells y = g + e_q pulled from it
-    // (none when y bounced back, i.e. when the ghost cell is SOLID)
-    // (the links word and the adjoint value are loaded independently and
-    // combined afterwards: one memory round trip instead of two)
+    // lamHt at the ghost: what the interior cells y = g + e_q pulled from it,
+    // nothing when the ghost cell is SOLID (they bounced back instead).  Bit q
+    // of y's links word is that solidity for every such y, so one word is
+    // read: that of the interior neighbour along the inward normal.
+    const int qn = 1 + 2 * F.axis + F.side;
+    const int ni = F.axis == 0 ? 1 - 2 * F.side : 0, nj = F.axis == 1 ? 1 - 2 * F.side : 0,
+              nk = F.axis == 2 ? 1 - 2 * F.side : 0;
+    // (loaded beside the adjoint values, not before them: one memory round trip)
+    const uint32_t lkn = __ldg(a.links + L.cell(gi + ni, gj + nj, gk + nk));
     float lh[Q];
-    uint32_t lk[Q];
 #pragma unroll
     for (int q = 0; q < Q; ++q)
     {
         const int di = gi + ex(q), dj = gj + ey(q), dk = gk + ez(q);
-        const bool in = interior(L, di, dj, dk);
-        lk[q] = in ? __ldg(a.links + L.cell(di, dj, dk)) : 1u << q;
-        lh[q] = in ? __ldg(a.lam_in + L.elem(q, di, dj, dk)) : 0.f;
+        lh[q] = interior(L, di, dj, dk) ? __ldg(a.lam_in + L.elem(q, di, dj, dk)) : 0.f;
     }
+    if ((lkn >> qn) & 1u)
+    {
 #pragma unroll
-    for (int q = 0; q < Q; ++q)
-        if ((lk[q] >> q) & 1u) lh[q] = 0.f;
+        for (int q = 0; q < Q; ++q) lh[q] = 0.f;
+    }
     // moments of the interior cell the ghost was built from
     const float4 m = __ldg(a.face_mom + t);
-    const float rho = m.x, jx = m.y, jy = m.z, jz = m.w;
-    D4 D[Q];
-    nscbc_delta4(D4{rho, {1.f, 0.f, 0.f, 0.f}}, D4{jx, {0.f, 1.f, 0.f, 0.f}}, D4{jy, {0.f, 0.f, 1.f, 0.f}},
-                 D4{jz, {0.f, 0.f, 0.f, 1.f}}, F.axis, F.side, D);
-    float vk[4] = {0.f, 0.f, 0.f, 0.f};
+    // J_ghost^T lam = grad_m sum_q lam_q D_q(m), through lam's weighted moments
+    LamMoments A{};
 #pragma unroll
     for (int q = 0; q < Q; ++q)
-#pragma unroll
-        for (int m = 0; m < 4; ++m) vk[m] += lh[q] * D[q].d[m];
+    {
+        const float wl = wf(q) * lh[q];
+        A.a0 += wl;
+        if (ex(q)) A.a1[0] += ex(q) * wl;
+        if (ey(q)) A.a1[1] += ey(q) * wl;
+        if (ez(q)) A.a1[2] += ez(q) * wl;
+        if (ex(q)) A.a2[0] += wl;
+        if (ey(q)) A.a2[1] += wl;
+        if (ez(q)) A.a2[2] += wl;
+        if (ex(q) * ey(q)) A.a2[3] += ex(q) * ey(q) * wl;
+        if (ex(q) * ez(q)) A.a2[4] += ex(q) * ez(q) * wl;
+        if (ey(q) * ez(q)) A.a2[5] += ey(q) * ez(q) * wl;
+    }
+    const D4 S = nscbc_lam4(A, D4{m.x, {1.f, 0.f, 0.f, 0.f}}, D4{m.y, {0.f, 1.f, 0.f, 0.f}},
+                            D4{m.z, {0.f, 0.f, 1.f, 0.f}}, D4{m.w, {0.f, 0.f, 0.f, 1.f}}, F.axis, F.side);
+    const float vk[4] = {S.d[0], S.d[1], S.d[2], S.d[3]};
     const long long n = (long long)F.nu * F.nv, off = a.gadj_off[F.axis * 2 + F.side];
 #pragma unroll
     for (int p = 0; p < Q; ++p)
