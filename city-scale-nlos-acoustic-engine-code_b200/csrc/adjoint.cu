@@ -302,6 +302,37 @@ __device__ __forceinline__ float2 shifted_pair(const float* row, int lane, const
 // a = (1 - sigma)(1 - omega), b = (1 - sigma) omega; SOLID cells copy.
 // lamH (gather of lamF^s with the bounce-back terms and, at the open faces,
 // the ghost-adjoint terms) stays in registers for the output.
+// L2 prefetch of the adjoint lines and the moments that the row `dist` rows
+// after (j, k) reads, for the CELLS columns from col0 (one block's share):
+// the first threads take one interleaved block each (19 lines), the next
+// ones one 128-byte line of moments each.
+template <int CELLS>
+__device__ __forceinline__ void adj_prefetch_rows(const AdjStepArgs& a, int j, int k, int col0)
+{
+    constexpr int BC = 32, NBLK = (CELLS + BC - 1) / BC, NMOM = (CELLS * 8 + 127) / 128;
+    const Layout& L = a.L;
+    const int t = threadIdx.x;
+    if (t >= NBLK + NMOM) return;
+    const int r = (k - 1) * L.ny + (j - 1) + a.prefetch_rows;
+    if (r >= L.ny * L.nz) return;
+    const int jj = 1 + r % L.ny, kk = 1 + r / L.ny;
+    if (t < NBLK)
+    {
+        const int col = col0 + t * BC;
+        if (col >= L.nx) return;
+#pragma unroll
+        for (int q = 0; q < Q; ++q)
+            asm volatile("prefetch.global.L2 [%0];" ::"l"(a.lam_in + L.elem(q, col + 1, jj + ey(q), kk + ez(q))));
+    }
+    else
+    {
+        const int col = col0 + (t - NBLK) * 16;
+        if (col >= L.nx) return;
+        const long long mi = ((long long)(kk - 1) * L.ny + (jj - 1)) * L.nx + col;
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(a.mom_prev + mi));
+    }
+}
+
 template <int BLOCK, int MINB>
 __global__ void __launch_bounds__(BLOCK, MINB) k_adj_step(AdjStepArgs a)
 {
@@ -314,6 +345,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_adj_step(AdjStepArgs a)
     const int j = blockIdx.y + 1, k = blockIdx.z + 1;
     const long long e0 = L.elem(0, c0 + 1, j, k);
     const long long rs = L.row_stride, ps = L.plane_stride;
+    if (a.prefetch_rows > 0) adj_prefetch_rows<2 * BLOCK>(a, j, k, 2 * BLOCK * blockIdx.x);
 
     uint32_t lk0 = 0, lk1 = 0;
     if (active)
