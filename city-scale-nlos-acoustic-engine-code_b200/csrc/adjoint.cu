@@ -162,7 +162,7 @@ __global__ void __launch_bounds__(128) k_adj_ghost(AdjGhostArgs a)
     while (fi + 1 < a.ga.nfaces && t >= a.ga.face[fi + 1].first) ++fi;
     const GhostFace F = a.ga.face[fi];
     const int lt = (int)(t - F.first);
-    const int u = lt % F.nu, v = lt / F.nu;
+    const int v = lt / F.nu, u = lt - v * F.nu;
     const Layout& L = a.L;
     // ghost cell g (the forward ghost kernel's enumeration of the face)
     int gi, gj, gk;

@@ -937,6 +937,8 @@ extern "C" int lbm_init(lbm_handle* h)
         gf.nu = gf.axis == 0 ? ny : nx;
         gf.nv = gf.axis == 2 ? ny : nz;
         gf.first = first;
+        // the ghost kernels index within a face in 32 bits
+        if ((long long)gf.nu * gf.nv > 0x7fffffffLL) return h->fail(LBM_ERR_UNSUPPORTED, "an open face of 2^31 cells or more");
         first += (long long)gf.nu * gf.nv;
         h->ga.face[h->ga.nfaces++] = gf;
     }

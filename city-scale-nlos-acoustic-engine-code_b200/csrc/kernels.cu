@@ -1190,8 +1190,8 @@ __global__ void __launch_bounds__(128) k_ghost(S* __restrict__ f, Layout L, Ghos
     int fi = 0;
     while (fi + 1 < a.nfaces && t >= a.face[fi + 1].first) ++fi;
     const GhostFace F = a.face[fi];
-    const long long lt = t - F.first;
-    const int u = (int)(lt % F.nu), v = (int)(lt / F.nu);
+    const int lt = (int)(t - F.first);   // a face has fewer than 2^31 cells (nu, nv are ints of one grid)
+    const int v = lt / F.nu, u = lt - v * F.nu;
     const float inv_scale = 1.0f / a.scale;
     float G[Q];
     if (F.axis == 0)

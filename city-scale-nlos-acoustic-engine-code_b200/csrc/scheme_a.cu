@@ -346,30 +346,32 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step_a(const float* __restrict_
 __global__ void __launch_bounds__(128) k_copy_a(const float* __restrict__ fin, float* __restrict__ fout, Layout L,
                                                  StepArgs a, SchemeAArgs b)
 {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const long long nyt = L.ny + 2, nzt = L.nz + 2;
-    const long long nX = 2 * nyt * nzt, nY = 2LL * L.nx * nzt, nZ = 2LL * L.nx * L.ny;
+    // 32-bit index arithmetic: launch_copy_a rejects grids with 2^31 halo cells or more
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nyt = L.ny + 2, nzt = L.nz + 2;
+    const int pX = nyt * nzt, pY = L.nx * nzt, pZ = L.nx * L.ny;   // cells of one face
     int ih, jh, kh;
-    if (t < nX)
+    if (t < 2 * pX)
     {
-        const long long r = t % (nyt * nzt);
-        ih = t < nyt * nzt ? 0 : L.nx + 1;
-        jh = (int)(r % nyt);
-        kh = (int)(r / nyt);
+        const int r = t < pX ? t : t - pX;
+        ih = t < pX ? 0 : L.nx + 1;
+        kh = r / nyt;
+        jh = r - kh * nyt;
     }
-    else if (t < nX + nY)
+    else if (t < 2 * pX + 2 * pY)
     {
-        const long long u = t - nX, r = u % (L.nx * nzt);
-        jh = u < L.nx * nzt ? 0 : L.ny + 1;
-        ih = 1 + (int)(r % L.nx);
-        kh = (int)(r / L.nx);
+        const int u = t - 2 * pX, r = u < pY ? u : u - pY;
+        jh = u < pY ? 0 : L.ny + 1;
+        kh = r / L.nx;
+        ih = 1 + r - kh * L.nx;
     }
-    else if (t < nX + nY + nZ)
+    else if (t < 2 * pX + 2 * pY + 2 * pZ)
     {
-        const long long u = t - nX - nY, r = u % ((long long)L.nx * L.ny);
-        kh = u < (long long)L.nx * L.ny ? 0 : L.nz + 1;
-        ih = 1 + (int)(r % L.nx);
-        jh = 1 + (int)(r / L.nx);
+        const int u = t - 2 * pX - 2 * pY, r = u < pZ ? u : u - pZ;
+        kh = u < pZ ? 0 : L.nz + 1;
+        const int jr = r / L.nx;
+        ih = 1 + r - jr * L.nx;
+        jh = 1 + jr;
     }
     else
     {
@@ -572,6 +574,7 @@ cudaError_t launch_copy_a(const float* fin, float* fout, const Layout& L, const 
                           cudaStream_t stream)
 {
     const long long n = 2LL * (L.ny + 2) * (L.nz + 2) + 2LL * L.nx * (L.nz + 2) + 2LL * L.nx * L.ny;
+    if (n + 127 > 0x7fffffffLL) return cudaErrorInvalidValue;   // the kernel indexes in 32 bits
     k_copy_a<<<(unsigned)((n + 127) / 128), 128, 0, stream>>>(fin, fout, L, a, b);
     return cudaGetLastError();
 }
