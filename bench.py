@@ -177,12 +177,18 @@ def measure(name, storage, steps, warmup, device, torch, barrier, reduce_max, ke
     solid = np.count_nonzero(s.get_mask().reshape(nz + 2, ny + 2, nx + 2)[1:-1, 1:-1, 1:-1])
     fluid_fraction = 1.0 - solid / ncell
     s.step(warmup)
-    s.set_kernel_timing(kernel_timing)
+    # the timed steps run as the library runs them (CUDA graphs); the step
+    # kernel's own duration comes from as many further steps with per-launch
+    # events (which replace the graphs by direct launches)
     l0 = s.launch_count
     ms = device_timed_steps(s, steps, torch, barrier)
     launches = s.launch_count - l0
-    kms, kn = s.kernel_time()
-    s.set_kernel_timing(False)
+    kms, kn = 0.0, 0
+    if kernel_timing:
+        s.set_kernel_timing(True)
+        s.step(steps)
+        kms, kn = s.kernel_time()
+        s.set_kernel_timing(False)
     ms_max = reduce_max(ms)
     probes = s.get_probes()
     res = dict(name=name, storage="fp16" if s.bytes_per_cell == 76 else "fp32", cells=ncell, dims=[nx, ny, nz],
