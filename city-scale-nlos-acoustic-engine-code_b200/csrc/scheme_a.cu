@@ -467,7 +467,8 @@ __global__ void __launch_bounds__(128) k_zper_a(float* __restrict__ f, Layout L,
 // ---------------------------------------------------------------- initial density
 // 01's pulse (01:187-205): every FLUID cell starts at f = feq(1 + rho', u0)
 // = (1 + rho') (w_q + base_q), an equilibrium, which the collision keeps, so
-// the stored post-collision deviation is rho' (w_q + base_q).  A SOLID
+// the stored post-collision deviation is rho' (w_q + base_q); zero-gradient
+// halo cells take the value of their nearest interior cell.  A SOLID
 // cell's slot q holds the value its neighbour D = cell + e_q bounces back in
 // the first step, f(D) of direction inv(q): base_inv(q) - base_q +
 // rho'(D) (w_q + base_inv(q)) for FLUID interior D (w_inv(q) = w_q).  Other
@@ -490,13 +491,21 @@ __global__ void __launch_bounds__(128) k_set_density_a(float* __restrict__ f, fl
     const bool solid = mref(i0, j, k) != 0;
     if (!solid)
     {
-        if (!interior(i0, j, k)) return;
-        const float r = rho_at(i0, j, k);
+        // a zero-gradient halo cell repeats its nearest interior cell I, and
+        // collides what I holds (03:175-237): the same equilibrium, I's rho'
+        const bool in = interior(i0, j, k);
+        if (!in && !b.copy) return;
+        const int ii = min(max(i0, 1), L.nx), jj = min(max(j, 1), L.ny), kk = min(max(k, 1), L.nz);
+        if (!in && mref(ii, jj, kk) != 0) return;   // a SOLID I holds no density of its own
+        const float r = rho_at(ii, jj, kk);
 #pragma unroll
         for (int q = 0; q < Q; ++q)
         {
-            const long long e = L.elem(q, i0, j, k);
-            if (LBM_IN(kChkAStore, e, L.total)) f[e] = r * (wf(q) + b.base[q]);
+            const float v = r * (wf(q) + b.base[q]);
+            if (i0 == 0 || i0 == L.nx + 1)
+                xgh[XFace{nullptr, nullptr}.gh_index(i0 == 0 ? 0 : 1, q, j, k, L.ny, L.nz)] = v;
+            else if (LBM_IN(kChkAStore, L.elem(q, i0, j, k), L.total))
+                f[L.elem(q, i0, j, k)] = v;
         }
         return;
     }

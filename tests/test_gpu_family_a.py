@@ -143,6 +143,25 @@ def test_wall_faces_with_initial_pulse_match_oracle(gpu):
     assert np.max(np.abs(g.get_rho().astype(np.float64) - fo)) <= FIELD_TOL * np.max(np.abs(fo))
 
 
+def test_copy_halos_with_initial_pulse_match_oracle(gpu):
+    """Zero-gradient halos (03) and background flow with an initial density
+    pulse that already covers the high x face: the first step pulls the
+    halo copies of the pulse, not rest."""
+    sc = scenarios.family_a("doppler_a", steps=30)
+    n, dx = 40, 0.25
+    c = (np.arange(n) + 0.5) * dx
+    z, y, x = np.meshgrid(c, c, c, indexing="ij")
+    sc["rho0"] = (1e-3 * np.exp(-((x - (n * dx - 0.6)) ** 2 + (y - 5.0) ** 2 + (z - 5.0) ** 2) / 2.0)).ravel()
+    sc["sources"] = []
+    g, o = _solver(sc), _oracle(sc)
+    g.step(sc["steps"])
+    o.step(sc["steps"])
+    assert rel_l2(g.get_probes(), o.get_probes()) <= PROBE_TOL
+    fo = o.get_rho().reshape(n + 2, n + 2, n + 2)[1:-1, 1:-1, 1:-1] - 1.0
+    assert np.max(np.abs(fo[:, :, -1])) > 1e-5
+    assert np.max(np.abs(g.get_rho().astype(np.float64) - fo)) <= FIELD_TOL * np.max(np.abs(fo))
+
+
 def test_periodic_z_direct_calls_equal_batched_steps(gpu):
     sc = _scattering_3d(10)
     a = _solver(sc)
