@@ -112,18 +112,6 @@ __device__ __forceinline__ void moments(const float (&G)[Q], float& rho, float& 
     }
 }
 
-__device__ __forceinline__ float dot_c(int q, float x, float y, float z)
-{
-    float r = 0.f;
-    if (ex(q) > 0) r += x;
-    if (ex(q) < 0) r -= x;
-    if (ey(q) > 0) r += y;
-    if (ey(q) < 0) r -= y;
-    if (ez(q) > 0) r += z;
-    if (ez(q) < 0) r -= z;
-    return r;
-}
-
 __device__ __forceinline__ uint32_t near_bits(const StepArgs& a, const Layout& L, int col, int j, int k)
 {
     return a.near[((long long)k * (L.ny + 2) + j) * L.words_per_row + (col >> 5)] >> (col & 31);
@@ -1126,12 +1114,6 @@ __global__ void __launch_bounds__(512) k_source(S* __restrict__ f, Layout L, Ste
 // pressure carry only the outgoing invariant (incoming invariant zero).  In
 // stored deviation units (Gs = scale * g):
 //   geq(rho', r, u) = w (rho' + r (3 c.u + (4.5 (c.u)^2 - 1.5 u^2) / scale)).
-__device__ __forceinline__ float geq_dev(int q, float rho, float r, float ux, float uy, float uz, float inv_scale)
-{
-    const float cu = dot_c(q, ux, uy, uz);
-    const float u2 = ux * ux + uy * uy + uz * uz;
-    return wf(q) * fmaf(r, fmaf(inv_scale, 4.5f * cu * cu - 1.5f * u2, 3.0f * cu), rho);
-}
 
 __device__ __forceinline__ void nscbc(float (&G)[Q], int axis, int side, float inv_scale)
 {
@@ -1170,9 +1152,30 @@ __device__ __forceinline__ void nscbc(float (&G)[Q], int axis, int side, float i
     const float rhoB = pB / cs2;
     const float rB = fmaf(rhoB, inv_scale, 1.0f);
     const float bx = axis == 0 ? unB : ux, by = axis == 1 ? unB : uy, bz = axis == 2 ? unB : uz;
+    // geq(B) - geq(I) = w_q (d0 + c.v + c^T M c), a quadratic form in
+    // c_q whose ten coefficients are taken once per cell
+    const float k45 = 4.5f * inv_scale;
+    const float d0 = (rhoB - rho) - 1.5f * inv_scale * (rB * (bx * bx + by * by + bz * bz) - rI * (ux * ux + uy * uy + uz * uz));
+    const float vx = 3.0f * (rB * bx - rI * ux), vy = 3.0f * (rB * by - rI * uy), vz = 3.0f * (rB * bz - rI * uz);
+    const float mxx = k45 * (rB * bx * bx - rI * ux * ux), myy = k45 * (rB * by * by - rI * uy * uy),
+                mzz = k45 * (rB * bz * bz - rI * uz * uz);
+    const float mxy = 2.0f * k45 * (rB * bx * by - rI * ux * uy), mxz = 2.0f * k45 * (rB * bx * bz - rI * ux * uz),
+                myz = 2.0f * k45 * (rB * by * bz - rI * uy * uz);
 #pragma unroll
     for (int q = 0; q < Q; ++q)
-        G[q] += geq_dev(q, rhoB, rB, bx, by, bz, inv_scale) - geq_dev(q, rho, rI, ux, uy, uz, inv_scale);
+    {
+        float e = d0;
+        if (ex(q)) e += mxx;
+        if (ey(q)) e += myy;
+        if (ez(q)) e += mzz;
+        if (ex(q) * ey(q)) e += ex(q) * ey(q) * mxy;
+        if (ex(q) * ez(q)) e += ex(q) * ez(q) * mxz;
+        if (ey(q) * ez(q)) e += ey(q) * ez(q) * myz;
+        if (ex(q)) e += ex(q) * vx;
+        if (ey(q)) e += ey(q) * vy;
+        if (ez(q)) e += ez(q) * vz;
+        G[q] = fmaf(wf(q), e, G[q]);
+    }
 }
 
 __device__ __forceinline__ void store_moments(const float (&G)[Q], float4* out)
