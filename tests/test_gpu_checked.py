@@ -1,6 +1,7 @@
 """The bounds-checked library (liblbm_b200_check.so, NLOS_LBM_CHECK=1) on the
 GPU: its self-test trips exactly one check, and the forward (FP32, FP16 warp
-pipelines, register-held FP16), scheme-A and adjoint kernels run the parity
+pipelines, register-held FP16), scheme-A (03, and 01 with its blend sponge,
+periodic z and initial density) and adjoint kernels run the parity
 scenarios without a single out-of-range index, with the same results as the
 product library.  The checked library runs in a child process (a process
 loads one of the two libraries)."""
@@ -38,6 +39,7 @@ runs = {
     "fp16_city": scenarios.scenario("city_small", storage=abi.LBM_STORE_F16, f16_scale=1e3),
     "fp16_wide": tv.wide_box(),
     "scheme_a": scenarios.family_a("doppler_a", steps=20),
+    "scheme_a_01": scenarios.scattering_a(steps=20),
 }
 for name, s in runs.items():
     for variant in ((None, "4") if name.startswith("fp16") else (None,)):
@@ -45,6 +47,8 @@ for name, s in runs.items():
             os.environ["NLOS_LBM_STEP_VARIANT"] = variant
         g = Solver(s["cfg"], s["sources"], s["probes"], triangles=s.get("triangles"), mask=s.get("mask"))
         os.environ.pop("NLOS_LBM_STEP_VARIANT", None)
+        if s.get("rho0") is not None:
+            g.set_density(s["rho0"])
         g.step(min(s["steps"], 60))
         key = name + ("_v" + variant if variant else "")
         out[key] = {"status": g.check_status(), "probes": g.get_probes().tolist()}
@@ -65,10 +69,13 @@ def _product_runs():
         "fp16_city": scenarios.scenario("city_small", storage=abi.LBM_STORE_F16, f16_scale=1e3),
         "fp16_wide": tv.wide_box(),
         "scheme_a": scenarios.family_a("doppler_a", steps=20),
+        "scheme_a_01": scenarios.scattering_a(steps=20),
     }
     out = {}
     for name, s in runs.items():
         g = Solver(s["cfg"], s["sources"], s["probes"], triangles=s.get("triangles"), mask=s.get("mask"))
+        if s.get("rho0") is not None:
+            g.set_density(s["rho0"])
         g.step(min(s["steps"], 60))
         out[name] = g.get_probes()
     a = scenarios.adjoint_scenario(nx=32, ny=24, nz=16, steps=30, nprobe=6)
@@ -89,7 +96,7 @@ def test_checked_build_finds_no_out_of_range_index(gpu):
         if key not in ("selftest", "after_selftest"):
             assert v["status"] == [0, 0], (key, v["status"])
     ref = _product_runs()
-    for name in ("fp32_city", "fp16_city", "fp16_wide", "scheme_a"):
+    for name in ("fp32_city", "fp16_city", "fp16_wide", "scheme_a", "scheme_a_01"):
         assert np.array_equal(np.asarray(got[name]["probes"]), ref[name]), name
     assert got["adjoint"]["loss"] == ref["adjoint"][0]
     assert np.array_equal(np.asarray(got["adjoint"]["grad_pos"]), ref["adjoint"][1])
