@@ -77,6 +77,7 @@ struct lbm_handle
     int stl_status = LBM_OK;
     std::vector<uint8_t> mask_override;
     int mo_dims[3] = {0, 0, 0};
+    std::vector<double> blend_xy, field_xy;   // scheme A: caller's per-column fields (lbm_set_*_xy)
 
     std::vector<SourceState> srcs;
     std::vector<double> probe_xyz;
@@ -504,6 +505,13 @@ int upload_scheme_a_profiles(lbm_handle* h)
             }
             prof.push_back(sgv > 1e-6 ? (float)sgv : 0.0f);
         }
+    // the caller's per-column fields
+    if (!h->blend_xy.empty() && !c.sponge_blend)
+        return h->fail(LBM_ERR_BAD_CONFIG, "lbm_set_blend_xy needs sponge_blend = 1");
+    const size_t off_sg_xy = prof.size();
+    for (double v : h->blend_xy) prof.push_back(v > 1e-6 ? (float)v : 0.0f);
+    const size_t off_fld_xy = prof.size();
+    for (double v : h->field_xy) prof.push_back((float)v);
     if (!h->a_prof) CK(cudaMalloc(&h->a_prof, prof.size() * sizeof(float)), "scheme A profiles");
     CK(cudaMemcpyAsync(h->a_prof, prof.data(), prof.size() * sizeof(float), cudaMemcpyHostToDevice, h->stream),
        "scheme A profiles");
@@ -521,8 +529,16 @@ int upload_scheme_a_profiles(lbm_handle* h)
     b.sg_z = b.sg_y + L.ny;
     b.blend = c.sponge_blend ? 1 : 0;
     b.zper = c.face_bc[LBM_FACE_ZLO] == LBM_BC_PERIODIC ? 1 : 0;
+    b.sg_xy = h->blend_xy.empty() ? nullptr : h->a_prof + off_sg_xy;
+    b.fld_xy = h->field_xy.empty() ? nullptr : h->a_prof + off_fld_xy;
+    b.nx_col = L.nx;
+    b.ny_col = L.ny;
     b.om_bulk = (float)(1.0 / c.tau);
     b.field_mode = fs ? fs->field_mode : -1;
+    // a pre-step source enters the step that computes its arrivals, one step
+    // ahead: nothing carries a value at t = 0 into the initial state
+    if (fs && fs->field_mode == LBM_FIELD_PRE && source_entry(h->srcs[(size_t)fsi], 0.0, h->dt).mass != 0.0)
+        return h->fail(LBM_ERR_UNSUPPORTED, "a LBM_FIELD_PRE source must be 0 at t = 0");
     b.src_index = fsi;
     b.nsrc = (int)h->srcs.size();
     double u2 = 0.0;
@@ -667,6 +683,32 @@ extern "C" int lbm_set_geometry_triangles(lbm_handle* h, const float* tris, int 
     return LBM_OK;
 }
 
+namespace {
+int set_columns(lbm_handle* h, const double* v, long count, std::vector<double>& out, const char* what)
+{
+    if (!h || !v) return LBM_ERR_INVALID_ARGUMENT;
+    if (h->inited) return h->fail(LBM_ERR_STATE, "per-column fields are set before lbm_init");
+    if (h->cfg.scheme != LBM_SCHEME_A) return h->fail(LBM_ERR_UNSUPPORTED, "per-column fields are scheme A");
+    int nx = 0, ny = 0, nz = 0;
+    grid_size(h->cfg, nx, ny, nz);
+    if (count != (long)nx * ny) return h->fail(LBM_ERR_INVALID_ARGUMENT, what);
+    out.assign(v, v + count);
+    return LBM_OK;
+}
+}  // namespace
+
+extern "C" int lbm_set_blend_xy(lbm_handle* h, const double* s_xy, long count)
+{
+    if (!h) return LBM_ERR_INVALID_ARGUMENT;
+    return set_columns(h, s_xy, count, h->blend_xy, "blend field size mismatch");
+}
+
+extern "C" int lbm_set_field_weights_xy(lbm_handle* h, const double* w_xy, long count)
+{
+    if (!h) return LBM_ERR_INVALID_ARGUMENT;
+    return set_columns(h, w_xy, count, h->field_xy, "weight field size mismatch");
+}
+
 extern "C" int lbm_set_mask(lbm_handle* h, const uint8_t* mask, int nx_t, int ny_t, int nz_t)
 {
     if (!h || !mask || nx_t < 3 || ny_t < 3 || nz_t < 3) return LBM_ERR_INVALID_ARGUMENT;
@@ -693,7 +735,7 @@ extern "C" int lbm_add_source(lbm_handle* h, const lbm_source* s)
             return h->fail(LBM_ERR_UNSUPPORTED, "scheme A takes field sources (LBM_INJECT_FIELD) only");
         if (!h->srcs.empty()) return h->fail(LBM_ERR_UNSUPPORTED, "scheme A takes one field source");
         if (!(s->sigma_cells > 0)) return h->fail(LBM_ERR_INVALID_ARGUMENT, "field source needs sigma_cells > 0");
-        if (s->field_mode != LBM_FIELD_DST && s->field_mode != LBM_FIELD_FORCE)
+        if (s->field_mode != LBM_FIELD_DST && s->field_mode != LBM_FIELD_FORCE && s->field_mode != LBM_FIELD_PRE)
             return h->fail(LBM_ERR_INVALID_ARGUMENT, "unknown field_mode");
     }
     else if (s->injection == LBM_INJECT_FIELD)

@@ -179,7 +179,7 @@ struct SchemeAArgs
     const float* fld_x;        // source weight factors, halo-inclusive index 0..n+1;
     const float* fld_y;        //   weight(i,j,k) = fld_x[i] fld_y[j] fld_z[k]
     const float* fld_z;
-    int field_mode;            // -1: no field source, 0: LBM_FIELD_DST, 1: LBM_FIELD_FORCE
+    int field_mode;            // -1: no field source, 0: LBM_FIELD_DST, 1: LBM_FIELD_FORCE, 2: LBM_FIELD_PRE
     int src_index;             // which source of the schedule is the field source
     int nsrc;
     float flow[3];             // background velocity u0 (lattice units)
@@ -196,6 +196,9 @@ struct SchemeAArgs
     const float* sg_z;         //   of the three, 0 outside the layer
     int blend;                 // 1: populations that left a fluid cell are blended, (1-s) f + s w_q
     int zper;                  // 1: periodic z, halo planes 0 / nz+1 repeat planes nz / 1
+    const float* sg_xy;        // nullptr or per-column blend strengths [(j-1) nx + (i-1)] (max with sg_*)
+    const float* fld_xy;       // nullptr or per-column source weights, replacing fld_x fld_y fld_z
+    int nx_col, ny_col;        // column grid of sg_xy / fld_xy (nx, ny)
 };
 
 // ---- launchers (kernels.cu) ----------------------------------------------

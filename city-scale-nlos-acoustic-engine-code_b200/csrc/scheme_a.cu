@@ -43,15 +43,24 @@ __device__ __forceinline__ float cell_omega(const SchemeAArgs& b, int i, int j, 
     return fminf(b.om_x[i - 1], fminf(b.om_y[j - 1], b.om_z[k - 1]));
 }
 
+// source weight of cell (i, j, k), halo-inclusive (a halo cell takes its
+// nearest column's per-column weight)
 __device__ __forceinline__ float field_weight(const SchemeAArgs& b, int i, int j, int k)
 {
+    if (b.fld_xy)
+    {
+        const int ci = min(max(i, 1), b.nx_col) - 1, cj = min(max(j, 1), b.ny_col) - 1;
+        return b.fld_xy[cj * b.nx_col + ci];
+    }
     return b.fld_x[i] * b.fld_y[j] * b.fld_z[k];
 }
 
-// strength of the destination blend at interior cell (i, j, k) (01:207-225)
+// strength of the destination blend at interior cell (i, j, k) (01:207-225,
+// 04:177-209)
 __device__ __forceinline__ float cell_blend(const SchemeAArgs& b, int i, int j, int k)
 {
-    return fmaxf(b.sg_x[i - 1], fmaxf(b.sg_y[j - 1], b.sg_z[k - 1]));
+    const float s = fmaxf(b.sg_x[i - 1], fmaxf(b.sg_y[j - 1], b.sg_z[k - 1]));
+    return b.sg_xy ? fmaxf(s, b.sg_xy[(j - 1) * b.nx_col + (i - 1)]) : s;
 }
 
 // BGK of one cell on deviations d = f - feq(1, u0): with rho' = sum d,
@@ -228,6 +237,15 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step_a(const float* __restrict_
             if (!((lk0 >> q) & 1u)) G[q].x = v.x;
             if (!((lk1 >> q) & 1u)) G[q].y = v.y;
         }
+    }
+    // pre-step source of the next step (04:212-235): every population of the
+    // cell, before it is bounced back or collided next step
+    if (b.field_mode == 2)
+    {
+        const float m = field_mass(b, 1);
+        const float2 S = make_float2(m * field_weight(b, c0 + 1, j, k), has1 ? m * field_weight(b, c0 + 2, j, k) : 0.f);
+#pragma unroll
+        for (int q = 0; q < Q; ++q) G[q] = fma2(f2(wf(q)), S, G[q]);
     }
     // pre-collision values for the SOLID neighbours' slots: the next step
     // pulls direction q from the SOLID cell dst - e_q and must read this

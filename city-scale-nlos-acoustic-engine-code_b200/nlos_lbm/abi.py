@@ -30,7 +30,7 @@ LBM_NOALLOC_MAX_CELLS = 8388608
 
 LBM_BC_NSCBC, LBM_BC_REST, LBM_BC_WALL, LBM_BC_COPY, LBM_BC_PERIODIC = 0, 1, 2, 3, 4
 LBM_SCHEME_B, LBM_SCHEME_A = 0, 1
-LBM_FIELD_DST, LBM_FIELD_FORCE = 0, 1
+LBM_FIELD_DST, LBM_FIELD_FORCE, LBM_FIELD_PRE = 0, 1, 2
 FACE_XLO, FACE_XHI, FACE_YLO, FACE_YHI, FACE_ZLO, FACE_ZHI = range(6)
 LBM_STORE_F32, LBM_STORE_F16 = 0, 1
 LBM_WAVE_GAUSS, LBM_WAVE_SINE, LBM_WAVE_RICKER, LBM_WAVE_TABLE = 0, 1, 2, 3
@@ -197,6 +197,8 @@ def bind_product(lib):
         "lbm_get_f": (ctypes.c_int, [P, c_double_p, ctypes.c_long]),
         "lbm_set_f": (ctypes.c_int, [P, c_double_p, ctypes.c_long]),
         "lbm_set_density": (ctypes.c_int, [P, c_double_p, ctypes.c_long]),
+        "lbm_set_blend_xy": (ctypes.c_int, [P, c_double_p, ctypes.c_long]),
+        "lbm_set_field_weights_xy": (ctypes.c_int, [P, c_double_p, ctypes.c_long]),
         "lbm_get_mask": (ctypes.c_int, [P, c_uint8_p, ctypes.c_long]),
         "lbm_set_kernel_timing": (ctypes.c_int, [P, ctypes.c_int]),
         "lbm_get_kernel_time": (ctypes.c_int, [P, c_double_p, c_long_p]),

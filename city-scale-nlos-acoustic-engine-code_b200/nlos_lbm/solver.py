@@ -46,7 +46,7 @@ class Solver:
     """One solver handle: config + geometry + sources + probes -> device state."""
 
     def __init__(self, cfg, sources=(), probes=None, triangles=None, stl=None, stl_offset=(0.0, 0.0, 0.0),
-                 mask=None):
+                 mask=None, blend_xy=None, field_xy=None):
         self.lib = library()
         self.cfg = cfg
         h = ctypes.c_void_p()
@@ -68,6 +68,12 @@ class Solver:
             ny = int(round((cfg.y_max - cfg.y_min) / cfg.dx)) + 2
             nz = int(round((cfg.z_max - cfg.z_min) / cfg.dx)) + 2
             self._check(self.lib.lbm_set_mask(self.h, _ptr(m, abi.c_uint8_p), nx, ny, nz), "lbm_set_mask")
+        # scheme A: per-column blend strengths and source weights (nx*ny, x fastest)
+        for arr, fn, what in ((blend_xy, self.lib.lbm_set_blend_xy, "lbm_set_blend_xy"),
+                              (field_xy, self.lib.lbm_set_field_weights_xy, "lbm_set_field_weights_xy")):
+            if arr is not None:
+                a = np.ascontiguousarray(arr, dtype=np.float64).ravel()
+                self._check(fn(self.h, _ptr(a), a.size), what)
         for s in sources:
             self._check(self.lib.lbm_add_source(self.h, ctypes.byref(s)), "lbm_add_source")
         self.nprobe = 0

@@ -95,8 +95,11 @@ enum
 {
     LBM_FIELD_DST = 0,   /* w_q * weight(dst) * val(t) * dt added to every population streamed
                             from a fluid cell, after the collision (02:373, 02:405) */
-    LBM_FIELD_FORCE = 1  /* forcing at the cell being collided: w_q * weight * val(t) * dt
+    LBM_FIELD_FORCE = 1, /* forcing at the cell being collided: w_q * weight * val(t) * dt
                             * (1 + 3 c_q.flow) * (1 - 1/(2 tau)) (03:74-78, 03:424-435) */
+    LBM_FIELD_PRE = 2    /* w_q * weight * val(t) * dt added to every population of every
+                            fluid cell before the step at time t (apply_source 04:212-235);
+                            val(0) must be 0 */
 };
 
 /* Solver configuration: the member fields of LBMSolver (06:244-268), the
@@ -208,6 +211,15 @@ int lbm_set_geometry_triangles(lbm_handle* h, const float* tris, int ntris, doub
 /* Override the voxelised mask: nx_t*ny_t*nz_t bytes (0 FLUID, 1 SOLID) in the
  * reference's halo-inclusive order i + j*nx_t + k*nx_t*ny_t (06:206-209). */
 int lbm_set_mask(lbm_handle* h, const uint8_t* mask, int nx_t, int ny_t, int nz_t);
+/* Scheme A, before lbm_init: per-column (x, y) fields that are the same at
+ * every height, count = nx*ny, x fastest (both programs that use them are
+ * z-invariant: 01 and 04).  Blend strengths s of the destination blend
+ * (sponge_blend = 1; a cell takes the larger of this and the face profile;
+ * s <= 1e-6 is no blend), e.g. 04's radial layer (04:177-209).  Weights of
+ * the field source, replacing its Gaussian, e.g. 04's line source with its
+ * cutoff (04:212-235). */
+int lbm_set_blend_xy(lbm_handle* h, const double* s_xy, long count);
+int lbm_set_field_weights_xy(lbm_handle* h, const double* w_xy, long count);
 
 /* The mask lbm_init builds for this config and triangle set (init_domain
  * 06:453-532), computed on the host; needs no device.  n3_halo receives

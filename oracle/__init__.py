@@ -65,6 +65,8 @@ def _load():
             "orc_get_f": (None, [P, _dp]),
             "orc_set_f": (None, [P, _dp]),
             "orc_set_density": (None, [P, _dp]),
+            "orc_set_blend_xy": (ctypes.c_int, [P, _dp]),
+            "orc_set_field_xy": (ctypes.c_int, [P, _dp]),
             "orc_get_mask": (None, [P, abi.c_uint8_p]),
             "orc_get_rho": (None, [P, _dp]),
             "orc_get_sponge": (None, [P, _dp]),
@@ -115,13 +117,17 @@ class OracleSolver:
     """FP64 restatement with the same call surface as the reference LBMSolver."""
 
     def __init__(self, cfg, sources=(), probes=None, triangles=None, stl=None, stl_offset=(0.0, 0.0, 0.0),
-                 mask=None, threads=None):
+                 mask=None, threads=None, blend_xy=None, field_xy=None):
         self.lib = _load()
         if threads:
             self.lib.orc_set_threads(int(threads))
         self.cfg = cfg
         self.h = self.lib.orc_create(ctypes.byref(cfg))
         self._keep = []
+        for arr, fn in ((blend_xy, self.lib.orc_set_blend_xy), (field_xy, self.lib.orc_set_field_xy)):
+            if arr is not None:
+                a = np.ascontiguousarray(arr, dtype=np.float64).ravel()
+                fn(self.h, _ptr(a))
         if stl is not None:
             self.stl_status = self.lib.orc_set_geometry_stl(self.h, stl.encode(), 1.0, *stl_offset)
         elif triangles is not None:
@@ -245,7 +251,8 @@ def refa_available(which):
 
 class RefASolver:
     """An unmodified family-A reference program (01 acoustic scattering, 02
-    Lloyd's mirror or 03 Doppler) through oracle/ref_harness_a.cpp: set-up, then steps of
+    Lloyd's mirror, 03 Doppler or 04 scalability benchmark) through
+    oracle/ref_harness_a.cpp: set-up, then steps of [apply_source() (04)] +
     exchange_halos() + step(); fields in the reference's own layout."""
 
     def __init__(self, which, **params):

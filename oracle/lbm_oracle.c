@@ -56,6 +56,7 @@ struct orc_handle
     double dt;
     double *f_curr, *f_next, *rho, *sponge, *gH;
     double *tau_a, *field_a;   /* scheme A: per-cell tau (ramp sponge) and source weight */
+    double *blend_xy, *field_xy;   /* scheme A: caller's per-column blend strengths, source weights */
     unsigned char* mask;
     int mask_override;
     /* geometry (GeometryEngine 06:60-193) */
@@ -117,7 +118,7 @@ void orc_destroy(orc_handle* h)
 {
     if (!h) return;
     free(h->f_curr); free(h->f_next); free(h->rho); free(h->sponge); free(h->gH); free(h->mask);
-    free(h->tau_a); free(h->field_a);
+    free(h->tau_a); free(h->field_a); free(h->blend_xy); free(h->field_xy);
     free(h->tris); free(h->bin_start); free(h->bin_items);
     for (int i = 0; i < h->nsrc; ++i) free(h->srcs[i].table);
     free(h->srcs); free(h->probe_xyz); free(h->probe_idx); free(h->series);
@@ -262,6 +263,29 @@ int orc_set_geometry_stl(orc_handle* h, const char* path, double scale, double s
     orc_set_geometry_triangles(h, v, (int)n, scale, sx, sy, sz);
     free(v);
     return LBM_OK;
+}
+
+static double* copy_xy(const orc_handle* h, const double* v)
+{
+    const lbm_config* c = &h->cfg;
+    const size_t n = (size_t)(int)((c->x_max - c->x_min) / c->dx + 0.5) * (size_t)(int)((c->y_max - c->y_min) / c->dx + 0.5);
+    double* out = (double*)malloc(n * sizeof(double));
+    if (out) memcpy(out, v, n * sizeof(double));
+    return out;
+}
+
+int orc_set_blend_xy(orc_handle* h, const double* s_xy)
+{
+    free(h->blend_xy);
+    h->blend_xy = copy_xy(h, s_xy);
+    return h->blend_xy ? LBM_OK : LBM_ERR_OUT_OF_MEMORY;
+}
+
+int orc_set_field_xy(orc_handle* h, const double* w_xy)
+{
+    free(h->field_xy);
+    h->field_xy = copy_xy(h, w_xy);
+    return h->field_xy ? LBM_OK : LBM_ERR_OUT_OF_MEMORY;
 }
 
 int orc_set_mask(orc_handle* h, const unsigned char* mask)
@@ -428,6 +452,8 @@ static void init_scheme_a(orc_handle* h)
     const lbm_config* c = &h->cfg;
     const unsigned sf = c->sponge_faces;
     const int w = (int)c->sponge_width;
+    free(h->tau_a);
+    free(h->field_a);   /* a second orc_init (after orc_set_mask) rebuilds both */
     h->tau_a = (double*)malloc(h->Nloc * sizeof(double));
     h->field_a = (double*)calloc(h->Nloc, sizeof(double));
     const src_t* fs = NULL;
@@ -462,6 +488,10 @@ static void init_scheme_a(orc_handle* h)
                     const double z = c->z_min + (gz + 0.5) * c->dx - fs->s.sz;
                     h->field_a[idx] = exp(-(x * x + y * y + z * z) / (2.0 * sig * sig));
                 }
+                /* a caller's per-column weights (nearest column for halo cells) */
+                const int cx = gx < 0 ? 0 : (gx >= h->nx ? h->nx - 1 : gx);
+                const int cy = gy < 0 ? 0 : (gy >= h->ny ? h->ny - 1 : gy);
+                if (h->field_xy) h->field_a[idx] = h->field_xy[(size_t)cy * h->nx + cx];
                 for (int q = 0; q < Q; ++q) h->f_curr[idx * Q + q] = feq_a(q, 1.0, c->flow[0], c->flow[1], c->flow[2]);
                 if (c->sponge_blend)
                 {
@@ -486,6 +516,7 @@ static void init_scheme_a(orc_handle* h)
                         const double r_ratio = dist_max / th;
                         sig = c->sponge_strength * r_ratio * r_ratio;
                     }
+                    if (h->blend_xy && h->blend_xy[(size_t)cy * h->nx + cx] > sig) sig = h->blend_xy[(size_t)cy * h->nx + cx];
                     h->sponge[idx] = sig;
                 }
             }
@@ -542,7 +573,22 @@ static void step_a(orc_handle* h, long s)
         if (h->srcs[i].s.injection == LBM_INJECT_FIELD) fs = &h->srcs[i];
     const double mass = fs ? source_value(h, fs, t) * h->dt * fs->s.gain : 0.0;
     const int force = fs && fs->s.field_mode == LBM_FIELD_FORCE;
+    const int pre = fs && fs->s.field_mode == LBM_FIELD_PRE;
     const double fx = c->flow[0], fy = c->flow[1], fz = c->flow[2];
+    if (pre)
+    {
+        /* 04:212-235: every population of every interior fluid cell, before the
+           halo exchange and the step */
+        #pragma omp parallel for collapse(2)
+        for (int k = 1; k <= h->nz; ++k)
+            for (int j = 1; j <= h->ny; ++j)
+                for (int i = 1; i <= h->nx; ++i)
+                {
+                    const size_t idx = loc(h, i, j, k);
+                    if (h->mask[idx] == SOLID) continue;
+                    for (int q = 0; q < Q; ++q) h->f_curr[idx * Q + q] += W[q] * (h->field_a[idx] * mass);
+                }
+    }
     halos_a(h);
     const int nx = h->nx, ny = h->ny, nz = h->nz;
     #pragma omp parallel for collapse(2)
@@ -588,7 +634,7 @@ static void step_a(orc_handle* h, long s)
                             const double cu = EXA[q] * fx + EYA[q] * fy + EZA[q] * fz;
                             fn += W[q] * (h->field_a[src] * mass) * (1.0 + 3.0 * cu) * (1.0 - 0.5 / tau_s);
                         }
-                        else if (fs)
+                        else if (fs && !pre)
                         {
                             fn += W[q] * (h->field_a[dst] * mass);
                         }

@@ -32,6 +32,10 @@ int orc_set_geometry_triangles(orc_handle* h, const float* tris, int ntris, doub
                                double sy, double sz);
 int orc_set_geometry_stl(orc_handle* h, const char* path, double scale, double sx, double sy, double sz);
 int orc_set_mask(orc_handle* h, const unsigned char* mask);
+/* Scheme A, before orc_init: per-column blend strengths and field-source
+ * weights (nx*ny, x fastest), as lbm_set_blend_xy / lbm_set_field_weights_xy. */
+int orc_set_blend_xy(orc_handle* h, const double* s_xy);
+int orc_set_field_xy(orc_handle* h, const double* w_xy);
 int orc_add_source(orc_handle* h, const lbm_source* src);
 int orc_set_probes(orc_handle* h, const double* xyz, int n);
 int orc_init(orc_handle* h);

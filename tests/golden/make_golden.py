@@ -9,10 +9,11 @@ oracle/_ref/libref06.so or libref08.so (the reference's own apply_source /
 exchange_halos / step_collision_bgk, 06:1077-1092) and stores the probe
 series, the voxelised mask, a window of the final populations and two FP64
 checksums of the whole population array.  The family-A fixtures (lloyd_a,
-doppler_a, scattering_a) run 02_lloyds_mirror.cpp / 03_doppler_effect.cpp /
-01_acoustic_scattering.cpp through oracle/_ref/libref02.so / libref03.so /
-libref01.so (exchange_halos + step, 02:543-546, 03:540-541, 01:527-528) and
-store the final density field.  `python tests/golden/make_golden.py NAME ...`
+doppler_a, scattering_a, hpc_a) run 02_lloyds_mirror.cpp / 03_doppler_effect.cpp /
+01_acoustic_scattering.cpp / 04_hpc_scalability.cpp through oracle/_ref/libref02.so /
+libref03.so / libref01.so / libref04.so (exchange_halos + step, 02:543-546,
+03:540-541, 01:527-528; 04 with apply_source first, 04:383-389) and store the
+final density field.  `python tests/golden/make_golden.py NAME ...`
 regenerates only the named fixtures.  The fixtures pin the oracle (and,
 within tolerance, the CUDA solver) to the reference on machines where the
 reference itself is absent.
@@ -77,11 +78,11 @@ def reference_run(name):
                 f_checksums=checksums(f), dims_halo=np.array(ref.dims_halo), steps=np.array(sc["steps"]))
 
 
-FAMILY_A = ("lloyd_a", "doppler_a", "scattering_a")
+FAMILY_A = ("lloyd_a", "doppler_a", "scattering_a", "hpc_a")
 
 
 def reference_run_a(name):
-    """A family-A program (01, 02 or 03) on its reduced scenario: rho - 1 of every
+    """A family-A program (01, 02, 03 or 04) on its reduced scenario: rho - 1 of every
     interior cell after the scenario's steps (SOLID cells as 0), its tau and
     source-weight fields and the mask."""
     sc = scenarios.family_a(name)

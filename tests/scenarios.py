@@ -221,7 +221,55 @@ def family_a(name, n=40, steps=60):
         return dict(cfg=cfg, sources=[src], probes=probes, mask=None, steps=steps, ref="03", ref_params=ref_params)
     if name == "scattering_a":
         return scattering_a(steps=steps)
+    if name == "hpc_a":
+        return hpc_a(steps=steps)
     raise KeyError(name)
+
+
+def hpc_columns(dx, lo=-13.0, n=None, cyl_r=4.0, r0=10.0, th=3.0, strength=0.5, src_y=-6.0, b=2.0):
+    """04_hpc_scalability.cpp's z-invariant set-up on an n x n column grid
+    from lo at dx, with 04's own cell-centre expression lo + g dx + dx/2
+    (04:187-188): SOLID cylinder r < cyl_r (04:191-194), radial blend layer
+    0.5 min((r - 10)/3, 1)^2 beyond r = 10 (04:198-203), line-source weights
+    exp(-ln2 d^2 / b) for d^2 = x^2 + (y - src_y)^2 <= 36 (04:220-224).
+    Returns (solid[ny+2, nx+2] halo-inclusive, blend[ny, nx], weight[ny, nx])."""
+    g = np.arange(-1, n + 1)
+    c = lo + g * dx + 0.5 * dx
+    x, y = c[None, :], c[:, None]
+    r = np.sqrt(x * x + y * y)
+    solid = r < cyl_r
+    ratio = np.minimum((r - r0) / th, 1.0)
+    blend = np.where(~solid & (r > r0), strength * ratio * ratio, 0.0)
+    d2 = x * x + (y - src_y) * (y - src_y)
+    weight = np.where(d2 > 36.0, 0.0, np.exp(-np.log(2.0) * d2 / b))
+    return solid, blend[1:-1, 1:-1], weight[1:-1, 1:-1]
+
+
+def hpc_a(steps=40, dx=0.5, half=13.0):
+    """04_hpc_scalability.cpp (the reference's scaling benchmark) on a reduced
+    grid: [-13, 13]^3 at dx 0.5 instead of 0.125 (04:52-54, 04:21); tau 0.51
+    (04:301); periodic z and rest x/y halos (04:51, 04:237-297); the radial
+    blend layer and the line source of hpc_columns, a sine of amplitude 0.01
+    and angular frequency pi/15 added before each step (04:65-67, 04:212-235);
+    dt = 0.577350269 dx (04:22-26).  Probes at cell centres in the fluid."""
+    n = int(2 * half / dx + 0.5)
+    cfg = abi.reference_config(x_min=-half, x_max=half, y_min=-half, y_max=half, z_min=-half, z_max=half, dx=dx,
+                               c_phys=1.0, tau=0.51, use_geometry=0,
+                               face_bc=(abi.LBM_BC_REST,) * 4 + (abi.LBM_BC_PERIODIC,) * 2,
+                               sponge_faces=0, sponge_width=0.0, sponge_blend=1, sky_z=1e30,
+                               scheme=abi.LBM_SCHEME_A, tau_sponge_max=0.0, dt=0.577350269 * dx)
+    solid, blend, weight = hpc_columns(dx, -half, n)
+    mask = np.broadcast_to(solid, (n + 2,) + solid.shape).astype(np.uint8)
+    src = abi.reference_source(sx=0.0, sy=-6.0, sz=0.0, ex=0.0, ey=-6.0, ez=0.0, amp=0.01, freq=1.0 / 30.0,
+                               waveform=abi.LBM_WAVE_SINE, injection=abi.LBM_INJECT_FIELD, sigma_cells=1.0,
+                               field_mode=abi.LBM_FIELD_PRE)
+    cell = lambda v: -half + (np.floor((v + half) / dx) + 0.5) * dx
+    pts = [(0.0, -6.0), (6.0, 0.0), (-6.0, 0.0), (0.0, 7.0), (9.0, 9.0)]
+    zc = -half + (n // 2 + 0.5) * dx
+    probes = np.array([(cell(px), cell(py), zc) for px, py in pts])
+    ref_params = dict(x_min=-half, x_max=half, y_min=-half, y_max=half, z_min=-half, z_max=half, dx=dx, amp=0.01)
+    return dict(cfg=cfg, sources=[src], probes=probes, mask=np.ascontiguousarray(mask).ravel(), blend_xy=blend.ravel(),
+                field_xy=weight.ravel(), steps=steps, ref="04", ref_params=ref_params)
 
 
 def scattering_a(steps=60, dx=0.1, x=(-3.0, 6.0), y=(-3.0, 3.0), z=(-0.2, 0.2), amp=0.01):

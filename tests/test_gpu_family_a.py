@@ -7,6 +7,7 @@ Tolerances: FP32 deviation storage against FP64, probe (density) series
 relative L2 <= 1e-5 and field max error <= 1e-5 of the field's largest
 deviation, the FP32 bars of the scheme-B parity tests.
 """
+import ctypes
 import os
 
 import numpy as np
@@ -25,20 +26,22 @@ GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
 
 def _solver(sc, **kw):
-    g = Solver(sc["cfg"], sc["sources"], sc["probes"], mask=sc["mask"], **kw)
+    g = Solver(sc["cfg"], sc["sources"], sc["probes"], mask=sc["mask"], blend_xy=sc.get("blend_xy"),
+               field_xy=sc.get("field_xy"), **kw)
     if sc.get("rho0") is not None:
         g.set_density(sc["rho0"])
     return g
 
 
 def _oracle(sc):
-    o = OracleSolver(sc["cfg"], sc["sources"], sc["probes"], mask=sc["mask"])
+    o = OracleSolver(sc["cfg"], sc["sources"], sc["probes"], mask=sc["mask"], blend_xy=sc.get("blend_xy"),
+                     field_xy=sc.get("field_xy"))
     if sc.get("rho0") is not None:
         o.set_density(sc["rho0"])
     return o
 
 
-@pytest.mark.parametrize("name", ["lloyd_a", "doppler_a", "scattering_a"])
+@pytest.mark.parametrize("name", ["lloyd_a", "doppler_a", "scattering_a", "hpc_a"])
 def test_scheme_a_matches_oracle(name, gpu):
     sc = scenarios.family_a(name)
     g = _solver(sc)
@@ -57,7 +60,7 @@ def test_scheme_a_matches_oracle(name, gpu):
     assert np.max(np.abs(fg - fo)) <= FIELD_TOL * np.max(np.abs(fo))
 
 
-@pytest.mark.parametrize("name", ["lloyd_a", "doppler_a", "scattering_a"])
+@pytest.mark.parametrize("name", ["lloyd_a", "doppler_a", "scattering_a", "hpc_a"])
 def test_scheme_a_matches_reference_fixture(name, gpu):
     path = os.path.join(GOLDEN, name + ".npz")
     gold = np.load(path)
@@ -189,6 +192,46 @@ def test_set_density_rules(gpu):
     lat = Solver(scenarios.lattice_config(16, 16, 8, 0.52, use_geometry=0), [], None)
     with pytest.raises(LBMError) as e:
         lat.set_density(np.zeros(16 * 16 * 8))
+    assert e.value.status == abi.LBM_ERR_UNSUPPORTED
+
+
+def test_pre_step_source_direct_calls_equal_batched_steps(gpu):
+    sc = scenarios.family_a("hpc_a", steps=12)
+    a = _solver(sc)
+    a.step(sc["steps"])
+    b = _solver(sc)
+    for s in range(sc["steps"]):
+        b.step_collision_bgk()
+        b.record_probes()
+    assert np.array_equal(a.get_probes(), b.get_probes())
+    assert np.array_equal(a.get_rho(), b.get_rho())
+
+
+def test_column_field_rules(gpu):
+    sc = scenarios.family_a("hpc_a", steps=2)
+    n = 52
+    with pytest.raises(LBMError) as e:                      # count
+        Solver(sc["cfg"], sc["sources"], None, mask=sc["mask"], blend_xy=np.zeros(n * n - 1))
+    assert e.value.status == abi.LBM_ERR_INVALID_ARGUMENT
+    lat = scenarios.lattice_config(16, 16, 8, 0.52, use_geometry=0)
+    with pytest.raises(LBMError) as e:                      # scheme B
+        Solver(lat, [], None, field_xy=np.zeros(16 * 16))
+    assert e.value.status == abi.LBM_ERR_UNSUPPORTED
+    c = sc["cfg"]
+    c.sponge_blend = 0
+    with pytest.raises(LBMError) as e:                      # blend strengths without the blend
+        Solver(c, sc["sources"], None, mask=sc["mask"], blend_xy=sc["blend_xy"])
+    assert e.value.status == abi.LBM_ERR_BAD_CONFIG
+    c.sponge_blend = 1
+    g = _solver(sc)
+    a = np.ascontiguousarray(sc["blend_xy"], dtype=np.float64)
+    assert g.lib.lbm_set_blend_xy(g.h, a.ctypes.data_as(abi.c_double_p), a.size) == abi.LBM_ERR_STATE   # after init
+    src = abi.LbmSource()
+    ctypes.pointer(src)[0] = sc["sources"][0]
+    src.waveform = abi.LBM_WAVE_GAUSS                     # nonzero at t = 0
+    src.t0, src.sigma_t = 0.0, 1.0
+    with pytest.raises(LBMError) as e:
+        Solver(c, [src], None, mask=sc["mask"], field_xy=sc["field_xy"], blend_xy=sc["blend_xy"])
     assert e.value.status == abi.LBM_ERR_UNSUPPORTED
 
 

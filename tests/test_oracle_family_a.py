@@ -1,10 +1,11 @@
 """The oracle's scheme-A (family 01-04) restatement against the unmodified
-01_acoustic_scattering.cpp, 02_lloyds_mirror.cpp and 03_doppler_effect.cpp
-(built by oracle/Makefile's
+01_acoustic_scattering.cpp, 02_lloyds_mirror.cpp, 03_doppler_effect.cpp and
+04_hpc_scalability.cpp (built by oracle/Makefile's
 `ref` target through oracle/ref_harness_a.cpp where the reference sources
 are present) and against the fixtures they produced (tests/golden, always).
 
-Measured agreement: 01 and 03 bit-identical; 02 within 1e-14 of the field's
+Measured agreement: 01 and 03 bit-identical; 04 within 2.4e-13 of the
+field's largest deviation (its source term is summed in another order); 02 within 1e-14 of the field's
 largest deviation, from the source weight written as exp(-r^2/(2 sigma^2))
 instead of 02's exp(-ln2 r^2/b) with the same width.  Bound: 1e-12.
 """
@@ -22,7 +23,8 @@ GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
 
 def _oracle_rho(sc):
-    o = OracleSolver(sc["cfg"], sc["sources"], sc["probes"], mask=sc["mask"])
+    o = OracleSolver(sc["cfg"], sc["sources"], sc["probes"], mask=sc["mask"], blend_xy=sc.get("blend_xy"),
+                     field_xy=sc.get("field_xy"))
     if sc.get("rho0") is not None:
         o.set_density(sc["rho0"])
     o.step(sc["steps"])
@@ -33,7 +35,7 @@ def _oracle_rho(sc):
     return o, rho
 
 
-@pytest.mark.parametrize("name", ["lloyd_a", "doppler_a", "scattering_a"])
+@pytest.mark.parametrize("name", ["lloyd_a", "doppler_a", "scattering_a", "hpc_a"])
 def test_oracle_matches_family_a_fixture(name):
     gold = np.load(os.path.join(GOLDEN, name + ".npz"))
     sc = scenarios.family_a(name, steps=int(gold["steps"]))
@@ -46,7 +48,7 @@ def test_oracle_matches_family_a_fixture(name):
     assert np.max(np.abs(rho - ref)) <= TOL * np.max(np.abs(ref))
 
 
-@pytest.mark.parametrize("name", ["lloyd_a", "doppler_a", "scattering_a"])
+@pytest.mark.parametrize("name", ["lloyd_a", "doppler_a", "scattering_a", "hpc_a"])
 def test_oracle_matches_family_a_reference(name):
     sc = scenarios.family_a(name, steps=25)
     if not oracle.refa_available(sc["ref"]):
@@ -58,7 +60,12 @@ def test_oracle_matches_family_a_reference(name):
     assert np.array_equal(mask, o.get_mask())
     assert np.max(np.abs(ref.get_tau()[fluid] - o.get_tau_a()[fluid])) <= 1e-15
     if sc["cfg"].sponge_blend:
-        assert np.max(np.abs(ref.get_sponge()[fluid] - o.get_sponge()[fluid])) <= 1e-15
+        # interior cells (04 also fills its halo cells, which are never updated)
+        nx, ny, nz = ref.dims_halo
+        inner = (slice(1, -1),) * 3
+        fi = fluid.reshape(nz, ny, nx)[inner]
+        sr, so = ref.get_sponge().reshape(nz, ny, nx)[inner], o.get_sponge().reshape(nz, ny, nx)[inner]
+        assert np.max(np.abs(sr[fi] - so[fi])) <= 1e-15
     ref.step(sc["steps"])
     nx, ny, nz = ref.dims_halo
     rr = ref.get_rho().reshape(nz, ny, nx)[1:-1, 1:-1, 1:-1] - 1.0
