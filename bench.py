@@ -144,7 +144,8 @@ def make_solver(name, storage, device):
     w = workloads.build(name, storage=storage)
     w["cfg"].device = device
     t0 = time.time()
-    s = nlos_lbm.Solver(w["cfg"], w["sources"], w["probes"], triangles=w["triangles"], mask=w.get("mask"))
+    s = nlos_lbm.Solver(w["cfg"], w["sources"], w["probes"], triangles=w["triangles"], mask=w.get("mask"),
+                        blend_xy=w.get("blend_xy"), field_xy=w.get("field_xy"))
     if w.get("rho0") is not None:
         s.set_density(w["rho0"])
     return s, w, time.time() - t0
@@ -284,17 +285,19 @@ def adjoint_measure(device, torch, reps=2, ckpt=(200, 0), workload="adjoint256",
 
 
 def family_a_cpu(name, seconds=5.0):
-    """The unmodified family-A reference program (01, 02 or 03 through
-    oracle/_ref, FP64, OpenMP on all host threads) on its own domain (01) or a
-    sub-domain of its own set-up (02, 03), in GLUPS; None where the harness
-    was not built."""
+    """The unmodified family-A reference program (01, 02, 03 or 04 through
+    oracle/_ref, FP64, OpenMP on all host threads) on its own domain (01, 04)
+    or a sub-domain of its own set-up (02, 03), in GLUPS; None where the
+    harness was not built."""
     import oracle
 
-    which = {"scattering_a": "01", "lloyd_a": "02", "doppler_a": "03"}[name]
+    which = {"scattering_a": "01", "lloyd_a": "02", "doppler_a": "03", "hpc_a": "04"}[name]
     if not oracle.refa_available(which):
         return None
     if which == "01":
         p = dict(x_min=-8.0, x_max=8.0, y_min=-8.0, y_max=8.0, z_min=-0.2, z_max=0.2, dx=0.05, amp=0.01)
+    elif which == "04":
+        p = dict(x_min=-13.0, x_max=13.0, y_min=-13.0, y_max=13.0, z_min=-13.0, z_max=13.0, dx=0.125, amp=0.01)
     elif which == "02":
         p = dict(x_min=-10.0, x_max=10.0, y_min=-10.0, y_max=10.0, z_min=-2.0, z_max=10.0, dx=0.2, amp=0.5,
                  b_param=2.0)
@@ -311,7 +314,7 @@ def family_a_cpu(name, seconds=5.0):
         t += time.perf_counter() - t0
         n += 2
     return {"value": nx * ny * nz * n / t / 1e9, "unit": "GLUPS", "cores": os.cpu_count(), "kind": "reference",
-            "sample": f"{nx}x{ny}x{nz} {'domain' if which == '01' else 'sub-domain'}, {n} steps of "
+            "sample": f"{nx}x{ny}x{nz} {'domain' if which in ('01', '04') else 'sub-domain'}, {n} steps of "
                       "exchange_halos+step, FP64"}
 
 
@@ -434,12 +437,22 @@ def run_our_arm(args):
     family_a = {}
     if world == 1 and not args.headline_only:
         # the reference's family-A programs at their own sizes on scheme A (FP32)
-        for nm in ("lloyd_a", "doppler_a", "scattering_a"):
+        for nm in ("lloyd_a", "doppler_a", "scattering_a", "hpc_a"):
             s2, _, r = measure(nm, None, args.steps, args.warmup, local, torch, barrier, reduce_max)
             family_a[nm] = {k: r[k] for k in ("glups_rank", "ms", "kernel_ms_avg", "dims", "bytes_per_cell",
                                                "description", "fluid_fraction")}
             family_a[nm]["hbm_frac_kernel"] = (r["cells"] * r["bytes_per_cell"] / (r["kernel_ms_avg"] / 1e3) / 1e9
                                                / hbm_peak)
+            if nm == "hpc_a":
+                # 04's own benchmark: 2000 steps after 100 (04:360-404), its MLUPS over all cells
+                from nlos_lbm import workloads
+
+                s2.step(max(0, 100 - s2.step_count))
+                w2 = workloads.build(nm)
+                ms2 = device_timed_steps(s2, w2["steps"], torch, barrier)
+                family_a[nm]["program_steps"] = w2["steps"]
+                family_a[nm]["program_ms"] = ms2
+                family_a[nm]["mlups"] = r["cells"] * w2["steps"] / (ms2 / 1e3) / 1e6
             if not args.no_cpu:
                 family_a[nm]["cpu_reference"] = family_a_cpu(nm)
             del s2
@@ -510,7 +523,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="city2048",
                     choices=["city2048", "city1024", "city512", "lloyd", "scatter", "lloyd_a", "lloyd_a_small",
-                             "doppler_a", "scattering_a"])
+                             "doppler_a", "scattering_a", "hpc_a"])
     ap.add_argument("--storage", default=None, choices=["fp32", "fp16"],
                     help="population storage of the headline workload (default: the workload's own)")
     ap.add_argument("--headline-only", action="store_true")

@@ -44,10 +44,11 @@ __device__ __forceinline__ float cell_omega(const SchemeAArgs& b, int i, int j, 
 }
 
 // source weight of cell (i, j, k), halo-inclusive (a halo cell takes its
-// nearest column's per-column weight)
+// nearest column's per-column weight); COLS = false: per-axis factors only
+template <bool COLS = true>
 __device__ __forceinline__ float field_weight(const SchemeAArgs& b, int i, int j, int k)
 {
-    if (b.fld_xy)
+    if (COLS && b.fld_xy)
     {
         const int ci = min(max(i, 1), b.nx_col) - 1, cj = min(max(j, 1), b.ny_col) - 1;
         return b.fld_xy[cj * b.nx_col + ci];
@@ -57,10 +58,11 @@ __device__ __forceinline__ float field_weight(const SchemeAArgs& b, int i, int j
 
 // strength of the destination blend at interior cell (i, j, k) (01:207-225,
 // 04:177-209)
+template <bool COLS = true>
 __device__ __forceinline__ float cell_blend(const SchemeAArgs& b, int i, int j, int k)
 {
     const float s = fmaxf(b.sg_x[i - 1], fmaxf(b.sg_y[j - 1], b.sg_z[k - 1]));
-    return b.sg_xy ? fmaxf(s, b.sg_xy[(j - 1) * b.nx_col + (i - 1)]) : s;
+    return COLS && b.sg_xy ? fmaxf(s, b.sg_xy[(j - 1) * b.nx_col + (i - 1)]) : s;
 }
 
 // BGK of one cell on deviations d = f - feq(1, u0): with rho' = sum d,
@@ -142,8 +144,11 @@ __device__ __forceinline__ void pull_a(const float* __restrict__ f, const Layout
 
 // ---------------------------------------------------------------- step
 // Two x-adjacent cells per thread, aligned float2 loads with warp shuffles
-// for the +-1 x shift (the same access scheme as the scheme-B step).
-template <int BLOCK, int MINB>
+// for the +-1 x shift (the same access scheme as the scheme-B step).  FEAT:
+// 0 = the update of 02 and 03; 1 = with 01's destination blend and periodic
+// z; 2 = also with per-column fields and the pre-step source (04).  Each is
+// its own instance, so the simpler programs keep the leaner kernel.
+template <int BLOCK, int MINB, int FEAT>
 __global__ void __launch_bounds__(BLOCK, MINB) k_step_a(const float* __restrict__ fin, float* __restrict__ fout,
                                                         Layout L, StepArgs a, SchemeAArgs b)
 {
@@ -165,7 +170,20 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step_a(const float* __restrict_
         if (nb & 2u) lk1 = a.links[cl + 1];
     }
     const bool any_link = __any_sync(kFull, (lk0 | lk1) != 0u);
-
+    // FEAT 2: the pair's source weights, per column or per axis, taken once
+    // before the populations are loaded (the per-column lookup inside each
+    // source term spilled registers)
+    float2 fw = f2(0.f);
+    if constexpr (FEAT == 2)
+    {
+        if (b.field_mode >= 0)
+            fw = make_float2(field_weight(b, c0 + 1, j, k), c0 + 1 < L.nx ? field_weight(b, c0 + 2, j, k) : 0.f);
+    }
+    const auto pair_weight = [&](float m) -> float2 {
+        if constexpr (FEAT == 2) return mul2(f2(m), fw);
+        return make_float2(m * field_weight<false>(b, c0 + 1, j, k),
+                           c0 + 1 < L.nx ? m * field_weight<false>(b, c0 + 2, j, k) : 0.f);
+    };
     // pair load (the bounds-checked build tests the index first)
     const auto ldc = [&](const float* p) {
         return LBM_IN(kChkALoad, p - fin, L.total - 1) ? ldg2(p) : make_float2(0.f, 0.f);
@@ -215,8 +233,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step_a(const float* __restrict_
     // destination source, for populations that left a fluid cell (02:373, 02:405)
     if (b.field_mode == 0)
     {
-        const float m = field_mass(b, 0);
-        const float2 S = make_float2(m * field_weight(b, c0 + 1, j, k), has1 ? m * field_weight(b, c0 + 2, j, k) : 0.f);
+        const float2 S = pair_weight(field_mass(b, 0));
 #pragma unroll
         for (int q = 0; q < Q; ++q)
         {
@@ -226,9 +243,10 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step_a(const float* __restrict_
         }
     }
     // destination blend toward rest, same populations (01:343-347)
-    if (b.blend)
+    if (FEAT >= 1 && b.blend)
     {
-        const float2 sg = make_float2(cell_blend(b, c0 + 1, j, k), has1 ? cell_blend(b, c0 + 2, j, k) : 0.f);
+        const float2 sg = make_float2(cell_blend<FEAT == 2>(b, c0 + 1, j, k),
+                                      has1 ? cell_blend<FEAT == 2>(b, c0 + 2, j, k) : 0.f);
         const float2 keep = sub2(f2(1.0f), sg);
 #pragma unroll
         for (int q = 0; q < Q; ++q)
@@ -240,10 +258,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step_a(const float* __restrict_
     }
     // pre-step source of the next step (04:212-235): every population of the
     // cell, before it is bounced back or collided next step
-    if (b.field_mode == 2)
+    if (FEAT == 2 && b.field_mode == 2)
     {
-        const float m = field_mass(b, 1);
-        const float2 S = make_float2(m * field_weight(b, c0 + 1, j, k), has1 ? m * field_weight(b, c0 + 2, j, k) : 0.f);
+        const float2 S = pair_weight(field_mass(b, 1));
 #pragma unroll
         for (int q = 0; q < Q; ++q) G[q] = fma2(f2(wf(q)), S, G[q]);
     }
@@ -314,8 +331,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step_a(const float* __restrict_
     // forcing of this cell for the populations it sends next (03:424-435)
     if (b.field_mode == 1)
     {
-        const float m = field_mass(b, 1);
-        const float s0 = m * field_weight(b, c0 + 1, j, k), s1 = has1 ? m * field_weight(b, c0 + 2, j, k) : 0.f;
+        const float2 sp = pair_weight(field_mass(b, 1));
+        const float s0 = sp.x, s1 = sp.y;
 #pragma unroll
         for (int q = 0; q < Q; ++q)
         {
@@ -346,7 +363,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step_a(const float* __restrict_
     store(e0);
     // periodic z (01:286-299): planes nz and 1 are also the next step's halo
     // planes 0 and nz + 1, stored twice here instead of copied afterwards
-    if (b.zper)
+    if (FEAT >= 1 && b.zper)
     {
         if (k == L.nz) store(e0 - (long long)L.nz * ps);
         if (k == 1) store(e0 + (long long)L.nz * ps);
@@ -593,7 +610,12 @@ cudaError_t launch_step_a(const float* fin, float* fout, const Layout& L, const 
     if (L.bc != BC) return cudaErrorInvalidValue;
     constexpr int kBlock = 128;
     const dim3 g((unsigned)((L.nx + 2 * kBlock - 1) / (2 * kBlock)), (unsigned)L.ny, (unsigned)L.nz);
-    k_step_a<kBlock, 7><<<g, kBlock, 0, stream>>>(fin, fout, L, a, b);
+    if (b.field_mode == 2 || b.sg_xy || b.fld_xy)
+        k_step_a<kBlock, 5, 2><<<g, kBlock, 0, stream>>>(fin, fout, L, a, b);
+    else if (b.blend || b.zper)
+        k_step_a<kBlock, 7, 1><<<g, kBlock, 0, stream>>>(fin, fout, L, a, b);
+    else
+        k_step_a<kBlock, 7, 0><<<g, kBlock, 0, stream>>>(fin, fout, L, a, b);
     return cudaGetLastError();
 }
 

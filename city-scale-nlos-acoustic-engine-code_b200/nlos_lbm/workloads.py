@@ -28,6 +28,10 @@ reference's heightmap ray cast.
              320x320x8 at dx 0.05, cylinder of radius 0.5, initial pulse,
              destination blend sponge 0.5 deep, periodic z, 402 steps (to
              T = 11 s plus 01's 20 extra steps)
+  hpc_a      04_hpc_scalability.cpp (the reference's MLUPS benchmark) at its
+             own size (scheme A): 208^3 at dx 0.125, cylinder of radius 4,
+             radial blend layer beyond r = 10, sine line source added before
+             each step, periodic z, 2000 timed steps after 100
 """
 import numpy as np
 
@@ -206,7 +210,47 @@ def build(name, storage=None, seed=2024):
                     rho0=np.ascontiguousarray(rho0).ravel(), steps=max_steps + 1,
                     description=f"acoustic scattering (01) {n}x{n}x{nz}, scheme A, cylinder, blend sponge, "
                                 "periodic z")
+    if name == "hpc_a":
+        # 04:21-26, 04:52-54, 04:65-71, 04:177-235, 04:301, 04:360-404
+        dx, half = 0.125, 13.0
+        n = int(2 * half / dx + 0.5)
+        cfg = lattice_config(n, n, n, 0.51, x_min=-half, x_max=half, y_min=-half, y_max=half, z_min=-half,
+                             z_max=half, dx=dx, c_phys=1.0,
+                             face_bc=(abi.LBM_BC_REST,) * 4 + (abi.LBM_BC_PERIODIC,) * 2, sponge_faces=0,
+                             sponge_width=0.0, sponge_blend=1, scheme=abi.LBM_SCHEME_A, dt=0.577350269 * dx)
+        solid, blend, weight = hpc_columns(dx, -half, n)
+        mask = np.broadcast_to(solid, (n + 2,) + solid.shape).astype(np.uint8)
+        src = abi.reference_source(sx=0.0, sy=-6.0, sz=0.0, ex=0.0, ey=-6.0, ez=0.0, amp=0.01, freq=1.0 / 30.0,
+                                   waveform=abi.LBM_WAVE_SINE, injection=abi.LBM_INJECT_FIELD, sigma_cells=1.0,
+                                   field_mode=abi.LBM_FIELD_PRE)
+        zc = -half + (n // 2 + 0.5) * dx
+        probes = np.array([[-half + (np.floor((px + half) / dx) + 0.5) * dx,
+                            -half + (np.floor((py + half) / dx) + 0.5) * dx, zc]
+                           for px, py in ((0.0, 7.0), (7.0, 0.0), (-7.0, 0.0), (0.0, -9.0))])
+        return dict(cfg=cfg, sources=[src], probes=probes, triangles=None, mask=np.ascontiguousarray(mask).ravel(),
+                    blend_xy=blend.ravel(), field_xy=weight.ravel(), steps=2000,
+                    description=f"scalability benchmark (04) {n}^3, scheme A, cylinder, radial blend layer, line "
+                                "source, periodic z")
     raise KeyError(name)
+
+
+def hpc_columns(dx, lo=-13.0, n=None, cyl_r=4.0, r0=10.0, th=3.0, strength=0.5, src_y=-6.0, b=2.0):
+    """04_hpc_scalability.cpp's z-invariant set-up on an n x n column grid
+    from lo at dx, with 04's own cell-centre expression lo + g dx + dx/2
+    (04:187-188): SOLID cylinder r < cyl_r (04:191-194), radial blend layer
+    0.5 min((r - 10)/3, 1)^2 beyond r = 10 (04:198-203), line-source weights
+    exp(-ln2 d^2 / b) for d^2 = x^2 + (y - src_y)^2 <= 36 (04:220-224).
+    Returns (solid[n+2, n+2] halo-inclusive, blend[n, n], weight[n, n])."""
+    g = np.arange(-1, n + 1)
+    c = lo + g * dx + 0.5 * dx
+    x, y = c[None, :], c[:, None]
+    r = np.sqrt(x * x + y * y)
+    solid = r < cyl_r
+    ratio = np.minimum((r - r0) / th, 1.0)
+    blend = np.where(~solid & (r > r0), strength * ratio * ratio, 0.0)
+    d2 = x * x + (y - src_y) * (y - src_y)
+    weight = np.where(d2 > 36.0, 0.0, np.exp(-np.log(2.0) * d2 / b))
+    return solid, blend[1:-1, 1:-1], weight[1:-1, 1:-1]
 
 
 def _cube(a, b):

@@ -6,7 +6,7 @@ and the FP64 oracle are built from the same description.
 """
 import numpy as np
 
-from nlos_lbm import abi
+from nlos_lbm import abi, workloads
 
 ALL_FACES = (1 << 6) - 1
 FIVE_FACES = ALL_FACES & ~(1 << abi.FACE_ZLO)
@@ -226,30 +226,11 @@ def family_a(name, n=40, steps=60):
     raise KeyError(name)
 
 
-def hpc_columns(dx, lo=-13.0, n=None, cyl_r=4.0, r0=10.0, th=3.0, strength=0.5, src_y=-6.0, b=2.0):
-    """04_hpc_scalability.cpp's z-invariant set-up on an n x n column grid
-    from lo at dx, with 04's own cell-centre expression lo + g dx + dx/2
-    (04:187-188): SOLID cylinder r < cyl_r (04:191-194), radial blend layer
-    0.5 min((r - 10)/3, 1)^2 beyond r = 10 (04:198-203), line-source weights
-    exp(-ln2 d^2 / b) for d^2 = x^2 + (y - src_y)^2 <= 36 (04:220-224).
-    Returns (solid[ny+2, nx+2] halo-inclusive, blend[ny, nx], weight[ny, nx])."""
-    g = np.arange(-1, n + 1)
-    c = lo + g * dx + 0.5 * dx
-    x, y = c[None, :], c[:, None]
-    r = np.sqrt(x * x + y * y)
-    solid = r < cyl_r
-    ratio = np.minimum((r - r0) / th, 1.0)
-    blend = np.where(~solid & (r > r0), strength * ratio * ratio, 0.0)
-    d2 = x * x + (y - src_y) * (y - src_y)
-    weight = np.where(d2 > 36.0, 0.0, np.exp(-np.log(2.0) * d2 / b))
-    return solid, blend[1:-1, 1:-1], weight[1:-1, 1:-1]
-
-
 def hpc_a(steps=40, dx=0.5, half=13.0):
     """04_hpc_scalability.cpp (the reference's scaling benchmark) on a reduced
     grid: [-13, 13]^3 at dx 0.5 instead of 0.125 (04:52-54, 04:21); tau 0.51
     (04:301); periodic z and rest x/y halos (04:51, 04:237-297); the radial
-    blend layer and the line source of hpc_columns, a sine of amplitude 0.01
+    blend layer and the line source of workloads.hpc_columns, a sine of amplitude 0.01
     and angular frequency pi/15 added before each step (04:65-67, 04:212-235);
     dt = 0.577350269 dx (04:22-26).  Probes at cell centres in the fluid."""
     n = int(2 * half / dx + 0.5)
@@ -258,7 +239,7 @@ def hpc_a(steps=40, dx=0.5, half=13.0):
                                face_bc=(abi.LBM_BC_REST,) * 4 + (abi.LBM_BC_PERIODIC,) * 2,
                                sponge_faces=0, sponge_width=0.0, sponge_blend=1, sky_z=1e30,
                                scheme=abi.LBM_SCHEME_A, tau_sponge_max=0.0, dt=0.577350269 * dx)
-    solid, blend, weight = hpc_columns(dx, -half, n)
+    solid, blend, weight = workloads.hpc_columns(dx, -half, n)
     mask = np.broadcast_to(solid, (n + 2,) + solid.shape).astype(np.uint8)
     src = abi.reference_source(sx=0.0, sy=-6.0, sz=0.0, ex=0.0, ey=-6.0, ez=0.0, amp=0.01, freq=1.0 / 30.0,
                                waveform=abi.LBM_WAVE_SINE, injection=abi.LBM_INJECT_FIELD, sigma_cells=1.0,
