@@ -303,8 +303,10 @@ int lbm_get_f(lbm_handle* h, double* out, long capacity);
 int lbm_set_f(lbm_handle* h, const double* in, long count);
 /* Scheme A: initial state at rest with density 1 + rho_minus_1 at every
  * interior fluid cell (count = nx*ny*nz, x fastest), i.e. f = feq(1 + rho',
- * flow) (the pulse initial condition of 01:183-205); SOLID cells are
- * unchanged.  After lbm_init, before the first step. */
+ * flow) (the pulse initial condition of 01:183-205); SOLID cells keep theirs,
+ * the bounce-back slots next to them and zero-gradient (LBM_BC_COPY) halo
+ * cells follow the new values, periodic halo planes repeat them.  After
+ * lbm_init, before the first step (LBM_ERR_STATE otherwise). */
 int lbm_set_density(lbm_handle* h, const double* rho_minus_1, long count);
 /* Voxelised mask, halo-inclusive, 0 FLUID / 1 SOLID (06:469-531). */
 int lbm_get_mask(lbm_handle* h, uint8_t* out, long capacity);
