@@ -11,7 +11,7 @@ reference's heightmap ray cast.
   city512    512x512x128 city (profiler-sized), 2 Ricker sources, 64 probes
   city1024   1024x1024x256 city, 4 Ricker sources at street level, 256 probes
   city2048   2048x2048x256 city, one source flying at z = 120 at Mach 0.15,
-             512 probes (FP16 deviation storage, scale 1/amplitude)
+             512 probes (FP16 deviation storage, scale F16_HEADROOM/amplitude)
   adjoint256 256x256x128 city patch, tau 0.52, true source at street level
              emitting a Ricker wavelet (period 30 steps), 64 street-level
              receivers, 3000 steps; the trial source (the unknown of the
@@ -38,6 +38,14 @@ import numpy as np
 from . import abi
 
 ALL_FACES = (1 << 6) - 1
+# FP16 storage scale = F16_HEADROOM / source amplitude.  Probes far from a
+# source see density deviations about 1e-3 of its amplitude; at a scale of
+# 1/amplitude their populations fall into FP16's subnormal range (the 128^3
+# scattering box over its 2000 steps: probe rel-L2 3.1e-3 against the FP64
+# oracle).  A hundred times more keeps them normal (2.4e-4) and still leaves
+# the stored values a factor ~650 below FP16's largest for peaks above the
+# source amplitude.
+F16_HEADROOM = 100.0
 FIVE_FACES = ALL_FACES & ~(1 << abi.FACE_ZLO)
 MACH_TO_CELLS = abi.CS   # cells/step per unit Mach (c = cs in lattice units)
 
@@ -77,7 +85,7 @@ def city(nx, ny, nz, seed, storage, tau=0.51, sponge=32):
                                margin=sponge + 8)
     amp = 1e-3
     cfg = lattice_config(nx, ny, nz, tau, sponge_width=float(sponge), sponge_faces=FIVE_FACES, storage=storage,
-                         f16_scale=1.0 / amp)
+                         f16_scale=F16_HEADROOM / amp)
     return cfg, tris, cov, amp
 
 
@@ -87,7 +95,8 @@ def build(name, storage=None, seed=2024):
         n = 128
         cfg = lattice_config(n, n, n, 0.55, face_bc=(abi.LBM_BC_NSCBC,) * 6, sponge_faces=ALL_FACES,
                              sponge_width=20.0, sponge_strength=0.5,
-                             storage=abi.LBM_STORE_F32 if storage is None else storage, f16_scale=1e3)
+                             storage=abi.LBM_STORE_F32 if storage is None else storage,
+                             f16_scale=F16_HEADROOM / 1e-3)
         c = n / 2
         tris = _cube(c - 8, c + 8)
         src = abi.reference_source(sx=c - 24 + 0.5, sy=c + 0.5, sz=c + 0.5, ex=c - 24 + 0.5, ey=c + 0.5,
@@ -98,7 +107,8 @@ def build(name, storage=None, seed=2024):
                     description="acoustic scattering 128^3, cube 16^3, Gaussian pulse")
     if name == "lloyd":
         cfg = lattice_config(256, 128, 128, 0.52, sponge_width=16.0, sponge_faces=FIVE_FACES,
-                             storage=abi.LBM_STORE_F32 if storage is None else storage, f16_scale=2e3)
+                             storage=abi.LBM_STORE_F32 if storage is None else storage,
+                             f16_scale=F16_HEADROOM / 5e-4)
         v = 0.1 * MACH_TO_CELLS
         src = abi.reference_source(sx=40.0, sy=64.0, sz=20.0, ex=250.0, ey=64.0, ez=20.0, speed=v, amp=5e-4,
                                    freq=1 / 50.0, waveform=abi.LBM_WAVE_SINE, injection=abi.LBM_INJECT_TRILINEAR)

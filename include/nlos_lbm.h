@@ -118,7 +118,9 @@ typedef struct lbm_config
     double sponge_strength;                          /* 06:456: 0.35 */
     double sky_z;                                    /* cells above this z are FLUID (06:458,489) */
     int storage;                                     /* LBM_STORE_F32 or LBM_STORE_F16 */
-    double f16_scale;                                /* FP16 stores (f_q - w_q) * f16_scale */
+    double f16_scale;                                /* FP16 stores (f_q - w_q) * f16_scale; about
+                                                        100 / (source density amplitude) keeps
+                                                        far-field values out of FP16's subnormals */
     int device;                                      /* CUDA device ordinal */
     int use_graphs;                                  /* replay multi-step runs as CUDA graphs */
     int verbose;                                     /* print the reference's progress lines */

@@ -64,6 +64,29 @@ def test_fp32_matches_reference_fixture(name, gpu):
     assert rel_l2(g.get_probes(), gold["probes"]) <= FP32_PROBE_TOL
 
 
+@pytest.mark.parametrize("fixture", ["oracle_scatter_2000", "oracle_lloyd_6000"])
+def test_full_size_workload_matches_oracle_series(fixture, gpu):
+    """The full-size 128^3 scattering box (2000 steps) and 256x128x128 Lloyd's
+    mirror (6000 steps) benchmark workloads, FP32 and FP16 storage (the
+    workload's scale, 100/amplitude), against the FP64 oracle's series
+    (tests/golden/make_oracle_series.py)."""
+    from nlos_lbm import workloads
+
+    path = os.path.join(GOLDEN, fixture + ".npz")
+    if not os.path.exists(path):
+        pytest.skip("oracle series not generated")
+    gold = np.load(path)
+    name, steps = fixture.split("_")[1], int(gold["steps"])
+    for storage, tol in ((abi.LBM_STORE_F32, FP32_PROBE_TOL), (abi.LBM_STORE_F16, FP16_PROBE_TOL)):
+        w = workloads.build(name, storage=storage)
+        g = nlos_lbm.Solver(w["cfg"], w["sources"], w["probes"], triangles=w["triangles"])
+        assert g.dims_halo == tuple(gold["dims_halo"])
+        g.step(steps)
+        err = rel_l2(g.get_probes(), gold["probes"])
+        assert err <= tol, (name, storage, err)
+        g.close()
+
+
 @pytest.mark.parametrize("name", ["scatter_small", "lloyd_small", "city_small"])
 def test_fp16_storage_matches_oracle(name, gpu):
     amp = {"scatter_small": 1e-3, "lloyd_small": 5e-4, "city_small": 1e-3}[name]
