@@ -196,7 +196,8 @@ def measure(name, storage, steps, warmup, device, torch, barrier, reduce_max, ke
                steps=steps, ms=ms_max, ms_local=ms, setup_s=setup_s, glups_rank=ncell * steps / (ms_max / 1e3) / 1e9,
                kernel_ms_avg=kms / max(kn, 1), kernel_launches=kn, launches=launches,
                bytes_per_cell=s.bytes_per_cell, probes_finite=bool(np.all(np.isfinite(probes))),
-               description=w["description"], coverage=w.get("coverage"), fluid_fraction=fluid_fraction)
+               description=w["description"], coverage=w.get("coverage"), fluid_fraction=fluid_fraction,
+               f16_scale=w["cfg"].f16_scale if s.bytes_per_cell == 76 else None)
     return s, w, res
 
 
@@ -481,7 +482,7 @@ def run_our_arm(args):
         "data": "synthetic (seeded box city voxelised from STL triangles)",
         "config": {"workload": f"{headline}: {head['description']}", "grid": head["dims"],
                    "storage": head["storage"], "plan_coverage": head["coverage"],
-                   "fluid_fraction": head["fluid_fraction"],
+                   "fluid_fraction": head["fluid_fraction"], "f16_scale": head["f16_scale"],
                    "parallelism": f"replicas x{n}" if n > 1 else "single GPU",
                    "l2": ("inputs larger than L2 (populations %.1f GB per step)" if cells * head["bytes_per_cell"] > 2 * L2_BYTES
                           else "inputs about the size of L2 (populations %.2f GB per step)")

@@ -195,6 +195,31 @@ def test_set_density_rules(gpu):
     assert e.value.status == abi.LBM_ERR_UNSUPPORTED
 
 
+@pytest.mark.parametrize("name", ["lloyd_a", "doppler_a"])
+def test_column_source_weights_with_other_source_forms(name, gpu):
+    """Per-column source weights (a line source) with 02's destination source
+    and 03's forcing (and its zero-gradient halos, which take their nearest
+    column's weight), against the oracle."""
+    sc = scenarios.family_a(name, steps=40)
+    cfg = sc["cfg"]
+    nx = int(round((cfg.x_max - cfg.x_min) / cfg.dx))
+    ny = int(round((cfg.y_max - cfg.y_min) / cfg.dx))
+    s0 = sc["sources"][0]
+    xc = cfg.x_min + (np.arange(nx) + 0.5) * cfg.dx
+    yc = cfg.y_min + (np.arange(ny) + 0.5) * cfg.dx
+    d2 = (xc[None, :] - s0.sx) ** 2 + (yc[:, None] - s0.sy) ** 2
+    sc["field_xy"] = np.where(d2 > 4.0, 0.0, np.exp(-d2 / 0.5)).ravel()
+    g, o = _solver(sc), _oracle(sc)
+    g.step(sc["steps"])
+    o.step(sc["steps"])
+    assert np.max(np.abs(o.get_probes())) > 0
+    assert rel_l2(g.get_probes(), o.get_probes()) <= PROBE_TOL
+    nx_, ny_, nz_ = g.dims
+    fo = o.get_rho().reshape(nz_ + 2, ny_ + 2, nx_ + 2)[1:-1, 1:-1, 1:-1] - 1.0
+    fo[o.get_mask().reshape(nz_ + 2, ny_ + 2, nx_ + 2)[1:-1, 1:-1, 1:-1] == 1] = 0.0
+    assert np.max(np.abs(g.get_rho().astype(np.float64) - fo)) <= FIELD_TOL * np.max(np.abs(fo))
+
+
 def test_pre_step_source_direct_calls_equal_batched_steps(gpu):
     sc = scenarios.family_a("hpc_a", steps=12)
     a = _solver(sc)
