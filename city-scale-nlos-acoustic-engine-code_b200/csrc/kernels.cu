@@ -1212,6 +1212,58 @@ __global__ void __launch_bounds__(128) k_ghost(S* __restrict__ f, Layout L, Ghos
         for (int q = 0; q < Q; ++q) a.xf.xgh[a.xf.gh_index(F.side, q, j, k, L.ny, L.nz)] = G[q];
         return;
     }
+    if constexpr (std::is_same<S, __half>::value)
+    {
+        // y and z faces in FP16: the first half of the face's threads take two
+        // x-adjacent cells each, one half2 per direction (a 64-cell block
+        // holds both cells of an even-aligned pair); same values as one cell
+        // per thread, half as many 2-byte accesses
+        const int npair = (F.nu + 1) >> 1;
+        if (lt >= npair * F.nv) return;
+        const int vp = lt / npair, up = 2 * (lt - vp * npair);
+        const bool two = up + 1 < F.nu;
+        const int pi = 1 + up;
+        const int pj = F.axis == 1 ? (F.side ? L.ny : 1) : 1 + vp, pk = F.axis == 1 ? 1 + vp : (F.side ? L.nz : 1);
+        const int qj = F.axis == 1 ? (F.side ? L.ny + 1 : 0) : pj, qk = F.axis == 1 ? pk : (F.side ? L.nz + 1 : 0);
+        constexpr int BCH = block_cells(sizeof(S));
+        if (!LBM_IN(kChkGhost, L.elem(18, pi + (two ? 1 : 0), pj, pk), L.total) ||
+            !LBM_IN(kChkGhost, L.elem(18, pi + (two ? 1 : 0), qj, qk), L.total))
+            return;
+        const __half* I = f + L.elem(0, pi, pj, pk);
+        __half* B = f + L.elem(0, pi, qj, qk);
+        float G1[Q];
+#pragma unroll
+        for (int q = 0; q < Q; ++q)
+        {
+            if (two)
+            {
+                const float2 v2 = __half22float2(__ldg(reinterpret_cast<const __half2*>(I + q * BCH)));
+                G[q] = v2.x;
+                G1[q] = v2.y;
+            }
+            else
+            {
+                G[q] = Io<S>::ld(I + q * BCH);
+                G1[q] = 0.f;
+            }
+        }
+        const long long cell = F.first + (long long)vp * F.nu + up;   // the face enumeration of one cell a thread
+        if (a.face_mom) store_moments(G, a.face_mom + cell);
+        nscbc(G, F.axis, F.side, inv_scale);
+        if (two)
+        {
+            if (a.face_mom) store_moments(G1, a.face_mom + cell + 1);
+            nscbc(G1, F.axis, F.side, inv_scale);
+#pragma unroll
+            for (int q = 0; q < Q; ++q) *reinterpret_cast<__half2*>(B + q * BCH) = __floats2half2_rn(G[q], G1[q]);
+        }
+        else
+        {
+#pragma unroll
+            for (int q = 0; q < Q; ++q) Io<S>::st(B + q * BCH, G[q]);
+        }
+        return;
+    }
     int ci, cj, ck, gj, gk;
     if (F.axis == 1)
     {
