@@ -32,13 +32,6 @@ namespace {
 constexpr int kTableRows = 4096;   // source-schedule rows resident on the device
 constexpr int kBcCut = 100;        // face of a z-slab that borders the next slab (internal face type)
 constexpr int kProbeRows = 4096;   // probe-series rows buffered on the device
-// Fused-step implementation and L2 prefetch distance per storage type, from
-// launch-shape sweeps on the 1024x1024x256 city (B200): FP32 is fastest with
-// the plain pair kernel; FP16 with the warp pipelines of cp.async copies,
-// two blocks in flight per warp and 20 warps per SM (the prefetch distance
-// applies to the register-held FP16 variants 4-7 only).
-constexpr int kDefaultStepVariant[2] = {0, 10};
-constexpr int kDefaultPrefetchRows[2] = {0, 96};
 // Register cap of the adjoint step kernel (launch_adj_step variant).
 constexpr int kDefaultAdjointVariant = 1;
 // L2 prefetch distance of the adjoint step in rows (measured on the 256x256x128 patch: 192 rows
@@ -70,7 +63,6 @@ struct lbm_handle
     std::string err;
     int storage = LBM_STORE_F32;
     float scale = 1.0f;
-    int step_variant = 0;              // fused-step implementation (NLOS_LBM_STEP_VARIANT overrides)
 
     // geometry / mask
     HeightField geo;
@@ -114,6 +106,7 @@ struct lbm_handle
     long long probe_pending = 0;        // rows recorded on the device, not yet on the host
     std::vector<double> series;
     bool halo_dirty = false;
+    std::vector<float> rho0;             // scheme A: the initial density deviation lbm_set_density set
 
     long long step = 0;                // completed time steps
     long launches = 0;
@@ -607,6 +600,7 @@ extern "C" const char* lbm_status_string(int s)
     case LBM_OK: return "ok";
     case LBM_WARN_STL_NOT_LOADED: return "warning: STL not loaded, using empty geometry";
     case LBM_WARN_PROBE_IN_SOLID: return "warning: probe inside a SOLID cell";
+    case LBM_WARN_STL_TRUNCATED: return "warning: STL truncated, missing triangles read as zeros";
     case LBM_ERR_INVALID_ARGUMENT: return "invalid argument";
     case LBM_ERR_BAD_CONFIG: return "bad configuration";
     case LBM_ERR_OUT_OF_MEMORY: return "out of device memory";
@@ -668,9 +662,14 @@ extern "C" const char* lbm_last_error(lbm_handle* h) { return h ? h->err.c_str()
 extern "C" int lbm_set_geometry_stl(lbm_handle* h, const char* path, double scale, double sx, double sy, double sz)
 {
     if (!h || !path) return LBM_ERR_INVALID_ARGUMENT;
-    const bool ok = h->geo.load_stl(path, scale, sx, sy, sz);
-    h->stl_status = ok ? LBM_OK : LBM_WARN_STL_NOT_LOADED;
-    if (!ok) h->err = std::string("STL not loaded: ") + path;
+    const int r = h->geo.load_stl(path, scale, sx, sy, sz);
+    h->stl_status = r == HeightField::kStlLoaded ? LBM_OK
+                  : r == HeightField::kStlNotOpened ? LBM_WARN_STL_NOT_LOADED
+                                                    : LBM_WARN_STL_TRUNCATED;
+    if (r == HeightField::kStlNotOpened) h->err = std::string("STL not loaded: ") + path;
+    if (r == HeightField::kStlTruncated)
+        h->err = std::string("STL ends before the triangle count of its header; missing records read as zeros: ") +
+                 path;
     return h->stl_status;
 }
 
@@ -836,6 +835,22 @@ extern "C" int lbm_init(lbm_handle* h)
     L.plane_stride = L.row_stride * nyt;
     L.total = kFrontElems + L.plane_stride * nzt + kBackElems;
 
+    // The two population buffers and the links words must fit in the free
+    // device memory: a grid that cannot fit fails here, before any host or
+    // device allocation (later allocations still report their own failure).
+    {
+        const double need = 2.0 * (double)L.total * (h->storage == LBM_STORE_F16 ? 2 : 4) + 4.0 * (double)L.plane * nzt;
+        size_t free_b = 0, total_b = 0;
+        CK(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
+        if (need > (double)free_b)
+        {
+            char msg[160];
+            std::snprintf(msg, sizeof msg, "the grid needs at least %.1f GB of device memory, %.1f GB free", need / 1e9,
+                          (double)free_b / 1e9);
+            return h->fail(LBM_ERR_OUT_OF_MEMORY, msg);
+        }
+    }
+
     // Mask (init_domain 06:453-532).
     if (!h->mask_override.empty())
     {
@@ -904,6 +919,7 @@ extern "C" int lbm_init(lbm_handle* h)
     h->xf.xgh = dalloc<float>(n_xgh_all, e);
     h->ctl = dalloc<Control>(1, e);
     if (e != cudaSuccess) return h->cuda_fail(e, "device allocation");
+    CK(cudaMemsetAsync(h->ctl, 0, sizeof(Control), h->stream), "memset control");
     CK(cudaMemsetAsync(h->links, 0, cells * sizeof(uint32_t), h->stream), "memset links");
     CK(cudaMemsetAsync(h->near, 0, near_words * sizeof(uint32_t), h->stream), "memset near");
     CK(cudaMemsetAsync(h->xf.xexp, 0, n_xexp * sizeof(float), h->stream), "memset x faces");
@@ -911,6 +927,7 @@ extern "C" int lbm_init(lbm_handle* h)
     h->xgh_par[0] = h->xf.xgh;
     h->xgh_par[1] = h->xf.xgh + (h->scheme_a() ? n_xgh : 0);
     CK(cudaMallocHost(&h->ctl_host, sizeof(Control)), "cudaMallocHost");
+    *h->ctl_host = Control{};
     CK(cudaMemcpyAsync(h->sig, sx.data(), sx.size() * 4, cudaMemcpyHostToDevice, h->stream), "upload sponge");
     CK(cudaMemcpyAsync(h->sig + nx, sy.data(), sy.size() * 4, cudaMemcpyHostToDevice, h->stream), "upload sponge");
     CK(cudaMemcpyAsync(h->sig + nx + ny, sz.data(), sz.size() * 4, cudaMemcpyHostToDevice, h->stream),
@@ -954,16 +971,10 @@ extern "C" int lbm_init(lbm_handle* h)
     h->sa.sig_z = h->sig + nx + ny;
     h->sa.omega = (float)(1.0 / c.tau);
     h->sa.xf = h->xf;
-    const int si = h->storage == LBM_STORE_F16 ? 1 : 0;
-    h->step_variant = kDefaultStepVariant[si];
-    if (const char* v = std::getenv("NLOS_LBM_STEP_VARIANT")) h->step_variant = std::atoi(v);
-    if (h->step_variant < 0 || h->step_variant > 13) return h->fail(LBM_ERR_BAD_CONFIG, "NLOS_LBM_STEP_VARIANT out of range");
     {
-        const cudaError_t e = prepare_step(h->storage == LBM_STORE_F16 ? 1 : 0, h->step_variant);
+        const cudaError_t e = prepare_step(h->storage == LBM_STORE_F16 ? 1 : 0);
         if (e != cudaSuccess) return h->cuda_fail(e, "step set-up");
     }
-    h->sa.prefetch_rows = kDefaultPrefetchRows[si];
-    if (const char* v = std::getenv("NLOS_LBM_PREFETCH_ROWS")) h->sa.prefetch_rows = std::max(0, std::atoi(v));
 
     // Open faces for the ghost kernel.
     h->ga = GhostArgs{};
@@ -1082,6 +1093,7 @@ ProbeArgs probe_args(lbm_handle* h, bool batched, long long direct_row)
     a.ctl = batched ? h->ctl : nullptr;
     a.direct_row = direct_row;
     a.scale = h->scale;
+    a.nonfinite = &h->ctl->nonfinite;
     return a;
 }
 
@@ -1111,7 +1123,7 @@ cudaError_t timed_step_launch(lbm_handle* h, int parity, bool batched, long long
 {
     const auto launch = [&]() {
         if (!h->scheme_a())
-            return launch_step(h->storage, h->f[parity], h->f[parity ^ 1], h->L, h->sa, h->scale, h->step_variant,
+            return launch_step(h->storage, h->f[parity], h->f[parity ^ 1], h->L, h->sa, h->scale,
                                h->stream);
         StepArgs sa;
         SchemeAArgs b;
@@ -1345,6 +1357,25 @@ int check_ready(lbm_handle* h)
     return LBM_OK;
 }
 
+// Field before the first step: rho is 1 everywhere (06:368) unless
+// lbm_set_density gave scheme A an initial pulse, which is then the field at
+// FLUID cells (01:197); SOLID cells read 0 as after a step.
+void field_rho_initial(const lbm_handle* h, float* out, size_t n)
+{
+    if (h->rho0.size() != n)
+    {
+        std::fill(out, out + n, 0.0f);
+        return;
+    }
+    const Layout& L = h->L;
+    const size_t nxt = (size_t)L.nx + 2, nyt = (size_t)L.ny + 2;
+    size_t c = 0;
+    for (int k = 1; k <= L.nz; ++k)
+        for (int j = 1; j <= L.ny; ++j)
+            for (int i = 1; i <= L.nx; ++i, ++c)
+                out[c] = h->mask[(size_t)i + nxt * ((size_t)j + nyt * (size_t)k)] == 1 ? 0.0f : h->rho0[c];
+}
+
 // (float)(rho - 1) of the last step into d (device, interior cells).
 cudaError_t field_rho_last_step(lbm_handle* h, float* d)
 {
@@ -1515,8 +1546,9 @@ extern "C" int lbm_step(lbm_handle* h, int nsteps)
         // the probe row of step s is s - probe_base: rows continue after the
         // ones already buffered
         h->ctl_host->probe_base = h->step - h->probe_pending;
-        CK(cudaMemcpyAsync(h->ctl, h->ctl_host, sizeof(Control), cudaMemcpyHostToDevice, h->stream), "control");
-        h->h2d_bytes += (long)sizeof(Control);
+        CK(cudaMemcpyAsync(h->ctl, h->ctl_host, offsetof(Control, nonfinite), cudaMemcpyHostToDevice, h->stream),
+           "control");
+        h->h2d_bytes += (long)offsetof(Control, nonfinite);
         long long done = 0;
         while (done < chunk)
         {
@@ -1537,11 +1569,20 @@ extern "C" int lbm_step(lbm_handle* h, int nsteps)
                 done += 1;
             }
         }
+        if (np)
+        {
+            CK(cudaMemcpyAsync(&h->ctl_host->nonfinite, &h->ctl->nonfinite, sizeof(int), cudaMemcpyDeviceToHost,
+                               h->stream),
+               "probe flag");
+            h->d2h_bytes += (long)sizeof(int);
+        }
         // the control block upload must not be overwritten before the copy ran
         CK(cudaStreamSynchronize(h->stream), "step sync");
         h->step += chunk;
         if (np) h->probe_pending += chunk;
         left -= chunk;
+        if (np && h->ctl_host->nonfinite)
+            return h->fail(LBM_ERR_NAN, "non-finite probe value by step " + std::to_string(h->step));
         st = harvest_timing(h);
         if (st) return st;
         if (np && h->probe_pending >= kProbeRows)
@@ -1643,7 +1684,7 @@ extern "C" int lbm_get_rho(lbm_handle* h, float* out, long capacity)
     if (!out || (long)n > capacity) return h->fail(LBM_ERR_CAPACITY, "rho buffer too small");
     if (h->step == 0)
     {
-        std::fill(out, out + n, 0.0f);   // rho initialised to 1 (06:368)
+        field_rho_initial(h, out, n);
         return LBM_OK;
     }
     CK(cudaSetDevice(h->device), "cudaSetDevice");
@@ -1674,7 +1715,7 @@ extern "C" int lbm_get_rho_noalloc(lbm_handle* h, float* out, long capacity)
     if (!out || (long long)capacity < n) return h->fail(LBM_ERR_CAPACITY, "rho buffer too small");
     if (h->step == 0)
     {
-        std::fill(out, out + n, 0.0f);   // rho initialised to 1 (06:368)
+        field_rho_initial(h, out, (size_t)n);
         return LBM_OK;
     }
     CK(cudaSetDevice(h->device), "cudaSetDevice");
@@ -1759,6 +1800,7 @@ extern "C" int lbm_set_density(lbm_handle* h, const double* rho_minus_1, long co
     cudaFree(d_rp);
     cudaFree(d_mask);
     if (e != cudaSuccess) return h->cuda_fail(e, "set_density");
+    h->rho0 = std::move(rp);
     h->launches += h->aa.zper ? 2 : 1;
     return LBM_OK;
 }
@@ -2281,7 +2323,7 @@ extern "C" int lbm_adjoint_grad(lbm_handle* h, int nsteps, const double* observe
     };
     // pull + collide of step s (Ht^s -> G^{s+1}), optionally with its probe record
     const auto collide = [&](int s, bool probe) {
-        cudaError_t r = launch_step(h->storage, h->f[h->cur], h->f[h->cur ^ 1], L, h->sa, h->scale, h->step_variant,
+        cudaError_t r = launch_step(h->storage, h->f[h->cur], h->f[h->cur ^ 1], L, h->sa, h->scale,
                                     h->stream);
         kernels++;
         if (r == cudaSuccess && probe)

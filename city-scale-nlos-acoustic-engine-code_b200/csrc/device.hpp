@@ -27,6 +27,7 @@
 #include <cuda_runtime.h>
 
 #include "check.cuh"
+#include "nlos_lbm.h"
 
 namespace lbm {
 
@@ -68,6 +69,8 @@ struct Control
     long long step;        // time step index of the step being executed
     long long table_base;  // step index of source-table row 0
     long long probe_base;  // step index of probe-buffer row 0
+    int nonfinite;         // set by the probe kernels when an owned probe reads a non-finite value
+                           // (the host uploads only the fields above it)
 };
 
 struct SourceStatic
@@ -144,7 +147,6 @@ struct StepArgs
     const float* sig_z;
     float omega;               // 1 / tau
     XFace xf;
-    int prefetch_rows;         // > 0: each block prefetches into L2 the lines the row this far ahead will read
 };
 
 struct ProbeArgs
@@ -156,6 +158,7 @@ struct ProbeArgs
     Control* ctl;              // nullptr: row = direct_row, no counter update
     long long direct_row;
     float scale;
+    int* nonfinite;            // set to 1 when an owned probe reads a non-finite value
 };
 
 // Scheme A (the reference's 01-04 family).  The stored state is the
@@ -208,20 +211,13 @@ cudaError_t launch_build_links(const uint8_t* mask_ref, uint32_t* links, uint32_
 cudaError_t launch_source(int storage, void* f, const Layout& L, const StepArgs& sa, const SourceArgs& a,
                           cudaStream_t stream);
 cudaError_t launch_ghost(int storage, void* f, const Layout& L, const GhostArgs& a, cudaStream_t stream);
-// variant: implementation of the fused step, same work in all.  0-3: two
-// cells per thread (0: 128 threads, 1: 128 threads with at most 64
-// registers, 2: 256 threads, 3: 64 threads); 4-7: FP16 storage only, kept
-// packed as half2 through the update (cells per thread / register cap:
-// 4: 2/64, 5: 4/85, 6: 2/51, 7: 4/102, 128 threads); 8-12: FP16 storage,
-// warp pipelines of cp.async copies into shared memory (blocks in flight per
-// warp / warps per CTA: 8: 4/4, 9: 3/4, 10: 2/4, 11: 6/2, 12: 4/8), whose
-// collision takes fewer operations in another rounding order; 13: as 10 with
-// the collision of 4-7; FP32 storage runs variant 0 instead of 4-13.
+// Fused step: FP32 storage runs the two-cells-per-thread pair kernel, FP16
+// storage the warp pipelines of cp.async copies.
 cudaError_t launch_step(int storage, const void* fin, void* fout, const Layout& L, const StepArgs& a,
-                        float scale, int variant, cudaStream_t stream);
-// One-time set-up of a step variant on the current device (shared-memory
+                        float scale, cudaStream_t stream);
+// One-time set-up of the fused step on the current device (shared-memory
 // attribute, occupancy); call before the first launch or capture.
-cudaError_t prepare_step(int storage, int variant);
+cudaError_t prepare_step(int storage);
 // Fused step (FP32 storage, the default implementation) that also writes the
 // moments (rho', jx, jy, jz) of every cell's pulled populations to `mom`,
 // dense cell order ((k-1) ny + (j-1)) nx + (i-1), as two FP16 pairs per cell
@@ -280,7 +276,7 @@ cudaError_t launch_check_selftest(cudaStream_t stream);
 // lbm_get_rho_noalloc, and the device address of that array on `device`
 // (looked up on first use with the device current; must not run during
 // stream capture).
-constexpr long long kNoAllocFieldCells = 8388608;   // 2^23 floats = 32 MiB
+constexpr long long kNoAllocFieldCells = LBM_NOALLOC_MAX_CELLS;   // 2^23 floats = 32 MiB, the API's limit
 constexpr int kMaxDevices = 64;
 cudaError_t field_scratch_address(int device, float** ptr);
 

@@ -41,28 +41,40 @@ void HeightField::set_triangles(const float* v, int ntris, double scale, double 
     build_bins();
 }
 
-bool HeightField::load_stl(const std::string& path, double scale, double sx, double sy, double sz)
+int HeightField::load_stl(const std::string& path, double scale, double sx, double sy, double sz)
 {
     std::ifstream file(path, std::ios::binary);
     if (!file)
     {
         set_triangles(nullptr, 0, scale, sx, sy, sz);
-        return false;
+        return kStlNotOpened;
     }
+    file.seekg(0, std::ios::end);
+    const long long size = (long long)file.tellg();
+    file.seekg(0, std::ios::beg);
     char header[80];
     file.read(header, 80);
     uint32_t n = 0;
     file.read(reinterpret_cast<char*>(&n), 4);
     if (!file) n = 0;
-    std::vector<float> v((size_t)n * 9, 0.0f);
-    for (uint32_t i = 0; i < n; ++i)
+    // The reference reads n records whatever the file holds; a short read
+    // leaves a record's missing bytes zero (its StlTriangle st{}, 06:82-85).
+    // Records past the end of the file are all-zero triangles: degenerate at
+    // the offset point, they never hit a ray and add only that point to the
+    // bounding box, so one of them stands for all (the mask is the same, and
+    // a corrupt count cannot make this allocate more than the file holds).
+    const long long avail = size > 84 ? (size - 84 + 49) / 50 : 0;   // records with at least one byte
+    const bool truncated = (long long)n > (size > 84 ? (size - 84) / 50 : 0);
+    const long long kept = std::min<long long>(n, avail) + ((long long)n > avail ? 1 : 0);
+    std::vector<float> v((size_t)kept * 9, 0.0f);
+    for (long long i = 0; i < std::min<long long>(n, avail); ++i)
     {
         unsigned char rec[50] = {0};
-        file.read(reinterpret_cast<char*>(rec), 50);   // a short read leaves zeros, as the reference's st{} does
+        file.read(reinterpret_cast<char*>(rec), 50);
         std::memcpy(&v[(size_t)i * 9], rec + 12, 36);
     }
-    set_triangles(v.data(), (int)n, scale, sx, sy, sz);
-    return true;
+    set_triangles(v.data(), (int)kept, scale, sx, sy, sz);
+    return truncated ? kStlTruncated : kStlLoaded;
 }
 
 void HeightField::build_bins()

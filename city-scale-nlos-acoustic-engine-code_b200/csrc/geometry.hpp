@@ -19,8 +19,12 @@ public:
     // GeometryEngine::load (06:70-111) from memory: 9 floats per triangle,
     // vertex * scale + offset in FP64.
     void set_triangles(const float* tris, int ntris, double scale, double sx, double sy, double sz);
-    // Returns false (and leaves the geometry empty) when the file cannot be opened.
-    bool load_stl(const std::string& path, double scale, double sx, double sy, double sz);
+    // GeometryEngine::load (06:70-111) from a binary STL file: kStlNotOpened
+    // (geometry left empty) when the file cannot be opened, kStlTruncated
+    // when it ends before the triangle count of its header (the missing
+    // records read as zeros, as in the reference), else kStlLoaded.
+    static constexpr int kStlLoaded = 0, kStlNotOpened = 1, kStlTruncated = 2;
+    int load_stl(const std::string& path, double scale, double sx, double sy, double sz);
     // GeometryEngine::getGroundHeight (06:144-192): highest hit of the ray
     // from z = 10000 straight down, -1e30 when there is none.
     double ground_height(double x, double y) const;

@@ -140,32 +140,9 @@ __device__ __forceinline__ void pull_cell(const S* __restrict__ f, const Layout&
     }
 }
 
-// ---------------------------------------------------------------- L2 prefetch
+// y and z components of the velocities, for per-lane index arithmetic
 __constant__ signed char c_ey[19] = {0, 0, 0, 1, -1, 0, 0, 1, -1, 1, -1, 0, 0, 0, 0, 1, 1, -1, -1};
 __constant__ signed char c_ez[19] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1};
-
-// Each thread of a block asks L2 for one (or more) of the lines that the
-// same block position `prefetch_rows` rows later will load: direction q of
-// each interleaved block of the tile, from source row (j - ey, k - ez).
-// Prefetches hold no registers, so they add memory-level parallelism that
-// the register-bound demand loads cannot; those later loads then hit L2.
-template <typename S, int CELLS_PER_BLOCK>
-__device__ __forceinline__ void prefetch_rows_ahead(const S* f, const Layout& L, int dist, int j, int k, int col0)
-{
-    constexpr int BC = block_cells(sizeof(S));
-    constexpr int NBLK = (CELLS_PER_BLOCK + BC - 1) / BC;   // interleaved blocks in this tile
-    const long long r = (long long)(k - 1) * L.ny + (j - 1) + dist;
-    if (r >= (long long)L.ny * L.nz) return;
-    const int jj = 1 + (int)(r % L.ny), kk = 1 + (int)(r / L.ny);
-    for (int t = threadIdx.x; t < 19 * NBLK; t += blockDim.x)
-    {
-        const int q = t / NBLK, b = t - q * NBLK;
-        const int col = col0 + b * BC;
-        if (col >= L.nx) continue;
-        const S* p = f + L.elem(q, col + 1, jj - c_ey[q], kk - c_ez[q]);
-        asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
-    }
-}
 
 // ---------------------------------------------------------------- step
 // Packed FP32x2 arithmetic (sm_100): both cells of a thread's pair in one
@@ -271,7 +248,6 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step(const S* __restrict__ fin,
     const long long e0 = L.elem(0, c0 + 1, j, k);
     const S* own = fin + e0;
     const long long rs = L.row_stride, ps = L.plane_stride;
-    if (a.prefetch_rows > 0) prefetch_rows_ahead<S, 2 * BLOCK>(fin, L, a.prefetch_rows, j, k, 2 * BLOCK * blockIdx.x);
 
     // pair load (the bounds-checked build tests the index first)
     const auto ldp = [&](const S* p) -> typename P::V {
@@ -395,65 +371,7 @@ __device__ __forceinline__ unsigned set_hi(unsigned w, float v)
     return (w & 0x0000ffffu) | ((unsigned)__half_as_ushort(__float2half_rn(v)) << 16);
 }
 
-// collide2() on packed words (same formulas, FP32x2 arithmetic).
-__device__ __forceinline__ void collide2_packed(unsigned (&w)[Q], float inv_scale, float omega, float2 sigma,
-                                                bool solid0, bool solid1)
-{
-    float2 rho = h2f(w[0]);
-    float2 jx = f2(0.f), jy = f2(0.f), jz = f2(0.f);
-#pragma unroll
-    for (int q = 1; q < Q; ++q)
-    {
-        const float2 g = h2f(w[q]);
-        rho = add2(rho, g);
-        if (ex(q) > 0) jx = add2(jx, g);
-        if (ex(q) < 0) jx = sub2(jx, g);
-        if (ey(q) > 0) jy = add2(jy, g);
-        if (ey(q) < 0) jy = sub2(jy, g);
-        if (ez(q) > 0) jz = add2(jz, g);
-        if (ez(q) < 0) jz = sub2(jz, g);
-    }
-    float2 r = fma2(rho, f2(inv_scale), f2(1.0f));
-    if (r.x <= 0.f) r.x = 1e-12f;   // 06:948
-    if (r.y <= 0.f) r.y = 1e-12f;
-    const float2 irs = make_float2(__fdividef(inv_scale, r.x), __fdividef(inv_scale, r.y));
-    const float2 j2 = fma2(jz, jz, fma2(jy, jy, mul2(jx, jx)));
-    const float2 base = fma2(mul2(irs, j2), f2(-1.5f), rho);
-    const float2 k45 = mul2(irs, f2(4.5f));
-    const float2 keep = sub2(f2(1.0f), sigma);
-    float2 cA = mul2(keep, f2(1.0f - omega));
-    float2 cB = mul2(keep, f2(omega));
-    if (solid0) cA.x = 1.0f, cB.x = 0.0f;
-    if (solid1) cA.y = 1.0f, cB.y = 0.0f;
-    const float2 cBw1 = mul2(cB, f2(wf(1))), cBw2 = mul2(cB, f2(wf(7)));
-    const float2 cBt1 = mul2(cB, f2(3.0f * wf(1))), cBt2 = mul2(cB, f2(3.0f * wf(7)));
-    w[0] = f2h(fma2(cA, h2f(w[0]), mul2(mul2(cB, f2(wf(0))), base)));
-#pragma unroll
-    for (int p = 0; p < 9; ++p)
-    {
-        const int q = pair_head(p);
-        const int qb = inv(q);
-        float2 cj;
-        if (p == 0) cj = jx;
-        else if (p == 1) cj = jy;
-        else if (p == 2) cj = jz;
-        else if (p == 3) cj = add2(jx, jy);
-        else if (p == 4) cj = sub2(jx, jy);
-        else if (p == 5) cj = add2(jx, jz);
-        else if (p == 6) cj = sub2(jx, jz);
-        else if (p == 7) cj = add2(jy, jz);
-        else cj = sub2(jy, jz);
-        const float2 cBw = q < 7 ? cBw1 : cBw2;
-        const float2 cBt = q < 7 ? cBt1 : cBt2;
-        const float2 e = mul2(cBw, fma2(k45, mul2(cj, cj), base));
-        const float2 o = mul2(cBt, cj);
-        w[q] = f2h(fma2(cA, h2f(w[q]), add2(e, o)));
-        w[qb] = f2h(fma2(cA, h2f(w[qb]), sub2(e, o)));
-    }
-}
-
-// collide2_packed() in fewer operations, for kernels with registers to
-// spare: each word is converted to FP32 once; the moments share partial sums
+// collide2() on packed FP16 words: each word is converted to FP32 once; the moments share partial sums
 // (rho = g0 + rest + S(x+) + S(x-), jx = S(x+) - S(x-)); each direction of a
 // pair (q, inv q) is two FMAs from the pair's equilibrium term
 //   e = (cB w k45) (c.J)^2 + cB w base,   G'_q = cA G_q + e +- 3 cB w (c.J).
@@ -512,164 +430,6 @@ __device__ __forceinline__ void collide2_grouped(unsigned (&w)[Q], float inv_sca
     }
 }
 
-// FP16 fused step, CELLS = 2 or 4 x-adjacent cells per thread (one aligned
-// 4- or 8-byte vector per direction).  Same pull / bounce-back / x-face /
-// collision semantics as k_step.
-template <int CELLS, int BLOCK, int MINB>
-__global__ void __launch_bounds__(BLOCK, MINB) k_step_h(const __half* __restrict__ fin, __half* __restrict__ fout,
-                                                        Layout L, StepArgs a, float inv_scale)
-{
-    constexpr int NW = CELLS / 2;   // half2 words per direction
-    constexpr int BC = block_cells(2);   // cells per interleaved block
-    constexpr int BE = 19 * BC;          // elements per block
-    const int lane = threadIdx.x & 31;
-    const int c0r = CELLS * (blockIdx.x * BLOCK + threadIdx.x);
-    const bool active = c0r < L.nx;
-    const int c0 = active ? c0r : ((L.nx - 1) & ~(CELLS - 1));
-    const int j = blockIdx.y + 1;
-    const int k = blockIdx.z + 1;
-    const long long e0 = L.elem(0, c0 + 1, j, k);
-    const __half* own = fin + e0;
-    const long long rs = L.row_stride, ps = L.plane_stride;
-    if (a.prefetch_rows > 0)
-        prefetch_rows_ahead<__half, CELLS * BLOCK>(fin, L, a.prefetch_rows, j, k, CELLS * BLOCK * blockIdx.x);
-
-    uint32_t lk[CELLS];
-#pragma unroll
-    for (int c = 0; c < CELLS; ++c) lk[c] = 0u;
-    if (active)
-    {
-        const uint32_t b = near_bits(a, L, c0, j, k) & ((1u << CELLS) - 1u);
-        if (b)
-        {
-            const long long cl = L.cell(c0 + 1, j, k);
-#pragma unroll
-            for (int c = 0; c < CELLS; ++c)
-                if ((b >> c) & 1u) lk[c] = a.links[cl + c];
-        }
-    }
-    uint32_t lka = 0u;
-#pragma unroll
-    for (int c = 0; c < CELLS; ++c) lka |= lk[c];
-    const bool any_link = __any_sync(kFull, lka != 0u);
-
-    // w[h][q]: cells (c0 + 2h, c0 + 2h + 1) of direction q, already shifted
-    unsigned w[NW][Q];
-#pragma unroll
-    for (int q = 0; q < Q; ++q)
-    {
-        const __half* row = own - (ey(q) * rs + ez(q) * ps) + q * BC;
-        unsigned cur[NW];
-        if constexpr (NW == 1)
-        {
-            cur[0] = __ldg(reinterpret_cast<const unsigned*>(row));
-        }
-        else
-        {
-            const uint2 v = __ldg(reinterpret_cast<const uint2*>(row));
-            cur[0] = v.x;
-            cur[1] = v.y;
-        }
-        if (ex(q) == 0)
-        {
-#pragma unroll
-            for (int h = 0; h < NW; ++h) w[h][q] = cur[h];
-        }
-        else if (ex(q) > 0)
-        {
-            // lane 0 starts a block: its left neighbour is the previous block's last pair
-            unsigned prev = __shfl_up_sync(kFull, cur[NW - 1], 1);
-            if (lane == 0) prev = __ldg(reinterpret_cast<const unsigned*>(row - BE + (BC - 2)));
-            w[0][q] = __byte_perm(prev, cur[0], 0x5432);
-#pragma unroll
-            for (int h = 1; h < NW; ++h) w[h][q] = __byte_perm(cur[h - 1], cur[h], 0x5432);
-        }
-        else
-        {
-            // lane 31 ends a block: its right neighbour is the next block's first pair
-            unsigned next = __shfl_down_sync(kFull, cur[0], 1);
-            if (lane == 31)
-                next = __ldg(reinterpret_cast<const unsigned*>(row + BE - (BC - CELLS)));
-#pragma unroll
-            for (int h = 0; h < NW - 1; ++h) w[h][q] = __byte_perm(cur[h], cur[h + 1], 0x5432);
-            w[NW - 1][q] = __byte_perm(cur[NW - 1], next, 0x5432);
-        }
-    }
-    if (any_link)
-    {
-#pragma unroll
-        for (int q = 0; q < Q; ++q)
-        {
-            if ((lka >> q) & 1u)
-            {
-#pragma unroll
-                for (int h = 0; h < NW; ++h)
-                {
-                    const unsigned o = __ldg(reinterpret_cast<const unsigned*>(own + inv(q) * BC + 2 * h));
-                    const unsigned m = (((lk[2 * h] >> q) & 1u) ? 0x0000ffffu : 0u) |
-                                       (((lk[2 * h + 1] >> q) & 1u) ? 0xffff0000u : 0u);
-                    w[h][q] = (w[h][q] & ~m) | (o & m);
-                }
-            }
-        }
-    }
-    if (!active) return;
-
-    // x faces: sources in the x halo come from the x-face ghosts.
-    const int last = L.nx - 1 - c0;   // position of cell nx-1 in this group when in 0..CELLS-1
-    const bool xlo = c0 == 0;
-    const bool xhi = last >= 0 && last < CELLS;
-    if (xlo | xhi)
-    {
-#pragma unroll
-        for (int q = 0; q < Q; ++q)
-        {
-            if (ex(q) == 0) continue;
-            const float g = a.xf.xgh[a.xf.gh_index(ex(q) > 0 ? 0 : 1, q, j - ey(q), k - ez(q), L.ny, L.nz)];
-            if (ex(q) > 0 && xlo && !((lk[0] >> q) & 1u)) w[0][q] = set_lo(w[0][q], g);
-#pragma unroll
-            for (int h = 0; h < NW; ++h)
-            {
-                if (ex(q) < 0 && xhi && last == 2 * h && !((lk[2 * h] >> q) & 1u)) w[h][q] = set_lo(w[h][q], g);
-                if (ex(q) < 0 && xhi && last == 2 * h + 1 && !((lk[2 * h + 1] >> q) & 1u))
-                    w[h][q] = set_hi(w[h][q], g);
-            }
-        }
-    }
-
-    const float syz = fmaxf(a.sig_y[j - 1], a.sig_z[k - 1]);
-#pragma unroll
-    for (int h = 0; h < NW; ++h)
-    {
-        const int ca = c0 + 2 * h;
-        const float2 sg = make_float2(fmaxf(ca < L.nx ? a.sig_x[ca] : 0.f, syz),
-                                      fmaxf(ca + 1 < L.nx ? a.sig_x[ca + 1] : 0.f, syz));
-        collide2_packed(w[h], inv_scale, a.omega, sg, (lk[2 * h] & kSolidSelfBit) != 0u,
-                        (lk[2 * h + 1] & kSolidSelfBit) != 0u);
-    }
-    __half* out = fout + e0;
-#pragma unroll
-    for (int q = 0; q < Q; ++q)
-    {
-        if constexpr (NW == 1) *reinterpret_cast<unsigned*>(out + q * BC) = w[0][q];
-        else *reinterpret_cast<uint2*>(out + q * BC) = make_uint2(w[0][q], w[1][q]);
-    }
-    if (xlo | xhi)
-    {
-#pragma unroll
-        for (int q = 0; q < Q; ++q)
-        {
-            if (xlo) a.xf.xexp[a.xf.exp_index(0, q, j, k, L.ny, L.nz)] = h2f(w[0][q]).x;
-#pragma unroll
-            for (int h = 0; h < NW; ++h)
-            {
-                if (xhi && last == 2 * h) a.xf.xexp[a.xf.exp_index(1, q, j, k, L.ny, L.nz)] = h2f(w[h][q]).x;
-                if (xhi && last == 2 * h + 1) a.xf.xexp[a.xf.exp_index(1, q, j, k, L.ny, L.nz)] = h2f(w[h][q]).y;
-            }
-        }
-    }
-}
-
 // ---------------------------------------------------------------- FP16 step, warp pipelines
 // Each warp walks whole rows one interleaved block (64 cells, two per lane)
 // at a time and keeps the source lines of its next P blocks in flight as
@@ -718,7 +478,7 @@ __host__ __device__ constexpr int ghost_slot(int q)
     return t[q];
 }
 
-template <int P, int WARPS, int MINB, bool GROUPED = true>
+template <int P, int WARPS, int MINB>
 __global__ void __launch_bounds__(32 * WARPS, MINB) k_step_hw(const __half* __restrict__ fin,
                                                                __half* __restrict__ fout, Layout L, StepArgs a,
                                                                float inv_scale)
@@ -931,10 +691,7 @@ __global__ void __launch_bounds__(32 * WARPS, MINB) k_step_hw(const __half* __re
         if (active)
         {
             const float2 sg = make_float2(fmaxf(sx0, syz), fmaxf(sx1, syz));
-            if constexpr (GROUPED)
-                collide2_grouped(w, inv_scale, a.omega, sg, (lk0 & kSolidSelfBit) != 0u, (lk1 & kSolidSelfBit) != 0u);
-            else
-                collide2_packed(w, inv_scale, a.omega, sg, (lk0 & kSolidSelfBit) != 0u, (lk1 & kSolidSelfBit) != 0u);
+            collide2_grouped(w, inv_scale, a.omega, sg, (lk0 & kSolidSelfBit) != 0u, (lk1 & kSolidSelfBit) != 0u);
 #pragma unroll
             for (int q = 0; q < Q; ++q)
                 if (LBM_IN(kChkHwStore, 2 * (outp - reinterpret_cast<unsigned*>(fout)) + 64 * q, L.total - 1))
@@ -1322,6 +1079,7 @@ __global__ void __launch_bounds__(256) k_probe(const S* __restrict__ f, Layout L
             else if (1.0f + rp <= 0.f) val = 1e-12 - 1.0;
             else val = (double)rp;
             a.energy[p] += val * val;
+            if (!isfinite(val)) *a.nonfinite = 1;
         }
         a.out[row * a.n + p] = val;
     }
@@ -1417,6 +1175,8 @@ __global__ void k_check_selftest()
 // (rho - 1) passes through it instead of a temporary cudaMalloc buffer.  It
 // exists on every GPU that loads this library, for the life of the process.
 static __device__ __align__(256) float g_field_scratch[kNoAllocFieldCells];
+static_assert(sizeof(g_field_scratch) == sizeof(float) * LBM_NOALLOC_MAX_CELLS,
+              "the static field array must hold the grid size lbm_get_rho_noalloc accepts");
 
 dim3 row_grid(const Layout& L) { return dim3((unsigned)((L.nx + 127) / 128), (unsigned)L.ny, (unsigned)L.nz); }
 dim3 pair_grid(const Layout& L, int block)
@@ -1432,7 +1192,7 @@ dim3 grid_n(const Layout& L, int cells, int block)
 // Warp-pipelined FP16 step: dynamic shared memory (one ring per warp) and a
 // grid of as many CTAs as the GPU holds at once (every warp then walks rows
 // all_warps apart).  The attribute and the occupancy are set up once per device.
-template <int P, int WARPS, int MINB, bool GROUPED = true>
+template <int P, int WARPS, int MINB>
 cudaError_t hw_ctas(int* out)
 {
     constexpr int smem = WARPS * (P + 2) * wp::kSlotBytes;
@@ -1445,10 +1205,10 @@ cudaError_t hw_ctas(int* out)
     std::lock_guard<std::mutex> lock(mu);
     if (!ctas[dev])
     {
-        e = cudaFuncSetAttribute(k_step_hw<P, WARPS, MINB, GROUPED>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        e = cudaFuncSetAttribute(k_step_hw<P, WARPS, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         int per_sm = 0, sms = 0;
         if (e == cudaSuccess)
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_hw<P, WARPS, MINB, GROUPED>, 32 * WARPS, smem);
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_hw<P, WARPS, MINB>, 32 * WARPS, smem);
         if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         if (e != cudaSuccess) return e;
         if (per_sm < 1) return cudaErrorInvalidConfiguration;
@@ -1458,49 +1218,28 @@ cudaError_t hw_ctas(int* out)
     return cudaSuccess;
 }
 
-template <int P, int WARPS, int MINB, bool GROUPED = true>
+template <int P, int WARPS, int MINB>
 cudaError_t launch_hw(const __half* fin, __half* fout, const Layout& L, const StepArgs& a, float inv_scale,
                       cudaStream_t stream)
 {
     // the per-lane source offsets are 32-bit
     if (L.plane_stride + L.row_stride + 19 * 64 > 0x7fffffffLL) return cudaErrorInvalidValue;
     int ctas = 0;
-    const cudaError_t e = hw_ctas<P, WARPS, MINB, GROUPED>(&ctas);
+    const cudaError_t e = hw_ctas<P, WARPS, MINB>(&ctas);
     if (e != cudaSuccess) return e;
     const long long need = ((long long)L.ny * L.nz + WARPS - 1) / WARPS;
     const int grid = (int)(need < ctas ? need : ctas);
-    k_step_hw<P, WARPS, MINB, GROUPED><<<grid, 32 * WARPS, WARPS * (P + 2) * wp::kSlotBytes, stream>>>(fin, fout, L, a, inv_scale);
+    k_step_hw<P, WARPS, MINB><<<grid, 32 * WARPS, WARPS * (P + 2) * wp::kSlotBytes, stream>>>(fin, fout, L, a, inv_scale);
     return cudaGetLastError();
 }
 
 template <typename S>
-cudaError_t launch_step_t(const S* fin, S* fout, const Layout& L, const StepArgs& a, float inv_scale, int variant,
+cudaError_t launch_step_t(const S* fin, S* fout, const Layout& L, const StepArgs& a, float inv_scale,
                           cudaStream_t stream)
 {
     if constexpr (std::is_same<S, __half>::value)
-    {
-        switch (variant)
-        {
-        case 8: return launch_hw<4, 4, 3>(fin, fout, L, a, inv_scale, stream);
-        case 9: return launch_hw<3, 4, 4>(fin, fout, L, a, inv_scale, stream);
-        case 10: return launch_hw<2, 4, 5>(fin, fout, L, a, inv_scale, stream);
-        case 11: return launch_hw<6, 2, 4>(fin, fout, L, a, inv_scale, stream);
-        case 12: return launch_hw<4, 8, 1>(fin, fout, L, a, inv_scale, stream);
-        case 13: return launch_hw<2, 4, 5, false>(fin, fout, L, a, inv_scale, stream);
-        case 4: k_step_h<2, 128, 8><<<grid_n(L, 2, 128), 128, 0, stream>>>(fin, fout, L, a, inv_scale); return cudaGetLastError();
-        case 5: k_step_h<4, 128, 6><<<grid_n(L, 4, 128), 128, 0, stream>>>(fin, fout, L, a, inv_scale); return cudaGetLastError();
-        case 6: k_step_h<2, 128, 10><<<grid_n(L, 2, 128), 128, 0, stream>>>(fin, fout, L, a, inv_scale); return cudaGetLastError();
-        case 7: k_step_h<4, 128, 5><<<grid_n(L, 4, 128), 128, 0, stream>>>(fin, fout, L, a, inv_scale); return cudaGetLastError();
-        default: break;
-        }
-    }
-    switch (variant)
-    {
-    case 1: k_step<S, 128, 8><<<pair_grid(L, 128), 128, 0, stream>>>(fin, fout, L, a, inv_scale); break;
-    case 2: k_step<S, 256, 4><<<pair_grid(L, 256), 256, 0, stream>>>(fin, fout, L, a, inv_scale); break;
-    case 3: k_step<S, 64, 0><<<pair_grid(L, 64), 64, 0, stream>>>(fin, fout, L, a, inv_scale); break;
-    default: k_step<S, 128, 0><<<pair_grid(L, 128), 128, 0, stream>>>(fin, fout, L, a, inv_scale); break;
-    }
+        return launch_hw<2, 4, 5>(fin, fout, L, a, inv_scale, stream);
+    k_step<S, 128, 0><<<pair_grid(L, 128), 128, 0, stream>>>(fin, fout, L, a, inv_scale);
     return cudaGetLastError();
 }
 
@@ -1541,27 +1280,18 @@ cudaError_t launch_build_links(const uint8_t* mask_ref, uint32_t* links, uint32_
     return cudaGetLastError();
 }
 
-cudaError_t prepare_step(int storage, int variant)
+cudaError_t prepare_step(int storage)
 {
     if (storage == 0) return cudaSuccess;
     int ctas = 0;
-    switch (variant)
-    {
-    case 8: return hw_ctas<4, 4, 3>(&ctas);
-    case 9: return hw_ctas<3, 4, 4>(&ctas);
-    case 10: return hw_ctas<2, 4, 5>(&ctas);
-    case 11: return hw_ctas<6, 2, 4>(&ctas);
-    case 12: return hw_ctas<4, 8, 1>(&ctas);
-    case 13: return hw_ctas<2, 4, 5, false>(&ctas);
-    default: return cudaSuccess;
-    }
+    return hw_ctas<2, 4, 5>(&ctas);
 }
 
 cudaError_t launch_step(int storage, const void* fin, void* fout, const Layout& L, const StepArgs& a,
-                        float scale, int variant, cudaStream_t stream)
+                        float scale, cudaStream_t stream)
 {
-    if (storage == 0) return launch_step_t<float>((const float*)fin, (float*)fout, L, a, 1.0f, variant, stream);
-    return launch_step_t<__half>((const __half*)fin, (__half*)fout, L, a, 1.0f / scale, variant, stream);
+    if (storage == 0) return launch_step_t<float>((const float*)fin, (float*)fout, L, a, 1.0f, stream);
+    return launch_step_t<__half>((const __half*)fin, (__half*)fout, L, a, 1.0f / scale, stream);
 }
 
 cudaError_t launch_step_moments(const float* fin, float* fout, const Layout& L, const StepArgs& a,

@@ -580,6 +580,7 @@ __global__ void __launch_bounds__(256) k_probe_a(const float* __restrict__ f, La
             for (int q = 0; q < Q; ++q) rho += G[q];
             val = (lk & kSolidSelfBit) ? 0.0 : (double)rho;
             a.energy[p] += val * val;
+            if (!isfinite(val)) *a.nonfinite = 1;
         }
         a.out[row * a.n + p] = val;
     }

@@ -16,6 +16,7 @@ c_long_p = ctypes.POINTER(ctypes.c_long)
 LBM_OK = 0
 LBM_WARN_STL_NOT_LOADED = 1
 LBM_WARN_PROBE_IN_SOLID = 2
+LBM_WARN_STL_TRUNCATED = 3
 LBM_ERR_INVALID_ARGUMENT = -1
 LBM_ERR_BAD_CONFIG = -2
 LBM_ERR_OUT_OF_MEMORY = -3

@@ -36,11 +36,22 @@ typedef enum lbm_status
     LBM_OK = 0,
     LBM_WARN_STL_NOT_LOADED = 1,   /* 06:397-410: geometry left empty, run continues */
     LBM_WARN_PROBE_IN_SOLID = 2,   /* 06:432-435: probe cell is SOLID, run continues */
+    LBM_WARN_STL_TRUNCATED = 3,    /* the STL ends before its header's triangle count; the missing
+                                      records read as zeros, as the reference's loader leaves them
+                                      (06:82-85), and the run continues */
     LBM_ERR_INVALID_ARGUMENT = -1,
     LBM_ERR_BAD_CONFIG = -2,
     LBM_ERR_OUT_OF_MEMORY = -3,
     LBM_ERR_CUDA = -4,
-    LBM_ERR_NAN = -5,
+    LBM_ERR_NAN = -5,              /* an owned probe read a non-finite value.  The probe kernel
+                                      sets a device flag that lbm_step / lbm_run read at the end
+                                      of each batch of steps (at most 4096 steps, usually the
+                                      whole call): the call in which the value appeared returns
+                                      this code, with the steps taken; the flag stays set, so
+                                      every later lbm_step call returns it too.  Standalone
+                                      lbm_record_probes calls are checked at the next lbm_step
+                                      or lbm_get_probes.  A grid without probes is not checked
+                                      (the reference checks nothing). */
     LBM_ERR_STATE = -6,            /* call out of order, e.g. step before init */
     LBM_ERR_CAPACITY = -7,         /* caller's output buffer too small */
     LBM_ERR_NO_DEVICE = -8,
@@ -205,7 +216,10 @@ const char* lbm_last_error(lbm_handle* h);
 
 /* Binary STL file; vertices * scale + (sx,sy,sz) as GeometryEngine::load
  * (06:70-111).  Returns LBM_WARN_STL_NOT_LOADED and keeps an empty geometry
- * when the file cannot be read, as the reference does (06:397-410). */
+ * when the file cannot be read, as the reference does (06:397-410), and
+ * LBM_WARN_STL_TRUNCATED when the file holds fewer records than its header
+ * counts (the mask is the reference's: missing records are zero triangles).
+ * The status is also returned by lbm_init when no probe warning replaces it. */
 int lbm_set_geometry_stl(lbm_handle* h, const char* path, double scale, double sx, double sy, double sz);
 /* Same, from memory: tris holds ntris * 9 floats (v1, v2, v3). */
 int lbm_set_geometry_triangles(lbm_handle* h, const float* tris, int ntris, double scale, double sx,
@@ -276,7 +290,9 @@ long lbm_get_step(lbm_handle* h);
 int lbm_get_probes(lbm_handle* h, double* out, long capacity, long* nsteps);
 /* Per-probe sum over recorded steps of (rho-1)^2, accumulated in FP64. */
 int lbm_get_probe_energy(lbm_handle* h, double* out);
-/* Interior field (float)(rho-1) of the last step, i fastest (06:979-985). */
+/* Interior field (float)(rho-1) of the last step, i fastest (06:979-985).
+ * Before the first step it is 0 (rho starts at 1, 06:368), or, after
+ * lbm_set_density, the initial pulse at FLUID cells (01:197). */
 int lbm_get_rho(lbm_handle* h, float* out, long capacity);
 /* Largest grid (interior cells) lbm_get_rho_noalloc accepts. */
 #define LBM_NOALLOC_MAX_CELLS 8388608L
@@ -292,8 +308,10 @@ int lbm_get_rho(lbm_handle* h, float* out, long capacity);
  * reserved statically in the library: every GPU that loads the library
  * holds it until the process exits, and nothing is allocated per call.
  * Grids with more interior cells are rejected with LBM_ERR_UNSUPPORTED.
- * The first call on a device looks up the array's address; make that first
- * call before any CUDA stream capture.  All handles on a device share the
+ * The first call on a device looks up the array's address and keeps it for
+ * the life of the process; make that first call before any CUDA stream
+ * capture, and do not reset the device (cudaDeviceReset) while the library
+ * is in use: the kept address, like every handle's memory, would be stale.  All handles on a device share the
  * array: calls that overlap on the GPU (handles used from different host
  * threads at the same time) race and may return each other's field, so
  * serialise them.  The array keeps the last call's contents; every call

@@ -32,6 +32,13 @@ _dp = abi.c_double_p
 _lib = None
 
 
+def reference_dir():
+    """Directory of the reference sources: NLOS_REFERENCE_DIR, else the
+    default written in oracle/Makefile."""
+    r = subprocess.run(["make", "-s", "-C", HERE, "print-ref-dir"], check=True, capture_output=True, text=True)
+    return r.stdout.strip()
+
+
 def build(ref=False):
     """Compile the restatement (and the reference harness when ref=True)."""
     cmd = ["make", "-s", "-C", HERE, "all"] + (["ref"] if ref else [])

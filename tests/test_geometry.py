@@ -101,3 +101,22 @@ def test_city_generator_properties():
         gap = np.maximum(gx, gy)
         gap[i] = np.inf
         assert gap.min() >= 8
+
+
+@pytest.mark.skipif(not oracle.ref_available("06"), reason="reference harness not built here")
+@pytest.mark.parametrize("keep,extra", [(30, 0), (30, 17)])
+def test_truncated_stl_oracle_matches_live_reference(keep, extra, tmp_path):
+    """GeometryEngine::load on a file shorter than its header's count (06:74-85):
+    the missing bytes stay zero.  The oracle reads it the same way, which the
+    GPU tests then hold the library's mask to."""
+    nx, ny, nz = 96, 80, 40
+    tris, _ = nlos_lbm.city_triangles(nx, ny, seed=7, height=(5, 30), fp=(10, 24), street=6)
+    path = str(tmp_path / "t.stl")
+    nlos_lbm.stl_write(path, tris)
+    raw = open(path, "rb").read()
+    open(path, "wb").write(raw[:84 + 50 * keep + extra])
+    cfg = abi.reference_config(x_min=0, x_max=nx, y_min=0, y_max=ny, z_min=0, z_max=nz, dx=1.0)
+    ref = oracle.RefSolver("06", (0, nx), (0, ny), (0, nz), 1.0, 0.55, (1, 1, 1, 1, 1, 1, 0, 0, 0), stl=path)
+    o = oracle.OracleSolver(cfg, [], None, stl=path)
+    assert np.array_equal(o.get_mask(), ref.get_mask())
+    assert o.get_mask().sum() > 0

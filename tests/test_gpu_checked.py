@@ -1,6 +1,6 @@
 """The bounds-checked library (liblbm_b200_check.so, NLOS_LBM_CHECK=1) on the
 GPU: its self-test trips exactly one check, and the forward (FP32, FP16 warp
-pipelines, register-held FP16), scheme-A (03, and 01 with its blend sponge,
+pipelines), scheme-A (03, and 01 with its blend sponge,
 periodic z and initial density) and adjoint kernels run the parity
 scenarios without a single out-of-range index, with the same results as the
 product library.  The checked library runs in a child process (a process
@@ -26,7 +26,7 @@ sys.path[:0] = [sys.argv[1], os.path.join(sys.argv[1], "city-scale-nlos-acoustic
 import numpy as np
 import scenarios
 from nlos_lbm import Solver, abi
-import test_gpu_step_variants as tv
+import test_gpu_fp16_step as tv
 assert abi.CHECKED
 out = {}
 sc = scenarios.scenario("lloyd_small")
@@ -42,16 +42,11 @@ runs = {
     "scheme_a_01": scenarios.scattering_a(steps=20),
 }
 for name, s in runs.items():
-    for variant in ((None, "4") if name.startswith("fp16") else (None,)):
-        if variant:
-            os.environ["NLOS_LBM_STEP_VARIANT"] = variant
-        g = Solver(s["cfg"], s["sources"], s["probes"], triangles=s.get("triangles"), mask=s.get("mask"))
-        os.environ.pop("NLOS_LBM_STEP_VARIANT", None)
-        if s.get("rho0") is not None:
-            g.set_density(s["rho0"])
-        g.step(min(s["steps"], 60))
-        key = name + ("_v" + variant if variant else "")
-        out[key] = {"status": g.check_status(), "probes": g.get_probes().tolist()}
+    g = Solver(s["cfg"], s["sources"], s["probes"], triangles=s.get("triangles"), mask=s.get("mask"))
+    if s.get("rho0") is not None:
+        g.set_density(s["rho0"])
+    g.step(min(s["steps"], 60))
+    out[name] = {"status": g.check_status(), "probes": g.get_probes().tolist()}
 a = scenarios.adjoint_scenario(nx=32, ny=24, nz=16, steps=30, nprobe=6)
 g = Solver(a["cfg"], [a["trial"]], a["probes"], triangles=a["triangles"])
 L, gp, gs, _ = g.adjoint_grad(a["observed"], 10, 0)
@@ -62,7 +57,7 @@ print(json.dumps(out))
 
 def _product_runs():
     import scenarios
-    import test_gpu_step_variants as tv
+    import test_gpu_fp16_step as tv
 
     runs = {
         "fp32_city": scenarios.scenario("city_small"),

@@ -19,10 +19,6 @@ from nlos_lbm import abi
 
 pytestmark = pytest.mark.gpu
 
-# field values are FP32; the tolerance of the FP32 parity tests
-RTOL = 1e-5
-
-
 def rho_alloc(s):
     return s.get_rho().ravel()
 
@@ -35,9 +31,11 @@ def rho_noalloc(s):
     return out
 
 
-def close(a, b):
+def same(a, b):
+    """Both entry points run the same field kernel on the same state: the
+    results must be equal bit for bit, and not trivially zero."""
     assert a.shape == b.shape
-    assert np.linalg.norm(a.astype(np.float64) - b) <= RTOL * np.linalg.norm(b.astype(np.float64))
+    assert np.array_equal(a, b)
     assert np.max(np.abs(b)) > 0
 
 
@@ -51,18 +49,38 @@ def test_noalloc_field_matches_allocating_call_twice_in_a_row(gpu):
     # two calls in a row on one handle
     first, second = rho_noalloc(a), rho_noalloc(a)
     ref_a = rho_alloc(a)
-    close(first, ref_a)
-    close(second, ref_a)
+    same(first, ref_a)
+    same(second, ref_a)
     # a smaller grid after a larger one: the shared array's leftovers must not leak
-    close(rho_noalloc(b), rho_alloc(b))
+    same(rho_noalloc(b), rho_alloc(b))
     # state moves on: the next call returns the new field
     a.step(7)
-    close(rho_noalloc(a), rho_alloc(a))
+    same(rho_noalloc(a), rho_alloc(a))
     # FP16 storage goes through the same path
     h16 = scenarios.scenario("scatter_small", storage=abi.LBM_STORE_F16, f16_scale=1e3)
     c = nlos_lbm.Solver(h16["cfg"], h16["sources"], h16["probes"], triangles=h16["triangles"])
     c.step(40)
-    close(rho_noalloc(c), rho_alloc(c))
+    same(rho_noalloc(c), rho_alloc(c))
+
+
+def test_noalloc_field_of_scheme_a_with_initial_pulse(gpu):
+    """01's set-up (scheme A, initial density pulse, periodic z): before the
+    first step both entry points return the pulse at FLUID cells (01:197),
+    after steps the scheme-A field kernel's output, through the static array."""
+    sc = scenarios.scattering_a(steps=20)
+    g = nlos_lbm.Solver(sc["cfg"], sc["sources"], sc["probes"], mask=sc.get("mask"))
+    g.set_density(sc["rho0"])
+    before = rho_noalloc(g)
+    same(before, rho_alloc(g))
+    nx, ny, nz = g.dims
+    mask = g.get_mask().reshape(nz + 2, ny + 2, nx + 2)[1:-1, 1:-1, 1:-1].ravel()   # interior, i fastest
+    pulse = np.asarray(sc["rho0"], dtype=np.float64).ravel().astype(np.float32)
+    assert np.array_equal(before, np.where(mask == 1, np.float32(0), pulse))
+    g.step(5)
+    first, second = rho_noalloc(g), rho_noalloc(g)
+    same(first, rho_alloc(g))
+    same(second, first)
+    assert not np.array_equal(first, before)
 
 
 def test_noalloc_rejects_grids_beyond_its_array(gpu):
