@@ -37,9 +37,9 @@ METRIC = "D3Q19 GLUPS, %HBM peak: FP16-store vs FP32 @<=1e-3 probe L2; adjoint g
 NCU_TRAFFIC_PER_CELL = {"fp16": 2.644e9 / 33554432, "fp32": 5.132e9 / 33554432}
 UNIT = "GLUPS"
 L2_BYTES = 126e6   # B200 L2
-# steps of the FP16-vs-FP32 probe comparison on the 1024x1024x256 city (the
-# Ricker sources' first periods reach the nearer street-level probes)
-ERR_STEPS = 400
+# steps of the FP16-vs-FP32 probe comparison on the 1024x1024x256 city: the
+# workload's whole configured length
+ERR_STEPS = 4000
 
 
 def measured_peaks():
@@ -319,19 +319,41 @@ def family_a_cpu(name, seconds=5.0):
                       "exchange_halos+step, FP64"}
 
 
-def cpu_baseline(steps_hint=None):
-    """Reference CPU step on a bounded sub-domain of the city (rank 0, N=1)."""
+# The reference arm's sample: a 256x256 plan window of the headline city (the
+# 2048x2048x256 generator, seed 2024), 128 layers.  An FP64 run of the whole
+# headline grid would need about 330 GB of host memory (19 x 8 B x 2 buffers
+# per cell), so the reference is timed on this window as a rate.
+REF_WINDOW = (896, 896, 256, 128)   # x0, y0, width, layers
+
+
+def reference_sample():
+    """Triangles of the window, built by the pure-Python restatement of the
+    city generator (oracle/city.py), so the reference arm maps no library of
+    the product."""
+    from oracle import city
+
+    x0, y0, w, _ = REF_WINDOW
+    boxes, _ = city.city_boxes(2048, 2048, 2024, fp=(20, 60), height=(10, 80), coverage=0.40, street=8, margin=40)
+    part = city.crop_boxes(boxes, x0, y0, x0 + w, y0 + w)
+    tris = np.concatenate([city.box_triangles(*b) for b in part]) if part else np.zeros((0, 9), np.float32)
+    return tris
+
+
+def cpu_baseline(steps_hint=None, seconds=12.0):
+    """The reference's CPU step on the bounded sample (rank 0, N=1): the
+    unmodified 06 (oracle/_ref/libref06.so: apply_source, exchange_halos,
+    step_collision_bgk, FP64, OpenMP on every host thread), or the FP64 port
+    where the reference was not built."""
     import oracle
+    from oracle import city
 
-    from nlos_lbm import workloads
-    from nlos_lbm.solver import city_triangles, stl_write
-
-    nx, ny, nz = 256, 256, 128
-    tris, _ = city_triangles(nx, ny, seed=2024, fp=(20, 60), height=(10, 80), coverage=0.40, street=8, margin=40)
+    _, _, w, nz = REF_WINDOW
+    nx = ny = w
+    tris = reference_sample()
     threads = os.cpu_count() or 1
     if oracle.ref_available("06"):
-        stl = "/tmp/bench_city_sample.stl"
-        stl_write(stl, tris)
+        stl = "/tmp/bench_city_window.stl"
+        city.stl_write(stl, tris)
         ref = oracle.RefSolver("06", (0, nx), (0, ny), (0, nz), 1.0, 0.51, (128.5, 128.5, 2.5, 128.5, 128.5, 2.5,
                                                                            0.0, 10.0, 0.0), stl=stl)
         kind = "reference"
@@ -339,8 +361,9 @@ def cpu_baseline(steps_hint=None):
         def run(n):
             ref.step(n)
     else:
-        cfg = workloads.lattice_config(nx, ny, nz, 0.51)
         from nlos_lbm import abi
+        cfg = abi.reference_config(x_min=0.0, x_max=float(nx), y_min=0.0, y_max=float(ny), z_min=0.0,
+                                   z_max=float(nz), dx=1.0, c_phys=abi.CS, tau=0.51)
         src = abi.reference_source(sx=128.5, sy=128.5, sz=2.5, ex=128.5, ey=128.5, ez=2.5, amp=1e-3, t0=40.0,
                                    sigma_t=8.0)
         orc = oracle.OracleSolver(cfg, [src], None, triangles=tris)
@@ -352,14 +375,15 @@ def cpu_baseline(steps_hint=None):
     t0 = time.perf_counter()
     run(2)
     per = (time.perf_counter() - t0) / 2
-    n = steps_hint or max(2, min(200, int(12.0 / max(per, 1e-6))))
+    n = steps_hint or max(2, min(200, int(seconds / max(per, 1e-6))))
     t0 = time.perf_counter()
     run(n)
     dt = time.perf_counter() - t0
     cells = nx * ny * nz
+    x0, y0 = REF_WINDOW[:2]
     return dict(value=cells * n / dt / 1e9, unit=UNIT, cores=threads, kind=kind,
-                sample=f"{nx}x{ny}x{nz} sub-domain of the seeded city, {n} full steps "
-                       f"(apply_source+exchange_halos+step_collision_bgk), FP64, {threads} OpenMP threads",
+                sample=f"{nx}x{ny}x{nz} window [{x0},{x0 + nx})x[{y0},{y0 + ny}) of the 2048x2048x256 city, "
+                       f"{n} full steps (apply_source+exchange_halos+step_collision_bgk), FP64, {threads} threads",
                 seconds=dt, steps=n)
 
 
@@ -370,18 +394,75 @@ def run_reference_arm(args):
     import oracle
 
     oracle_kind = "reference" if oracle.ref_available("06") else "port"
-    # warm-up + timed steps on the bounded sample
+    # each timed step of the sample is one reference step; the whole run is bounded
     b = cpu_baseline(steps_hint=max(1, args.steps))
     line = {"metric": METRIC, "value": b["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": b["steps"],
             "warmup": args.warmup, "ms_per_step": b["seconds"] / b["steps"] * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "impl": "reference",
-            "config": {"workload": "synthetic city (seeded boxes), 256x256x128 sub-domain of the city workload",
+            "config": {"workload": "city2048 (2048x2048x256 seeded box city) timed as a rate on a "
+                                   "256x256x128 window of it: the FP64 reference on the whole grid needs ~330 GB",
                        "sample": b["sample"]},
             "cpu_baseline": {"value": b["value"], "unit": UNIT, "cores": b["cores"], "kind": oracle_kind,
                              "sample": b["sample"]},
             "e2e": {"value": b["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_slab_arm(args, torch, dist, world, rank, local, barrier, reduce_max):
+    """Strong scaling: one z-slab of the headline grid per rank, the cut
+    messages (crossing populations only) moved by NCCL point-to-point."""
+    import nlos_lbm
+    from nlos_lbm import ranks, workloads
+
+    hbm_peak, peak_kind = measured_peaks()
+    storage = None if args.storage is None else (1 if args.storage == "fp16" else 0)
+    w = workloads.build(args.workload, storage=storage)
+    r = ranks.SlabRank(w["cfg"], dist, w["sources"], w["probes"], triangles=w["triangles"], device=local,
+                       staging="device")
+    nx, ny, nz = workloads.cells(w["cfg"])
+    cells = nx * ny * nz
+    r.step(args.warmup)
+    stream = r.stream
+    l0 = r.solver.launch_count
+    with ClockSampler(local) as clk:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        barrier()
+        e0.record(stream)
+        r.step(args.steps)
+        e1.record(stream)
+        e1.synchronize()
+        torch.cuda.synchronize()
+        barrier()
+    ms = reduce_max(e0.elapsed_time(e1))
+    launches = r.solver.launch_count - l0
+    h0, d0 = r.solver.transfer_bytes()
+    t0 = time.perf_counter()
+    r.step(args.steps)
+    r.solver.get_probes()
+    e2e_ms = reduce_max((time.perf_counter() - t0) * 1e3)
+    h1, d1 = r.solver.transfer_bytes()
+    clocks = clk.summary()
+    value = cells * args.steps / (ms / 1e3) / 1e9
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "fp16-store/fp32-compute" if w["cfg"].storage == 1 else "fp32",
+            "data": "synthetic (seeded box city voxelised from STL triangles)",
+            "config": {"workload": f"{args.workload}: {w['description']}", "grid": [nx, ny, nz],
+                       "parallelism": f"z-slabs x{world}", "slab_bounds": r.bounds,
+                       "message_bytes_per_cut": r.lib.lbm_slab_message_bytes(r.h)},
+            "e2e": {"value": cells * args.steps / (e2e_ms / 1e3) / 1e9, "unit": UNIT,
+                    "h2d_bytes_per_step": (h1 - h0) / args.steps, "d2h_bytes_per_step": (d1 - d0) / args.steps},
+            "gpu_launches": launches, "clocks": {k: clocks[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
+            "roofline": {"bound": "hbm", "peak": hbm_peak, "unit": "GB/s", "peak_kind": peak_kind,
+                         "achieved": cells / world * (76 if w["cfg"].storage == 1 else 152) / (ms / args.steps / 1e3) / 1e9,
+                         "traffic": None}}
+    line["roofline"]["frac"] = line["roofline"]["achieved"] / hbm_peak
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    r.close()
     return 0
 
 
@@ -400,6 +481,12 @@ def run_our_arm(args):
                                 device_id=torch.device("cuda", local))
 
     barrier, reduce_max = make_reducers(dist, "cuda")
+    if args.split == "slab":
+        rc = run_slab_arm(args, torch, dist, world, rank, local, barrier, reduce_max)
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+        return rc
 
     hbm_peak, peak_kind = measured_peaks()
     headline = args.workload
@@ -474,41 +561,50 @@ def run_our_arm(args):
     # moves cells times that.
     per_cell = NCU_TRAFFIC_PER_CELL.get(head["storage"])
     traffic = None if per_cell is None else per_cell * cells
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                "frac": achieved / hbm_peak, "traffic": traffic, "peak_kind": peak_kind,
+                "kernel": "k_step_hw" if head["storage"] == "fp16" else "k_step",
+                "kernel_ms": head["kernel_ms_avg"], "bytes_per_cell": head["bytes_per_cell"]}
+    for key in ("city1024_fp32", "city1024_fp16"):
+        if key in secondary:
+            roofline[key + "_frac"] = secondary[key]["hbm_frac_kernel"]
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": n, "steps": steps, "warmup": args.warmup,
-        "fluid_glups": value * head["fluid_fraction"],
         "ms_per_step": head["ms"] / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "fp16-store/fp32-compute" if head["storage"] == "fp16" else "fp32",
         "data": "synthetic (seeded box city voxelised from STL triangles)",
         "config": {"workload": f"{headline}: {head['description']}", "grid": head["dims"],
-                   "storage": head["storage"], "plan_coverage": head["coverage"],
-                   "fluid_fraction": head["fluid_fraction"], "f16_scale": head["f16_scale"],
+                   "storage": head["storage"], "fluid_fraction": round(head["fluid_fraction"], 4),
                    "parallelism": f"replicas x{n}" if n > 1 else "single GPU",
-                   "l2": ("inputs larger than L2 (populations %.1f GB per step)" if cells * head["bytes_per_cell"] > 2 * L2_BYTES
-                          else "inputs about the size of L2 (populations %.2f GB per step)")
-                   % (cells * head["bytes_per_cell"] / 1e9)},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                     "frac": achieved / hbm_peak, "traffic": traffic, "peak_kind": peak_kind,
-                     "kernel": "k_step (fused pull-stream + bounce-back + BGK + sponge)",
-                     "kernel_ms": head["kernel_ms_avg"], "bytes_per_cell": head["bytes_per_cell"]},
+                   "l2": "inputs larger than L2" if cells * head["bytes_per_cell"] > 2 * L2_BYTES
+                         else "inputs about the size of L2"},
+        "roofline": roofline,
         "e2e": {"value": n * cells * steps / (e2e_ms / 1e3) / 1e9, "unit": UNIT, "h2d_bytes_per_step": h2d_ps,
                 "d2h_bytes_per_step": d2h_ps},
         "gpu_launches": head["launches"],
-        "clocks": clocks,
-        "probes_finite": head["probes_finite"],
-        "secondary": secondary,
+        "clocks": {k: clocks[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
+        "fluid_glups": value * head["fluid_fraction"],
     }
-    if adjoint is not None:
-        line["adjoint"] = adjoint
-    if family_a:
-        line["family_a"] = family_a
     if secondary.get("city1024_fp32") and secondary.get("city1024_fp16"):
         line["fp16_over_fp32"] = secondary["city1024_fp16"]["glups_rank"] / secondary["city1024_fp32"]["glups_rank"]
         line["fp16_probe_rel_l2"] = secondary["fp16_probe_rel_l2_vs_fp32"]
+    if adjoint is not None:
+        line["adjoint_grad_per_s"] = adjoint["grad_per_s"]
     if world == 1 and rank == 0 and not args.no_cpu:
         line["cpu_baseline"] = {k: v for k, v in cpu_baseline().items() if k in ("value", "unit", "cores", "kind",
                                                                                   "sample")}
     if rank == 0:
+        # the legs first, one JSON object per line; the headline line last
+        if secondary:
+            print(json.dumps({"leg": "city1024 FP32 and FP16 storage, FP16 probe error against FP32",
+                              **secondary}), flush=True)
+        for nm, v in family_a.items():
+            print(json.dumps({"leg": "family_a " + nm, **v}), flush=True)
+        if adjoint is not None:
+            print(json.dumps({"leg": "adjoint", **adjoint}), flush=True)
+        print(json.dumps({"leg": "headline details", "probes_finite": head["probes_finite"],
+                          "plan_coverage": head["coverage"], "f16_scale": head["f16_scale"],
+                          "clock_samples": clocks.get("samples")}), flush=True)
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()
@@ -527,6 +623,9 @@ def main():
                              "doppler_a", "scattering_a", "hpc_a"])
     ap.add_argument("--storage", default=None, choices=["fp32", "fp16"],
                     help="population storage of the headline workload (default: the workload's own)")
+    ap.add_argument("--split", default="replicas", choices=["replicas", "slab"],
+                    help="multi-GPU form: independent replicas (weak scaling, the default) or one z-slab of the "
+                         "headline grid per rank (strong scaling)")
     ap.add_argument("--headline-only", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")

@@ -122,6 +122,13 @@ struct lbm_handle
     float* xgh_par[2] = {nullptr, nullptr};
     bool scheme_a() const { return cfg.scheme == LBM_SCHEME_A; }
 
+    // z-slab exchange between handles of one process: message buffers
+    // [send to lower | send to upper | received from lower | received from upper]
+    // and the events that order the two handles' streams (lbm_slab_exchange)
+    void* slab_buf = nullptr;
+    size_t slab_msg_bytes = 0;
+    cudaEvent_t ev_packed = nullptr, ev_read = nullptr;
+
     // adjoint workspace (checkpoints, stored moments, adjoint populations),
     // kept between lbm_adjoint_grad calls; lbm_adjoint_release frees it
     void* adj_ws = nullptr;
@@ -177,6 +184,12 @@ struct lbm_handle
         ctl_host = nullptr; h_table = nullptr; h_probe_out = nullptr;
         if (adj_ws) cudaFree(adj_ws);
         adj_ws = nullptr;
+        if (slab_buf) cudaFree(slab_buf);
+        slab_buf = nullptr;
+        slab_msg_bytes = 0;
+        if (ev_packed) cudaEventDestroy(ev_packed);
+        if (ev_read) cudaEventDestroy(ev_read);
+        ev_packed = ev_read = nullptr;
         adj_ws_bytes = 0;
         if (stream) cudaStreamDestroy(stream);
         stream = nullptr;
@@ -606,6 +619,7 @@ extern "C" const char* lbm_status_string(int s)
     case LBM_ERR_OUT_OF_MEMORY: return "out of device memory";
     case LBM_ERR_CUDA: return "CUDA error";
     case LBM_ERR_NAN: return "non-finite value in probe series";
+    case LBM_ERR_TIMEOUT: return "a device-side wait gave up";
     case LBM_ERR_STATE: return "call out of order";
     case LBM_ERR_CAPACITY: return "output buffer too small";
     case LBM_ERR_NO_DEVICE: return "no CUDA device";
@@ -826,7 +840,7 @@ extern "C" int lbm_init(lbm_handle* h)
     Layout& L = h->L;
     L.nx = nx; L.ny = ny; L.nz = nz;
     L.pitch = (nx + 2 + 31) / 32 * 32;
-    L.words_per_row = L.pitch / 32;
+    L.words_per_row = (L.pitch / 32 + 1) & ~1;   // even: a block's two words load as one 8-byte word
     L.plane = (long long)L.pitch * nyt;
     L.bc = block_cells(h->storage == LBM_STORE_F16 ? 2 : 4);
     L.bc_shift = L.bc == 64 ? 6 : 5;
@@ -912,7 +926,9 @@ extern "C" int lbm_init(lbm_handle* h)
     h->links = dalloc<uint32_t>(cells, e);
     const size_t near_words = (size_t)nzt * nyt * L.words_per_row;
     h->near = dalloc<uint32_t>(near_words, e);
-    h->sig = dalloc<float>((size_t)nx + ny + nz, e);
+    // sig_x padded with zeros to whole 64-cell blocks (the FP16 step loads a pair per lane unguarded)
+    const int nxs = (nx + 63) / 64 * 64;
+    h->sig = dalloc<float>((size_t)nxs + ny + nz, e);
     const size_t n_xexp = (size_t)2 * Q * ny * nz, n_xgh = (size_t)2 * Q * nyt * nzt;
     h->xf.xexp = dalloc<float>(n_xexp, e);
     const size_t n_xgh_all = n_xgh * (h->scheme_a() ? 2 : 1);   // scheme A: one array per step parity
@@ -928,9 +944,10 @@ extern "C" int lbm_init(lbm_handle* h)
     h->xgh_par[1] = h->xf.xgh + (h->scheme_a() ? n_xgh : 0);
     CK(cudaMallocHost(&h->ctl_host, sizeof(Control)), "cudaMallocHost");
     *h->ctl_host = Control{};
+    CK(cudaMemsetAsync(h->sig, 0, (size_t)nxs * 4, h->stream), "memset sponge");
     CK(cudaMemcpyAsync(h->sig, sx.data(), sx.size() * 4, cudaMemcpyHostToDevice, h->stream), "upload sponge");
-    CK(cudaMemcpyAsync(h->sig + nx, sy.data(), sy.size() * 4, cudaMemcpyHostToDevice, h->stream), "upload sponge");
-    CK(cudaMemcpyAsync(h->sig + nx + ny, sz.data(), sz.size() * 4, cudaMemcpyHostToDevice, h->stream),
+    CK(cudaMemcpyAsync(h->sig + nxs, sy.data(), sy.size() * 4, cudaMemcpyHostToDevice, h->stream), "upload sponge");
+    CK(cudaMemcpyAsync(h->sig + nxs + ny, sz.data(), sz.size() * 4, cudaMemcpyHostToDevice, h->stream),
        "upload sponge");
     {
         uint8_t* d_mask = nullptr;
@@ -967,10 +984,11 @@ extern "C" int lbm_init(lbm_handle* h)
     h->sa.links = h->links;
     h->sa.near = h->near;
     h->sa.sig_x = h->sig;
-    h->sa.sig_y = h->sig + nx;
-    h->sa.sig_z = h->sig + nx + ny;
+    h->sa.sig_y = h->sig + (nx + 63) / 64 * 64;
+    h->sa.sig_z = h->sa.sig_y + ny;
     h->sa.omega = (float)(1.0 / c.tau);
     h->sa.xf = h->xf;
+    h->sa.err = &h->ctl->step_error;
     {
         const cudaError_t e = prepare_step(h->storage == LBM_STORE_F16 ? 1 : 0);
         if (e != cudaSuccess) return h->cuda_fail(e, "step set-up");
@@ -1569,18 +1587,19 @@ extern "C" int lbm_step(lbm_handle* h, int nsteps)
                 done += 1;
             }
         }
-        if (np)
-        {
-            CK(cudaMemcpyAsync(&h->ctl_host->nonfinite, &h->ctl->nonfinite, sizeof(int), cudaMemcpyDeviceToHost,
-                               h->stream),
-               "probe flag");
-            h->d2h_bytes += (long)sizeof(int);
-        }
+        // the probe kernels' non-finite flag and the step's wait flag
+        CK(cudaMemcpyAsync(&h->ctl_host->nonfinite, &h->ctl->nonfinite, 2 * sizeof(int), cudaMemcpyDeviceToHost,
+                           h->stream),
+           "device flags");
+        h->d2h_bytes += (long)(2 * sizeof(int));
         // the control block upload must not be overwritten before the copy ran
         CK(cudaStreamSynchronize(h->stream), "step sync");
         h->step += chunk;
         if (np) h->probe_pending += chunk;
         left -= chunk;
+        if (h->ctl_host->step_error)
+            return h->fail(LBM_ERR_TIMEOUT, "a wait of the step kernel for its own copies gave up by step " +
+                                                std::to_string(h->step));
         if (np && h->ctl_host->nonfinite)
             return h->fail(LBM_ERR_NAN, "non-finite probe value by step " + std::to_string(h->step));
         st = harvest_timing(h);
@@ -2507,6 +2526,77 @@ extern "C" int lbm_adjoint_grad(lbm_handle* h, int nsteps, const double* observe
 
 // ---------------------------------------------------------------- z-slabs
 
+namespace {
+
+// side 0: the cut below the slab (toward slab_k0 - 1), side 1: the cut above it.
+bool has_cut(const lbm_handle* h, int side)
+{
+    return h->slab && h->lcfg.face_bc[side ? LBM_FACE_ZHI : LBM_FACE_ZLO] == kBcCut;
+}
+
+int slab_msg_check(lbm_handle* h, int side, const void* msg)
+{
+    int st = check_ready(h);
+    if (st) return st;
+    if (side != 0 && side != 1) return h->fail(LBM_ERR_INVALID_ARGUMENT, "side is 0 (below) or 1 (above)");
+    if (!has_cut(h, side)) return h->fail(LBM_ERR_STATE, "this z-slab has no cut on that side");
+    if (!msg || ((uintptr_t)msg & 15u)) return h->fail(LBM_ERR_INVALID_ARGUMENT, "message buffer: 16-byte aligned device memory");
+    return LBM_OK;
+}
+
+// pack: the plane next to the cut of `side` (plane 1 below, nz above), its
+// directions toward the neighbour; unpack: the halo plane of that side, the
+// neighbour's directions toward this slab.
+cudaError_t slab_msg(lbm_handle* h, bool pack, int side, void* msg)
+{
+    const Layout& L = h->L;
+    const int k = pack ? (side ? L.nz : 1) : (side ? L.nz + 1 : 0);
+    const int up = pack ? side : 1 - side;
+    return launch_slab_msg(pack, h->f[h->cur], h->xf.xgh, msg, L, k, up, h->storage == LBM_STORE_F16 ? 2 : 4,
+                           h->stream);
+}
+
+int slab_buffers(lbm_handle* h)
+{
+    if (h->slab_buf) return LBM_OK;
+    CK(cudaSetDevice(h->device), "cudaSetDevice");
+    h->slab_msg_bytes = (size_t)(slab_message_bytes(h->L) + 255) / 256 * 256;
+    CK(cudaMalloc(&h->slab_buf, 4 * h->slab_msg_bytes), "slab message buffers");
+    CK(cudaEventCreateWithFlags(&h->ev_packed, cudaEventDisableTiming), "slab events");
+    CK(cudaEventCreateWithFlags(&h->ev_read, cudaEventDisableTiming), "slab events");
+    return LBM_OK;
+}
+
+char* slab_part(lbm_handle* h, int n) { return (char*)h->slab_buf + (size_t)n * h->slab_msg_bytes; }
+
+}  // namespace
+
+extern "C" long lbm_slab_message_bytes(lbm_handle* h)
+{
+    if (check_ready(h)) return 0;
+    return h->slab ? (long)slab_message_bytes(h->L) : 0;
+}
+
+extern "C" int lbm_slab_pack(lbm_handle* h, int side, void* msg)
+{
+    int st = slab_msg_check(h, side, msg);
+    if (st) return st;
+    CK(cudaSetDevice(h->device), "cudaSetDevice");
+    CK(slab_msg(h, true, side, msg), "slab pack");
+    h->launches++;
+    return LBM_OK;
+}
+
+extern "C" int lbm_slab_unpack(lbm_handle* h, int side, const void* msg)
+{
+    int st = slab_msg_check(h, side, msg);
+    if (st) return st;
+    CK(cudaSetDevice(h->device), "cudaSetDevice");
+    CK(slab_msg(h, false, side, const_cast<void*>(msg)), "slab unpack");
+    h->launches++;
+    return LBM_OK;
+}
+
 extern "C" int lbm_slab_exchange(lbm_handle* lo, lbm_handle* hi)
 {
     NvtxRange range("lbm_slab_exchange");
@@ -2520,64 +2610,46 @@ extern "C" int lbm_slab_exchange(lbm_handle* lo, lbm_handle* hi)
         return lo->fail(LBM_ERR_INVALID_ARGUMENT, "the upper slab does not start where the lower one ends");
     if (lo->L.nx != hi->L.nx || lo->L.ny != hi->L.ny || lo->storage != hi->storage)
         return lo->fail(LBM_ERR_INVALID_ARGUMENT, "slabs of different grids");
-    const Layout &A = lo->L, &B = hi->L;
-    const size_t esz = lo->storage == LBM_STORE_F16 ? 2 : 4;
-    const size_t plane = (size_t)A.plane_stride * esz;   // one z-plane, all rows (y-ghost rows included)
-    char* a = (char*)lo->f[lo->cur];
-    char* b = (char*)hi->f[hi->cur];
-    const auto plane_at = [&](char* f, int k) { return f + ((size_t)kFrontElems + (size_t)k * A.plane_stride) * esz; };
-    // x-face ghost rows of one plane: 38 rows of ny + 2 floats, (nz + 2)(ny + 2) floats apart
-    const size_t row = (size_t)(A.ny + 2) * sizeof(float);
-    const size_t pitch_a = (size_t)(A.nz + 2) * row, pitch_b = (size_t)(B.nz + 2) * row;
-    const auto gh_row = [&](const lbm_handle* h, int k) { return (char*)(h->xf.xgh + (size_t)k * (h->L.ny + 2)); };
-    const auto copy_into = [&](lbm_handle* to, char* dst_plane, char* dst_gh, size_t dst_pitch, const lbm_handle* from,
-                               const char* src_plane, const char* src_gh, size_t src_pitch) {
-        cudaError_t e;
-        if (to->device == from->device)
+    st = slab_buffers(lo);
+    if (st) return st;
+    st = slab_buffers(hi);
+    if (st) return st;
+    const size_t bytes = (size_t)slab_message_bytes(lo->L);
+    // Only the populations that cross the cut travel: lower's top plane, ez = +1
+    // (send part 1), into upper's halo plane 0; upper's bottom plane, ez = -1
+    // (send part 0), into lower's halo plane nz + 1.  Each side packs on its own
+    // stream after its halo fill; the receiver waits for that, copies the
+    // message to its own GPU when the handles live on different ones, and
+    // unpacks on its stream; each sender then waits until the receiver has
+    // read its message before it packs the next one.
+    const auto receive = [&](lbm_handle* to, int to_side, lbm_handle* from, int from_part) -> cudaError_t {
+        cudaError_t e = cudaSetDevice(to->device);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(to->stream, from->ev_packed, 0);
+        const void* src = slab_part(from, from_part);
+        if (e == cudaSuccess && to->device != from->device)
         {
-            e = cudaMemcpyAsync(dst_plane, src_plane, plane, cudaMemcpyDeviceToDevice, to->stream);
-            if (e == cudaSuccess)
-                e = cudaMemcpy2DAsync(dst_gh, dst_pitch, src_gh, src_pitch, row, 2 * Q, cudaMemcpyDeviceToDevice,
-                                      to->stream);
-            return e;
+            e = cudaMemcpyPeerAsync(slab_part(to, 2 + to_side), to->device, src, from->device, bytes, to->stream);
+            src = slab_part(to, 2 + to_side);
         }
-        e = cudaMemcpyPeerAsync(dst_plane, to->device, src_plane, from->device, plane, to->stream);
-        for (int r = 0; r < 2 * Q && e == cudaSuccess; ++r)
-            e = cudaMemcpyPeerAsync(dst_gh + r * dst_pitch, to->device, src_gh + r * src_pitch, from->device, row,
-                                    to->stream);
+        if (e == cudaSuccess) e = slab_msg(to, false, to_side, const_cast<void*>(src));
+        if (e == cudaSuccess) e = cudaEventRecord(to->ev_read, to->stream);
         return e;
     };
-    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
-    cudaError_t e = cudaSuccess;
-    for (int n = 0; n < 4 && e == cudaSuccess; ++n)
-    {
-        e = cudaSetDevice(n % 2 ? hi->device : lo->device);
-        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev[n], cudaEventDisableTiming);
-    }
-    // ev0: lower's halo fill done; ev1: upper's; ev2: copies into upper done; ev3: into lower
-    if (e == cudaSuccess) e = cudaSetDevice(lo->device);
-    if (e == cudaSuccess) e = cudaEventRecord(ev[0], lo->stream);
+    cudaError_t e = cudaSetDevice(lo->device);
+    if (e == cudaSuccess) e = slab_msg(lo, true, 1, slab_part(lo, 1));
+    if (e == cudaSuccess) e = cudaEventRecord(lo->ev_packed, lo->stream);
     if (e == cudaSuccess) e = cudaSetDevice(hi->device);
-    if (e == cudaSuccess) e = cudaEventRecord(ev[1], hi->stream);
-    // upper's halo plane 0 <- lower's plane nz; the lower's plane must have its halo fill
-    if (e == cudaSuccess) e = cudaStreamWaitEvent(hi->stream, ev[0], 0);
-    if (e == cudaSuccess)
-        e = copy_into(hi, plane_at(b, 0), gh_row(hi, 0), pitch_b, lo, plane_at(a, A.nz), gh_row(lo, A.nz), pitch_a);
-    if (e == cudaSuccess) e = cudaEventRecord(ev[2], hi->stream);
-    // lower's halo plane nz + 1 <- upper's plane 1
-    if (e == cudaSuccess) e = cudaSetDevice(lo->device);
-    if (e == cudaSuccess) e = cudaStreamWaitEvent(lo->stream, ev[1], 0);
-    if (e == cudaSuccess)
-        e = copy_into(lo, plane_at(a, A.nz + 1), gh_row(lo, A.nz + 1), pitch_a, hi, plane_at(b, 1), gh_row(hi, 1),
-                      pitch_b);
-    if (e == cudaSuccess) e = cudaEventRecord(ev[3], lo->stream);
-    // neither slab overwrites the buffer the other one reads before that copy is done
-    if (e == cudaSuccess) e = cudaStreamWaitEvent(lo->stream, ev[2], 0);
+    if (e == cudaSuccess) e = slab_msg(hi, true, 0, slab_part(hi, 0));
+    if (e == cudaSuccess) e = cudaEventRecord(hi->ev_packed, hi->stream);
+    if (e == cudaSuccess) e = receive(hi, 0, lo, 1);
+    if (e == cudaSuccess) e = receive(lo, 1, hi, 0);
+    // neither handle packs into a buffer the other one is still reading
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(lo->stream, hi->ev_read, 0);
     if (e == cudaSuccess) e = cudaSetDevice(hi->device);
-    if (e == cudaSuccess) e = cudaStreamWaitEvent(hi->stream, ev[3], 0);
-    for (int n = 0; n < 4; ++n)
-        if (ev[n]) cudaEventDestroy(ev[n]);   // released once the streams pass them
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(hi->stream, lo->ev_read, 0);
     cudaSetDevice(lo->device);
     if (e != cudaSuccess) return lo->cuda_fail(e, "slab exchange");
+    lo->launches += 2;
+    hi->launches += 2;
     return LBM_OK;
 }

@@ -71,6 +71,7 @@ struct Control
     long long probe_base;  // step index of probe-buffer row 0
     int nonfinite;         // set by the probe kernels when an owned probe reads a non-finite value
                            // (the host uploads only the fields above it)
+    int step_error;        // set by the FP16 step when a wait for its own copies gave up
 };
 
 struct SourceStatic
@@ -147,6 +148,7 @@ struct StepArgs
     const float* sig_z;
     float omega;               // 1 / tau
     XFace xf;
+    int* err;                  // device flag: set to 1 when a kernel's bounded wait gave up
 };
 
 struct ProbeArgs
@@ -263,6 +265,13 @@ cudaError_t launch_zper_a(float* f, const Layout& L, const StepArgs& sa, cudaStr
 // of SOLID cells next to them.  mask_ref: the halo-inclusive mask.
 cudaError_t launch_set_density_a(float* f, float* xgh, const float* rho_prime, const uint8_t* mask_ref,
                                  const Layout& L, const SchemeAArgs& b, cudaStream_t stream);
+
+// z-slab messages: the 5 crossing directions of one plane as whole lines plus
+// its two crossing x-face ghost rows (kernels.cu); pack: plane k -> msg,
+// otherwise msg -> plane k.  up: the directions with ez = +1 (else -1).
+long long slab_message_bytes(const Layout& L);
+cudaError_t launch_slab_msg(bool pack, void* f, float* xgh, void* msg, const Layout& L, int k, int up, int esz,
+                            cudaStream_t stream);
 
 // Bounds-checked builds (-DLBM_CHECK): read and clear the first failed check
 // of each kernel file (site 0: none; always 0 in the product build), and a

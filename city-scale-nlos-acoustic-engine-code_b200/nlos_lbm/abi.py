@@ -27,6 +27,7 @@ LBM_ERR_CAPACITY = -7
 LBM_ERR_NO_DEVICE = -8
 LBM_ERR_IO = -9
 LBM_ERR_UNSUPPORTED = -10
+LBM_ERR_TIMEOUT = -11
 LBM_NOALLOC_MAX_CELLS = 8388608
 
 LBM_BC_NSCBC, LBM_BC_REST, LBM_BC_WALL, LBM_BC_COPY, LBM_BC_PERIODIC = 0, 1, 2, 3, 4
@@ -215,6 +216,9 @@ def bind_product(lib):
                                             ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]),
         "lbm_adjoint_release": (ctypes.c_int, [P]),
         "lbm_slab_exchange": (ctypes.c_int, [P, P]),
+        "lbm_slab_message_bytes": (ctypes.c_long, [P]),
+        "lbm_slab_pack": (ctypes.c_int, [P, ctypes.c_int, P]),
+        "lbm_slab_unpack": (ctypes.c_int, [P, ctypes.c_int, P]),
         "lbm_city_generate": (ctypes.c_int, [ctypes.POINTER(LbmCityParams), c_float_p, ctypes.c_int,
                                              c_int_p, c_double_p]),
         "lbm_stl_write": (ctypes.c_int, [ctypes.c_char_p, c_float_p, ctypes.c_int]),

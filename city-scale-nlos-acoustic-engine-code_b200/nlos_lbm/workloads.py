@@ -8,6 +8,8 @@ reference's heightmap ray cast.
 
   scatter    128^3 open box, rigid 16^3 cube, Gaussian pulse, 20-cell sponge
   lloyd      256x128x128, ground wall, moving sine source (Mach 0.1), trilinear
+  city256    256x256x128 city patch with city1024's physics, 4 Ricker sources,
+             64 probes, 4000 steps (its FP64 oracle series is a test fixture)
   city512    512x512x128 city (profiler-sized), 2 Ricker sources, 64 probes
   city1024   1024x1024x256 city, 4 Ricker sources at street level, 256 probes
   city2048   2048x2048x256 city, one source flying at z = 120 at Mach 0.15,
@@ -124,6 +126,19 @@ def build(name, storage=None, seed=2024):
                 for p in pts[:4]]
         return dict(cfg=cfg, sources=srcs, probes=pts[4:], triangles=tris, steps=4000, coverage=cov,
                     description="synthetic city 1024x1024x256, 4 Ricker sources, 256 street probes")
+    if name == "city256":
+        # C3's physics on a 256x256x128 patch (tau 0.51, 32-cell sponge on the
+        # sides and top, ground bounce-back, 4 Ricker sources at street
+        # level, street-level probes) for its full 4000 steps: small enough
+        # for the FP64 oracle to run its whole length on the host
+        st = abi.LBM_STORE_F32 if storage is None else storage
+        cfg, tris, cov, amp = city(256, 256, 128, seed, st)
+        pts = street_points(tris, 256, 256, 4 + 64, 2.5, seed)
+        srcs = [abi.reference_source(sx=p[0], sy=p[1], sz=p[2], ex=p[0], ey=p[1], ez=p[2], amp=amp, freq=1 / 40.0,
+                                     t0=60.0, waveform=abi.LBM_WAVE_RICKER, injection=abi.LBM_INJECT_TRILINEAR)
+                for p in pts[:4]]
+        return dict(cfg=cfg, sources=srcs, probes=pts[4:], triangles=tris, steps=4000, coverage=cov,
+                    description="synthetic city patch 256x256x128, C3 physics, 4 Ricker sources, 64 street probes")
     if name == "city512":
         # a few-GB version of the city for profiler captures
         st = abi.LBM_STORE_F32 if storage is None else storage

@@ -56,7 +56,11 @@ typedef enum lbm_status
     LBM_ERR_CAPACITY = -7,         /* caller's output buffer too small */
     LBM_ERR_NO_DEVICE = -8,
     LBM_ERR_IO = -9,
-    LBM_ERR_UNSUPPORTED = -10
+    LBM_ERR_UNSUPPORTED = -10,
+    LBM_ERR_TIMEOUT = -11          /* a bounded device-side wait gave up (the FP16 step waits on
+                                      its own copies with an iteration limit); reported by
+                                      lbm_step / lbm_run at the end of the batch, results of
+                                      that batch are not valid */
 } lbm_status;
 
 /* Boundary treatment of one face of the box. */
@@ -372,17 +376,38 @@ int lbm_adjoint_release(lbm_handle* h);
 
 /* ---- z-slab decomposition --------------------------------------------------- */
 
-/* Halo exchange between two z-slab handles of one domain (no counterpart in
- * this form; the reference's MPI decomposition exchanges every face through
- * exchange_halos, 06:837-903).  `lower` holds the layers just below
- * `upper`.  Call it once per time step, after lbm_apply_source and
- * lbm_exchange_halos of both handles and before their
- * lbm_step_collision_bgk: the boundary interior plane of each slab (its
- * y-ghost rows included) and the x-face ghost rows of that plane are copied
- * into the other slab's halo.  The copies run on the receiving handle's
- * stream, ordered against both streams with events, so the handles may live
- * on different GPUs (peer copies) or on the same one. */
+/* Halo exchange between two z-slab handles of one process (the reference's
+ * MPI decomposition exchanges every face through exchange_halos, 06:837-903,
+ * all 19 populations of each face cell, 06:840-845).  `lower` holds the
+ * layers just below `upper`.  Call it once per time step, after
+ * lbm_apply_source and lbm_exchange_halos of both handles and before their
+ * lbm_step_collision_bgk.  Only what the next step pulls across the cut
+ * travels: the 5 populations with ez toward the neighbour of each slab's
+ * boundary plane (its y-halo rows included) and the 2 of its x-face ghost rows
+ * among them, as one message each way (lbm_slab_pack / lbm_slab_unpack).  The
+ * copies run on the receiving handle's stream, ordered against both streams
+ * with events, so the handles may live on different GPUs (a peer copy of the
+ * message) or on the same one.  The handles keep their message buffers (4
+ * messages each) until lbm_destroy. */
 int lbm_slab_exchange(lbm_handle* lower, lbm_handle* upper);
+/* Size in bytes of one cut's message of this z-slab handle: 5 directions x
+ * (ny + 2) rows x ceil(nx / cells per line) lines of 128 B, plus 2 x (ny + 2)
+ * floats of x-face ghosts.  0 for a handle that is not a z-slab. */
+long lbm_slab_message_bytes(lbm_handle* h);
+/* For one z-slab per process (a rank per GPU): pack, on the handle's stream,
+ * the message toward the neighbour on `side` (0: below, the directions with
+ * ez = -1 of the slab's first plane; 1: above, ez = +1 of its last plane) into
+ * `msg`, 16-byte aligned device memory of the handle's GPU of
+ * lbm_slab_message_bytes bytes.  Call after lbm_exchange_halos.  The caller
+ * moves the message to the neighbour's GPU (for example an NCCL send/recv),
+ * ordered after this call's work on the handle's stream (lbm_get_stream). */
+int lbm_slab_pack(lbm_handle* h, int side, void* msg);
+/* Unpack the neighbour's message on `side` (0: from the slab below, into halo
+ * plane 0; 1: from the slab above, into halo plane nz + 1), on the handle's
+ * stream, before lbm_step_collision_bgk.  The message must be complete in
+ * device memory of this handle's GPU before the handle's stream reaches this
+ * call (order the transfer's stream before it). */
+int lbm_slab_unpack(lbm_handle* h, int side, const void* msg);
 
 /* ---- measurement ---------------------------------------------------------- */
 

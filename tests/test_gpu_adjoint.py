@@ -62,9 +62,11 @@ def test_adjoint_matches_fp64_adjoint(case, gpu):
 
 
 def test_adjoint_matches_central_fd_of_gpu_forward(case, gpu):
+    """Every case: the trilinear misfit is piecewise quadratic in the shift
+    (exact central differences inside a cell), the Gaussian stencil's adds an
+    O(h^2) term (3e-5 relative at h = 1e-2 in the FP64 oracle's own check);
+    both sit inside the 1e-4 bar."""
     name, sc, _ = case
-    if name != "trilinear":
-        pytest.skip("central-difference check on the stationary trilinear case")
     g = Solver(sc["cfg"], [sc["trial"]], sc["probes"], triangles=sc["triangles"])
     L, gp, gs, _ = g.adjoint_grad(sc["observed"])
     g.close()

@@ -64,12 +64,13 @@ def test_fp32_matches_reference_fixture(name, gpu):
     assert rel_l2(g.get_probes(), gold["probes"]) <= FP32_PROBE_TOL
 
 
-@pytest.mark.parametrize("fixture", ["oracle_scatter_2000", "oracle_lloyd_6000"])
+@pytest.mark.parametrize("fixture", ["oracle_scatter_2000", "oracle_lloyd_6000", "oracle_city256_4000"])
 def test_full_size_workload_matches_oracle_series(fixture, gpu):
     """The full-size 128^3 scattering box (2000 steps) and 256x128x128 Lloyd's
-    mirror (6000 steps) benchmark workloads, FP32 and FP16 storage (the
-    workload's scale, 100/amplitude), against the FP64 oracle's series
-    (tests/golden/make_oracle_series.py)."""
+    mirror (6000 steps) benchmark workloads, and the 256x256x128 city patch
+    with the 1024x1024x256 city's physics over its 4000 steps, FP32 and FP16
+    storage (the workload's scale, 100/amplitude), against the FP64 oracle's
+    series (tests/golden/make_oracle_series.py)."""
     from nlos_lbm import workloads
 
     path = os.path.join(GOLDEN, fixture + ".npz")
