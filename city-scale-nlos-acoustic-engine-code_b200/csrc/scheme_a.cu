@@ -144,19 +144,26 @@ __device__ __forceinline__ void pull_a(const float* __restrict__ f, const Layout
 
 // ---------------------------------------------------------------- step
 // Two x-adjacent cells per thread, aligned float2 loads with warp shuffles
-// for the +-1 x shift (the same access scheme as the scheme-B step).  FEAT:
-// 0 = the update of 02 and 03; 1 = with 01's destination blend and periodic
-// z; 2 = also with per-column fields and the pre-step source (04).  Each is
-// its own instance, so the simpler programs keep the leaner kernel.
-template <int BLOCK, int MINB, int FEAT>
-__global__ void __launch_bounds__(BLOCK, MINB) k_step_a(const float* __restrict__ fin, float* __restrict__ fout,
-                                                        Layout L, StepArgs a, SchemeAArgs b)
+// for the +-1 x shift (the same access scheme as the scheme-B step); each
+// thread updates its pair in KZ consecutive planes, so what does not depend
+// on z (the omega and blend profiles of the column, the source weights of
+// the column, the step's source masses) is looked up once.  FEAT: 0 = the
+// update of 02 and 03; 1 = with 01's destination blend and periodic z; 2 =
+// also with per-column fields and the pre-step source (04).  Each is its own
+// instance, so the simpler programs keep the leaner kernel.
+struct ColumnValues
 {
-    const int lane = threadIdx.x & 31;
-    const int c0r = 2 * (blockIdx.x * BLOCK + threadIdx.x);
-    const bool active = c0r < L.nx;
-    const int c0 = active ? c0r : ((L.nx - 1) & ~1);   // inactive lanes shadow a valid pair
-    const int j = blockIdx.y + 1, k = blockIdx.z + 1;
+    float2 om;      // min(om_x, om_y) of the two cells
+    float2 blend;   // max(sg_x, sg_y[, sg_xy]) of the two cells
+    float2 fw;      // source weight per column (fld_xy), else fld_x fld_y
+    float mass0, mass1;   // source mass of this step and of the next
+};
+
+template <int FEAT>
+__device__ __forceinline__ void step_a_pair(const float* __restrict__ fin, float* __restrict__ fout, const Layout& L,
+                                            const StepArgs& a, const SchemeAArgs& b, const ColumnValues& z,
+                                            int lane, bool active, bool has1, int c0, int j, int k)
+{
     const long long e0 = L.elem(0, c0 + 1, j, k);
     const float* own = fin + e0;
     const long long rs = L.row_stride, ps = L.plane_stride;
@@ -170,19 +177,21 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step_a(const float* __restrict_
         if (nb & 2u) lk1 = a.links[cl + 1];
     }
     const bool any_link = __any_sync(kFull, (lk0 | lk1) != 0u);
-    // FEAT 2: the pair's source weights, per column or per axis, taken once
-    // before the populations are loaded (the per-column lookup inside each
-    // source term spilled registers)
-    float2 fw = f2(0.f);
-    if constexpr (FEAT == 2)
-    {
-        if (b.field_mode >= 0)
-            fw = make_float2(field_weight(b, c0 + 1, j, k), c0 + 1 < L.nx ? field_weight(b, c0 + 2, j, k) : 0.f);
-    }
+    // the pair's source weights: per column (04), or the product of the
+    // per-axis factors with this plane's z factor
     const auto pair_weight = [&](float m) -> float2 {
-        if constexpr (FEAT == 2) return mul2(f2(m), fw);
+        if constexpr (FEAT == 2)
+        {
+            if (b.fld_xy) return mul2(f2(m), z.fw);
+            const float fz = b.fld_z[k];
+            return make_float2(m * (z.fw.x * fz), c0 + 1 < L.nx ? m * (z.fw.y * fz) : 0.f);
+        }
         return make_float2(m * field_weight<false>(b, c0 + 1, j, k),
                            c0 + 1 < L.nx ? m * field_weight<false>(b, c0 + 2, j, k) : 0.f);
+    };
+    const auto mass = [&](int ahead) -> float {
+        if constexpr (FEAT == 2) return ahead ? z.mass1 : z.mass0;
+        return field_mass(b, ahead);
     };
     // pair load (the bounds-checked build tests the index first)
     const auto ldc = [&](const float* p) {
@@ -211,7 +220,6 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step_a(const float* __restrict_
             G[q] = make_float2(cur.y, next);
         }
     }
-    const bool has1 = c0 + 1 < L.nx;
     const bool xlo = active && c0 == 0, xhi0 = active && c0 == L.nx - 1, xhi1 = active && c0 + 1 == L.nx - 1;
     if (xlo | xhi0 | xhi1)
     {
@@ -233,7 +241,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step_a(const float* __restrict_
     // destination source, for populations that left a fluid cell (02:373, 02:405)
     if (b.field_mode == 0)
     {
-        const float2 S = pair_weight(field_mass(b, 0));
+        const float2 S = pair_weight(mass(0));
 #pragma unroll
         for (int q = 0; q < Q; ++q)
         {
@@ -245,8 +253,16 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step_a(const float* __restrict_
     // destination blend toward rest, same populations (01:343-347)
     if (FEAT >= 1 && b.blend)
     {
-        const float2 sg = make_float2(cell_blend<FEAT == 2>(b, c0 + 1, j, k),
-                                      has1 ? cell_blend<FEAT == 2>(b, c0 + 2, j, k) : 0.f);
+        float2 sg;
+        if constexpr (FEAT == 2)
+        {
+            const float szk = b.sg_z[k - 1];
+            sg = make_float2(fmaxf(z.blend.x, szk), has1 ? fmaxf(z.blend.y, szk) : 0.f);
+        }
+        else
+        {
+            sg = make_float2(cell_blend<false>(b, c0 + 1, j, k), has1 ? cell_blend<false>(b, c0 + 2, j, k) : 0.f);
+        }
         const float2 keep = sub2(f2(1.0f), sg);
 #pragma unroll
         for (int q = 0; q < Q; ++q)
@@ -260,7 +276,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step_a(const float* __restrict_
     // cell, before it is bounced back or collided next step
     if (FEAT == 2 && b.field_mode == 2)
     {
-        const float2 S = pair_weight(field_mass(b, 1));
+        const float2 S = pair_weight(mass(1));
 #pragma unroll
         for (int q = 0; q < Q; ++q) G[q] = fma2(f2(wf(q)), S, G[q]);
     }
@@ -287,7 +303,16 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step_a(const float* __restrict_
     }
 
     // BGK with each cell's own omega, FP32x2
-    const float2 om = make_float2(cell_omega(b, c0 + 1, j, k), has1 ? cell_omega(b, c0 + 2, j, k) : 1.0f);
+    float2 om;
+    if constexpr (FEAT == 2)
+    {
+        const float ozk = b.om_z[k - 1];
+        om = make_float2(fminf(z.om.x, ozk), has1 ? fminf(z.om.y, ozk) : 1.0f);
+    }
+    else
+    {
+        om = make_float2(cell_omega(b, c0 + 1, j, k), has1 ? cell_omega(b, c0 + 2, j, k) : 1.0f);
+    }
     {
         float2 rho = f2(0.f), jx = f2(0.f), jy = f2(0.f), jz = f2(0.f);
 #pragma unroll
@@ -331,7 +356,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step_a(const float* __restrict_
     // forcing of this cell for the populations it sends next (03:424-435)
     if (b.field_mode == 1)
     {
-        const float2 sp = pair_weight(field_mass(b, 1));
+        const float2 sp = pair_weight(mass(1));
         const float s0 = sp.x, s1 = sp.y;
 #pragma unroll
         for (int q = 0; q < Q; ++q)
@@ -367,6 +392,52 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step_a(const float* __restrict_
     {
         if (k == L.nz) store(e0 - (long long)L.nz * ps);
         if (k == 1) store(e0 + (long long)L.nz * ps);
+    }
+}
+
+template <int BLOCK, int MINB, int FEAT, int KZ>
+__global__ void __launch_bounds__(BLOCK, MINB) k_step_a(const float* __restrict__ fin, float* __restrict__ fout,
+                                                        Layout L, StepArgs a, SchemeAArgs b)
+{
+    const int lane = threadIdx.x & 31;
+    const int c0r = 2 * (blockIdx.x * BLOCK + threadIdx.x);
+    const bool active = c0r < L.nx;
+    const int c0 = active ? c0r : ((L.nx - 1) & ~1);   // inactive lanes shadow a valid pair
+    const bool has1 = c0 + 1 < L.nx;
+    const int j = blockIdx.y + 1;
+    if constexpr (FEAT < 2)
+    {
+        step_a_pair<FEAT>(fin, fout, L, a, b, ColumnValues{}, lane, active, has1, c0, j, blockIdx.z + 1);
+    }
+    else
+    {
+        const int i0 = c0 + 1, i1 = has1 ? c0 + 2 : c0 + 1;
+        ColumnValues z{};
+        z.om = make_float2(fminf(b.om_x[i0 - 1], b.om_y[j - 1]), fminf(b.om_x[i1 - 1], b.om_y[j - 1]));
+        if (b.blend)
+        {
+            z.blend = make_float2(fmaxf(b.sg_x[i0 - 1], b.sg_y[j - 1]), fmaxf(b.sg_x[i1 - 1], b.sg_y[j - 1]));
+            if (b.sg_xy)
+                z.blend = make_float2(fmaxf(z.blend.x, b.sg_xy[(j - 1) * b.nx_col + (i0 - 1)]),
+                                      fmaxf(z.blend.y, b.sg_xy[(j - 1) * b.nx_col + (i1 - 1)]));
+        }
+        if (b.field_mode >= 0)
+        {
+            if (b.fld_xy)
+                z.fw = make_float2(field_weight(b, i0, j, 1), has1 ? field_weight(b, i1, j, 1) : 0.f);
+            else
+                z.fw = make_float2(b.fld_x[i0] * b.fld_y[j], b.fld_x[i1] * b.fld_y[j]);
+        }
+        z.mass0 = b.field_mode == 0 ? field_mass(b, 0) : 0.f;
+        z.mass1 = b.field_mode >= 1 ? field_mass(b, 1) : 0.f;
+        const int k0 = blockIdx.z * KZ + 1;
+#pragma unroll 1
+        for (int kk = 0; kk < KZ; ++kk)
+        {
+            const int k = k0 + kk;
+            if (k > L.nz) break;
+            step_a_pair<FEAT>(fin, fout, L, a, b, z, lane, active, has1, c0, j, k);
+        }
     }
 }
 
@@ -609,14 +680,17 @@ cudaError_t launch_step_a(const float* fin, float* fout, const Layout& L, const 
                           cudaStream_t stream)
 {
     if (L.bc != BC) return cudaErrorInvalidValue;
-    constexpr int kBlock = 128;
-    const dim3 g((unsigned)((L.nx + 2 * kBlock - 1) / (2 * kBlock)), (unsigned)L.ny, (unsigned)L.nz);
+    // 04's instance walks 4 planes per thread (its column lookups are the
+    // costly part); the lean instances, at 72 registers, take one plane each
+    // (a plane loop there spilled)
+    constexpr int kBlock = 128, kZ = 4;
+    const unsigned gx = (unsigned)((L.nx + 2 * kBlock - 1) / (2 * kBlock));
     if (b.field_mode == 2 || b.sg_xy || b.fld_xy)
-        k_step_a<kBlock, 5, 2><<<g, kBlock, 0, stream>>>(fin, fout, L, a, b);
+        k_step_a<kBlock, 5, 2, kZ><<<dim3(gx, L.ny, (L.nz + kZ - 1) / kZ), kBlock, 0, stream>>>(fin, fout, L, a, b);
     else if (b.blend || b.zper)
-        k_step_a<kBlock, 7, 1><<<g, kBlock, 0, stream>>>(fin, fout, L, a, b);
+        k_step_a<kBlock, 7, 1, 1><<<dim3(gx, L.ny, L.nz), kBlock, 0, stream>>>(fin, fout, L, a, b);
     else
-        k_step_a<kBlock, 7, 0><<<g, kBlock, 0, stream>>>(fin, fout, L, a, b);
+        k_step_a<kBlock, 7, 0, 1><<<dim3(gx, L.ny, L.nz), kBlock, 0, stream>>>(fin, fout, L, a, b);
     return cudaGetLastError();
 }
 
