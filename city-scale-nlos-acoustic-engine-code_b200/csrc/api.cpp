@@ -2308,7 +2308,7 @@ extern "C" int lbm_adjoint_grad(lbm_handle* h, int nsteps, const double* observe
     SourceArgs sargs = source_args(h, false);
     int adj_variant = kDefaultAdjointVariant;
     if (const char* v = std::getenv("NLOS_LBM_ADJ_VARIANT")) adj_variant = std::atoi(v);
-    if (adj_variant < 0 || adj_variant > 2) return h->fail(LBM_ERR_BAD_CONFIG, "NLOS_LBM_ADJ_VARIANT out of range");
+    if (adj_variant < 0 || adj_variant > 4) return h->fail(LBM_ERR_BAD_CONFIG, "NLOS_LBM_ADJ_VARIANT out of range");
     // L2 prefetch distance of the adjoint step in rows (NLOS_LBM_ADJ_PREFETCH_ROWS, 0 = off)
     int adj_prefetch = kDefaultAdjointPrefetchRows;
     if (const char* v = std::getenv("NLOS_LBM_ADJ_PREFETCH_ROWS")) adj_prefetch = std::max(0, std::atoi(v));

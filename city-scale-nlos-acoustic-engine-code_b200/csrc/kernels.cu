@@ -15,6 +15,7 @@
 #include "check.cuh"
 #include "device.hpp"
 #include "lattice.cuh"
+#include "pipeline.cuh"
 
 namespace lbm {
 namespace {
@@ -733,46 +734,9 @@ constexpr int kLinesBytes = 19 * 128;           // a block's 19 source lines
 constexpr int kLinkOff = kLinesBytes;           // its links words (near-solid blocks only)
 constexpr int kSlotBytes = kLinesBytes + 256;
 constexpr unsigned kNear = 1u, kFirst = 2u, kLast = 4u;   // block flags
-constexpr int kSpinLimit = 1 << 22;             // try_wait rounds before a slot wait gives up (seconds)
 template <int S>
 __host__ __device__ constexpr int warp_bytes() { return (S * kSlotBytes + S * 8 + 127) / 128 * 128; }
 }  // namespace hb
-
-__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count) : "memory");
-}
-__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory"); }
-__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
-__device__ __forceinline__ void mbar_arrive_expect_tx(uint32_t bar, uint32_t bytes)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity)
-{
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(ok)
-        : "r"(bar), "r"(parity)
-        : "memory");
-    return ok != 0u;
-}
-// Bounded wait for the phase of parity `parity`; false when it gave up.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
-{
-    for (int i = 0; i < hb::kSpinLimit; ++i)
-        if (mbar_try_wait(bar, parity)) return true;
-    return false;
-}
-// One bulk copy global -> this CTA's shared memory, completed on `bar`
-// (16-byte aligned addresses, size a multiple of 16).
-__device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar)
-{
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(dst),
-                 "l"(src), "r"(bytes), "r"(bar)
-                 : "memory");
-}
 
 template <int P, int WARPS, int MINB>
 __global__ void __launch_bounds__(32 * WARPS, MINB) k_step_hb(const __half* __restrict__ fin,
