@@ -36,10 +36,25 @@ METRIC = "D3Q19 GLUPS, %HBM peak: FP16-store vs FP32 @<=1e-3 probe L2; adjoint g
 # 2.644e9 B, k_step<float>: 5.132e9 B for 33.55e6 cells)
 NCU_TRAFFIC_PER_CELL = {"fp16": 2.644e9 / 33554432, "fp32": 5.132e9 / 33554432}
 UNIT = "GLUPS"
+DATA = "synthetic (seeded box city voxelised from STL triangles)"
 L2_BYTES = 126e6   # B200 L2
 # steps of the FP16-vs-FP32 probe comparison on the 1024x1024x256 city: the
 # workload's whole configured length
 ERR_STEPS = 4000
+
+
+def headline_config(name, storage, n):
+    """The `config` of both arms' lines: the workload, its grid and storage,
+    the multi-GPU form and the L2 rule (known without building the workload)."""
+    from nlos_lbm import workloads
+
+    dims, default_storage, desc = workloads.CITY_SUMMARY[name]
+    storage = storage or default_storage
+    cells = dims[0] * dims[1] * dims[2]
+    pop_bytes = cells * (76 if storage == "fp16" else 152)
+    return {"workload": f"{name}: {desc}", "grid": list(dims), "storage": storage,
+            "parallelism": f"replicas x{n}" if n > 1 else "single GPU",
+            "l2": "inputs larger than L2" if pop_bytes > 2 * L2_BYTES else "inputs about the size of L2"}
 
 
 def measured_peaks():
@@ -382,8 +397,9 @@ def cpu_baseline(steps_hint=None, seconds=12.0):
     cells = nx * ny * nz
     x0, y0 = REF_WINDOW[:2]
     return dict(value=cells * n / dt / 1e9, unit=UNIT, cores=threads, kind=kind,
-                sample=f"{nx}x{ny}x{nz} window [{x0},{x0 + nx})x[{y0},{y0 + ny}) of the 2048x2048x256 city, "
-                       f"{n} full steps (apply_source+exchange_halos+step_collision_bgk), FP64, {threads} threads",
+                sample=f"{nx}x{ny}x{nz} window [{x0},{x0 + nx})x[{y0},{y0 + ny}) of the 2048x2048x256 city (an FP64 "
+                       f"run of the whole grid needs ~330 GB of host memory), timed as a rate: {n} full steps "
+                       f"(apply_source+exchange_halos+step_collision_bgk), FP64, {threads} threads",
                 seconds=dt, steps=n)
 
 
@@ -398,11 +414,9 @@ def run_reference_arm(args):
     b = cpu_baseline(steps_hint=max(1, args.steps))
     line = {"metric": METRIC, "value": b["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": b["steps"],
             "warmup": args.warmup, "ms_per_step": b["seconds"] / b["steps"] * 1e3, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": DATA,
             "impl": "reference",
-            "config": {"workload": "city2048 (2048x2048x256 seeded box city) timed as a rate on a "
-                                   "256x256x128 window of it: the FP64 reference on the whole grid needs ~330 GB",
-                       "sample": b["sample"]},
+            "config": headline_config(args.workload, args.storage, args.gpus),
             "cpu_baseline": {"value": b["value"], "unit": UNIT, "cores": b["cores"], "kind": oracle_kind,
                              "sample": b["sample"]},
             "e2e": {"value": b["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -449,7 +463,7 @@ def run_slab_arm(args, torch, dist, world, rank, local, barrier, reduce_max):
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "strong",
             "vs_baseline": None, "dtype": "fp16-store/fp32-compute" if w["cfg"].storage == 1 else "fp32",
-            "data": "synthetic (seeded box city voxelised from STL triangles)",
+            "data": DATA,
             "config": {"workload": f"{args.workload}: {w['description']}", "grid": [nx, ny, nz],
                        "parallelism": f"z-slabs x{world}", "slab_bounds": r.bounds,
                        "message_bytes_per_cut": r.lib.lbm_slab_message_bytes(r.h)},
@@ -572,12 +586,8 @@ def run_our_arm(args):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": n, "steps": steps, "warmup": args.warmup,
         "ms_per_step": head["ms"] / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "fp16-store/fp32-compute" if head["storage"] == "fp16" else "fp32",
-        "data": "synthetic (seeded box city voxelised from STL triangles)",
-        "config": {"workload": f"{headline}: {head['description']}", "grid": head["dims"],
-                   "storage": head["storage"], "fluid_fraction": round(head["fluid_fraction"], 4),
-                   "parallelism": f"replicas x{n}" if n > 1 else "single GPU",
-                   "l2": "inputs larger than L2" if cells * head["bytes_per_cell"] > 2 * L2_BYTES
-                         else "inputs about the size of L2"},
+        "data": DATA,
+        "config": headline_config(headline, head["storage"], n),
         "roofline": roofline,
         "e2e": {"value": n * cells * steps / (e2e_ms / 1e3) / 1e9, "unit": UNIT, "h2d_bytes_per_step": h2d_ps,
                 "d2h_bytes_per_step": d2h_ps},
@@ -603,8 +613,8 @@ def run_our_arm(args):
         if adjoint is not None:
             print(json.dumps({"leg": "adjoint", **adjoint}), flush=True)
         print(json.dumps({"leg": "headline details", "probes_finite": head["probes_finite"],
-                          "plan_coverage": head["coverage"], "f16_scale": head["f16_scale"],
-                          "clock_samples": clocks.get("samples")}), flush=True)
+                          "fluid_fraction": head["fluid_fraction"], "plan_coverage": head["coverage"],
+                          "f16_scale": head["f16_scale"], "clock_samples": clocks.get("samples")}), flush=True)
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()

@@ -52,6 +52,19 @@ FIVE_FACES = ALL_FACES & ~(1 << abi.FACE_ZLO)
 MACH_TO_CELLS = abi.CS   # cells/step per unit Mach (c = cs in lattice units)
 
 
+# grid, default storage and description of the city workloads, known without
+# building their geometry (bench.py's reference arm reports the headline
+# workload's configuration without loading the library)
+CITY_SUMMARY = {
+    "city2048": ((2048, 2048, 256), "fp16", "synthetic city 2048x2048x256, source flying at z=120 Mach 0.15, "
+                                            "512 probes"),
+    "city1024": ((1024, 1024, 256), "fp32", "synthetic city 1024x1024x256, 4 Ricker sources, 256 street probes"),
+    "city512": ((512, 512, 128), "fp32", "synthetic city 512x512x128, 2 Ricker sources, 64 street probes"),
+    "city256": ((256, 256, 128), "fp32", "synthetic city patch 256x256x128, C3 physics, 4 Ricker sources, "
+                                         "64 street probes"),
+}
+
+
 def lattice_config(nx, ny, nz, tau, **kw):
     base = dict(x_min=0.0, x_max=float(nx), y_min=0.0, y_max=float(ny), z_min=0.0, z_max=float(nz), dx=1.0,
                 c_phys=abi.CS, tau=tau, sky_z=1e30)
@@ -125,7 +138,7 @@ def build(name, storage=None, seed=2024):
                                      t0=60.0, waveform=abi.LBM_WAVE_RICKER, injection=abi.LBM_INJECT_TRILINEAR)
                 for p in pts[:4]]
         return dict(cfg=cfg, sources=srcs, probes=pts[4:], triangles=tris, steps=4000, coverage=cov,
-                    description="synthetic city 1024x1024x256, 4 Ricker sources, 256 street probes")
+                    description=CITY_SUMMARY["city1024"][2])
     if name == "city256":
         # C3's physics on a 256x256x128 patch (tau 0.51, 32-cell sponge on the
         # sides and top, ground bounce-back, 4 Ricker sources at street
@@ -138,7 +151,7 @@ def build(name, storage=None, seed=2024):
                                      t0=60.0, waveform=abi.LBM_WAVE_RICKER, injection=abi.LBM_INJECT_TRILINEAR)
                 for p in pts[:4]]
         return dict(cfg=cfg, sources=srcs, probes=pts[4:], triangles=tris, steps=4000, coverage=cov,
-                    description="synthetic city patch 256x256x128, C3 physics, 4 Ricker sources, 64 street probes")
+                    description=CITY_SUMMARY["city256"][2])
     if name == "city512":
         # a few-GB version of the city for profiler captures
         st = abi.LBM_STORE_F32 if storage is None else storage
@@ -148,7 +161,7 @@ def build(name, storage=None, seed=2024):
                                      t0=60.0, waveform=abi.LBM_WAVE_RICKER, injection=abi.LBM_INJECT_TRILINEAR)
                 for p in pts[:2]]
         return dict(cfg=cfg, sources=srcs, probes=pts[2:], triangles=tris, steps=4000, coverage=cov,
-                    description="synthetic city 512x512x128, 2 Ricker sources, 64 street probes")
+                    description=CITY_SUMMARY["city512"][2])
     if name == "city2048":
         st = abi.LBM_STORE_F16 if storage is None else storage
         cfg, tris, cov, amp = city(2048, 2048, 256, seed, st)
@@ -157,7 +170,7 @@ def build(name, storage=None, seed=2024):
         src = abi.reference_source(sx=400.0, sy=600.0, sz=120.0, ex=1650.0, ey=1450.0, ez=120.0, speed=v, amp=amp,
                                    freq=1 / 40.0, waveform=abi.LBM_WAVE_SINE, injection=abi.LBM_INJECT_TRILINEAR)
         return dict(cfg=cfg, sources=[src], probes=probes, triangles=tris, steps=4000, coverage=cov,
-                    description="synthetic city 2048x2048x256, source flying at z=120 Mach 0.15, 512 probes")
+                    description=CITY_SUMMARY["city2048"][2])
     if name in ("adjoint256", "adjoint128"):
         from .solver import city_triangles
 
