@@ -710,7 +710,7 @@ __global__ void __launch_bounds__(32 * WARPS, MINB) k_adj_hb(AdjStepArgs a)
         const unsigned char* slot = ring + st * ahb::kSlotBytes;
         const bool active = c0 < L.nx;
         const bool has1 = c0 + 1 < L.nx;
-        const long long e0 = L.elem(0, min(c0, L.nx - 1) + 1, j, k);
+        const long long e0 = L.elem(0, (active ? c0 : ((L.nx - 1) & ~1)) + 1, j, k);   // inactive lanes shadow a valid pair
 
         // ---- moments of F^{s-1} and links of the pair
         const uint4 mw = *reinterpret_cast<const uint4*>(slot + ahb::kMomOff + 16 * lane);
