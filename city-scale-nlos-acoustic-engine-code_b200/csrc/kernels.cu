@@ -738,7 +738,9 @@ template <int S>
 __host__ __device__ constexpr int warp_bytes() { return (S * kSlotBytes + S * 8 + 127) / 128 * 128; }
 }  // namespace hb
 
-template <int P, int WARPS, int MINB>
+// BULK = false feeds the same pipeline with per-lane 16-byte cp.async copies
+// (five per lane and block, cp.async groups instead of mbarriers).
+template <int P, int WARPS, int MINB, bool BULK = true>
 __global__ void __launch_bounds__(32 * WARPS, MINB) k_step_hb(const __half* __restrict__ fin,
                                                                __half* __restrict__ fout, Layout L, StepArgs a,
                                                                float inv_scale)
@@ -755,13 +757,25 @@ __global__ void __launch_bounds__(32 * WARPS, MINB) k_step_hb(const __half* __re
     const int all_warps = gridDim.x * WARPS;
     const int r0 = blockIdx.x * WARPS + warp;   // rows r0, r0 + all_warps, ...; r = (k-1) ny + (j-1)
     if (r0 >= nrows) return;
-    if (lane < S) mbar_init(bar_s + 8 * lane, 1);
-    fence_mbar_init();
-    __syncwarp();
+    if constexpr (BULK)
+    {
+        if (lane < S) mbar_init(bar_s + 8 * lane, 1);
+        fence_mbar_init();
+        __syncwarp();
+    }
 
-    // lane q < 19 copies line q: element offset from the destination block's own position
+    // BULK: lane q < 19 copies line q; its element offset from the destination block's own position
     const int ql = lane < Q ? lane : 0;
-    const int loff = -(c_ey[ql] * (int)L.row_stride + c_ez[ql] * (int)L.plane_stride) + ql * 64;
+    const int loff = BULK ? -(c_ey[ql] * (int)L.row_stride + c_ez[ql] * (int)L.plane_stride) + ql * 64 : 0;
+    // cp.async: this lane's five 16-byte pieces (piece p = 32 i + lane of the block's 19 lines)
+    int poff[5];
+#pragma unroll
+    for (int i = 0; i < 5; ++i)
+    {
+        const int p = i * 32 + lane;
+        const int q = min(p >> 3, 18);
+        poff[i] = BULK ? 0 : -(c_ey[q] * (int)L.row_stride + c_ez[q] * (int)L.plane_stride) + q * 64 + (p & 7) * 8;
+    }
     // lanes 0-4: low-face ghosts (directions with ex > 0) of a row, lanes 5-9: high-face ghosts (ex < 0)
     const int gq = wp::ghost_dir(lane < 10 ? lane : 0);
     const int goff = (lane < 5 ? 0 : 19) * (L.nz + 2) * (L.ny + 2) + gq * (L.nz + 2) * (L.ny + 2) -
@@ -785,6 +799,17 @@ __global__ void __launch_bounds__(32 * WARPS, MINB) k_step_hb(const __half* __re
     };
     const auto issue = [&](unsigned flags) {
         const uint32_t dst = ring_s + ci_slot * hb::kSlotBytes;
+        if constexpr (!BULK)
+        {
+#pragma unroll
+            for (int i = 0; i < 5; ++i)
+                if ((i < 4 || lane < 24) && LBM_IN(kChkHwLine, (ci_src - fin) + poff[i], L.total - 7))
+                    cp_async16(dst + (i * 32 + lane) * 16, ci_src + poff[i]);
+            if ((flags & hb::kNear) && 64 * ci_b + 2 * lane < L.pitch &&
+                LBM_IN(kChkHwLinks, ci_link + 64 * ci_b + 2 * lane - a.links, links_extent(L) - 1))
+                cp_async8(dst + hb::kLinkOff + lane * 8, ci_link + 64 * ci_b + 2 * lane);
+            return;
+        }
         const uint32_t bar = bar_s + 8 * ci_slot;
         // links words of the block's 64 cells, within the row's pitch (16-byte multiples)
         const int nlink = (flags & hb::kNear) ? min(64, L.pitch - 64 * ci_b) : 0;
@@ -873,10 +898,12 @@ __global__ void __launch_bounds__(32 * WARPS, MINB) k_step_hb(const __half* __re
             ci_next();
             if (ci_r < nrows) nf = ci_flags();
         }
+        if constexpr (!BULK) cp_async_commit();
     }
     uint32_t ph = 0u;   // bit s: parity of slot s's next phase
     int st = 0;         // slot of block t
-    bool ok = mbar_wait(bar_s, 0u);
+    bool ok = true;
+    if constexpr (BULK) ok = mbar_wait(bar_s, 0u);
     if (ok)
     {
         ph ^= 1u;
@@ -897,7 +924,14 @@ __global__ void __launch_bounds__(32 * WARPS, MINB) k_step_hb(const __half* __re
         const int sp = st == 0 ? S - 1 : st - 1;
         const int sn = st == S - 1 ? 0 : st + 1;
         // block t + 1 must have landed too: lane 31 reads its first word
-        if (inflight > 0)
+        if constexpr (!BULK)
+        {
+            cp_async_commit();
+            cp_async_wait<P - 1>();   // every group but the newest P - 1: blocks up to t + 1
+            __syncwarp();
+            if (inflight > 0) --inflight;
+        }
+        else if (inflight > 0)
         {
             ok = mbar_wait(bar_s + 8 * sn, (ph >> sn) & 1u);
             if (ok)
@@ -1009,6 +1043,7 @@ __global__ void __launch_bounds__(32 * WARPS, MINB) k_step_hb(const __half* __re
         cc_next();
         st = sn;
     }
+    if constexpr (!BULK) cp_async_wait<0>();
     if (!__all_sync(kFull, ok))
     {
         // a slot never completed: record it, then let the copies still in flight land before exiting
@@ -1588,7 +1623,7 @@ cudaError_t launch_hw(const __half* fin, __half* fout, const Layout& L, const St
     return cudaGetLastError();
 }
 
-template <int P, int WARPS, int MINB>
+template <int P, int WARPS, int MINB, bool BULK = true>
 cudaError_t hb_ctas(int* out)
 {
     constexpr int smem = WARPS * hb::warp_bytes<P + 2>();
@@ -1601,10 +1636,10 @@ cudaError_t hb_ctas(int* out)
     std::lock_guard<std::mutex> lock(mu);
     if (!ctas[dev])
     {
-        e = cudaFuncSetAttribute(k_step_hb<P, WARPS, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        e = cudaFuncSetAttribute(k_step_hb<P, WARPS, MINB, BULK>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         int per_sm = 0, sms = 0;
         if (e == cudaSuccess)
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_hb<P, WARPS, MINB>, 32 * WARPS, smem);
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_hb<P, WARPS, MINB, BULK>, 32 * WARPS, smem);
         if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         if (e != cudaSuccess) return e;
         if (per_sm < 1) return cudaErrorInvalidConfiguration;
@@ -1614,23 +1649,24 @@ cudaError_t hb_ctas(int* out)
     return cudaSuccess;
 }
 
-template <int P, int WARPS, int MINB>
+template <int P, int WARPS, int MINB, bool BULK = true>
 cudaError_t launch_hb(const __half* fin, __half* fout, const Layout& L, const StepArgs& a, float inv_scale,
                       cudaStream_t stream)
 {
     // the per-lane line offsets are 32-bit
     if (L.plane_stride + L.row_stride + 19 * 64 > 0x7fffffffLL) return cudaErrorInvalidValue;
     int ctas = 0;
-    const cudaError_t e = hb_ctas<P, WARPS, MINB>(&ctas);
+    const cudaError_t e = hb_ctas<P, WARPS, MINB, BULK>(&ctas);
     if (e != cudaSuccess) return e;
     const long long need = ((long long)L.ny * L.nz + WARPS - 1) / WARPS;
     const int grid = (int)(need < ctas ? need : ctas);
-    k_step_hb<P, WARPS, MINB><<<grid, 32 * WARPS, WARPS * hb::warp_bytes<P + 2>(), stream>>>(fin, fout, L, a, inv_scale);
+    k_step_hb<P, WARPS, MINB, BULK><<<grid, 32 * WARPS, WARPS * hb::warp_bytes<P + 2>(), stream>>>(fin, fout, L, a, inv_scale);
     return cudaGetLastError();
 }
 
-// FP16 step implementation: 0 = bulk-copy pipelines (k_step_hb), 1 = cp.async
-// pipelines (k_step_hw); NLOS_LBM_F16_STEP selects while both are built.
+// FP16 step implementation (NLOS_LBM_F16_STEP while the candidates are built):
+// 0, 1 = cp.async pipelines (k_step_hw); 2 = bulk-copy pipelines (k_step_hb);
+// 4, 5 = k_step_hb fed by cp.async (4 or 1 warps per CTA).
 int f16_impl()
 {
     static const int v = [] {
@@ -1649,9 +1685,10 @@ cudaError_t launch_step_t(const S* fin, S* fout, const Layout& L, const StepArgs
         switch (f16_impl())
         {
         case 1: return launch_hw<2, 4, 5>(fin, fout, L, a, inv_scale, stream);
-        case 2: return launch_hb<2, 1, 20>(fin, fout, L, a, inv_scale, stream);
-        case 3: return launch_hb<3, 4, 4>(fin, fout, L, a, inv_scale, stream);
-        default: return launch_hb<2, 4, 5>(fin, fout, L, a, inv_scale, stream);
+        case 2: return launch_hb<2, 4, 5>(fin, fout, L, a, inv_scale, stream);
+        case 4: return launch_hb<2, 4, 5, false>(fin, fout, L, a, inv_scale, stream);
+        case 5: return launch_hb<2, 1, 20, false>(fin, fout, L, a, inv_scale, stream);
+        default: return launch_hw<2, 4, 5>(fin, fout, L, a, inv_scale, stream);
         }
     }
     k_step<S, 128, 0><<<pair_grid(L, 128), 128, 0, stream>>>(fin, fout, L, a, inv_scale);
@@ -1716,9 +1753,10 @@ cudaError_t prepare_step(int storage)
     switch (f16_impl())
     {
     case 1: return hw_ctas<2, 4, 5>(&ctas);
-    case 2: return hb_ctas<2, 1, 20>(&ctas);
-    case 3: return hb_ctas<3, 4, 4>(&ctas);
-    default: return hb_ctas<2, 4, 5>(&ctas);
+    case 2: return hb_ctas<2, 4, 5>(&ctas);
+    case 4: return hb_ctas<2, 4, 5, false>(&ctas);
+    case 5: return hb_ctas<2, 1, 20, false>(&ctas);
+    default: return hw_ctas<2, 4, 5>(&ctas);
     }
 }
 

@@ -134,4 +134,16 @@ class SlabRank:
         return out
 
     def close(self):
+        """Frees the message buffers (after the library's stream has finished
+        with them) and then the slab handle.  Pinned host buffers record an
+        event on the streams that used them when they are freed, so they must
+        go while the CUDA context is alive: call close() before the process
+        ends rather than leaving them to interpreter shutdown."""
+        if getattr(self, "solver", None) is None:
+            return
+        self.stream.synchronize()
+        self.send, self.recv = {}, {}
+        self.send_h, self.recv_h = {}, {}
+        self.torch.cuda.synchronize(self.stream.device)
         self.solver.close()
+        self.solver = None

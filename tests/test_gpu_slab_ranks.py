@@ -47,7 +47,9 @@ def _worker(rank, world, port, name, storage, steps, q):
     q.put((rank, p, rho, r.bounds))
     dist.barrier()
     r.close()
+    del r
     dist.destroy_process_group()
+    torch.cuda.synchronize()
 
 
 @pytest.mark.parametrize("name,storage,world", [("city_small", "fp32", 2), ("scatter_small", "fp16", 2),
