@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <cstdlib>
 
 #include "check.cuh"
 #include "device.hpp"
@@ -686,7 +687,22 @@ cudaError_t launch_step_a(const float* fin, float* fout, const Layout& L, const 
     constexpr int kBlock = 128, kZ = 4;
     const unsigned gx = (unsigned)((L.nx + 2 * kBlock - 1) / (2 * kBlock));
     if (b.field_mode == 2 || b.sg_xy || b.fld_xy)
-        k_step_a<kBlock, 5, 2, kZ><<<dim3(gx, L.ny, (L.nz + kZ - 1) / kZ), kBlock, 0, stream>>>(fin, fout, L, a, b);
+    {
+        static const int v = [] {
+            const char* e = std::getenv("NLOS_LBM_A04");
+            return e ? std::atoi(e) : 0;
+        }();
+        const dim3 g4(gx, L.ny, (L.nz + kZ - 1) / kZ), g1(gx, L.ny, L.nz);
+        switch (v)
+        {
+        case 1: k_step_a<kBlock, 5, 2, 1><<<g1, kBlock, 0, stream>>>(fin, fout, L, a, b); break;
+        case 2: k_step_a<kBlock, 6, 2, kZ><<<g4, kBlock, 0, stream>>>(fin, fout, L, a, b); break;
+        case 3: k_step_a<kBlock, 6, 2, 1><<<g1, kBlock, 0, stream>>>(fin, fout, L, a, b); break;
+        case 4: k_step_a<kBlock, 7, 2, 1><<<g1, kBlock, 0, stream>>>(fin, fout, L, a, b); break;
+        case 5: k_step_a<kBlock, 6, 2, 2><<<dim3(gx, L.ny, (L.nz + 1) / 2), kBlock, 0, stream>>>(fin, fout, L, a, b); break;
+        default: k_step_a<kBlock, 5, 2, kZ><<<g4, kBlock, 0, stream>>>(fin, fout, L, a, b); break;
+        }
+    }
     else if (b.blend || b.zper)
         k_step_a<kBlock, 7, 1, 1><<<dim3(gx, L.ny, L.nz), kBlock, 0, stream>>>(fin, fout, L, a, b);
     else
