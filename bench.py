@@ -43,12 +43,16 @@ L2_BYTES = 126e6   # B200 L2
 ERR_STEPS = 4000
 
 
-def headline_config(name, storage, n):
+def headline_config(name, storage, n, dims=None, desc=None):
     """The `config` of both arms' lines: the workload, its grid and storage,
-    the multi-GPU form and the L2 rule (known without building the workload)."""
+    the multi-GPU form and the L2 rule (known without building the city
+    workloads; other workloads pass their grid and description)."""
     from nlos_lbm import workloads
 
-    dims, default_storage, desc = workloads.CITY_SUMMARY[name]
+    if name in workloads.CITY_SUMMARY:
+        dims, default_storage, desc = workloads.CITY_SUMMARY[name]
+    else:
+        default_storage = "fp32"
     storage = storage or default_storage
     cells = dims[0] * dims[1] * dims[2]
     pop_bytes = cells * (76 if storage == "fp16" else 152)
@@ -587,7 +591,7 @@ def run_our_arm(args):
         "ms_per_step": head["ms"] / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "fp16-store/fp32-compute" if head["storage"] == "fp16" else "fp32",
         "data": DATA,
-        "config": headline_config(headline, head["storage"], n),
+        "config": headline_config(headline, head["storage"], n, head["dims"], head["description"]),
         "roofline": roofline,
         "e2e": {"value": n * cells * steps / (e2e_ms / 1e3) / 1e9, "unit": UNIT, "h2d_bytes_per_step": h2d_ps,
                 "d2h_bytes_per_step": d2h_ps},
