@@ -7,12 +7,10 @@
 
 #include <cmath>
 #include <cstdint>
-#include <mutex>
 
 #include "adjoint.hpp"
 #include "check.cuh"
 #include "lattice.cuh"
-#include "pipeline.cuh"
 
 namespace lbm {
 namespace {
@@ -527,388 +525,6 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_adj_step(AdjStepArgs a)
     }
 }
 
-// ---------------------------------------------------------------- adjoint step, bulk-copy pipelines
-// k_adj_step with its loads taken off the critical path: each warp walks
-// whole rows 64 cells (two 32-cell blocks, two cells per lane) at a time and
-// keeps the next P units in flight in its own ring of shared-memory slots.
-// A slot holds the unit's 19 adjoint lines of both blocks, gathered from the
-// rows (j + ey, k + ez) (lanes 0-18, one or two copies each), the 16 bytes
-// beyond each end of the lines that the unit's edge cells pull (lanes 19-28:
-// the first four cells of the next unit for the 5 directions with ex > 0,
-// the last four of the previous unit for the 5 with ex < 0), the stored
-// moments of its 64 cells (lane 29) and, for units with a SOLID cell or
-// neighbour, their links words (lane 30); copies complete on the slot's
-// mbarrier.  A slot is thus complete by itself: the warp waits only for the
-// unit it updates.  The arithmetic is k_adj_step's, in the same order, so
-// the two give bit-identical gradients.  Needs an even nx (the moment rows
-// are then 16-byte aligned).
-namespace ahb {
-constexpr int kLamBytes = 19 * 256;          // [q][64 cells] of lamF^s
-constexpr int kRightOff = kLamBytes;         // [5][4] cells 64 .. 67, directions with ex > 0
-constexpr int kLeftOff = kRightOff + 80;     // [5][4] cells -4 .. -1, directions with ex < 0
-constexpr int kMomOff = kLeftOff + 80;       // [64] PackedMoments
-constexpr int kLinkOff = kMomOff + 512;      // [64] links words (near-solid units)
-constexpr int kSlotBytes = kLinkOff + 256;
-constexpr unsigned kNear = 1u, kFirst = 2u, kLast = 4u;
-template <int S>
-__host__ __device__ constexpr int warp_bytes() { return (S * kSlotBytes + S * 8 + 127) / 128 * 128; }
-// the directions with ex > 0 (right pieces) and ex < 0 (left pieces), and a direction's place among them
-__host__ __device__ constexpr int right_dir(int i) { return i == 0 ? 1 : i == 1 ? 7 : i == 2 ? 8 : i == 3 ? 11 : 12; }
-__host__ __device__ constexpr int left_dir(int i) { return i == 0 ? 2 : i == 1 ? 9 : i == 2 ? 10 : i == 3 ? 13 : 14; }
-__host__ __device__ constexpr int piece_of(int q)
-{
-    return q == 1 || q == 2 ? 0 : q == 7 || q == 9 ? 1 : q == 8 || q == 10 ? 2 : q == 11 || q == 13 ? 3 : 4;
-}
-}  // namespace ahb
-
-__constant__ signed char c_aey[19] = {0, 0, 0, 1, -1, 0, 0, 1, -1, 1, -1, 0, 0, 0, 0, 1, 1, -1, -1};
-__constant__ signed char c_aez[19] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1};
-
-template <int P, int WARPS, int MINB>
-__global__ void __launch_bounds__(32 * WARPS, MINB) k_adj_hb(AdjStepArgs a)
-{
-    constexpr int S = P + 1;   // ring slots: units t .. t + P
-    constexpr int BC = 32, BE = 19 * BC;
-    extern __shared__ __align__(128) unsigned char ahb_smem[];
-    const Layout& L = a.L;
-    const int lane = threadIdx.x & 31;
-    const int warp = threadIdx.x >> 5;
-    unsigned char* ring = ahb_smem + warp * ahb::warp_bytes<S>();
-    const uint32_t ring_s = (uint32_t)__cvta_generic_to_shared(ring);
-    const uint32_t bar_s = ring_s + S * ahb::kSlotBytes;
-    const int nrows = L.ny * L.nz;
-    const int nu = (L.nx + 63) >> 6;          // units per row
-    const int all_warps = gridDim.x * WARPS;
-    const int r0 = blockIdx.x * WARPS + warp;
-    if (r0 >= nrows) return;
-    if (lane < S) mbar_init(bar_s + 8 * lane, 1);
-    fence_mbar_init();
-    __syncwarp();
-
-    // element offset of this lane's copy from the unit's own position (block 2u, line 0, cell 0):
-    // lanes 0-18 line q of block 2u; 19-23 the next unit's first cells; 24-28 the previous unit's last cells
-    const int qd = lane < Q ? lane : lane < 24 ? ahb::right_dir(lane - 19) : lane < 29 ? ahb::left_dir(lane - 24) : 0;
-    const int roff = c_aey[qd] * (int)L.row_stride + c_aez[qd] * (int)L.plane_stride + qd * BC;
-    const int loff = lane < Q ? roff : lane < 24 ? roff + 2 * BE : lane < 29 ? roff - BE + (BC - 4) : 0;
-    const uint32_t dlane = lane < Q ? lane * 256 : lane < 24 ? ahb::kRightOff + (lane - 19) * 16
-                                                    : ahb::kLeftOff + (lane - 24) * 16;
-
-    // ---- copy cursor
-    int ci_r = r0, ci_u = 0, ci_slot = 0;
-    const float* ci_src = nullptr;      // this lane's source of the cursor's unit
-    const uint2* ci_near = nullptr;     // near-solid words of the row, two per unit
-    const uint32_t* ci_link = nullptr;  // links words of the row
-    long long ci_mom = 0;               // dense index of the row's first cell
-    const auto ci_row = [&]() {
-        const int k = 1 + ci_r / L.ny, j = 1 + ci_r - (k - 1) * L.ny;
-        ci_src = a.lam_in + L.elem(0, 1, j, k) + loff;
-        ci_near = reinterpret_cast<const uint2*>(a.sa.near + ((long long)k * (L.ny + 2) + j) * L.words_per_row);
-        ci_link = a.sa.links + L.cell(1, j, k);
-        ci_mom = ((long long)(k - 1) * L.ny + (j - 1)) * L.nx;
-    };
-    const auto ci_flags = [&]() -> unsigned {
-        uint2 nw = make_uint2(0u, 0u);
-        if (LBM_IN(kChkAdjLoad, (const uint32_t*)(ci_near + ci_u) - a.sa.near,
-                   (long long)L.words_per_row * (L.ny + 2) * (L.nz + 2) - 1))
-            nw = __ldg(ci_near + ci_u);
-        return ((nw.x | nw.y) != 0u ? ahb::kNear : 0u) | (ci_u == 0 ? ahb::kFirst : 0u) |
-               (ci_u == nu - 1 ? ahb::kLast : 0u);
-    };
-    const auto issue = [&](unsigned flags) {
-        const uint32_t dst = ring_s + ci_slot * ahb::kSlotBytes;
-        const uint32_t bar = bar_s + 8 * ci_slot;
-        const bool hasB = 2 * ci_u + 1 < L.nb;
-        const int ncell = min(64, L.nx - 64 * ci_u);                       // even: nx is even
-        const int nlink = (flags & ahb::kNear) ? min(64, L.pitch - 64 * ci_u) : 0;
-        if (lane == 0) mbar_arrive_expect_tx(bar, 19 * 128 * (hasB ? 2 : 1) + 10 * 16 + 8 * ncell + 4 * nlink);
-        fence_proxy_async();
-        __syncwarp();
-        if (lane < 29)
-        {
-            if (LBM_IN(kChkAdjLoad, ci_src - a.lam_in + 31, L.total)) bulk_load(dst + dlane, ci_src, lane < Q ? 128 : 16, bar);
-            if (lane < Q && hasB && LBM_IN(kChkAdjLoad, ci_src + BE - a.lam_in + 31, L.total))
-                bulk_load(dst + dlane + 128, ci_src + BE, 128, bar);
-        }
-        else if (lane == 29)
-        {
-            bulk_load(dst + ahb::kMomOff, a.mom_prev + ci_mom + 64 * ci_u, 8 * ncell, bar);
-        }
-        else if (lane == 30 && nlink > 0)
-        {
-            bulk_load(dst + ahb::kLinkOff, ci_link + 64 * ci_u, 4 * nlink, bar);
-        }
-    };
-    const auto ci_next = [&]() {
-        ci_src += 2 * BE;
-        ci_slot = ci_slot == S - 1 ? 0 : ci_slot + 1;
-        if (++ci_u == nu)
-        {
-            ci_u = 0;
-            ci_r += all_warps;
-            if (ci_r < nrows) ci_row();
-        }
-    };
-
-    // ---- update cursor
-    int cc_r = r0, cc_u = 0, cc_j = 0, cc_k = 0, c0 = 0;
-    float syz = 0.f;
-    const auto cc_row = [&]() {
-        cc_k = 1 + cc_r / L.ny;
-        cc_j = 1 + cc_r - (cc_k - 1) * L.ny;
-        c0 = 2 * lane;
-        syz = fmaxf(__ldg(a.sa.sig_y + cc_j - 1), __ldg(a.sa.sig_z + cc_k - 1));
-    };
-    const auto cc_next = [&]() {
-        c0 += 64;
-        if (++cc_u == nu)
-        {
-            cc_u = 0;
-            cc_r += all_warps;
-            if (cc_r < nrows) cc_row();
-        }
-    };
-
-    ci_row();
-    cc_row();
-    unsigned nf = ci_flags();
-    unsigned fq = 0u;   // flags of the units in flight, 4 bits each from unit t
-    int inflight = 0;   // units copied and not yet waited for
-#pragma unroll 1
-    for (int p = 0; p < P; ++p)
-    {
-        if (ci_r < nrows)
-        {
-            issue(nf);
-            fq |= nf << (4 * p);
-            ++inflight;
-            ci_next();
-            if (ci_r < nrows) nf = ci_flags();
-        }
-    }
-    uint32_t ph = 0u;
-    int st = 0;
-    bool ok = true;
-#pragma unroll 1
-    while (cc_r < nrows)
-    {
-        // unit t + P goes into the slot unit t - 1 left (free since the last iteration's __syncwarp)
-        if (ci_r < nrows)
-        {
-            issue(nf);
-            fq |= nf << (4 * inflight);
-            ++inflight;
-            ci_next();
-            if (ci_r < nrows) nf = ci_flags();
-        }
-        ok = mbar_wait(bar_s + 8 * st, (ph >> st) & 1u);
-        if (!__all_sync(kFull, ok)) break;
-        ph ^= 1u << st;
-        --inflight;
-        const unsigned f = fq & 15u;
-        fq >>= 4;
-        const int j = cc_j, k = cc_k;
-        const unsigned char* slot = ring + st * ahb::kSlotBytes;
-        const bool active = c0 < L.nx;
-        const bool has1 = c0 + 1 < L.nx;
-        const long long e0 = L.elem(0, (active ? c0 : ((L.nx - 1) & ~1)) + 1, j, k);   // inactive lanes shadow a valid pair
-
-        // ---- moments of F^{s-1} and links of the pair
-        const uint4 mw = *reinterpret_cast<const uint4*>(slot + ahb::kMomOff + 16 * lane);
-        const float4 m0 = unpack_moments(make_uint2(mw.x, mw.y));
-        const float4 m1 = has1 ? unpack_moments(make_uint2(mw.z, mw.w)) : m0;
-        const float2 rho = make_float2(m0.x, m1.x), jx = make_float2(m0.y, m1.y), jy = make_float2(m0.z, m1.z),
-                     jz = make_float2(m0.w, m1.w);
-        uint32_t lk0 = 0u, lk1 = 0u;
-        if (f & ahb::kNear)
-        {
-            const uint2 lw = *reinterpret_cast<const uint2*>(slot + ahb::kLinkOff + 8 * lane);
-            lk0 = active ? lw.x : 0u;
-            lk1 = has1 ? lw.y : 0u;
-        }
-        const bool any_link = __any_sync(kFull, (lk0 | lk1) != 0u);
-
-        // ---- lamH^s: transposed pull, element c + ex(q) of line q
-        const float* cur = reinterpret_cast<const float*>(slot) + 2 * lane;   // line q: cur[64 q]
-        const float* rpc = reinterpret_cast<const float*>(slot + ahb::kRightOff);
-        const float* lpc = reinterpret_cast<const float*>(slot + ahb::kLeftOff);
-        float2 lg[Q];
-#pragma unroll
-        for (int q = 0; q < Q; ++q)
-        {
-            if (ex(q) == 0) lg[q] = *reinterpret_cast<const float2*>(cur + 64 * q);
-            else if (ex(q) > 0) lg[q] = make_float2(cur[64 * q + 1], *(lane < 31 ? cur + 64 * q + 2 : rpc + 4 * ahb::piece_of(q)));
-            else lg[q] = make_float2(*(lane > 0 ? cur + 64 * q - 1 : lpc + 4 * ahb::piece_of(q) + 3), cur[64 * q]);
-        }
-        const bool xlo = c0 == 0, xhi0 = c0 == L.nx - 1, xhi1 = c0 + 1 == L.nx - 1;
-        const bool solid0 = (lk0 & kSolidSelfBit) != 0u, solid1 = (lk1 & kSolidSelfBit) != 0u;
-        if (f & (ahb::kFirst | ahb::kLast))
-        {
-            // columns outside the interior pulled nothing
-#pragma unroll
-            for (int q = 0; q < Q; ++q)
-            {
-                if (ex(q) < 0 && xlo) lg[q].x = 0.f;
-                if (ex(q) > 0 && xhi0) lg[q].x = 0.f;
-                if (ex(q) > 0 && xhi1) lg[q].y = 0.f;
-            }
-        }
-        if (any_link)
-        {
-#pragma unroll
-            for (int q = 0; q < Q; ++q)
-            {
-                if (solid0) lg[q].x = 0.f;
-                if (solid1) lg[q].y = 0.f;
-            }
-            const float* own = a.lam_in + e0;
-#pragma unroll
-            for (int q = 0; q < Q; ++q)
-            {
-                if (((lk0 | lk1) >> inv(q)) & 1u)
-                {
-                    const float2 o = ldg2c(own + inv(q) * BC, a.lam_in, L.total);
-                    if ((lk0 >> inv(q)) & 1u) lg[q].x += o.x;
-                    if ((lk1 >> inv(q)) & 1u) lg[q].y += o.y;
-                }
-            }
-        }
-        // ---- ghost-adjoint terms of the open faces the pair borders (as k_adj_step)
-        const bool yz = (j == 1 && a.gadj_off[2] >= 0) || (j == L.ny && a.gadj_off[3] >= 0) ||
-                        (k == 1 && a.gadj_off[4] >= 0) || (k == L.nz && a.gadj_off[5] >= 0);
-        if (active && yz)
-        {
-#pragma unroll
-            for (int fc = 2; fc < 6; ++fc)
-            {
-                const bool on = fc == 2 ? j == 1 : fc == 3 ? j == L.ny : fc == 4 ? k == 1 : k == L.nz;
-                if (!on || a.gadj_off[fc] < 0) continue;
-                const int axis = fc / 2;
-                const long long n = face_cells(L, axis);
-                const float* g = a.gadj + a.gadj_off[fc] + face_cell(L, axis, c0 + 1, j, k);
-#pragma unroll
-                for (int q = 0; q < Q; ++q)
-                {
-                    lg[q].x += __ldg(g + q * n);
-                    if (has1) lg[q].y += __ldg(g + q * n + 1);
-                }
-            }
-        }
-        if (active && (xlo | xhi0 | xhi1))
-        {
-            const long long n = face_cells(L, 0), c = face_cell(L, 0, 1, j, k);
-#pragma unroll
-            for (int fc = 0; fc < 2; ++fc)
-            {
-                if (a.gadj_off[fc] < 0) continue;
-                const bool to0 = fc == 0 ? xlo : xhi0, to1 = fc == 1 && xhi1;
-                if (!(to0 | to1)) continue;
-                const float* g = a.gadj + a.gadj_off[fc] + c;
-#pragma unroll
-                for (int q = 0; q < Q; ++q)
-                {
-                    const float v = __ldg(g + q * n);
-                    if (to0) lg[q].x += v;
-                    if (to1) lg[q].y += v;
-                }
-            }
-        }
-
-        // ---- J_C^T (k_adj_step's formulas and order)
-        const float2 sx = __ldg(reinterpret_cast<const float2*>(a.sa.sig_x) + (c0 >> 1));
-        const float sg0 = fmaxf(sx.x, syz), sg1 = fmaxf(has1 ? sx.y : 0.f, syz);
-        float2 ca = make_float2((1.0f - sg0) * (1.0f - a.sa.omega), (1.0f - sg1) * (1.0f - a.sa.omega));
-        float2 cb = make_float2((1.0f - sg0) * a.sa.omega, (1.0f - sg1) * a.sa.omega);
-        if (solid0) ca.x = 1.0f, cb.x = 0.0f;
-        if (solid1) ca.y = 1.0f, cb.y = 0.0f;
-        if (!has1) ca.y = 0.0f, cb.y = 0.0f;
-        float2 r = add2(rho, f2(1.0f));
-        if (r.x <= 0.f) r.x = 1e-12f;
-        if (r.y <= 0.f) r.y = 1e-12f;
-        const float2 ir = make_float2(1.0f / r.x, 1.0f / r.y);
-        const float2 ir2 = mul2(ir, ir);
-        const float2 j2 = fma2(jz, jz, fma2(jy, jy, mul2(jx, jx)));
-        float2 s0 = mul2(f2(wf(0)), lg[0]), s1 = f2(0.f);
-        float2 vx = f2(0.f), vy = vx, vz = vx, ux = vx, uy = vx, uz = vx;
-#pragma unroll
-        for (int p = 0; p < 9; ++p)
-        {
-            const int q = pair_head(p), qb = inv(q);
-            const float2 cj = cdot(q, jx, jy, jz);
-            const float2 spp = mul2(f2(wf(q)), add2(lg[q], lg[qb]));
-            const float2 dm = mul2(f2(wf(q)), sub2(lg[q], lg[qb]));
-            const float2 t = mul2(spp, cj);
-            s0 = add2(s0, spp);
-            s1 = fma2(t, cj, s1);
-            if (ex(q)) vx = ex(q) > 0 ? add2(vx, dm) : sub2(vx, dm), ux = ex(q) > 0 ? add2(ux, t) : sub2(ux, t);
-            if (ey(q)) vy = ey(q) > 0 ? add2(vy, dm) : sub2(vy, dm), uy = ey(q) > 0 ? add2(uy, t) : sub2(uy, t);
-            if (ez(q)) vz = ez(q) > 0 ? add2(vz, dm) : sub2(vz, dm), uz = ez(q) > 0 ? add2(uz, t) : sub2(uz, t);
-        }
-        const float2 A = sub2(mul2(s0, fma2(mul2(j2, ir2), f2(1.5f), f2(1.0f))), mul2(mul2(s1, ir2), f2(4.5f)));
-        const float2 Bx = fma2(vx, f2(3.0f), mul2(sub2(mul2(ux, f2(9.0f)), mul2(mul2(jx, s0), f2(3.0f))), ir));
-        const float2 By = fma2(vy, f2(3.0f), mul2(sub2(mul2(uy, f2(9.0f)), mul2(mul2(jy, s0), f2(3.0f))), ir));
-        const float2 Bz = fma2(vz, f2(3.0f), mul2(sub2(mul2(uz, f2(9.0f)), mul2(mul2(jz, s0), f2(3.0f))), ir));
-        if (active && LBM_IN(kChkAdjStore, e0 + 18 * BC + 1, L.total))
-        {
-            float* out = a.lam_out + e0;
-            const float2 cbA = mul2(cb, A);
-            *reinterpret_cast<float2*>(out) = fma2(ca, lg[0], cbA);
-#pragma unroll
-            for (int p = 0; p < 9; ++p)
-            {
-                const int q = pair_head(p), qb = inv(q);
-                const float2 cB = mul2(cb, cdot(q, Bx, By, Bz));
-                *reinterpret_cast<float2*>(out + q * BC) = fma2(ca, lg[q], add2(cbA, cB));
-                *reinterpret_cast<float2*>(out + qb * BC) = fma2(ca, lg[qb], sub2(cbA, cB));
-            }
-        }
-        __syncwarp();   // every lane is done with slot t before the next copy lands there
-        cc_next();
-        st = st == S - 1 ? 0 : st + 1;
-    }
-    if (!__all_sync(kFull, ok))
-    {
-        // a slot never completed: record it, then let the copies still in flight land before exiting
-        if (lane == 0 && a.sa.err) atomicExch(a.sa.err, 1);
-        int s = st;
-        for (int i = 0; i < inflight; ++i)
-        {
-            mbar_wait(bar_s + 8 * s, (ph >> s) & 1u);
-            s = s == S - 1 ? 0 : s + 1;
-        }
-    }
-}
-
-template <int P, int WARPS, int MINB>
-cudaError_t launch_adj_hb(const AdjStepArgs& a, cudaStream_t stream)
-{
-    constexpr int smem = WARPS * ahb::warp_bytes<P + 2>();
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return e;
-    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
-    static std::mutex mu;
-    static int ctas[kMaxDevices] = {};
-    {
-        std::lock_guard<std::mutex> lock(mu);
-        if (!ctas[dev])
-        {
-            e = cudaFuncSetAttribute(k_adj_hb<P, WARPS, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-            int per_sm = 0, sms = 0;
-            if (e == cudaSuccess)
-                e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_adj_hb<P, WARPS, MINB>, 32 * WARPS, smem);
-            if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-            if (e != cudaSuccess) return e;
-            if (per_sm < 1) return cudaErrorInvalidConfiguration;
-            ctas[dev] = per_sm * sms;
-        }
-    }
-    if (a.L.plane_stride + a.L.row_stride + 19 * 64 > 0x7fffffffLL) return cudaErrorInvalidValue;
-    const long long need = ((long long)a.L.ny * a.L.nz + WARPS - 1) / WARPS;
-    const int grid = (int)(need < ctas[dev] ? need : ctas[dev]);
-    k_adj_hb<P, WARPS, MINB><<<grid, 32 * WARPS, smem, stream>>>(a);
-    return cudaGetLastError();
-}
-
 // Residual of each probe enters the adjoint of every population it summed.
 __global__ void k_adj_probe(float* __restrict__ lam, AdjProbeArgs a)
 {
@@ -971,15 +587,6 @@ cudaError_t launch_adj_ghost(const AdjGhostArgs& a, cudaStream_t stream)
 cudaError_t launch_adj_step(const AdjStepArgs& a, int variant, cudaStream_t stream)
 {
     if (a.L.bc != 32) return cudaErrorInvalidValue;   // FP32 layout only
-    // the bulk-copy pipelines need an even nx (16-byte aligned moment rows)
-    if (variant >= 3 && (a.L.nx % 2) == 0)
-    {
-        switch (variant)
-        {
-        case 4: return launch_adj_hb<2, 4, 3>(a, stream);
-        default: return launch_adj_hb<1, 4, 4>(a, stream);
-        }
-    }
     // rows of up to 128 columns take 64-thread blocks, so no warp idles
     const int block = a.L.nx <= 128 ? 64 : 128;
     const dim3 g((unsigned)((a.L.nx + 2 * block - 1) / (2 * block)), (unsigned)a.L.ny, (unsigned)a.L.nz);

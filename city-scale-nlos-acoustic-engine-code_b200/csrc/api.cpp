@@ -619,7 +619,6 @@ extern "C" const char* lbm_status_string(int s)
     case LBM_ERR_OUT_OF_MEMORY: return "out of device memory";
     case LBM_ERR_CUDA: return "CUDA error";
     case LBM_ERR_NAN: return "non-finite value in probe series";
-    case LBM_ERR_TIMEOUT: return "a device-side wait gave up";
     case LBM_ERR_STATE: return "call out of order";
     case LBM_ERR_CAPACITY: return "output buffer too small";
     case LBM_ERR_NO_DEVICE: return "no CUDA device";
@@ -988,7 +987,6 @@ extern "C" int lbm_init(lbm_handle* h)
     h->sa.sig_z = h->sa.sig_y + ny;
     h->sa.omega = (float)(1.0 / c.tau);
     h->sa.xf = h->xf;
-    h->sa.err = &h->ctl->step_error;
     {
         const cudaError_t e = prepare_step(h->storage == LBM_STORE_F16 ? 1 : 0);
         if (e != cudaSuccess) return h->cuda_fail(e, "step set-up");
@@ -1587,19 +1585,19 @@ extern "C" int lbm_step(lbm_handle* h, int nsteps)
                 done += 1;
             }
         }
-        // the probe kernels' non-finite flag and the step's wait flag
-        CK(cudaMemcpyAsync(&h->ctl_host->nonfinite, &h->ctl->nonfinite, 2 * sizeof(int), cudaMemcpyDeviceToHost,
-                           h->stream),
-           "device flags");
-        h->d2h_bytes += (long)(2 * sizeof(int));
+        if (np)
+        {
+            // the probe kernels' non-finite flag
+            CK(cudaMemcpyAsync(&h->ctl_host->nonfinite, &h->ctl->nonfinite, sizeof(int), cudaMemcpyDeviceToHost,
+                               h->stream),
+               "probe flag");
+            h->d2h_bytes += (long)sizeof(int);
+        }
         // the control block upload must not be overwritten before the copy ran
         CK(cudaStreamSynchronize(h->stream), "step sync");
         h->step += chunk;
         if (np) h->probe_pending += chunk;
         left -= chunk;
-        if (h->ctl_host->step_error)
-            return h->fail(LBM_ERR_TIMEOUT, "a wait of the step kernel for its own copies gave up by step " +
-                                                std::to_string(h->step));
         if (np && h->ctl_host->nonfinite)
             return h->fail(LBM_ERR_NAN, "non-finite probe value by step " + std::to_string(h->step));
         st = harvest_timing(h);
@@ -2308,7 +2306,7 @@ extern "C" int lbm_adjoint_grad(lbm_handle* h, int nsteps, const double* observe
     SourceArgs sargs = source_args(h, false);
     int adj_variant = kDefaultAdjointVariant;
     if (const char* v = std::getenv("NLOS_LBM_ADJ_VARIANT")) adj_variant = std::atoi(v);
-    if (adj_variant < 0 || adj_variant > 4) return h->fail(LBM_ERR_BAD_CONFIG, "NLOS_LBM_ADJ_VARIANT out of range");
+    if (adj_variant < 0 || adj_variant > 2) return h->fail(LBM_ERR_BAD_CONFIG, "NLOS_LBM_ADJ_VARIANT out of range");
     // L2 prefetch distance of the adjoint step in rows (NLOS_LBM_ADJ_PREFETCH_ROWS, 0 = off)
     int adj_prefetch = kDefaultAdjointPrefetchRows;
     if (const char* v = std::getenv("NLOS_LBM_ADJ_PREFETCH_ROWS")) adj_prefetch = std::max(0, std::atoi(v));

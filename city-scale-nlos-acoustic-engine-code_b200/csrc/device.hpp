@@ -71,7 +71,6 @@ struct Control
     long long probe_base;  // step index of probe-buffer row 0
     int nonfinite;         // set by the probe kernels when an owned probe reads a non-finite value
                            // (the host uploads only the fields above it)
-    int step_error;        // set by the FP16 step when a wait for its own copies gave up
 };
 
 struct SourceStatic
@@ -148,7 +147,6 @@ struct StepArgs
     const float* sig_z;
     float omega;               // 1 / tau
     XFace xf;
-    int* err;                  // device flag: set to 1 when a kernel's bounded wait gave up
 };
 
 struct ProbeArgs

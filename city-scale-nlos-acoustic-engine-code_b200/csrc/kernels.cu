@@ -15,7 +15,6 @@
 #include "check.cuh"
 #include "device.hpp"
 #include "lattice.cuh"
-#include "pipeline.cuh"
 
 namespace lbm {
 namespace {
@@ -719,344 +718,6 @@ __global__ void __launch_bounds__(32 * WARPS, MINB) k_step_hw(const __half* __re
     cp_async_wait<0>();
 }
 
-// ---------------------------------------------------------------- FP16 step, bulk-copy pipelines
-// Each warp walks whole rows one 64-cell block at a time (two cells per lane)
-// and keeps the source lines of its next P blocks in flight in its own ring
-// of shared-memory slots: lanes 0-18 each start one 128-byte bulk copy (the
-// line of direction q from row (j - ey, k - ez)), completed on the slot's
-// mbarrier, and lane 19 the block's 64 links words when the block holds a
-// SOLID cell or a SOLID neighbour.  Blocks away from solids and from the row
-// ends (most of a city) take a path with no links, ghost or export code; the
-// near-solid bitmap word of a block is read one block ahead of its copy, the
-// x-face ghosts and the sponge strengths of a row one row ahead.
-namespace hb {
-constexpr int kLinesBytes = 19 * 128;           // a block's 19 source lines
-constexpr int kLinkOff = kLinesBytes;           // its links words (near-solid blocks only)
-constexpr int kSlotBytes = kLinesBytes + 256;
-constexpr unsigned kNear = 1u, kFirst = 2u, kLast = 4u;   // block flags
-template <int S>
-__host__ __device__ constexpr int warp_bytes() { return (S * kSlotBytes + S * 8 + 127) / 128 * 128; }
-}  // namespace hb
-
-// BULK = false feeds the same pipeline with per-lane 16-byte cp.async copies
-// (five per lane and block, cp.async groups instead of mbarriers).
-template <int P, int WARPS, int MINB, bool BULK = true>
-__global__ void __launch_bounds__(32 * WARPS, MINB) k_step_hb(const __half* __restrict__ fin,
-                                                               __half* __restrict__ fout, Layout L, StepArgs a,
-                                                               float inv_scale)
-{
-    constexpr int S = P + 2;   // ring slots: blocks t - 1 .. t + P
-    constexpr uint32_t kDirBits = (1u << Q) - 1u;
-    extern __shared__ __align__(128) unsigned char hb_smem[];
-    const int lane = threadIdx.x & 31;
-    const int warp = threadIdx.x >> 5;
-    unsigned char* ring = hb_smem + warp * hb::warp_bytes<S>();
-    const uint32_t ring_s = (uint32_t)__cvta_generic_to_shared(ring);
-    const uint32_t bar_s = ring_s + S * hb::kSlotBytes;
-    const int nrows = L.ny * L.nz;
-    const int all_warps = gridDim.x * WARPS;
-    const int r0 = blockIdx.x * WARPS + warp;   // rows r0, r0 + all_warps, ...; r = (k-1) ny + (j-1)
-    if (r0 >= nrows) return;
-    if constexpr (BULK)
-    {
-        if (lane < S) mbar_init(bar_s + 8 * lane, 1);
-        fence_mbar_init();
-        __syncwarp();
-    }
-
-    // BULK: lane q < 19 copies line q; its element offset from the destination block's own position
-    const int ql = lane < Q ? lane : 0;
-    const int loff = BULK ? -(c_ey[ql] * (int)L.row_stride + c_ez[ql] * (int)L.plane_stride) + ql * 64 : 0;
-    // cp.async: this lane's five 16-byte pieces (piece p = 32 i + lane of the block's 19 lines)
-    int poff[5];
-#pragma unroll
-    for (int i = 0; i < 5; ++i)
-    {
-        const int p = i * 32 + lane;
-        const int q = min(p >> 3, 18);
-        poff[i] = BULK ? 0 : -(c_ey[q] * (int)L.row_stride + c_ez[q] * (int)L.plane_stride) + q * 64 + (p & 7) * 8;
-    }
-    // lanes 0-4: low-face ghosts (directions with ex > 0) of a row, lanes 5-9: high-face ghosts (ex < 0)
-    const int gq = wp::ghost_dir(lane < 10 ? lane : 0);
-    const int goff = (lane < 5 ? 0 : 19) * (L.nz + 2) * (L.ny + 2) + gq * (L.nz + 2) * (L.ny + 2) -
-                     c_ez[gq] * (L.ny + 2) - c_ey[gq];
-
-    // ---- copy cursor: the next block whose lines are copied
-    int ci_r = r0, ci_b = 0, ci_slot = 0;
-    const __half* ci_src = nullptr;     // lane q: line q of the cursor's block
-    const uint32_t* ci_link = nullptr;  // links words of the cursor's row
-    const uint2* ci_near = nullptr;     // near-solid words of the cursor's row, two per block
-    const auto ci_row = [&]() {
-        const int k = 1 + ci_r / L.ny, j = 1 + ci_r - (k - 1) * L.ny;
-        ci_src = fin + L.elem(0, 1, j, k) + loff;
-        ci_link = a.links + L.cell(1, j, k);
-        ci_near = reinterpret_cast<const uint2*>(a.near + ((long long)k * (L.ny + 2) + j) * L.words_per_row);
-    };
-    const auto ci_flags = [&]() -> unsigned {
-        uint2 nw = make_uint2(0u, 0u);
-        if (LBM_IN(kChkHwNear, (const uint32_t*)(ci_near + ci_b) - a.near, near_extent(L) - 1)) nw = __ldg(ci_near + ci_b);
-        return ((nw.x | nw.y) != 0u ? hb::kNear : 0u) | (ci_b == 0 ? hb::kFirst : 0u) | (ci_b == L.nb - 1 ? hb::kLast : 0u);
-    };
-    const auto issue = [&](unsigned flags) {
-        const uint32_t dst = ring_s + ci_slot * hb::kSlotBytes;
-        if constexpr (!BULK)
-        {
-#pragma unroll
-            for (int i = 0; i < 5; ++i)
-                if ((i < 4 || lane < 24) && LBM_IN(kChkHwLine, (ci_src - fin) + poff[i], L.total - 7))
-                    cp_async16(dst + (i * 32 + lane) * 16, ci_src + poff[i]);
-            if ((flags & hb::kNear) && 64 * ci_b + 2 * lane < L.pitch &&
-                LBM_IN(kChkHwLinks, ci_link + 64 * ci_b + 2 * lane - a.links, links_extent(L) - 1))
-                cp_async8(dst + hb::kLinkOff + lane * 8, ci_link + 64 * ci_b + 2 * lane);
-            return;
-        }
-        const uint32_t bar = bar_s + 8 * ci_slot;
-        // links words of the block's 64 cells, within the row's pitch (16-byte multiples)
-        const int nlink = (flags & hb::kNear) ? min(64, L.pitch - 64 * ci_b) : 0;
-        if (lane == 0) mbar_arrive_expect_tx(bar, hb::kLinesBytes + 4 * nlink);
-        fence_proxy_async();   // this warp's earlier reads of the slot come before the copies' writes
-        __syncwarp();
-        if (lane < Q)
-        {
-            if (LBM_IN(kChkHwLine, ci_src - fin, L.total - 63)) bulk_load(dst + lane * 128, ci_src, 128, bar);
-        }
-        else if (lane == Q && nlink > 0)
-        {
-            const uint32_t* src = ci_link + 64 * ci_b;
-            if (LBM_IN(kChkHwLinks, src - a.links + nlink - 1, links_extent(L))) bulk_load(dst + hb::kLinkOff, src, 4 * nlink, bar);
-        }
-    };
-    const auto ci_next = [&]() {
-        ci_src += 19 * 64;
-        ci_slot = ci_slot == S - 1 ? 0 : ci_slot + 1;
-        if (++ci_b == L.nb)
-        {
-            ci_b = 0;
-            ci_r += all_warps;
-            if (ci_r < nrows) ci_row();
-        }
-    };
-
-    // ---- per-row values, loaded one row ahead of the update cursor
-    const auto row_syz = [&](int r) -> float {
-        const int k = 1 + r / L.ny, j = 1 + r - (k - 1) * L.ny;
-        return fmaxf(__ldg(a.sig_y + j - 1), __ldg(a.sig_z + k - 1));
-    };
-    const auto row_gh = [&](int r) -> float {
-        const int k = 1 + r / L.ny, j = 1 + r - (k - 1) * L.ny;
-        const long long gi = ((long long)k * (L.ny + 2) + j) + goff;
-        return lane < 10 && LBM_IN(kChkHwGhost, gi, xgh_extent(L)) ? __ldg(a.xf.xgh + gi) : 0.f;
-    };
-
-    // ---- update cursor: the block being updated
-    int cc_r = r0, cc_b = 0, cc_j = 0, cc_k = 0, c0 = 0;
-    const unsigned* own = nullptr;   // this lane's word of line 0 of the block (line q: own[32 q])
-    unsigned* outp = nullptr;
-    float syz = row_syz(r0), gh = row_gh(r0);
-    float syz_n = 0.f, gh_n = 0.f;
-    const auto cc_row = [&]() {
-        cc_k = 1 + cc_r / L.ny;
-        cc_j = 1 + cc_r - (cc_k - 1) * L.ny;
-        const long long e = L.elem(0, 1, cc_j, cc_k);
-        own = reinterpret_cast<const unsigned*>(fin + e) + lane;
-        outp = reinterpret_cast<unsigned*>(fout + e) + lane;
-        c0 = 2 * lane;
-        const int rn = cc_r + all_warps;
-        if (rn < nrows)
-        {
-            syz_n = row_syz(rn);
-            gh_n = row_gh(rn);
-        }
-    };
-    const auto cc_next = [&]() {
-        own += 19 * 32;
-        outp += 19 * 32;
-        c0 += 64;
-        if (++cc_b == L.nb)
-        {
-            cc_b = 0;
-            cc_r += all_warps;
-            syz = syz_n;
-            gh = gh_n;
-            if (cc_r < nrows) cc_row();
-        }
-    };
-
-    ci_row();
-    cc_row();
-    unsigned nf = ci_flags();   // flags of the copy cursor's block, read one block ahead
-    unsigned fq = 0u;           // flags of the blocks in flight, 4 bits each from block t
-    int inflight = 0;           // blocks copied and not yet waited for
-#pragma unroll 1
-    for (int p = 0; p < P; ++p)
-    {
-        if (ci_r < nrows)
-        {
-            issue(nf);
-            fq |= nf << (4 * p);
-            ++inflight;
-            ci_next();
-            if (ci_r < nrows) nf = ci_flags();
-        }
-        if constexpr (!BULK) cp_async_commit();
-    }
-    uint32_t ph = 0u;   // bit s: parity of slot s's next phase
-    int st = 0;         // slot of block t
-    bool ok = true;
-    if constexpr (BULK) ok = mbar_wait(bar_s, 0u);
-    if (ok)
-    {
-        ph ^= 1u;
-        --inflight;
-    }
-#pragma unroll 1
-    while (cc_r < nrows)
-    {
-        if (!__all_sync(kFull, ok)) break;
-        if (ci_r < nrows)
-        {
-            issue(nf);
-            fq |= nf << (4 * (inflight + 1));
-            ++inflight;
-            ci_next();
-            if (ci_r < nrows) nf = ci_flags();
-        }
-        const int sp = st == 0 ? S - 1 : st - 1;
-        const int sn = st == S - 1 ? 0 : st + 1;
-        // block t + 1 must have landed too: lane 31 reads its first word
-        if constexpr (!BULK)
-        {
-            cp_async_commit();
-            cp_async_wait<P - 1>();   // every group but the newest P - 1: blocks up to t + 1
-            __syncwarp();
-            if (inflight > 0) --inflight;
-        }
-        else if (inflight > 0)
-        {
-            ok = mbar_wait(bar_s + 8 * sn, (ph >> sn) & 1u);
-            if (ok)
-            {
-                ph ^= 1u << sn;
-                --inflight;
-            }
-        }
-        const unsigned f = fq & 15u;
-        fq >>= 4;
-        const unsigned char* slot = ring + st * hb::kSlotBytes;
-
-        // sponge strengths of the two cells first, so that the load is in flight early
-        const float2 sx = __ldg(reinterpret_cast<const float2*>(a.sig_x) + (c0 >> 1));
-        // pulled words: line q of the slot, shifted by ex(q) across lanes / blocks
-        const unsigned* cur = reinterpret_cast<const unsigned*>(slot) + lane;   // line q: cur[32 q]
-        const unsigned* prv = lane > 0 ? cur - 1 : reinterpret_cast<const unsigned*>(ring + sp * hb::kSlotBytes) + 31;
-        const unsigned* nxt = lane < 31 ? cur + 1 : reinterpret_cast<const unsigned*>(ring + sn * hb::kSlotBytes);
-        unsigned w[Q];
-#pragma unroll
-        for (int q = 0; q < Q; ++q)
-        {
-            const unsigned v = cur[32 * q];
-            if (ex(q) == 0) w[q] = v;
-            else if (ex(q) > 0) w[q] = __byte_perm(prv[32 * q], v, 0x5432);
-            else w[q] = __byte_perm(v, nxt[32 * q], 0x5432);
-        }
-        uint32_t lk0 = 0u, lk1 = 0u;
-        if (f != 0u)
-        {
-            if (f & hb::kNear)
-            {
-                // links words came with the lines; halfway bounce-back from the cell's own opposite word
-                const uint2 lw = *reinterpret_cast<const uint2*>(slot + hb::kLinkOff + 8 * lane);
-                lk0 = lw.x;
-                lk1 = lw.y;
-                const uint32_t lka = (lk0 | lk1) & kDirBits;
-                if (__any_sync(kFull, lka != 0u))
-                {
-#pragma unroll
-                    for (int q = 0; q < Q; ++q)
-                    {
-                        const unsigned o =
-                            ((lka >> q) & 1u) &&
-                                    LBM_IN(kChkHwBounce,
-                                           2 * (own - reinterpret_cast<const unsigned*>(fin)) + inv(q) * 64, L.total - 1)
-                                ? __ldg(own + inv(q) * 32)
-                                : 0u;
-                        const unsigned m =
-                            ((0u - ((lk0 >> q) & 1u)) & 0x0000ffffu) | ((0u - ((lk1 >> q) & 1u)) & 0xffff0000u);
-                        w[q] = (w[q] & ~m) | (o & m);
-                    }
-                }
-            }
-            if (f & hb::kFirst)
-            {
-                // cell i = 1 pulls its ex > 0 directions from the low x-face ghosts
-#pragma unroll
-                for (int q = 0; q < Q; ++q)
-                {
-                    if (ex(q) <= 0) continue;
-                    const float g = __shfl_sync(kFull, gh, ghost_slot(q));
-                    if (lane == 0 && !((lk0 >> q) & 1u)) w[q] = set_lo(w[q], g);
-                }
-            }
-            if (f & hb::kLast)
-            {
-                // cell i = nx pulls its ex < 0 directions from the high x-face ghosts
-                const int last = L.nx - 1 - c0;
-#pragma unroll
-                for (int q = 0; q < Q; ++q)
-                {
-                    if (ex(q) >= 0) continue;
-                    const float g = __shfl_sync(kFull, gh, ghost_slot(q));
-                    if (last == 0 && !((lk0 >> q) & 1u)) w[q] = set_lo(w[q], g);
-                    if (last == 1 && !((lk1 >> q) & 1u)) w[q] = set_hi(w[q], g);
-                }
-            }
-        }
-        const float2 sg = make_float2(fmaxf(sx.x, syz), fmaxf(sx.y, syz));
-        collide2_grouped(w, inv_scale, a.omega, sg, (lk0 & kSolidSelfBit) != 0u, (lk1 & kSolidSelfBit) != 0u);
-        if (!(f & hb::kLast) || c0 < L.nx)
-        {
-#pragma unroll
-            for (int q = 0; q < Q; ++q)
-                if (LBM_IN(kChkHwStore, 2 * (outp - reinterpret_cast<unsigned*>(fout)) + 64 * q, L.total - 1))
-                    outp[32 * q] = w[q];
-        }
-        if (f & (hb::kFirst | hb::kLast))
-        {
-            // the cells next to the x faces export their results for the next ghost fill
-            const int last = L.nx - 1 - c0;
-            const bool xlo = (f & hb::kFirst) && lane == 0;
-            const bool xhi = (f & hb::kLast) && (last == 0 || last == 1);
-            if (xlo || xhi)
-            {
-#pragma unroll
-                for (int q = 0; q < Q; ++q)
-                {
-                    const float2 v = h2f(w[q]);
-                    const long long i0 = a.xf.exp_index(0, q, cc_j, cc_k, L.ny, L.nz);
-                    const long long i1 = a.xf.exp_index(1, q, cc_j, cc_k, L.ny, L.nz);
-                    if (xlo && LBM_IN(kChkHwExport, i0, xexp_extent(L))) a.xf.xexp[i0] = v.x;
-                    if (xhi && LBM_IN(kChkHwExport, i1, xexp_extent(L))) a.xf.xexp[i1] = last == 1 ? v.y : v.x;
-                }
-            }
-        }
-        __syncwarp();   // every lane is done with slot t - 1 before the next copy lands there
-        cc_next();
-        st = sn;
-    }
-    if constexpr (!BULK) cp_async_wait<0>();
-    if (!__all_sync(kFull, ok))
-    {
-        // a slot never completed: record it, then let the copies still in flight land before exiting
-        if (lane == 0 && a.err) atomicExch(a.err, 1);
-        int s = st;   // the first block not waited for successfully is block t
-        for (int i = 0; i < inflight; ++i)
-        {
-            mbar_wait(bar_s + 8 * s, (ph >> s) & 1u);
-            s = s == S - 1 ? 0 : s + 1;
-        }
-    }
-}
-
 // ---------------------------------------------------------------- z-slab messages
 // The populations that cross a z cut: the 5 directions with ez = +1 leave a
 // slab's top plane for the upper neighbour's halo plane 0, the 5 with ez = -1
@@ -1623,74 +1284,12 @@ cudaError_t launch_hw(const __half* fin, __half* fout, const Layout& L, const St
     return cudaGetLastError();
 }
 
-template <int P, int WARPS, int MINB, bool BULK = true>
-cudaError_t hb_ctas(int* out)
-{
-    constexpr int smem = WARPS * hb::warp_bytes<P + 2>();
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return e;
-    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
-    static std::mutex mu;
-    static int ctas[kMaxDevices] = {};
-    std::lock_guard<std::mutex> lock(mu);
-    if (!ctas[dev])
-    {
-        e = cudaFuncSetAttribute(k_step_hb<P, WARPS, MINB, BULK>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        int per_sm = 0, sms = 0;
-        if (e == cudaSuccess)
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_hb<P, WARPS, MINB, BULK>, 32 * WARPS, smem);
-        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (e != cudaSuccess) return e;
-        if (per_sm < 1) return cudaErrorInvalidConfiguration;
-        ctas[dev] = per_sm * sms;
-    }
-    *out = ctas[dev];
-    return cudaSuccess;
-}
-
-template <int P, int WARPS, int MINB, bool BULK = true>
-cudaError_t launch_hb(const __half* fin, __half* fout, const Layout& L, const StepArgs& a, float inv_scale,
-                      cudaStream_t stream)
-{
-    // the per-lane line offsets are 32-bit
-    if (L.plane_stride + L.row_stride + 19 * 64 > 0x7fffffffLL) return cudaErrorInvalidValue;
-    int ctas = 0;
-    const cudaError_t e = hb_ctas<P, WARPS, MINB, BULK>(&ctas);
-    if (e != cudaSuccess) return e;
-    const long long need = ((long long)L.ny * L.nz + WARPS - 1) / WARPS;
-    const int grid = (int)(need < ctas ? need : ctas);
-    k_step_hb<P, WARPS, MINB, BULK><<<grid, 32 * WARPS, WARPS * hb::warp_bytes<P + 2>(), stream>>>(fin, fout, L, a, inv_scale);
-    return cudaGetLastError();
-}
-
-// FP16 step implementation (NLOS_LBM_F16_STEP while the candidates are built):
-// 0, 1 = cp.async pipelines (k_step_hw); 2 = bulk-copy pipelines (k_step_hb);
-// 4, 5 = k_step_hb fed by cp.async (4 or 1 warps per CTA).
-int f16_impl()
-{
-    static const int v = [] {
-        const char* e = std::getenv("NLOS_LBM_F16_STEP");
-        return e ? std::atoi(e) : 0;
-    }();
-    return v;
-}
-
 template <typename S>
 cudaError_t launch_step_t(const S* fin, S* fout, const Layout& L, const StepArgs& a, float inv_scale,
                           cudaStream_t stream)
 {
     if constexpr (std::is_same<S, __half>::value)
-    {
-        switch (f16_impl())
-        {
-        case 1: return launch_hw<2, 4, 5>(fin, fout, L, a, inv_scale, stream);
-        case 2: return launch_hb<2, 4, 5>(fin, fout, L, a, inv_scale, stream);
-        case 4: return launch_hb<2, 4, 5, false>(fin, fout, L, a, inv_scale, stream);
-        case 5: return launch_hb<2, 1, 20, false>(fin, fout, L, a, inv_scale, stream);
-        default: return launch_hw<2, 4, 5>(fin, fout, L, a, inv_scale, stream);
-        }
-    }
+        return launch_hw<2, 4, 5>(fin, fout, L, a, inv_scale, stream);
     k_step<S, 128, 0><<<pair_grid(L, 128), 128, 0, stream>>>(fin, fout, L, a, inv_scale);
     return cudaGetLastError();
 }
@@ -1750,14 +1349,7 @@ cudaError_t prepare_step(int storage)
 {
     if (storage == 0) return cudaSuccess;
     int ctas = 0;
-    switch (f16_impl())
-    {
-    case 1: return hw_ctas<2, 4, 5>(&ctas);
-    case 2: return hb_ctas<2, 4, 5>(&ctas);
-    case 4: return hb_ctas<2, 4, 5, false>(&ctas);
-    case 5: return hb_ctas<2, 1, 20, false>(&ctas);
-    default: return hw_ctas<2, 4, 5>(&ctas);
-    }
+    return hw_ctas<2, 4, 5>(&ctas);
 }
 
 cudaError_t launch_step(int storage, const void* fin, void* fout, const Layout& L, const StepArgs& a,

@@ -27,7 +27,6 @@ LBM_ERR_CAPACITY = -7
 LBM_ERR_NO_DEVICE = -8
 LBM_ERR_IO = -9
 LBM_ERR_UNSUPPORTED = -10
-LBM_ERR_TIMEOUT = -11
 LBM_NOALLOC_MAX_CELLS = 8388608
 
 LBM_BC_NSCBC, LBM_BC_REST, LBM_BC_WALL, LBM_BC_COPY, LBM_BC_PERIODIC = 0, 1, 2, 3, 4

@@ -33,7 +33,7 @@ CU_SOURCES = ["kernels.cu", "adjoint.cu", "scheme_a.cu", "voxel.cu"]
 # voxel.cu must round every FP64 expression as the host does (no FMA contraction)
 CU_FLAGS = {"voxel.cu": ["-fmad=false"]}
 CXX_SOURCES = ["api.cpp", "geometry.cpp"]
-HEADERS = ["adjoint.hpp", "check.cuh", "device.hpp", "geometry.hpp", "lattice.cuh", "pipeline.cuh"]
+HEADERS = ["adjoint.hpp", "check.cuh", "device.hpp", "geometry.hpp", "lattice.cuh"]
 
 
 def _newer(target, deps):

@@ -56,11 +56,7 @@ typedef enum lbm_status
     LBM_ERR_CAPACITY = -7,         /* caller's output buffer too small */
     LBM_ERR_NO_DEVICE = -8,
     LBM_ERR_IO = -9,
-    LBM_ERR_UNSUPPORTED = -10,
-    LBM_ERR_TIMEOUT = -11          /* a bounded device-side wait gave up (the FP16 step waits on
-                                      its own copies with an iteration limit); reported by
-                                      lbm_step / lbm_run at the end of the batch, results of
-                                      that batch are not valid */
+    LBM_ERR_UNSUPPORTED = -10
 } lbm_status;
 
 /* Boundary treatment of one face of the box. */
