@@ -6,7 +6,6 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
-#include <cstdlib>
 
 #include "check.cuh"
 #include "device.hpp"
@@ -145,10 +144,11 @@ __device__ __forceinline__ void pull_a(const float* __restrict__ f, const Layout
 
 // ---------------------------------------------------------------- step
 // Two x-adjacent cells per thread, aligned float2 loads with warp shuffles
-// for the +-1 x shift (the same access scheme as the scheme-B step); each
-// thread updates its pair in KZ consecutive planes, so what does not depend
-// on z (the omega and blend profiles of the column, the source weights of
-// the column, the step's source masses) is looked up once.  FEAT: 0 = the
+// for the +-1 x shift (the same access scheme as the scheme-B step).  04's
+// instance looks up what does not depend on z (the omega and blend profiles
+// of the column, its source weights, the step's source masses) once per
+// thread, for KZ consecutive planes (the launcher uses one: more planes per
+// thread cost registers, and occupancy set this kernel's time).  FEAT: 0 = the
 // update of 02 and 03; 1 = with 01's destination blend and periodic z; 2 =
 // also with per-column fields and the pre-step source (04).  Each is its own
 // instance, so the simpler programs keep the leaner kernel.
@@ -681,28 +681,14 @@ cudaError_t launch_step_a(const float* fin, float* fout, const Layout& L, const 
                           cudaStream_t stream)
 {
     if (L.bc != BC) return cudaErrorInvalidValue;
-    // 04's instance walks 4 planes per thread (its column lookups are the
-    // costly part); the lean instances, at 72 registers, take one plane each
-    // (a plane loop there spilled)
-    constexpr int kBlock = 128, kZ = 4;
+    // every instance takes one plane per thread; 04's, with its column values
+    // hoisted, at the lean instances' 72 registers (28 warps per SM): on 04's
+    // 208^3 grid 0.309 ms against 0.326 ms at 96 registers with four planes per
+    // thread, 0.320 ms at 80 registers with two, 0.349-0.367 ms otherwise
+    constexpr int kBlock = 128;
     const unsigned gx = (unsigned)((L.nx + 2 * kBlock - 1) / (2 * kBlock));
     if (b.field_mode == 2 || b.sg_xy || b.fld_xy)
-    {
-        static const int v = [] {
-            const char* e = std::getenv("NLOS_LBM_A04");
-            return e ? std::atoi(e) : 0;
-        }();
-        const dim3 g4(gx, L.ny, (L.nz + kZ - 1) / kZ), g1(gx, L.ny, L.nz);
-        switch (v)
-        {
-        case 1: k_step_a<kBlock, 5, 2, 1><<<g1, kBlock, 0, stream>>>(fin, fout, L, a, b); break;
-        case 2: k_step_a<kBlock, 6, 2, kZ><<<g4, kBlock, 0, stream>>>(fin, fout, L, a, b); break;
-        case 3: k_step_a<kBlock, 6, 2, 1><<<g1, kBlock, 0, stream>>>(fin, fout, L, a, b); break;
-        case 4: k_step_a<kBlock, 7, 2, 1><<<g1, kBlock, 0, stream>>>(fin, fout, L, a, b); break;
-        case 5: k_step_a<kBlock, 6, 2, 2><<<dim3(gx, L.ny, (L.nz + 1) / 2), kBlock, 0, stream>>>(fin, fout, L, a, b); break;
-        default: k_step_a<kBlock, 5, 2, kZ><<<g4, kBlock, 0, stream>>>(fin, fout, L, a, b); break;
-        }
-    }
+        k_step_a<kBlock, 7, 2, 1><<<dim3(gx, L.ny, L.nz), kBlock, 0, stream>>>(fin, fout, L, a, b);
     else if (b.blend || b.zper)
         k_step_a<kBlock, 7, 1, 1><<<dim3(gx, L.ny, L.nz), kBlock, 0, stream>>>(fin, fout, L, a, b);
     else
