@@ -7,7 +7,6 @@
 
 #include <algorithm>
 #include <cmath>
-#include <cstdlib>
 #include <cstdint>
 #include <mutex>
 #include <type_traits>
@@ -718,319 +717,6 @@ __global__ void __launch_bounds__(32 * WARPS, MINB) k_step_hw(const __half* __re
     cp_async_wait<0>();
 }
 
-// FP16 step with self-contained ring slots: each slot also holds the 10 words
-// of the neighbour blocks that its edge cells pull (the previous block's last
-// word of the 5 lines with ex > 0, the next block's first word of the 5 with
-// ex < 0), so a warp waits only for the block it updates and keeps P + 1
-// slots instead of P + 2; with the collision of collide2_lean (each word
-// converted where it is used) the kernel fits fewer registers, for more warps
-// per SM.
-namespace hx {
-constexpr int kEdgeOff = wp::kSlotBytes;
-constexpr int kSlotBytes = kEdgeOff + 48;
-}
-
-// collide2_grouped() with each word converted to FP32 where it is used (twice:
-// in the moment sums and in its update) instead of all 19 at once, so that no
-// 19 x float2 array is live; same formulas, another summation order.
-__device__ __forceinline__ void collide2_lean(unsigned (&w)[Q], float inv_scale, float omega, float2 sigma,
-                                              bool solid0, bool solid1)
-{
-    float2 rho = h2f(w[0]);
-    float2 jx = f2(0.f), jy = f2(0.f), jz = f2(0.f);
-#pragma unroll
-    for (int q = 1; q < Q; ++q)
-    {
-        const float2 g = h2f(w[q]);
-        rho = add2(rho, g);
-        if (ex(q) > 0) jx = add2(jx, g);
-        if (ex(q) < 0) jx = sub2(jx, g);
-        if (ey(q) > 0) jy = add2(jy, g);
-        if (ey(q) < 0) jy = sub2(jy, g);
-        if (ez(q) > 0) jz = add2(jz, g);
-        if (ez(q) < 0) jz = sub2(jz, g);
-    }
-    float2 r = fma2(rho, f2(inv_scale), f2(1.0f));
-    if (r.x <= 0.f) r.x = 1e-12f;   // 06:948
-    if (r.y <= 0.f) r.y = 1e-12f;
-    const float2 irs = make_float2(__fdividef(inv_scale, r.x), __fdividef(inv_scale, r.y));
-    const float2 j2 = fma2(jz, jz, fma2(jy, jy, mul2(jx, jx)));
-    const float2 base = fma2(mul2(irs, j2), f2(-1.5f), rho);
-    const float2 k45 = mul2(irs, f2(4.5f));
-    const float2 keep = sub2(f2(1.0f), sigma);
-    float2 cA = mul2(keep, f2(1.0f - omega));
-    float2 cB = mul2(keep, f2(omega));
-    if (solid0) cA.x = 1.0f, cB.x = 0.0f;
-    if (solid1) cA.y = 1.0f, cB.y = 0.0f;
-    const float2 cBw1 = mul2(cB, f2(wf(1))), cBw2 = mul2(cB, f2(wf(7)));
-    const float2 K1 = mul2(cBw1, k45), K2 = mul2(cBw2, k45);
-    const float2 B1 = mul2(cBw1, base), B2 = mul2(cBw2, base);
-    const float2 T1 = mul2(cB, f2(3.0f * wf(1))), T2 = mul2(cB, f2(3.0f * wf(7)));
-    const float2 N1 = mul2(cB, f2(-3.0f * wf(1))), N2 = mul2(cB, f2(-3.0f * wf(7)));
-    w[0] = f2h(fma2(cA, h2f(w[0]), mul2(mul2(cB, f2(wf(0))), base)));
-#pragma unroll
-    for (int p = 0; p < 9; ++p)
-    {
-        const int q = pair_head(p);
-        const int qb = inv(q);
-        float2 cj;
-        if (p == 0) cj = jx;
-        else if (p == 1) cj = jy;
-        else if (p == 2) cj = jz;
-        else if (p == 3) cj = add2(jx, jy);
-        else if (p == 4) cj = sub2(jx, jy);
-        else if (p == 5) cj = add2(jx, jz);
-        else if (p == 6) cj = sub2(jx, jz);
-        else if (p == 7) cj = add2(jy, jz);
-        else cj = sub2(jy, jz);
-        const float2 e = fma2(q < 7 ? K1 : K2, mul2(cj, cj), q < 7 ? B1 : B2);
-        w[q] = f2h(fma2(q < 7 ? T1 : T2, cj, fma2(cA, h2f(w[q]), e)));
-        w[qb] = f2h(fma2(q < 7 ? N1 : N2, cj, fma2(cA, h2f(w[qb]), e)));
-    }
-}
-
-template <int P, int WARPS, int MINB>
-__global__ void __launch_bounds__(32 * WARPS, MINB) k_step_hx(const __half* __restrict__ fin,
-                                                               __half* __restrict__ fout, Layout L, StepArgs a,
-                                                               float inv_scale)
-{
-    constexpr int S = P + 1;   // ring slots: blocks t .. t + P (each slot holds its x-neighbour words)
-    constexpr uint32_t kDirBits = (1u << Q) - 1u;
-    extern __shared__ __align__(128) unsigned char wp_smem[];
-    const int lane = threadIdx.x & 31;
-    const int warp = threadIdx.x >> 5;
-    unsigned char* ring = wp_smem + warp * (S * hx::kSlotBytes);
-    const uint32_t ring_s = (uint32_t)__cvta_generic_to_shared(ring);
-    const int nrows = L.ny * L.nz;
-    const int all_warps = gridDim.x * WARPS;
-    const int r0 = blockIdx.x * WARPS + warp;   // rows r0, r0 + all_warps, ...; r = (k-1) ny + (j-1)
-    if (r0 >= nrows) return;
-
-    // element offsets of this lane's five 16-byte pieces from the destination block
-    int poff[5];
-#pragma unroll
-    for (int i = 0; i < 5; ++i)
-    {
-        const int p = i * 32 + lane;
-        const int q = min(p >> 3, 18);
-        poff[i] = -(c_ey[q] * (int)L.row_stride + c_ez[q] * (int)L.plane_stride) + q * 64 + (p & 7) * 8;
-    }
-
-    // lanes 0-4 copy the low-face ghosts of a row-start block, lanes 5-9 the
-    // high-face ghosts of a row-end block: ghost of direction q for row
-    // (j, k) is xgh[gh_index(side, q, j - ey, k - ez)] = row (k (ny+2) + j) + goff
-    const int gq = wp::ghost_dir(lane < 10 ? lane : 0);
-    const int goff = (lane < 5 ? 0 : 19) * (L.nz + 2) * (L.ny + 2) + gq * (L.nz + 2) * (L.ny + 2) -
-                     c_ez[gq] * (L.ny + 2) - c_ey[gq];
-    // lanes 10-14: the last word of the previous block's line q (ex > 0: cell 63 is the x
-    // neighbour of the block's cell 0); lanes 15-19: the first word of the next block's line q
-    // (ex < 0); stored at the slot's edge words in the order of ghost_slot
-    const int eq = wp::ghost_dir(lane >= 10 && lane < 20 ? lane - 10 : 0);
-    const int eoff = -(c_ey[eq] * (int)L.row_stride + c_ez[eq] * (int)L.plane_stride) + eq * 64 +
-                     (lane < 15 ? -19 * 64 + 62 : 19 * 64);
-
-    // ---- copy cursor: the next block whose lines are copied
-    int ci_r = r0, ci_b = 0;
-    const __half* ci_src = nullptr;     // the block's own position (lines are offset by poff)
-    const uint32_t* ci_near = nullptr;  // the block's two near-solid words
-    const uint32_t* ci_link = nullptr;  // links words of this lane's two cells
-    const float* ci_gh = nullptr;       // this lane's x-face ghost of the row
-    const auto ci_row = [&]() {
-        const int k = 1 + ci_r / L.ny, j = 1 + ci_r - (k - 1) * L.ny;
-        ci_src = fin + L.elem(0, 1, j, k);
-        ci_near = a.near + ((long long)k * (L.ny + 2) + j) * L.words_per_row;
-        ci_link = a.links + L.cell(1, j, k) + 2 * lane;
-        ci_gh = a.xf.xgh + ((long long)k * (L.ny + 2) + j) + goff;
-    };
-    const auto ci_next = [&]() {
-        ci_src += 19 * 64;
-        ci_near += 2;
-        ci_link += 64;
-        if (++ci_b == L.nb)
-        {
-            ci_b = 0;
-            ci_r += all_warps;
-            if (ci_r < nrows) ci_row();
-        }
-    };
-    uint32_t n0 = 0u, n1 = 0u;   // near words of the copy cursor's block, loaded one block ahead
-    const auto load_near = [&]() {
-        n0 = LBM_IN(kChkHwNear, ci_near - a.near, near_extent(L)) ? __ldg(ci_near) : 0u;
-        n1 = ci_b * 64 + 32 < L.nx && LBM_IN(kChkHwNear, ci_near + 1 - a.near, near_extent(L)) ? __ldg(ci_near + 1)
-                                                                                                   : 0u;
-    };
-    const auto issue = [&](int slot) {
-        const uint32_t dst = ring_s + slot * hx::kSlotBytes;
-#pragma unroll
-        for (int i = 0; i < 5; ++i)
-            if ((i < 4 || lane < 24) && LBM_IN(kChkHwLine, (ci_src - fin) + poff[i], L.total - 7))
-                cp_async16(dst + (i * 32 + lane) * 16, ci_src + poff[i]);
-        if (lane < 2) reinterpret_cast<uint32_t*>(ring + slot * hx::kSlotBytes + wp::kNearOff)[lane] = lane ? n1 : n0;
-        if ((n0 | n1) != 0u && ci_b * 64 + 2 * lane < L.nx &&
-            LBM_IN(kChkHwLinks, ci_link - a.links, links_extent(L) - 1))
-            cp_async8(dst + wp::kLinkOff + lane * 8, ci_link);
-        if (((ci_b == 0 && lane < 5) || (ci_b == L.nb - 1 && lane >= 5 && lane < 10)) &&
-            LBM_IN(kChkHwGhost, ci_gh - a.xf.xgh, xgh_extent(L)))
-            cp_async4(dst + wp::kGhostOff + lane * 4, ci_gh);
-        if (lane >= 10 && lane < 20 && LBM_IN(kChkHwLine, (ci_src - fin) + eoff, L.total - 1))
-            cp_async4(dst + hx::kEdgeOff + (lane - 10) * 4, ci_src + eoff);
-    };
-
-    // ---- update cursor: the block being updated
-    int cc_r = r0, cc_b = 0, cc_j = 0, cc_k = 0, c0 = 0;
-    const unsigned* own = nullptr;   // this lane's word of line 0 of the block (line q: own[32 q])
-    unsigned* outp = nullptr;
-    float syz = 0.f;
-    const auto cc_row = [&]() {
-        cc_k = 1 + cc_r / L.ny;
-        cc_j = 1 + cc_r - (cc_k - 1) * L.ny;
-        const long long e = L.elem(0, 1, cc_j, cc_k);
-        own = reinterpret_cast<const unsigned*>(fin + e) + lane;
-        outp = reinterpret_cast<unsigned*>(fout + e) + lane;
-        c0 = 2 * lane;
-        syz = fmaxf(__ldg(a.sig_y + cc_j - 1), __ldg(a.sig_z + cc_k - 1));
-    };
-    const auto cc_next = [&]() {
-        own += 19 * 32;
-        outp += 19 * 32;
-        c0 += 64;
-        if (++cc_b == L.nb)
-        {
-            cc_b = 0;
-            cc_r += all_warps;
-            if (cc_r < nrows) cc_row();
-        }
-    };
-
-    ci_row();
-    cc_row();
-#pragma unroll 1
-    for (int p = 0; p < P; ++p)
-    {
-        if (ci_r < nrows)
-        {
-            load_near();
-            issue(p);
-            ci_next();
-        }
-        cp_async_commit();
-    }
-    if (ci_r < nrows) load_near();
-
-    int st = 0;   // slot of block t
-#pragma unroll 1
-    while (cc_r < nrows)
-    {
-        const int sp = st == 0 ? S - 1 : st - 1;
-        const int sn = st == S - 1 ? 0 : st + 1;
-        int si = st + P;
-        if (si >= S) si -= S;
-        if (ci_r < nrows)
-        {
-            issue(si);
-            ci_next();
-            if (ci_r < nrows) load_near();
-        }
-        cp_async_commit();
-        cp_async_wait<P>();   // every group but the newest P: block t has landed
-        __syncwarp();
-
-        const int j = cc_j, k = cc_k;
-        const bool active = c0 < L.nx;
-        const int last = L.nx - 1 - c0;
-        const bool xlo = c0 == 0;
-        const bool xhi = last >= 0 && last < 2;
-        const bool edge = cc_b == 0 || cc_b == L.nb - 1;
-        const unsigned char* slot = ring + st * hx::kSlotBytes;
-
-        // links words of block t (they came with its lines, when a near-solid bit is set)
-        // sponge strengths of the two cells, first so that the loads are in flight early
-        const float sx0 = active ? __ldg(a.sig_x + c0) : 0.f;
-        const float sx1 = c0 + 1 < L.nx ? __ldg(a.sig_x + c0 + 1) : 0.f;
-        const uint2 nw = *reinterpret_cast<const uint2*>(slot + wp::kNearOff);
-        uint32_t lk0 = 0u, lk1 = 0u;
-        bool any_link = false;
-        if ((nw.x | nw.y) != 0u)
-        {
-            const uint32_t bits = active ? ((lane < 16 ? nw.x : nw.y) >> ((2 * lane) & 31)) & 3u : 0u;
-            const uint32_t* lw = reinterpret_cast<const uint32_t*>(slot + wp::kLinkOff) + 2 * lane;
-            lk0 = (bits & 1u) ? lw[0] : 0u;
-            lk1 = (bits & 2u) ? lw[1] : 0u;
-            any_link = __any_sync(kFull, ((lk0 | lk1) & kDirBits) != 0u);
-        }
-        const uint32_t lka = (lk0 | lk1) & kDirBits;
-
-        // pulled words: line q of the slot, shifted by ex(q) across lanes; the edge lanes take the
-        // neighbour blocks' words that came with the slot
-        const unsigned* cur = reinterpret_cast<const unsigned*>(slot) + lane;   // line q: cur[32 q]
-        const unsigned* ew = reinterpret_cast<const unsigned*>(slot + hx::kEdgeOff);
-        unsigned w[Q];
-#pragma unroll
-        for (int q = 0; q < Q; ++q)
-        {
-            const unsigned v = cur[32 * q];
-            if (ex(q) == 0) w[q] = v;
-            else if (ex(q) > 0) w[q] = __byte_perm(*(lane > 0 ? cur + 32 * q - 1 : ew + ghost_slot(q)), v, 0x5432);
-            else w[q] = __byte_perm(v, *(lane < 31 ? cur + 32 * q + 1 : ew + ghost_slot(q)), 0x5432);
-        }
-        if (any_link)
-        {
-            // halfway bounce-back: the own cell's word of the opposite direction
-#pragma unroll
-            for (int q = 0; q < Q; ++q)
-            {
-                const unsigned o =
-                    ((lka >> q) & 1u) &&
-                            LBM_IN(kChkHwBounce, 2 * (own - reinterpret_cast<const unsigned*>(fin)) + inv(q) * 64,
-                                   L.total - 1)
-                        ? __ldg(own + inv(q) * 32)
-                        : 0u;
-                const unsigned m = ((0u - ((lk0 >> q) & 1u)) & 0x0000ffffu) | ((0u - ((lk1 >> q) & 1u)) & 0xffff0000u);
-                w[q] = (w[q] & ~m) | (o & m);
-            }
-        }
-        if (edge)
-        {
-            // x-face ghosts of the row ends (they came with the block's lines)
-            const float* gs = reinterpret_cast<const float*>(slot + wp::kGhostOff);
-#pragma unroll
-            for (int q = 0; q < Q; ++q)
-            {
-                if (ex(q) == 0) continue;
-                const float g = gs[ghost_slot(q)];
-                if (ex(q) > 0 && xlo && !((lk0 >> q) & 1u)) w[q] = set_lo(w[q], g);
-                if (ex(q) < 0 && xhi && last == 0 && !((lk0 >> q) & 1u)) w[q] = set_lo(w[q], g);
-                if (ex(q) < 0 && xhi && last == 1 && !((lk1 >> q) & 1u)) w[q] = set_hi(w[q], g);
-            }
-        }
-        if (active)
-        {
-            const float2 sg = make_float2(fmaxf(sx0, syz), fmaxf(sx1, syz));
-            collide2_lean(w, inv_scale, a.omega, sg, (lk0 & kSolidSelfBit) != 0u, (lk1 & kSolidSelfBit) != 0u);
-#pragma unroll
-            for (int q = 0; q < Q; ++q)
-                if (LBM_IN(kChkHwStore, 2 * (outp - reinterpret_cast<unsigned*>(fout)) + 64 * q, L.total - 1))
-                    outp[32 * q] = w[q];
-            if (edge && (xlo | xhi))
-            {
-#pragma unroll
-                for (int q = 0; q < Q; ++q)
-                {
-                    if (!LBM_IN(kChkHwExport, a.xf.exp_index(xlo ? 0 : 1, q, j, k, L.ny, L.nz), xexp_extent(L)))
-                        continue;
-                    if (xlo) a.xf.xexp[a.xf.exp_index(0, q, j, k, L.ny, L.nz)] = h2f(w[q]).x;
-                    if (xhi && last == 0) a.xf.xexp[a.xf.exp_index(1, q, j, k, L.ny, L.nz)] = h2f(w[q]).x;
-                    if (xhi && last == 1) a.xf.xexp[a.xf.exp_index(1, q, j, k, L.ny, L.nz)] = h2f(w[q]).y;
-                }
-            }
-        }
-        __syncwarp();   // every lane is done with slot t before the next copy lands there
-        cc_next();
-        st = sn;
-    }
-    cp_async_wait<0>();
-}
-
 // ---------------------------------------------------------------- z-slab messages
 // The populations that cross a z cut: the 5 directions with ez = +1 leave a
 // slab's top plane for the upper neighbour's halo plane 0, the 5 with ez = -1
@@ -1597,74 +1283,12 @@ cudaError_t launch_hw(const __half* fin, __half* fout, const Layout& L, const St
     return cudaGetLastError();
 }
 
-template <int P, int WARPS, int MINB>
-cudaError_t hx_launch(const __half* fin, __half* fout, const Layout& L, const StepArgs& a, float inv_scale,
-                      cudaStream_t stream, bool prepare_only)
-{
-    constexpr int smem = WARPS * (P + 1) * hx::kSlotBytes;
-    if (L.plane_stride + L.row_stride + 19 * 64 > 0x7fffffffLL) return cudaErrorInvalidValue;
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return e;
-    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
-    static std::mutex mu;
-    static int ctas[kMaxDevices] = {};
-    {
-        std::lock_guard<std::mutex> lock(mu);
-        if (!ctas[dev])
-        {
-            e = cudaFuncSetAttribute(k_step_hx<P, WARPS, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-            int per_sm = 0, sms = 0;
-            if (e == cudaSuccess)
-                e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_hx<P, WARPS, MINB>, 32 * WARPS, smem);
-            if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-            if (e != cudaSuccess) return e;
-            if (per_sm < 1) return cudaErrorInvalidConfiguration;
-            ctas[dev] = per_sm * sms;
-        }
-    }
-    if (prepare_only) return cudaSuccess;
-    const long long need = ((long long)L.ny * L.nz + WARPS - 1) / WARPS;
-    const int grid = (int)(need < ctas[dev] ? need : ctas[dev]);
-    k_step_hx<P, WARPS, MINB><<<grid, 32 * WARPS, smem, stream>>>(fin, fout, L, a, inv_scale);
-    return cudaGetLastError();
-}
-
-// FP16 step implementation while the candidates are compared (NLOS_LBM_F16_STEP):
-// 0 = k_step_hw; 1-3 = k_step_hx with 1 / 2 / 1 blocks in flight at a 64 / 80 / 80 register cap.
-int f16_impl()
-{
-    static const int v = [] {
-        const char* e = std::getenv("NLOS_LBM_F16_STEP");
-        return e ? std::atoi(e) : 0;
-    }();
-    return v;
-}
-
-cudaError_t launch_f16(const __half* fin, __half* fout, const Layout& L, const StepArgs& a, float inv_scale,
-                       cudaStream_t stream, bool prepare_only)
-{
-    switch (f16_impl())
-    {
-    case 1: return hx_launch<1, 4, 8>(fin, fout, L, a, inv_scale, stream, prepare_only);
-    case 2: return hx_launch<2, 4, 6>(fin, fout, L, a, inv_scale, stream, prepare_only);
-    case 3: return hx_launch<1, 4, 6>(fin, fout, L, a, inv_scale, stream, prepare_only);
-    default:
-        if (prepare_only)
-        {
-            int ctas = 0;
-            return hw_ctas<2, 4, 5>(&ctas);
-        }
-        return launch_hw<2, 4, 5>(fin, fout, L, a, inv_scale, stream);
-    }
-}
-
 template <typename S>
 cudaError_t launch_step_t(const S* fin, S* fout, const Layout& L, const StepArgs& a, float inv_scale,
                           cudaStream_t stream)
 {
     if constexpr (std::is_same<S, __half>::value)
-        return launch_f16(fin, fout, L, a, inv_scale, stream, false);
+        return launch_hw<2, 4, 5>(fin, fout, L, a, inv_scale, stream);
     k_step<S, 128, 0><<<pair_grid(L, 128), 128, 0, stream>>>(fin, fout, L, a, inv_scale);
     return cudaGetLastError();
 }
@@ -1723,7 +1347,8 @@ cudaError_t launch_build_links(const uint8_t* mask_ref, uint32_t* links, uint32_
 cudaError_t prepare_step(int storage)
 {
     if (storage == 0) return cudaSuccess;
-    return launch_f16(nullptr, nullptr, Layout{}, StepArgs{}, 1.0f, nullptr, true);
+    int ctas = 0;
+    return hw_ctas<2, 4, 5>(&ctas);
 }
 
 cudaError_t launch_step(int storage, const void* fin, void* fout, const Layout& L, const StepArgs& a,
