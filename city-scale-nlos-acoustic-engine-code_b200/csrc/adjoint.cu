@@ -584,30 +584,14 @@ cudaError_t launch_adj_ghost(const AdjGhostArgs& a, cudaStream_t stream)
     return cudaGetLastError();
 }
 
-cudaError_t launch_adj_step(const AdjStepArgs& a, int variant, cudaStream_t stream)
+cudaError_t launch_adj_step(const AdjStepArgs& a, cudaStream_t stream)
 {
-    if (a.L.bc != 32) return cudaErrorInvalidValue;   // FP32 layout only
+    // 96 registers (the measured best against no cap and an 80-register cap);
     // rows of up to 128 columns take 64-thread blocks, so no warp idles
     const int block = a.L.nx <= 128 ? 64 : 128;
     const dim3 g((unsigned)((a.L.nx + 2 * block - 1) / (2 * block)), (unsigned)a.L.ny, (unsigned)a.L.nz);
-    if (block == 64)
-    {
-        switch (variant)
-        {
-        case 1: k_adj_step<64, 10><<<g, 64, 0, stream>>>(a); break;
-        case 2: k_adj_step<64, 12><<<g, 64, 0, stream>>>(a); break;
-        default: k_adj_step<64, 1><<<g, 64, 0, stream>>>(a); break;
-        }
-    }
-    else
-    {
-        switch (variant)
-        {
-        case 1: k_adj_step<128, 5><<<g, 128, 0, stream>>>(a); break;
-        case 2: k_adj_step<128, 6><<<g, 128, 0, stream>>>(a); break;
-        default: k_adj_step<128, 1><<<g, 128, 0, stream>>>(a); break;
-        }
-    }
+    if (block == 64) k_adj_step<64, 10><<<g, 64, 0, stream>>>(a);
+    else k_adj_step<128, 5><<<g, 128, 0, stream>>>(a);
     return cudaGetLastError();
 }
 

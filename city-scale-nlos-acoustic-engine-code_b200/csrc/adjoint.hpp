@@ -79,9 +79,8 @@ struct AdjProbeArgs
 cudaError_t launch_adj_ghost(const AdjGhostArgs& a, cudaStream_t stream);
 // J_C^T of the gathered lamF^s (plus, at the open faces, the ghost-adjoint
 // terms written by launch_adj_ghost for the same step) over every interior
-// cell.  variant: register cap of the step kernel (0: none, 1: 5 blocks of
-// 128 per SM, 2: 6 blocks); same work in all.
-cudaError_t launch_adj_step(const AdjStepArgs& a, int variant, cudaStream_t stream);
+// cell.
+cudaError_t launch_adj_step(const AdjStepArgs& a, cudaStream_t stream);
 cudaError_t launch_adj_source(const AdjSourceArgs& a, cudaStream_t stream);
 cudaError_t launch_adj_probe(float* lam, const AdjProbeArgs& a, cudaStream_t stream);
 

@@ -32,8 +32,6 @@ namespace {
 constexpr int kTableRows = 4096;   // source-schedule rows resident on the device
 constexpr int kBcCut = 100;        // face of a z-slab that borders the next slab (internal face type)
 constexpr int kProbeRows = 4096;   // probe-series rows buffered on the device
-// Register cap of the adjoint step kernel (launch_adj_step variant).
-constexpr int kDefaultAdjointVariant = 1;
 // L2 prefetch distance of the adjoint step in rows (measured on the 256x256x128 patch: 192 rows
 // ahead, 2-4 % less time per gradient than none; 48 to 1536 rows tried)
 constexpr int kDefaultAdjointPrefetchRows = 192;
@@ -2304,9 +2302,6 @@ extern "C" int lbm_adjoint_grad(lbm_handle* h, int nsteps, const double* observe
     CK(cudaMemsetAsync(d_out, 0, (size_t)T * 4 * sizeof(double), h->stream), "adjoint memset");
     const size_t pop_bytes = (size_t)L.total * sizeof(float);
     SourceArgs sargs = source_args(h, false);
-    int adj_variant = kDefaultAdjointVariant;
-    if (const char* v = std::getenv("NLOS_LBM_ADJ_VARIANT")) adj_variant = std::atoi(v);
-    if (adj_variant < 0 || adj_variant > 2) return h->fail(LBM_ERR_BAD_CONFIG, "NLOS_LBM_ADJ_VARIANT out of range");
     // L2 prefetch distance of the adjoint step in rows (NLOS_LBM_ADJ_PREFETCH_ROWS, 0 = off)
     int adj_prefetch = kDefaultAdjointPrefetchRows;
     if (const char* v = std::getenv("NLOS_LBM_ADJ_PREFETCH_ROWS")) adj_prefetch = std::max(0, std::atoi(v));
@@ -2457,7 +2452,7 @@ extern "C" int lbm_adjoint_grad(lbm_handle* h, int nsteps, const double* observe
             if (s == 0) continue;
             AdjStepArgs as{L, h->sa, lam[la], lam[la ^ 1], mom_of(s - 1 - cn), gadj, {}, adj_prefetch};
             std::copy(gadj_off, gadj_off + 6, as.gadj_off);
-            CK(launch_adj_step(as, adj_variant, h->stream), "adjoint step");
+            CK(launch_adj_step(as, h->stream), "adjoint step");
             kernels++;
             la ^= 1;
             pa.resid = d_resid + (size_t)(s - 1) * np;
