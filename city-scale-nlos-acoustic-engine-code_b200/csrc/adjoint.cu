@@ -3,6 +3,7 @@
 // pull-stream reads the adjoint populations of the neighbours that pulled
 // from a cell, mirroring the forward pull.
 #include <cuda_fp16.h>
+#include <cuda_fp8.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -240,11 +241,12 @@ __device__ __forceinline__ uint32_t near_bits(const StepArgs& a, const Layout& L
 
 __device__ __forceinline__ float2 ldg2(const float* p) { return __ldg(reinterpret_cast<const float2*>(p)); }
 
-// (rho', jx, jy, jz) from the two FP16 pairs of PackedMoments
-__device__ __forceinline__ float4 unpack_moments(uint2 u)
+// (rho', jx, jy, jz) from the four e5m2 bytes of PackedMoments (exact in FP16)
+__device__ __forceinline__ float4 unpack_moments(unsigned u)
 {
-    const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&u.x));
-    const float2 b = __half22float2(*reinterpret_cast<const __half2*>(&u.y));
+    const __half2_raw ra = __nv_cvt_fp8x2_to_halfraw2((__nv_fp8x2_storage_t)(u & 0xffffu), __NV_E5M2);
+    const __half2_raw rb = __nv_cvt_fp8x2_to_halfraw2((__nv_fp8x2_storage_t)(u >> 16), __NV_E5M2);
+    const float2 a = __half22float2(__half2(ra)), b = __half22float2(__half2(rb));
     return make_float4(a.x, a.y, b.x, b.y);
 }
 
@@ -309,7 +311,7 @@ __device__ __forceinline__ float2 shifted_pair(const float* row, int lane, const
 template <int CELLS>
 __device__ __forceinline__ void adj_prefetch_rows(const AdjStepArgs& a, int j, int k, int col0)
 {
-    constexpr int BC = 32, NBLK = (CELLS + BC - 1) / BC, NMOM = (CELLS * 8 + 127) / 128;
+    constexpr int BC = 32, NBLK = (CELLS + BC - 1) / BC, NMOM = (CELLS * (int)sizeof(PackedMoments) + 127) / 128;
     const Layout& L = a.L;
     const int t = threadIdx.x;
     if (t >= NBLK + NMOM) return;
@@ -326,7 +328,7 @@ __device__ __forceinline__ void adj_prefetch_rows(const AdjStepArgs& a, int j, i
     }
     else
     {
-        const int col = col0 + (t - NBLK) * 16;
+        const int col = col0 + (t - NBLK) * (128 / (int)sizeof(PackedMoments));
         if (col >= L.nx) return;
         const long long mi = ((long long)(kk - 1) * L.ny + (jj - 1)) * L.nx + col;
         asm volatile("prefetch.global.L2 [%0];" ::"l"(a.mom_prev + mi));
@@ -366,9 +368,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_adj_step(AdjStepArgs a)
     {
         const long long mi = ((long long)(k - 1) * L.ny + (j - 1)) * L.nx + c0;
         [[maybe_unused]] const long long ncell = (long long)L.nx * L.ny * L.nz;
-        const uint2* mp = reinterpret_cast<const uint2*>(a.mom_prev);
-        const uint2 p0 = LBM_IN(kChkAdjLoad, mi, ncell) ? __ldg(mp + mi) : make_uint2(0u, 0u);
-        const uint2 p1 = has1 && LBM_IN(kChkAdjLoad, mi + 1, ncell) ? __ldg(mp + mi + 1) : p0;
+        const unsigned* mp = reinterpret_cast<const unsigned*>(a.mom_prev);
+        const unsigned p0 = LBM_IN(kChkAdjLoad, mi, ncell) ? __ldg(mp + mi) : 0u;
+        const unsigned p1 = has1 && LBM_IN(kChkAdjLoad, mi + 1, ncell) ? __ldg(mp + mi + 1) : p0;
         const float4 m0 = unpack_moments(p0), m1 = unpack_moments(p1);
         rho = make_float2(m0.x, m1.x);
         jx = make_float2(m0.y, m1.y);

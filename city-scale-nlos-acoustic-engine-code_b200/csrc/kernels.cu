@@ -4,6 +4,7 @@
 // is FP32 (packed FP32x2 where two cells go together), with FP64 for the
 // source-weight reduction and the probe accumulators.
 #include <cuda_fp16.h>
+#include <cuda_fp8.h>
 
 #include <algorithm>
 #include <cmath>
@@ -224,12 +225,13 @@ __device__ __forceinline__ void collide2(float2 (&G)[Q], float inv_scale, float 
 // next to the x faces take their x-halo sources from the x-face ghosts and
 // export their results for the next ghost fill.
 // MOM: also write the moments (rho', J) of every cell's pulled populations to
-// `mom` (dense cell order, float4 per cell), the forward data the adjoint's
+// `mom` (dense cell order, PackedMoments), the forward data the adjoint's
 // BGK Jacobian needs.
 __device__ __forceinline__ PackedMoments pack_moments(float4 m)
 {
-    const __half2 a = __floats2half2_rn(m.x, m.y), b = __floats2half2_rn(m.z, m.w);
-    return PackedMoments{*reinterpret_cast<const unsigned*>(&a), *reinterpret_cast<const unsigned*>(&b)};
+    const unsigned lo = __nv_cvt_float2_to_fp8x2(make_float2(m.x, m.y), __NV_SATFINITE, __NV_E5M2);
+    const unsigned hi = __nv_cvt_float2_to_fp8x2(make_float2(m.z, m.w), __NV_SATFINITE, __NV_E5M2);
+    return PackedMoments{lo | (hi << 16)};
 }
 
 template <typename S, int BLOCK, int MINB, bool MOM = false>
