@@ -50,11 +50,29 @@ def exchange_messages(dist, send, recv, peers, group=None):
         r.wait()
 
 
+class _OneRank:
+    """The torch.distributed calls SlabRank makes, for a process that runs alone
+    (no process group): rank 0 of 1, and a gather that returns its own part."""
+
+    @staticmethod
+    def get_rank(group=None):
+        return 0
+
+    @staticmethod
+    def get_world_size(group=None):
+        return 1
+
+    @staticmethod
+    def all_gather_object(parts, obj, group=None):
+        parts[0] = obj
+
+
 class SlabRank:
     """This rank's z-slab of the grid `cfg`, stepped with the reference's
     loop body (source, halo fill, cut messages, collision, probes).
 
-    dist: torch.distributed, initialised; rank/world from it.  staging:
+    dist: torch.distributed, initialised, or None for one process holding the
+    whole grid (no cut, no messages); rank/world from it.  staging:
     "device" (NCCL: messages sent from device memory) or "host" (any
     backend: messages copied through pinned host memory)."""
 
@@ -62,10 +80,10 @@ class SlabRank:
         import torch
 
         self.torch = torch
-        self.dist = dist
+        self.dist = dist if dist is not None else _OneRank()
         self.group = group
-        self.rank = dist.get_rank(group)
-        self.world = dist.get_world_size(group)
+        self.rank = self.dist.get_rank(group)
+        self.world = self.dist.get_world_size(group)
         nz = int((cfg.z_max - cfg.z_min) / cfg.dx + 0.5)
         self.bounds = slab_bounds(nz, self.world)
         c = abi.LbmConfig.from_buffer_copy(cfg)

@@ -74,3 +74,12 @@ def test_slab_bounds_cover_the_grid():
         assert sizes.min() >= 1 and sizes.max() - sizes.min() <= 1
     with pytest.raises(ValueError):
         ranks.slab_bounds(3, 4)
+
+
+def test_single_process_stand_in():
+    one = ranks._OneRank()
+    assert one.get_rank() == 0 and one.get_world_size() == 1
+    parts = [None]
+    one.all_gather_object(parts, "mine")
+    assert parts == ["mine"]
+    assert ranks.neighbours(0, 1) == {}
