@@ -3,7 +3,6 @@
 // pull-stream reads the adjoint populations of the neighbours that pulled
 // from a cell, mirroring the forward pull.
 #include <cuda_fp16.h>
-#include <cuda_fp8.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -241,13 +240,20 @@ __device__ __forceinline__ uint32_t near_bits(const StepArgs& a, const Layout& L
 
 __device__ __forceinline__ float2 ldg2(const float* p) { return __ldg(reinterpret_cast<const float2*>(p)); }
 
-// (rho', jx, jy, jz) from the four e5m2 bytes of PackedMoments (exact in FP16)
-__device__ __forceinline__ float4 unpack_moments(unsigned u)
+// 12-bit float (PairMoments) -> float: it is FP16 with the 4 lowest mantissa bits zero
+__device__ __forceinline__ float from_f12(unsigned t)
 {
-    const __half2_raw ra = __nv_cvt_fp8x2_to_halfraw2((__nv_fp8x2_storage_t)(u & 0xffffu), __NV_E5M2);
-    const __half2_raw rb = __nv_cvt_fp8x2_to_halfraw2((__nv_fp8x2_storage_t)(u >> 16), __NV_E5M2);
-    const float2 a = __half22float2(__half2(ra)), b = __half22float2(__half2(rb));
-    return make_float4(a.x, a.y, b.x, b.y);
+    return __half2float(__ushort_as_half((unsigned short)((((t >> 11) & 1u) << 15) | ((t & 0x7ffu) << 4))));
+}
+
+// (rho', jx, jy, jz) of the two cells of a PairMoments record
+__device__ __forceinline__ void unpack_moments(const PairMoments& p, float4& m0, float4& m1)
+{
+    const unsigned w0 = p.w[0], w1 = p.w[1], w2 = p.w[2];
+    m0 = make_float4(from_f12(w0 & 0xfffu), from_f12((w0 >> 12) & 0xfffu), from_f12((w0 >> 24) | ((w1 & 0xfu) << 8)),
+                     from_f12((w1 >> 4) & 0xfffu));
+    m1 = make_float4(from_f12((w1 >> 16) & 0xfffu), from_f12((w1 >> 28) | ((w2 & 0xffu) << 4)),
+                     from_f12((w2 >> 8) & 0xfffu), from_f12(w2 >> 20));
 }
 
 // packed FP32x2 arithmetic (sm_100): both cells of a pair in one instruction
@@ -311,7 +317,7 @@ __device__ __forceinline__ float2 shifted_pair(const float* row, int lane, const
 template <int CELLS>
 __device__ __forceinline__ void adj_prefetch_rows(const AdjStepArgs& a, int j, int k, int col0)
 {
-    constexpr int BC = 32, NBLK = (CELLS + BC - 1) / BC, NMOM = (CELLS * (int)sizeof(PackedMoments) + 127) / 128;
+    constexpr int BC = 32, NBLK = (CELLS + BC - 1) / BC, NMOM = (CELLS / 2 * (int)sizeof(PairMoments) + 127) / 128;
     const Layout& L = a.L;
     const int t = threadIdx.x;
     if (t >= NBLK + NMOM) return;
@@ -328,10 +334,10 @@ __device__ __forceinline__ void adj_prefetch_rows(const AdjStepArgs& a, int j, i
     }
     else
     {
-        const int col = col0 + (t - NBLK) * (128 / (int)sizeof(PackedMoments));
-        if (col >= L.nx) return;
-        const long long mi = ((long long)(kk - 1) * L.ny + (jj - 1)) * L.nx + col;
-        asm volatile("prefetch.global.L2 [%0];" ::"l"(a.mom_prev + mi));
+        const int byte = (t - NBLK) * 128;   // within the tile's pair records
+        if (col0 + byte / (int)sizeof(PairMoments) * 2 >= L.nx) return;
+        const long long pi = ((long long)(kk - 1) * L.ny + (jj - 1)) * ((L.nx + 1) >> 1) + (col0 >> 1);
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(reinterpret_cast<const char*>(a.mom_prev + pi) + byte));
     }
 }
 
@@ -366,12 +372,13 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_adj_step(AdjStepArgs a)
     // ---- moments of F^{s-1}, stored by the forward recomputation
     float2 rho, jx, jy, jz;
     {
-        const long long mi = ((long long)(k - 1) * L.ny + (j - 1)) * L.nx + c0;
-        [[maybe_unused]] const long long ncell = (long long)L.nx * L.ny * L.nz;
-        const unsigned* mp = reinterpret_cast<const unsigned*>(a.mom_prev);
-        const unsigned p0 = LBM_IN(kChkAdjLoad, mi, ncell) ? __ldg(mp + mi) : 0u;
-        const unsigned p1 = has1 && LBM_IN(kChkAdjLoad, mi + 1, ncell) ? __ldg(mp + mi + 1) : p0;
-        const float4 m0 = unpack_moments(p0), m1 = unpack_moments(p1);
+        const long long pi = ((long long)(k - 1) * L.ny + (j - 1)) * ((L.nx + 1) >> 1) + (c0 >> 1);
+        [[maybe_unused]] const long long npair = (long long)((L.nx + 1) >> 1) * L.ny * L.nz;
+        PairMoments pm{{0u, 0u, 0u}};
+        if (LBM_IN(kChkAdjLoad, pi, npair)) pm = a.mom_prev[pi];
+        float4 m0, m1;
+        unpack_moments(pm, m0, m1);
+        if (!has1) m1 = m0;
         rho = make_float2(m0.x, m1.x);
         jx = make_float2(m0.y, m1.y);
         jy = make_float2(m0.z, m1.z);

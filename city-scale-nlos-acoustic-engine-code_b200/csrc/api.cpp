@@ -2092,7 +2092,7 @@ struct AdjPlan
     int Tt = 0;                                  // tail start (T: no tail), a multiple of K1
     int C = 0;                                   // store slots (steps of forward data)
     size_t pop = 0, ck_slot = 0, st_slot = 0;   // floats; st_slot: one step's stored moments
-    size_t mom_n = 0;                            // cells of packed moments (4 bytes each) per stored step
+    size_t mom_n = 0;                            // 4-byte words of pair moments per stored step
     long long gadj_n = 0;
     size_t bytes = 0;
     long long fwd_steps = 0;                     // forward steps run, recomputation included
@@ -2109,8 +2109,8 @@ AdjPlan adjoint_plan(const lbm_handle* h, int T, int ckpt_outer, int ckpt_inner)
     p.pop = round64((size_t)L.total);
     p.ck_slot = p.pop + round64((size_t)2 * Q * L.ny * L.nz);
     // stored per step: moments of F^s for every cell (two FP16 pairs), moments of H^s at every ghost's interior cell (FP32)
-    p.mom_n = round64((size_t)L.nx * L.ny * L.nz);
-    p.st_slot = p.mom_n + 4 * round64((size_t)std::max(h->ga.total, 1LL));   // FP8 cells, FP32 faces
+    p.mom_n = round64((size_t)((L.nx + 1) / 2) * L.ny * L.nz * (sizeof(PairMoments) / 4));
+    p.st_slot = p.mom_n + 4 * round64((size_t)std::max(h->ga.total, 1LL));   // 12-bit cell moments, FP32 faces
     for (int f = 0; f < h->ga.nfaces; ++f) p.gadj_n += (long long)Q * h->ga.face[f].nu * h->ga.face[f].nv;
     p.K1 = std::min(ckpt_outer > 0 ? ckpt_outer : 200, T);
     p.M = (T + p.K1 - 1) / p.K1;
@@ -2293,7 +2293,7 @@ extern "C" int lbm_adjoint_grad(lbm_handle* h, int nsteps, const double* observe
         Carve c{(char*)h->adj_ws, 0};
         carve(c);
     }
-    const auto mom_of = [&](long long slot) { return (PackedMoments*)(store + (size_t)slot * plan.st_slot); };
+    const auto mom_of = [&](long long slot) { return (PairMoments*)(store + (size_t)slot * plan.st_slot); };
     const auto face_mom_of = [&](long long slot) {
         return (float4*)(store + (size_t)slot * plan.st_slot + plan.mom_n);
     };

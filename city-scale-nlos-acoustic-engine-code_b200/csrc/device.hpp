@@ -219,20 +219,23 @@ cudaError_t launch_step(int storage, const void* fin, void* fout, const Layout& 
 // attribute, occupancy); call before the first launch or capture.
 cudaError_t prepare_step(int storage);
 // Fused step (FP32 storage, the default implementation) that also writes the
-// moments (rho', jx, jy, jz) of every cell's pulled populations to `mom`,
-// dense cell order ((k-1) ny + (j-1)) nx + (i-1), as four FP8 (e5m2) values in
-// one 32-bit word per cell (PackedMoments): the forward data of the adjoint's
-// BGK Jacobian.  They enter it only through terms of the wave's amplitude
-// (J^2, J / r, 1 / r with r = 1 + rho'), so their rounding moves the
-// gradient by a small multiple of the amplitude times the format's 2^-3
-// step, far below the 1e-4 bar, and 4 bytes per cell let the whole run's
-// moments be kept instead of recomputing the first segments.
-struct PackedMoments
+// moments (rho', jx, jy, jz) of every cell's pulled populations to `mom`: the
+// forward data of the adjoint's BGK Jacobian, where they enter only through
+// terms of the wave's amplitude (J^2, J / r, 1 / r with r = 1 + rho').  Each
+// value is kept as a 12-bit float (sign, FP16's 5-bit exponent, 6 mantissa
+// bits: FP16 rounded to nearest-even at its 4 lowest mantissa bits), the two
+// cells of an x pair (c, c + 1), c even, in one PairMoments of 96 bits, values
+// v0..v7 = rho', jx, jy, jz of cell c then of cell c + 1, v_i at bits 12 i;
+// pairs in dense order ((k-1) ny + (j-1)) ceil(nx / 2) + c / 2.  That is 6
+// bytes per cell, so most of a long run's moments stay in memory instead of
+// being recomputed, at a rounding step (2^-7) that moves the gradient far
+// less than the 1e-4 bar (8-bit floats, 2^-3, came within 12 % of it).
+struct PairMoments
 {
-    unsigned v;   // bytes 0-3: e5m2 of rho', jx, jy, jz
+    unsigned w[3];
 };
 cudaError_t launch_step_moments(const float* fin, float* fout, const Layout& L, const StepArgs& a,
-                                PackedMoments* mom, cudaStream_t stream);
+                                PairMoments* mom, cudaStream_t stream);
 cudaError_t launch_probe(int storage, const void* f, const Layout& L, const StepArgs& sa, const ProbeArgs& a,
                          cudaStream_t stream);
 // (float)(rho - 1) of every interior cell, pulled from the pre-step buffer `f`.

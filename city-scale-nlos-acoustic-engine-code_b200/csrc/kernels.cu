@@ -4,7 +4,6 @@
 // is FP32 (packed FP32x2 where two cells go together), with FP64 for the
 // source-weight reduction and the probe accumulators.
 #include <cuda_fp16.h>
-#include <cuda_fp8.h>
 
 #include <algorithm>
 #include <cmath>
@@ -225,19 +224,29 @@ __device__ __forceinline__ void collide2(float2 (&G)[Q], float inv_scale, float 
 // next to the x faces take their x-halo sources from the x-face ghosts and
 // export their results for the next ghost fill.
 // MOM: also write the moments (rho', J) of every cell's pulled populations to
-// `mom` (dense cell order, PackedMoments), the forward data the adjoint's
-// BGK Jacobian needs.
-__device__ __forceinline__ PackedMoments pack_moments(float4 m)
+// `mom` (PairMoments: 12-bit floats, one record per x pair), the forward data
+// the adjoint's BGK Jacobian needs.
+// FP16 bits of x rounded to nearest-even at their 4 lowest mantissa bits:
+// sign at bit 11, exponent at bits 6-10, 6 mantissa bits (finite values only).
+__device__ __forceinline__ unsigned to_f12(float x)
 {
-    const unsigned lo = __nv_cvt_float2_to_fp8x2(make_float2(m.x, m.y), __NV_SATFINITE, __NV_E5M2);
-    const unsigned hi = __nv_cvt_float2_to_fp8x2(make_float2(m.z, m.w), __NV_SATFINITE, __NV_E5M2);
-    return PackedMoments{lo | (hi << 16)};
+    const unsigned h = (unsigned)__half_as_ushort(__float2half_rn(x));
+    const unsigned mag = h & 0x7fffu;
+    const unsigned r = min((mag + 7u + ((mag >> 4) & 1u)) >> 4, 0x7bfu);
+    return ((h >> 15) << 11) | r;
+}
+__device__ __forceinline__ PairMoments pack_moments(float4 m0, float4 m1)
+{
+    const unsigned v0 = to_f12(m0.x), v1 = to_f12(m0.y), v2 = to_f12(m0.z), v3 = to_f12(m0.w);
+    const unsigned v4 = to_f12(m1.x), v5 = to_f12(m1.y), v6 = to_f12(m1.z), v7 = to_f12(m1.w);
+    return PairMoments{{v0 | (v1 << 12) | (v2 << 24), (v2 >> 8) | (v3 << 4) | (v4 << 16) | (v5 << 28),
+                        (v5 >> 4) | (v6 << 8) | (v7 << 20)}};
 }
 
 template <typename S, int BLOCK, int MINB, bool MOM = false>
 __global__ void __launch_bounds__(BLOCK, MINB) k_step(const S* __restrict__ fin, S* __restrict__ fout, Layout L,
                                                       StepArgs a, float inv_scale,
-                                                      PackedMoments* __restrict__ mom = nullptr)
+                                                      PairMoments* __restrict__ mom = nullptr)
 {
     using P = PairIo<S>;
     constexpr int BC = block_cells(sizeof(S));   // cells per interleaved block
@@ -332,9 +341,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step(const S* __restrict__ fin,
     collide2(G, inv_scale, a.omega, sg, (lk0 & kSolidSelfBit) != 0u, (lk1 & kSolidSelfBit) != 0u, m0, m1);
     if constexpr (MOM)
     {
-        const long long mi = ((long long)(k - 1) * L.ny + (j - 1)) * L.nx + c0;
-        mom[mi] = pack_moments(m0);
-        if (c0 + 1 < L.nx) mom[mi + 1] = pack_moments(m1);
+        const long long pi = ((long long)(k - 1) * L.ny + (j - 1)) * ((L.nx + 1) >> 1) + (c0 >> 1);
+        mom[pi] = pack_moments(m0, c0 + 1 < L.nx ? m1 : make_float4(0.f, 0.f, 0.f, 0.f));
     }
 
     S* out = fout + e0;
@@ -1361,7 +1369,7 @@ cudaError_t launch_step(int storage, const void* fin, void* fout, const Layout& 
 }
 
 cudaError_t launch_step_moments(const float* fin, float* fout, const Layout& L, const StepArgs& a,
-                                PackedMoments* mom, cudaStream_t stream)
+                                PairMoments* mom, cudaStream_t stream)
 {
     k_step<float, 128, 0, true><<<pair_grid(L, 128), 128, 0, stream>>>(fin, fout, L, a, 1.0f, mom);
     return cudaGetLastError();

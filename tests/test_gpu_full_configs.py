@@ -1,8 +1,8 @@
 """Parity at the configured sizes and lengths of the benchmark workloads.
 
 * The localisation gradient on the 256x256x128 patch over its 3000 steps
-  (64 receivers, 200-step checkpoints, the schedule the bench runs: the
-  whole run's moments kept from the first pass) against central differences of the GPU's own FP32 forward at
+  (64 receivers, 200-step checkpoints, the schedule the bench runs: most
+  of the run's moments kept from the first pass) against central differences of the GPU's own FP32 forward at
   h = 1e-2 cells, and its signal gradient against one directional
   difference.  Bound: 1e-4 relative (the north-star gradient bar).
 * The checkpoint schedule with recomputed segments AND a stored tail, at an
@@ -51,9 +51,9 @@ def test_full_size_gradient_matches_central_differences(gpu):
     trial = w["sources"][0]
     g = Solver(w["cfg"], [trial], w["probes"], triangles=w["triangles"])
     k_outer, k_inner, _, fwd = g.adjoint_plan(steps, 200, 0)
-    # the schedule the bench runs: with 4-byte moments the whole run's forward data fits, so every
-    # segment is reversed from the first pass's data (the recompute paths are the next test's)
-    assert k_outer == 200 and fwd == steps
+    # the schedule the bench runs: the first pass keeps the moments of as many 200-step segments
+    # as fit (most of the run at 6 bytes per cell), the rest are recomputed once
+    assert k_outer == 200 and steps <= fwd < 2 * steps - 1
     L, gp, gs, pred = g.adjoint_grad(observed, 200, 0)
     g.close()
     assert L == pytest.approx(_loss(w, trial, observed, steps), rel=1e-12)
