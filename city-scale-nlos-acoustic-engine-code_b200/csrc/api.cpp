@@ -2115,10 +2115,12 @@ AdjPlan adjoint_plan(const lbm_handle* h, int T, int ckpt_outer, int ckpt_inner)
     p.K1 = std::min(ckpt_outer > 0 ? ckpt_outer : 200, T);
     p.M = (T + p.K1 - 1) / p.K1;
     const int np = h->nprobe();
-    const auto bytes = [&](int K2, int C) {
-        const size_t ni = (size_t)((p.K1 + K2 - 1) / K2);
+    // Mr: outer segments reversed with a recompute (those before the tail); only they
+    // need a full-state checkpoint and, when there is one, the inner checkpoints
+    const auto bytes = [&](int K2, int C, int Mr) {
+        const size_t ni = Mr > 0 ? (size_t)((p.K1 + K2 - 1) / K2) : 0;
         Carve c;
-        c.get<float>((size_t)p.M * p.ck_slot);
+        c.get<float>((size_t)Mr * p.ck_slot);
         c.get<float>(ni * p.ck_slot);
         c.get<float>((size_t)std::max(C, K2 + 1) * p.st_slot);
         c.get<float>(p.pop);
@@ -2144,7 +2146,7 @@ AdjPlan adjoint_plan(const lbm_handle* h, int T, int ckpt_outer, int ckpt_inner)
         if (const char* v = std::getenv("NLOS_LBM_ADJ_BUDGET")) budget = std::min(budget, std::atof(v));
         p.K2 = 1;
         for (int K2 = p.K1; K2 >= 1; --K2)
-            if ((double)bytes(K2, K2 + 1) <= budget)
+            if ((double)bytes(K2, K2 + 1, p.M) <= budget)
             {
                 p.K2 = K2;
                 break;
@@ -2153,7 +2155,7 @@ AdjPlan adjoint_plan(const lbm_handle* h, int T, int ckpt_outer, int ckpt_inner)
         for (int m = 0; m < p.M; ++m)
         {
             const int Tt = m * p.K1, need = T - std::max(Tt - 1, 0);
-            if ((double)bytes(p.K2, need) <= budget)
+            if ((double)bytes(p.K2, need, m) <= budget)
             {
                 p.Tt = Tt;
                 break;
@@ -2163,7 +2165,7 @@ AdjPlan adjoint_plan(const lbm_handle* h, int T, int ckpt_outer, int ckpt_inner)
     p.C = std::max(p.K2 + 1, T - std::max(p.Tt - 1, 0));
     if (p.Tt == T) p.C = p.K2 + 1;
     p.NI = (p.K1 + p.K2 - 1) / p.K2;
-    p.bytes = bytes(p.K2, p.C);
+    p.bytes = bytes(p.K2, p.C, (p.Tt + p.K1 - 1) / p.K1);
     // forward steps (fused pull-collide launches): the first pass, the outer
     // recompute to the inner checkpoints and the recompute of every inner
     // segment before the tail (its last state needs only the source and ghost fill)
@@ -2233,7 +2235,7 @@ extern "C" int lbm_adjoint_grad(lbm_handle* h, int nsteps, const double* observe
 
     const int T = nsteps;
     const AdjPlan plan = adjoint_plan(h, T, ckpt_outer, ckpt_inner);
-    const int K1 = plan.K1, K2 = plan.K2, M = plan.M, NI = plan.NI, ncell = plan.ncell;
+    const int K1 = plan.K1, K2 = plan.K2, NI = plan.NI, ncell = plan.ncell;
     const int Tt = plan.Tt;                        // steps Tt .. T-1 are reversed from the first pass's data
     const int Mr = (Tt + K1 - 1) / K1;             // outer segments reversed with a recompute
     const Layout& L = h->L;
@@ -2268,8 +2270,8 @@ extern "C" int lbm_adjoint_grad(lbm_handle* h, int nsteps, const double* observe
     double *d_pred, *d_resid, *d_out;
     AdjSourceCell* d_cells;
     const auto carve = [&](Carve& c) {
-        outer = StateSlots{c.get<float>((size_t)M * plan.ck_slot), pop, plan.ck_slot - pop};
-        inner = StateSlots{c.get<float>((size_t)NI * plan.ck_slot), pop, plan.ck_slot - pop};
+        outer = StateSlots{c.get<float>((size_t)Mr * plan.ck_slot), pop, plan.ck_slot - pop};
+        inner = StateSlots{c.get<float>((size_t)(Mr > 0 ? NI : 0) * plan.ck_slot), pop, plan.ck_slot - pop};
         store = c.get<float>((size_t)plan.C * plan.st_slot);
         lam[0] = c.get<float>(pop);
         lam[1] = c.get<float>(pop);

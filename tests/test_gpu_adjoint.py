@@ -149,18 +149,32 @@ def test_adjoint_plan(gpu):
     assert g.adjoint_plan(45, 9, 1)[3] > g.adjoint_plan(45, 9, 9)[3]
 
 
+def _partial_tail_budget(g, steps, outer, monkeypatch):
+    """A memory cap under which the plan keeps the forward data of some but
+    not all segments (some recomputed, a stored tail): searched between the
+    all-recompute plan's bytes and the uncapped plan's."""
+    none = g.adjoint_plan(steps, outer, outer)        # explicit inner interval: every segment recomputed
+    full = g.adjoint_plan(steps, outer, 0)            # small grid: the whole run's forward data fits
+    assert full[3] == steps and none[3] > steps
+    for f in np.linspace(0.05, 0.95, 19):
+        budget = none[2] + f * (full[2] - none[2])
+        monkeypatch.setenv("NLOS_LBM_ADJ_BUDGET", str(budget))
+        plan = g.adjoint_plan(steps, outer, 0)
+        monkeypatch.delenv("NLOS_LBM_ADJ_BUDGET")
+        if steps < plan[3] < none[3]:
+            return budget, plan, none
+    raise AssertionError("no cap between the two plans gives a partial tail")
+
+
 def test_partial_stored_tail(gpu, monkeypatch):
-    """A memory cap that holds the forward data of the last two 10-step
-    segments: those are reversed from the first pass's data, the first three
-    with a recompute; the result is bit-identical to recomputing every segment."""
+    """A memory cap that holds the forward data of the last segments only:
+    those are reversed from the first pass's data, the others with a
+    recompute; the result is bit-identical to recomputing every segment."""
     sc = scenarios.adjoint_scenario(nx=32, ny=24, nz=16, steps=45, nprobe=6)
     g = Solver(sc["cfg"], [sc["trial"]], sc["probes"], triangles=sc["triangles"])
-    none = g.adjoint_plan(45, 10, 10)          # explicit inner interval: 11 store slots, no tail
-    full = g.adjoint_plan(45, 10, 0)           # everything fits: 45 store slots
-    slot = (full[2] - none[2]) / (45 - 11)
-    monkeypatch.setenv("NLOS_LBM_ADJ_BUDGET", str(none[2] + 5.5 * slot))   # 16 slots: steps 29..44
-    o, i, nbytes, fwd = g.adjoint_plan(45, 10, 0)
-    assert (o, i) == (10, 10) and fwd == 45 + 9 + 10 + 10
+    budget, plan, none = _partial_tail_budget(g, 45, 10, monkeypatch)
+    assert plan[:2] == (10, 10)
+    monkeypatch.setenv("NLOS_LBM_ADJ_BUDGET", str(budget))
     part = g.adjoint_grad(sc["observed"], 10, 0)
     monkeypatch.delenv("NLOS_LBM_ADJ_BUDGET")
     ref = g.adjoint_grad(sc["observed"], 10, 10)

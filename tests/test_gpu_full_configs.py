@@ -25,6 +25,7 @@ import scenarios
 from nlos_lbm import Solver, abi, workloads
 from oracle import OracleSolver
 from scenarios import rel_l2
+from test_gpu_adjoint import _partial_tail_budget
 
 pytestmark = pytest.mark.gpu
 
@@ -80,13 +81,10 @@ def test_stored_tail_and_recompute_schedule_matches_fp64_adjoint(gpu, monkeypatc
     sc = scenarios.adjoint_scenario(nx=112, ny=96, nz=48, steps=600, nprobe=24, seed=5)
     steps = sc["steps"]
     g = Solver(sc["cfg"], [sc["trial"]], sc["probes"], triangles=sc["triangles"])
-    none = g.adjoint_plan(steps, 200, 200)     # explicit inner interval: every segment recomputed
-    full = g.adjoint_plan(steps, 200, 0)       # uncapped: the whole run's forward data fits
-    assert none[3] > full[3] == steps
-    # a cap between the two: the last segment's forward data kept, the others recomputed
-    monkeypatch.setenv("NLOS_LBM_ADJ_BUDGET", str(none[2] + 0.55 * (full[2] - none[2])))
-    o, i, nbytes, fwd = g.adjoint_plan(steps, 200, 0)
-    assert (o, i) == (200, 200) and steps < fwd < none[3], (fwd, none[3])
+    # a cap under which the first segments are recomputed and the rest kept from the first pass
+    budget, plan, none = _partial_tail_budget(g, steps, 200, monkeypatch)
+    assert plan[:2] == (200, 200)
+    monkeypatch.setenv("NLOS_LBM_ADJ_BUDGET", str(budget))
     part = g.adjoint_grad(sc["observed"], 200, 0)
     monkeypatch.delenv("NLOS_LBM_ADJ_BUDGET")
     rec = g.adjoint_grad(sc["observed"], 200, 200)
