@@ -156,6 +156,7 @@ def _partial_tail_budget(g, steps, outer, monkeypatch):
     none = g.adjoint_plan(steps, outer, outer)        # explicit inner interval: every segment recomputed
     full = g.adjoint_plan(steps, outer, 0)            # small grid: the whole run's forward data fits
     assert full[3] == steps and none[3] > steps
+    assert full[2] > none[2], "storing every step must cost more than the checkpoints for a partial tail"
     for f in np.linspace(0.05, 0.95, 19):
         budget = none[2] + f * (full[2] - none[2])
         monkeypatch.setenv("NLOS_LBM_ADJ_BUDGET", str(budget))
@@ -170,14 +171,16 @@ def test_partial_stored_tail(gpu, monkeypatch):
     """A memory cap that holds the forward data of the last segments only:
     those are reversed from the first pass's data, the others with a
     recompute; the result is bit-identical to recomputing every segment."""
-    sc = scenarios.adjoint_scenario(nx=32, ny=24, nz=16, steps=45, nprobe=6)
+    # 120 steps in 20-step segments: keeping every step's forward data needs more memory than the
+    # full-state checkpoints of an all-recompute plan, so caps in between give a partial tail
+    sc = scenarios.adjoint_scenario(nx=32, ny=24, nz=16, steps=120, nprobe=6)
     g = Solver(sc["cfg"], [sc["trial"]], sc["probes"], triangles=sc["triangles"])
-    budget, plan, none = _partial_tail_budget(g, 45, 10, monkeypatch)
-    assert plan[:2] == (10, 10)
+    budget, plan, none = _partial_tail_budget(g, 120, 20, monkeypatch)
+    assert plan[:2] == (20, 20)
     monkeypatch.setenv("NLOS_LBM_ADJ_BUDGET", str(budget))
-    part = g.adjoint_grad(sc["observed"], 10, 0)
+    part = g.adjoint_grad(sc["observed"], 20, 0)
     monkeypatch.delenv("NLOS_LBM_ADJ_BUDGET")
-    ref = g.adjoint_grad(sc["observed"], 10, 10)
+    ref = g.adjoint_grad(sc["observed"], 20, 20)
     assert part[0] == ref[0]
     for a, b in zip(part[1:], ref[1:]):
         assert np.array_equal(a, b)
