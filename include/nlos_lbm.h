@@ -341,15 +341,17 @@ int lbm_get_mask(lbm_handle* h, uint8_t* out, long capacity);
  * 06:579-581, so dL/dtable[s] = amp * grad_signal[s] for LBM_WAVE_TABLE).
  * No counterpart in the reference, which has no adjoint or inverse solver;
  * the forward model is exactly lbm_step's (same kernels, FP32 storage).
- * A reverse-time discrete adjoint of the fused step: the forward pass keeps a
- * checkpoint every ckpt_outer steps (<= 0: 200), each segment is recomputed
- * with inner checkpoints every ckpt_inner steps, and each inner segment once
- * more, storing its states, before it is run backwards.  ckpt_inner <= 0
- * picks the largest interval up to ckpt_outer whose buffers fit in 90 % of the
- * free device memory (ckpt_inner = ckpt_outer stores whole outer segments and
- * needs no second recompute).  Device memory: about (nsteps/ckpt_outer +
- * ckpt_outer/ckpt_inner + ckpt_inner + 3) population buffers; lbm_adjoint_plan
- * gives the exact figure.  Requires FP32 storage, exactly one source and at least
+ * A reverse-time discrete adjoint of the fused step.  The backward pass needs
+ * each step's forward data: the moments of the pulled populations (6 bytes a
+ * cell) and those of the ghost cells.  The forward pass keeps them for a tail
+ * of whole ckpt_outer-step segments (<= 0: 200) and a full-state checkpoint at
+ * the start of every segment before that tail; those segments are recomputed,
+ * with inner checkpoints every ckpt_inner steps, before they are run
+ * backwards.  ckpt_inner <= 0 picks the largest inner interval, then the
+ * longest tail, that fit in 90 % of the free device memory (NLOS_LBM_ADJ_BUDGET
+ * caps it); when the whole run's forward data fits nothing is recomputed.  An
+ * explicit ckpt_inner > 0 keeps no tail.  lbm_adjoint_plan gives the schedule
+ * and its device bytes.  Requires FP32 storage, exactly one source and at least
  * one probe.  Observed entries that are NaN, probes outside the grid and the
  * probe rows of SOLID cells (which read 0 whatever the state) contribute no
  * gradient.  Starts from and returns to the rest state (step 0, empty probe
