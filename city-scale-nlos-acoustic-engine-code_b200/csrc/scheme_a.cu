@@ -315,17 +315,37 @@ __device__ __forceinline__ void step_a_pair(const float* __restrict__ fin, float
         om = make_float2(cell_omega(b, c0 + 1, j, k), has1 ? cell_omega(b, c0 + 2, j, k) : 1.0f);
     }
     {
-        float2 rho = f2(0.f), jx = f2(0.f), jy = f2(0.f), jz = f2(0.f);
-#pragma unroll
-        for (int q = 0; q < Q; ++q)
+        // moments; the 01 instance sums them one direction after another (with the
+        // shared partial sums below it spills at its register cap)
+        float2 rho, jx, jy, jz;
+        if constexpr (FEAT == 1)
         {
-            rho = add2(rho, G[q]);
-            if (ex(q) > 0) jx = add2(jx, G[q]);
-            if (ex(q) < 0) jx = sub2(jx, G[q]);
-            if (ey(q) > 0) jy = add2(jy, G[q]);
-            if (ey(q) < 0) jy = sub2(jy, G[q]);
-            if (ez(q) > 0) jz = add2(jz, G[q]);
-            if (ez(q) < 0) jz = sub2(jz, G[q]);
+            rho = jx = jy = jz = f2(0.f);
+#pragma unroll
+            for (int q = 0; q < Q; ++q)
+            {
+                rho = add2(rho, G[q]);
+                if (ex(q) > 0) jx = add2(jx, G[q]);
+                if (ex(q) < 0) jx = sub2(jx, G[q]);
+                if (ey(q) > 0) jy = add2(jy, G[q]);
+                if (ey(q) < 0) jy = sub2(jy, G[q]);
+                if (ez(q) > 0) jz = add2(jz, G[q]);
+                if (ez(q) < 0) jz = sub2(jz, G[q]);
+            }
+        }
+        else
+        {
+            // rho' = g0 + rest + S(x+) + S(x-), jx = S(x+) - S(x-)
+            const float2 sxp = add2(add2(add2(G[1], G[7]), add2(G[8], G[11])), G[12]);
+            const float2 sxn = add2(add2(add2(G[2], G[9]), add2(G[10], G[13])), G[14]);
+            const float2 rest =
+                add2(add2(add2(G[3], G[4]), add2(G[5], G[6])), add2(add2(G[15], G[16]), add2(G[17], G[18])));
+            rho = add2(add2(G[0], rest), add2(sxp, sxn));
+            jx = sub2(sxp, sxn);
+            jy = sub2(add2(add2(add2(G[3], G[7]), add2(G[9], G[15])), G[16]),
+                      add2(add2(add2(G[4], G[8]), add2(G[10], G[17])), G[18]));
+            jz = sub2(add2(add2(add2(G[5], G[11]), add2(G[13], G[15])), G[17]),
+                      add2(add2(add2(G[6], G[12]), add2(G[14], G[16])), G[18]));
         }
         float2 r = add2(rho, f2(1.0f));
         if (r.x <= 0.f) r.x = 1e-12f;
@@ -337,21 +357,59 @@ __device__ __forceinline__ void step_a_pair(const float* __restrict__ fin, float
         const float2 base = fma2(mul2(ir, E), f2(-1.5f), rho);
         const float2 k45 = mul2(ir, f2(4.5f));
         const float2 keep = sub2(f2(1.0f), om);
-#pragma unroll
-        for (int q = 0; q < Q; ++q)
+        if constexpr (FEAT == 1)
         {
-            float2 cj = f2(0.f);
-            if (ex(q) > 0) cj = add2(cj, jx);
-            if (ex(q) < 0) cj = sub2(cj, jx);
-            if (ey(q) > 0) cj = add2(cj, jy);
-            if (ey(q) < 0) cj = sub2(cj, jy);
-            if (ez(q) > 0) cj = add2(cj, jz);
-            if (ez(q) < 0) cj = sub2(cj, jz);
-            const float c0 = b.cu0[q];
-            // E_q = (2 c.u0 + c.J') c.J' - rho' (c.u0)^2
-            const float2 Eq = fma2(rho, f2(-c0 * c0), mul2(add2(f2(2.0f * c0), cj), cj));
-            const float2 geq = mul2(f2(wf(q)), fma2(cj, f2(3.0f), fma2(k45, Eq, base)));
-            G[q] = fma2(keep, G[q], mul2(om, geq));
+#pragma unroll
+            for (int q = 0; q < Q; ++q)
+            {
+                float2 cj = f2(0.f);
+                if (ex(q) > 0) cj = add2(cj, jx);
+                if (ex(q) < 0) cj = sub2(cj, jx);
+                if (ey(q) > 0) cj = add2(cj, jy);
+                if (ey(q) < 0) cj = sub2(cj, jy);
+                if (ez(q) > 0) cj = add2(cj, jz);
+                if (ez(q) < 0) cj = sub2(cj, jz);
+                const float c0 = b.cu0[q];
+                // E_q = (2 c.u0 + c.J') c.J' - rho' (c.u0)^2
+                const float2 Eq = fma2(rho, f2(-c0 * c0), mul2(add2(f2(2.0f * c0), cj), cj));
+                const float2 geq = mul2(f2(wf(q)), fma2(cj, f2(3.0f), fma2(k45, Eq, base)));
+                G[q] = fma2(keep, G[q], mul2(om, geq));
+            }
+        }
+        else
+        {
+            // rest direction: c = 0, so E_0 = -rho' (c.u0)^2 with c.u0 = 0
+            {
+                const float c0 = b.cu0[0];
+                const float2 Eq = fma2(rho, f2(-c0 * c0), mul2(f2(2.0f * c0), f2(0.f)));
+                G[0] = fma2(keep, G[0], mul2(om, mul2(f2(wf(0)), fma2(k45, Eq, base))));
+            }
+            // a direction q and its opposite share c.J' up to sign and, since
+            // c_{inv q}.u0 = -c_q.u0, the same E_q = (2 c.u0 + c.J') c.J' - rho' (c.u0)^2:
+            // om geq = om w (base + k45 E_q) +- 3 om w c.J'
+            const float2 omw1 = mul2(om, f2(wf(1))), omw2 = mul2(om, f2(wf(7)));
+#pragma unroll
+            for (int p = 0; p < 9; ++p)
+            {
+                const int q = pair_head(p), qb = inv(q);
+                float2 cj;
+                if (p == 0) cj = jx;
+                else if (p == 1) cj = jy;
+                else if (p == 2) cj = jz;
+                else if (p == 3) cj = add2(jx, jy);
+                else if (p == 4) cj = sub2(jx, jy);
+                else if (p == 5) cj = add2(jx, jz);
+                else if (p == 6) cj = sub2(jx, jz);
+                else if (p == 7) cj = add2(jy, jz);
+                else cj = sub2(jy, jz);
+                const float c0 = b.cu0[q];
+                const float2 Eq = fma2(rho, f2(-c0 * c0), mul2(add2(f2(2.0f * c0), cj), cj));
+                const float2 omw = q < 7 ? omw1 : omw2;
+                const float2 e = mul2(omw, fma2(k45, Eq, base));
+                const float2 t = mul2(omw, mul2(cj, f2(3.0f)));
+                G[q] = fma2(keep, G[q], add2(e, t));
+                G[qb] = fma2(keep, G[qb], sub2(e, t));
+            }
         }
     }
     // forcing of this cell for the populations it sends next (03:424-435)
