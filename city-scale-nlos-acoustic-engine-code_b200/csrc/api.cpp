@@ -556,6 +556,7 @@ int upload_scheme_a_profiles(lbm_handle* h)
         const double cu = ex(q) * c.flow[0] + ey(q) * c.flow[1] + ez(q) * c.flow[2];
         b.base[q] = (float)(wd(q) * (3.0 * cu + 4.5 * cu * cu - 1.5 * u2));
         b.cu0[q] = (float)cu;
+        b.fq[q] = (float)(wd(q) * (1.0 + 3.0 * cu));
     }
     b.u0sq = (float)u2;
     b.copy = c.face_bc[LBM_FACE_XLO] == LBM_BC_COPY ? 1 : 0;

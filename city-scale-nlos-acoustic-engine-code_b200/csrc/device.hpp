@@ -188,6 +188,7 @@ struct SchemeAArgs
     float flow[3];             // background velocity u0 (lattice units)
     float base[19];            // feq(1, u0) - w_q: stored values are deviations from feq(1, u0)
     float cu0[19];             // c_q . u0
+    float fq[19];              // w_q (1 + 3 c_q . u0): forcing weight of direction q (03:74-78)
     float u0sq;                // u0 . u0
     const SourceEntry* table;  // schedule rows [row][nsrc] (row = step - ctl->table_base), as SourceArgs
     const Control* ctl;        // nullptr: use mass_direct

@@ -107,7 +107,7 @@ __device__ __forceinline__ void collide1(float (&G)[Q], float om, const SchemeAA
 // forcing term of the collided cell (03:74-78, 03:422-435)
 __device__ __forceinline__ float force_term(const SchemeAArgs& b, int q, float s_amp, float om)
 {
-    return wf(q) * s_amp * (1.0f + 3.0f * b.cu0[q]) * (1.0f - 0.5f * om);
+    return b.fq[q] * (s_amp * (1.0f - 0.5f * om));
 }
 
 // Populations arriving at interior cell (i, j, k) in the step that reads f:
@@ -415,13 +415,24 @@ __device__ __forceinline__ void step_a_pair(const float* __restrict__ fin, float
     // forcing of this cell for the populations it sends next (03:424-435)
     if (b.field_mode == 1)
     {
-        const float2 sp = pair_weight(mass(1));
-        const float s0 = sp.x, s1 = sp.y;
+        // force_term() of both cells: w_q (1 + 3 c_q.u0) s (1 - om / 2)
+        const float2 sw = mul2(pair_weight(mass(1)), fma2(om, f2(-0.5f), f2(1.0f)));
 #pragma unroll
         for (int q = 0; q < Q; ++q)
         {
-            G[q].x += force_term(b, q, s0, om.x);
-            G[q].y += force_term(b, q, s1, om.y);
+            if constexpr (FEAT == 2)
+            {
+                // 04's instance forms the weight in place: reading fq from the
+                // parameter space costs it 36 more bytes of spills at its cap
+                const float w = wf(q) * (1.0f + 3.0f * b.cu0[q]);
+                G[q].x = fmaf(w, sw.x, G[q].x);
+                G[q].y = fmaf(w, sw.y, G[q].y);
+            }
+            else
+            {
+                G[q].x = fmaf(b.fq[q], sw.x, G[q].x);
+                G[q].y = fmaf(b.fq[q], sw.y, G[q].y);
+            }
         }
     }
 
@@ -741,8 +752,9 @@ cudaError_t launch_step_a(const float* fin, float* fout, const Layout& L, const 
     if (L.bc != BC) return cudaErrorInvalidValue;
     // every instance takes one plane per thread; 04's, with its column values
     // hoisted, at the lean instances' 72 registers (28 warps per SM): on 04's
-    // 208^3 grid 0.309 ms against 0.326 ms at 96 registers with four planes per
-    // thread, 0.320 ms at 80 registers with two, 0.349-0.367 ms otherwise
+    // 208^3 grid 0.309 ms (0.293 ms with the paired collision) against 0.326 ms
+    // at 96 registers with four planes per thread, 0.320 ms at 80 registers with
+    // two, 0.349-0.367 ms otherwise
     constexpr int kBlock = 128;
     const unsigned gx = (unsigned)((L.nx + 2 * kBlock - 1) / (2 * kBlock));
     if (b.field_mode == 2 || b.sg_xy || b.fld_xy)
