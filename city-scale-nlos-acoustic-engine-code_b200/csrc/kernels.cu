@@ -160,9 +160,12 @@ __device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b
 //   Geq_q = w_q (rho' + 3 c.J + (4.5 (c.J)^2 - 1.5 J^2) / (scale r))
 //   G'    = (1 - sigma) (G - omega (G - Geq))      [sponge blend toward w_q, 06:955-965]
 // A SOLID cell gets cA = 1, cB = 0, so its pulled values pass through
-// unchanged (06:933-938).
+// unchanged (06:933-938).  on_moments(rho', jx, jy, jz) receives the moments
+// of the pulled populations as soon as they are summed (the adjoint's forward
+// data), so nothing beyond the collision's own values stays live for them.
+template <typename OnMoments>
 __device__ __forceinline__ void collide2(float2 (&G)[Q], float inv_scale, float omega, float2 sigma, bool solid0,
-                                         bool solid1, float4& mom0, float4& mom1)
+                                         bool solid1, OnMoments&& on_moments)
 {
     // rho' and J in the family-B order (06:21-23)
     const float2 rho = add2(add2(add2(add2(G[0], G[1]), add2(G[2], G[3])), add2(add2(G[4], G[5]), add2(G[6], G[7]))),
@@ -174,8 +177,7 @@ __device__ __forceinline__ void collide2(float2 (&G)[Q], float inv_scale, float 
                            add2(add2(add2(G[4], G[8]), add2(G[10], G[17])), G[18]));
     const float2 jz = sub2(add2(add2(add2(G[5], G[11]), add2(G[13], G[15])), G[17]),
                            add2(add2(add2(G[6], G[12]), add2(G[14], G[16])), G[18]));
-    mom0 = make_float4(rho.x, jx.x, jy.x, jz.x);   // moments of the pulled populations
-    mom1 = make_float4(rho.y, jx.y, jy.y, jz.y);
+    on_moments(rho, jx, jy, jz);
     float2 r = fma2(rho, f2(inv_scale), f2(1.0f));
     if (r.x <= 0.f) r.x = 1e-12f;   // 06:948
     if (r.y <= 0.f) r.y = 1e-12f;
@@ -337,13 +339,16 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step(const S* __restrict__ fin,
 
     const float syz = fmaxf(a.sig_y[j - 1], a.sig_z[k - 1]);
     const float2 sg = make_float2(fmaxf(a.sig_x[c0], syz), fmaxf(c0 + 1 < L.nx ? a.sig_x[c0 + 1] : 0.f, syz));
-    float4 m0, m1;
-    collide2(G, inv_scale, a.omega, sg, (lk0 & kSolidSelfBit) != 0u, (lk1 & kSolidSelfBit) != 0u, m0, m1);
-    if constexpr (MOM)
-    {
-        const long long pi = ((long long)(k - 1) * L.ny + (j - 1)) * ((L.nx + 1) >> 1) + (c0 >> 1);
-        mom[pi] = pack_moments(m0, c0 + 1 < L.nx ? m1 : make_float4(0.f, 0.f, 0.f, 0.f));
-    }
+    collide2(G, inv_scale, a.omega, sg, (lk0 & kSolidSelfBit) != 0u, (lk1 & kSolidSelfBit) != 0u,
+             [&](float2 rho, float2 jx, float2 jy, float2 jz) {
+                 if constexpr (MOM)
+                 {
+                     const long long pi = ((long long)(k - 1) * L.ny + (j - 1)) * ((L.nx + 1) >> 1) + (c0 >> 1);
+                     mom[pi] = pack_moments(make_float4(rho.x, jx.x, jy.x, jz.x),
+                                            c0 + 1 < L.nx ? make_float4(rho.y, jx.y, jy.y, jz.y)
+                                                          : make_float4(0.f, 0.f, 0.f, 0.f));
+                 }
+             });
 
     S* out = fout + e0;
 #pragma unroll
