@@ -310,34 +310,36 @@ __device__ __forceinline__ float2 shifted_pair(const float* row, int lane, const
 // a = (1 - sigma)(1 - omega), b = (1 - sigma) omega; SOLID cells copy.
 // lamH (gather of lamF^s with the bounce-back terms and, at the open faces,
 // the ghost-adjoint terms) stays in registers for the output.
-// L2 prefetch of the adjoint lines and the moments that the row `dist` rows
-// after (j, k) reads, for the CELLS columns from col0 (one block's share):
-// the first threads take one interleaved block each (19 lines), the next
-// ones one 128-byte line of moments each.
+// L2 prefetch, one CTA's share, as two bulk prefetches issued by its first
+// thread: the columns of this CTA in the storage row first read `dist` rows
+// from now (a row of the adjoint layout is contiguous: its blocks' 19 lines
+// back to back; rows are first read by the target row one plane and one row
+// before them), and the moment records of the target row `dist` rows ahead.
 template <int CELLS>
 __device__ __forceinline__ void adj_prefetch_rows(const AdjStepArgs& a, int j, int k, int col0)
 {
-    constexpr int BC = 32, NBLK = (CELLS + BC - 1) / BC, NMOM = (CELLS / 2 * (int)sizeof(PairMoments) + 127) / 128;
+    if (threadIdx.x != 0) return;
     const Layout& L = a.L;
-    const int t = threadIdx.x;
-    if (t >= NBLK + NMOM) return;
-    const int r = (k - 1) * L.ny + (j - 1) + a.prefetch_rows;
-    if (r >= L.ny * L.nz) return;
-    const int jj = 1 + r % L.ny, kk = 1 + r / L.ny;
-    if (t < NBLK)
+    const long long rows_total = (long long)(L.nz + 2) * (L.ny + 2);
+    const long long R = (long long)k * (L.ny + 2) + j + (L.ny + 2) + 1 + a.prefetch_rows;
+    if (R < rows_total)
     {
-        const int col = col0 + t * BC;
-        if (col >= L.nx) return;
-#pragma unroll
-        for (int q = 0; q < Q; ++q)
-            asm volatile("prefetch.global.L2 [%0];" ::"l"(a.lam_in + L.elem(q, col + 1, jj + ey(q), kk + ez(q))));
+        constexpr int kBlocks = (CELLS + 31) / 32;
+        const int b0 = col0 >> 5, nbk = min(kBlocks, L.nb - b0);
+        const float* p = a.lam_in + kFrontElems + R * L.row_stride + (long long)b0 * (19 * 32);
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(nbk * 19 * 128) : "memory");
     }
-    else
+    const long long r = (long long)(k - 1) * L.ny + (j - 1) + a.prefetch_rows;
+    if (r < (long long)L.ny * L.nz)
     {
-        const int byte = (t - NBLK) * 128;   // within the tile's pair records
-        if (col0 + byte / (int)sizeof(PairMoments) * 2 >= L.nx) return;
-        const long long pi = ((long long)(kk - 1) * L.ny + (jj - 1)) * ((L.nx + 1) >> 1) + (col0 >> 1);
-        asm volatile("prefetch.global.L2 [%0];" ::"l"(reinterpret_cast<const char*>(a.mom_prev + pi) + byte));
+        const long long npr = (L.nx + 1) >> 1;
+        const long long first = r * npr + (col0 >> 1), last = min(first + CELLS / 2, (r + 1) * npr);
+        const long long total = npr * L.ny * L.nz * (long long)sizeof(PairMoments);
+        const long long lo = first * (long long)sizeof(PairMoments) & ~15LL;
+        const long long hi = min((last * (long long)sizeof(PairMoments) + 15) & ~15LL, total & ~15LL);
+        if (hi > lo)
+            asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(reinterpret_cast<const char*>(a.mom_prev) + lo),
+                         "r"((unsigned)(hi - lo)) : "memory");
     }
 }
 

@@ -32,7 +32,7 @@ struct AdjStepArgs
     const PairMoments* mom_prev;     // moments (rho', J) of F^{s-1}, dense pair order (launch_step_moments)
     const float* gadj;      // ghost-adjoint contributions of step s, per open face
     long long gadj_off[6];  // offset of face f in gadj, -1 = face not open
-    int prefetch_rows;      // > 0: each block prefetches into L2 what the row this far ahead reads
+    int prefetch_rows;      // > 0: each block prefetches into L2 the storage row first read this many rows ahead
 };
 
 struct AdjGhostArgs

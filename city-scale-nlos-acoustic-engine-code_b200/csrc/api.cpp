@@ -33,7 +33,8 @@ constexpr int kTableRows = 4096;   // source-schedule rows resident on the devic
 constexpr int kBcCut = 100;        // face of a z-slab that borders the next slab (internal face type)
 constexpr int kProbeRows = 4096;   // probe-series rows buffered on the device
 // L2 prefetch distance of the adjoint step in rows (measured on the 256x256x128 patch: 192 rows
-// ahead, 2-4 % less time per gradient than none; 48 to 1536 rows tried)
+// ahead; per-line prefetches gave 2-4 % less time per gradient than none, 48 to 1536 rows tried,
+// and one bulk prefetch of the whole storage row 4 % more)
 constexpr int kDefaultAdjointPrefetchRows = 192;
 
 struct SourceState
