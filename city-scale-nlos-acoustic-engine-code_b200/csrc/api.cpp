@@ -36,6 +36,10 @@ constexpr int kProbeRows = 4096;   // probe-series rows buffered on the device
 // ahead; per-line prefetches gave 2-4 % less time per gradient than none, 48 to 1536 rows tried,
 // and one bulk prefetch of the whole storage row 4 % more)
 constexpr int kDefaultAdjointPrefetchRows = 192;
+// The same for the scheme-A instance with per-column fields, latency-bound like the adjoint step
+// (04's 208^3 grid: 0.295 ms a launch without, 0.267 ms with 64-256 rows; the bandwidth-bound
+// instances and the forward pair kernel run slower with it)
+constexpr int kDefaultSchemeAPrefetchRows = 128;
 
 struct SourceState
 {
@@ -563,6 +567,10 @@ int upload_scheme_a_profiles(lbm_handle* h)
     b.copy = c.face_bc[LBM_FACE_XLO] == LBM_BC_COPY ? 1 : 0;
     b.table = h->d_table;
     b.ctl = h->ctl;
+    // L2 prefetch distance of the scheme-A instance with per-column fields (04's), in rows
+    // (NLOS_LBM_A_PREFETCH_ROWS, 0 = off)
+    b.prefetch_rows = kDefaultSchemeAPrefetchRows;
+    if (const char* v = std::getenv("NLOS_LBM_A_PREFETCH_ROWS")) b.prefetch_rows = std::max(0, std::atoi(v));
     return LBM_OK;
 }
 

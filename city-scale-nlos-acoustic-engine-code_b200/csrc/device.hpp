@@ -203,6 +203,8 @@ struct SchemeAArgs
     const float* sg_xy;        // nullptr or per-column blend strengths [(j-1) nx + (i-1)] (max with sg_*)
     const float* fld_xy;       // nullptr or per-column source weights, replacing fld_x fld_y fld_z
     int nx_col, ny_col;        // column grid of sg_xy / fld_xy (nx, ny)
+    int prefetch_rows;         // > 0: the instance with per-column fields (04's) prefetches into L2 the
+                               //   storage row first read this many rows ahead
 };
 
 // ---- launchers (kernels.cu) ----------------------------------------------

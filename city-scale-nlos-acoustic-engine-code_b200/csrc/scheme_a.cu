@@ -501,6 +501,19 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step_a(const float* __restrict_
         z.mass0 = b.field_mode == 0 ? field_mass(b, 0) : 0.f;
         z.mass1 = b.field_mode >= 1 ? field_mass(b, 1) : 0.f;
         const int k0 = blockIdx.z * KZ + 1;
+        if (b.prefetch_rows > 0 && threadIdx.x == 0)
+        {
+            // this CTA's columns of the storage row first read prefetch_rows rows
+            // from now, one bulk prefetch into L2 (a row of the layout is contiguous)
+            const long long R = (long long)k0 * (L.ny + 2) + j + (L.ny + 2) + 1 + b.prefetch_rows;
+            if (R < (long long)(L.nz + 2) * (L.ny + 2))
+            {
+                constexpr int kBlocks = 2 * BLOCK / BC;
+                const int b0 = 2 * BLOCK * (int)blockIdx.x / BC, nbk = min(kBlocks, L.nb - b0);
+                const float* p = fin + kFrontElems + R * L.row_stride + (long long)b0 * BE;
+                asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(nbk * BE * 4) : "memory");
+            }
+        }
 #pragma unroll 1
         for (int kk = 0; kk < KZ; ++kk)
         {
