@@ -131,6 +131,10 @@ struct lbm_handle
     void* slab_buf = nullptr;
     size_t slab_msg_bytes = 0;
     cudaEvent_t ev_packed = nullptr, ev_read = nullptr;
+    // lbm_adjoint_grad: a second stream for the small kernels that run beside a step
+    // (the forward pass's probe record, the reverse pass's source terms)
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
 
     // adjoint workspace (checkpoints, stored moments, adjoint populations),
     // kept between lbm_adjoint_grad calls; lbm_adjoint_release frees it
@@ -193,6 +197,11 @@ struct lbm_handle
         if (ev_packed) cudaEventDestroy(ev_packed);
         if (ev_read) cudaEventDestroy(ev_read);
         ev_packed = ev_read = nullptr;
+        if (ev_fork) cudaEventDestroy(ev_fork);
+        if (ev_join) cudaEventDestroy(ev_join);
+        ev_fork = ev_join = nullptr;
+        if (side) cudaStreamDestroy(side);
+        side = nullptr;
         adj_ws_bytes = 0;
         if (stream) cudaStreamDestroy(stream);
         stream = nullptr;
@@ -2346,17 +2355,25 @@ extern "C" int lbm_adjoint_grad(lbm_handle* h, int nsteps, const double* observe
         return r;
     };
     // pull + collide of step s (Ht^s -> G^{s+1}), optionally with its probe record
-    const auto collide = [&](int s, bool probe) {
-        cudaError_t r = launch_step(h->storage, h->f[h->cur], h->f[h->cur ^ 1], L, h->sa, h->scale,
-                                    h->stream);
+    // The probe record of step s reads the step's input buffer, which the step
+    // only reads: it runs on the side stream beside the step, joined before
+    // anything can overwrite that buffer (the next step writes into it).
+    const auto probe_beside = [&](int s) {
+        ProbeArgs pa = probe_args(h, false, s);
+        pa.out = d_pred;
+        cudaError_t r = cudaEventRecord(h->ev_fork, h->stream);
+        if (r == cudaSuccess) r = cudaStreamWaitEvent(h->side, h->ev_fork, 0);
+        if (r == cudaSuccess) r = launch_probe(h->storage, h->f[h->cur], L, h->sa, pa, h->side);
+        if (r == cudaSuccess) r = cudaEventRecord(h->ev_join, h->side);
         kernels++;
-        if (r == cudaSuccess && probe)
-        {
-            ProbeArgs pa = probe_args(h, false, s);
-            pa.out = d_pred;
-            r = launch_probe(h->storage, h->f[h->cur], L, h->sa, pa, h->stream);
-            kernels++;
-        }
+        return r;
+    };
+    const auto collide = [&](int s, bool probe) {
+        cudaError_t r = probe ? probe_beside(s) : cudaSuccess;
+        if (r == cudaSuccess)
+            r = launch_step(h->storage, h->f[h->cur], h->f[h->cur ^ 1], L, h->sa, h->scale, h->stream);
+        kernels++;
+        if (r == cudaSuccess && probe) r = cudaStreamWaitEvent(h->stream, h->ev_join, 0);
         h->cur ^= 1;
         return r;
     };
@@ -2379,20 +2396,23 @@ extern "C" int lbm_adjoint_grad(lbm_handle* h, int nsteps, const double* observe
     // probe_step >= 0: also the probe record of that step (first pass)
     const auto stored_collide = [&](long long slot, int probe_step = -1) {
         kernels++;
-        cudaError_t r =
-            launch_step_moments((const float*)h->f[h->cur], (float*)h->f[h->cur ^ 1], L, h->sa, mom_of(slot), h->stream);
-        if (r == cudaSuccess && probe_step >= 0)
-        {
-            ProbeArgs pa = probe_args(h, false, probe_step);
-            pa.out = d_pred;
-            r = launch_probe(h->storage, h->f[h->cur], L, h->sa, pa, h->stream);
-            kernels++;
-        }
+        cudaError_t r = probe_step >= 0 ? probe_beside(probe_step) : cudaSuccess;
+        if (r == cudaSuccess)
+            r = launch_step_moments((const float*)h->f[h->cur], (float*)h->f[h->cur ^ 1], L, h->sa, mom_of(slot),
+                                    h->stream);
+        if (r == cudaSuccess && probe_step >= 0) r = cudaStreamWaitEvent(h->stream, h->ev_join, 0);
         h->cur ^= 1;
         return r;
     };
     const auto ckpt_pos = [&](long long boundary) { return std::max(boundary - 1, 0LL); };
     const long long cnT = ckpt_pos(Tt);   // first step whose forward data the first pass stores
+
+    if (!h->side)
+    {
+        CK(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking), "adjoint side stream");
+        CK(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming), "adjoint events");
+        CK(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming), "adjoint events");
+    }
 
     // ---- forward pass: probe predictions, outer checkpoints G^{max(mK1-1,0)}
     // of the segments before the tail, and the tail's forward data
@@ -2457,19 +2477,28 @@ extern "C" int lbm_adjoint_grad(lbm_handle* h, int nsteps, const double* observe
                 CK(launch_adj_ghost(ga, h->stream), "adjoint ghost");
                 kernels++;
             }
+            // the source terms read lamF^s and the ghost-adjoint terms, which the
+            // adjoint step and the probe residuals do not write: they run on the
+            // side stream beside them, joined before the next ghost pass
             AdjSourceArgs sa{L, h->links, lam[la], gadj, {}, d_cells, ncell, s, d_out};
             std::copy(gadj_off, gadj_off + 6, sa.gadj_off);
-            CK(launch_adj_source(sa, h->stream), "adjoint source");
+            CK(cudaEventRecord(h->ev_fork, h->stream), "adjoint fork");
+            CK(cudaStreamWaitEvent(h->side, h->ev_fork, 0), "adjoint fork");
+            CK(launch_adj_source(sa, h->side), "adjoint source");
+            CK(cudaEventRecord(h->ev_join, h->side), "adjoint join");
             kernels++;
-            if (s == 0) continue;
-            AdjStepArgs as{L, h->sa, lam[la], lam[la ^ 1], mom_of(s - 1 - cn), gadj, {}, adj_prefetch};
-            std::copy(gadj_off, gadj_off + 6, as.gadj_off);
-            CK(launch_adj_step(as, h->stream), "adjoint step");
-            kernels++;
-            la ^= 1;
-            pa.resid = d_resid + (size_t)(s - 1) * np;
-            CK(launch_adj_probe(lam[la], pa, h->stream), "adjoint probe");
-            kernels++;
+            if (s > 0)
+            {
+                AdjStepArgs as{L, h->sa, lam[la], lam[la ^ 1], mom_of(s - 1 - cn), gadj, {}, adj_prefetch};
+                std::copy(gadj_off, gadj_off + 6, as.gadj_off);
+                CK(launch_adj_step(as, h->stream), "adjoint step");
+                kernels++;
+                la ^= 1;
+                pa.resid = d_resid + (size_t)(s - 1) * np;
+                CK(launch_adj_probe(lam[la], pa, h->stream), "adjoint probe");
+                kernels++;
+            }
+            CK(cudaStreamWaitEvent(h->stream, h->ev_join, 0), "adjoint join");
         }
         return LBM_OK;
     };
