@@ -2342,18 +2342,54 @@ extern "C" int lbm_adjoint_grad(lbm_handle* h, int nsteps, const double* observe
                                 h->stream);
         return r;
     };
+    // The ghost fill reads only the first interior layer of each open face (the
+    // x faces through their export arrays, which the source also updates);
+    // when step s's injection cells stay off that layer, source and ghost fill
+    // touch disjoint cells and the source runs on the side stream beside it.
+    std::vector<char> source_apart((size_t)T, 0);
+    for (int s = 0; s < T; ++s)
+    {
+        bool apart = true;
+        for (int b = 0; b < ncell && apart; ++b)
+        {
+            const AdjSourceCell& cc = cells[(size_t)s * ncell + b];
+            if (cc.i < 0) continue;
+            for (int f = 0; f < h->ga.nfaces; ++f)
+            {
+                const GhostFace& F = h->ga.face[f];
+                const int v = F.axis == 0 ? cc.i : F.axis == 1 ? cc.j : cc.k;
+                const int n = F.axis == 0 ? L.nx : F.axis == 1 ? L.ny : L.nz;
+                if (v == (F.side ? n : 1)) apart = false;
+            }
+        }
+        source_apart[(size_t)s] = apart;
+    }
     // source + ghost fill of step s on the current buffer (G^s -> Ht^s)
-    const auto source_ghost = [&](int s) {
+    const auto source_then_ghost = [&](int s, const GhostArgs& g) {
         sargs.direct[0] = entries[s];
-        cudaError_t r = launch_source(h->storage, h->f[h->cur], L, h->sa, sargs, h->stream);
+        cudaError_t r = cudaSuccess;
+        const bool beside = h->ga.total > 0 && source_apart[(size_t)s];
+        if (beside)
+        {
+            r = cudaEventRecord(h->ev_fork, h->stream);
+            if (r == cudaSuccess) r = cudaStreamWaitEvent(h->side, h->ev_fork, 0);
+            if (r == cudaSuccess) r = launch_source(h->storage, h->f[h->cur], L, h->sa, sargs, h->side);
+            if (r == cudaSuccess) r = cudaEventRecord(h->ev_join, h->side);
+        }
+        else
+        {
+            r = launch_source(h->storage, h->f[h->cur], L, h->sa, sargs, h->stream);
+        }
         kernels++;
         if (r == cudaSuccess && h->ga.total > 0)
         {
-            r = launch_ghost(h->storage, h->f[h->cur], L, h->ga, h->stream);
+            r = launch_ghost(h->storage, h->f[h->cur], L, g, h->stream);
             kernels++;
         }
+        if (r == cudaSuccess && beside) r = cudaStreamWaitEvent(h->stream, h->ev_join, 0);
         return r;
     };
+    const auto source_ghost = [&](int s) { return source_then_ghost(s, h->ga); };
     // pull + collide of step s (Ht^s -> G^{s+1}), optionally with its probe record
     // The probe record of step s reads the step's input buffer, which the step
     // only reads: it runs on the side stream beside the step, joined before
@@ -2381,17 +2417,9 @@ extern "C" int lbm_adjoint_grad(lbm_handle* h, int nsteps, const double* observe
     // recording the moments of H^s at the ghosts' interior cells, then the
     // fused step recording the moments of F^s, both into store slot `slot`.
     const auto stored_source_ghost = [&](int s, long long slot) {
-        sargs.direct[0] = entries[s];
-        cudaError_t r = launch_source(h->storage, h->f[h->cur], L, h->sa, sargs, h->stream);
-        kernels++;
-        if (r == cudaSuccess && h->ga.total > 0)
-        {
-            GhostArgs g = h->ga;
-            g.face_mom = face_mom_of(slot);
-            r = launch_ghost(h->storage, h->f[h->cur], L, g, h->stream);
-            kernels++;
-        }
-        return r;
+        GhostArgs g = h->ga;
+        g.face_mom = face_mom_of(slot);
+        return source_then_ghost(s, g);
     };
     // probe_step >= 0: also the probe record of that step (first pass)
     const auto stored_collide = [&](long long slot, int probe_step = -1) {
