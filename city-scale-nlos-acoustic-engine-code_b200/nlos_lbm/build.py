@@ -6,7 +6,7 @@ instead of the product when NLOS_LBM_CHECK=1).
 kernels.cu is compiled by nvcc for sm_100a only; the host C++ (api.cpp,
 geometry.cpp) by g++ with -ffp-contract=off so its FP64 arithmetic matches the
 reference's rounding.  The CUDA runtime is linked statically, so the library
-needs only the driver at run time.  Run ``python -m nlos_lbm.build`` or call
+needs only the NVIDIA driver at run time.  Run ``python -m nlos_lbm.build`` or call
 ``build()``.
 """
 import os

@@ -3,9 +3,10 @@ discrete adjoint of the oracle and against central finite differences of the
 GPU's own FP32 forward, on synthetic-city patches.
 
 Tolerances, stated per check:
-  - vs the FP64 adjoint: 1e-4 relative (the north-star gradient bar), on the
-    position gradient (max-norm) and on the per-step signal gradient
-    (relative L2); the forward series within the FP32 probe bar 1e-5;
+  - vs the FP64 adjoint: 1e-4 relative (the gradient accuracy target of the
+    localisation benchmark), on the position gradient (max-norm) and on the
+    per-step signal gradient (relative L2); the forward series within the FP32
+    probe bar 1e-5;
   - vs central differences of the FP32 forward at h = 1e-2 cells: 1e-4
     relative on the position gradient;
   - checkpoint schedules: bit-identical gradients (the recomputation is
