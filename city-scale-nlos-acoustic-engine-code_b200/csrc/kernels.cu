@@ -942,8 +942,22 @@ __global__ void __launch_bounds__(512) k_source(S* __restrict__ f, Layout L, Ste
 // stored deviation units (Gs = scale * g):
 //   geq(rho', r, u) = w (rho' + r (3 c.u + (4.5 (c.u)^2 - 1.5 u^2) / scale)).
 
-__device__ __forceinline__ void nscbc(float (&G)[Q], int axis, int side, float inv_scale)
+//
+// Only the 5 directions that point from the ghost into the interior (e_axis =
+// +1 on the low side, -1 on the high side) are ever pulled from a ghost cell
+// (by the step, the probes, the field output, the slab messages and the
+// adjoint); the fill computes and stores those and leaves the other 14 of the
+// ghost cell as they are.
+template <int AXIS, int SIDE>
+__host__ __device__ constexpr bool inward(int q)
 {
+    return (AXIS == 0 ? ex(q) : AXIS == 1 ? ey(q) : ez(q)) == (SIDE ? -1 : 1);
+}
+
+template <int AXIS, int SIDE>
+__device__ __forceinline__ void nscbc(float (&G)[Q], float inv_scale)
+{
+    constexpr int axis = AXIS, side = SIDE;
     float rho, jx, jy, jz;
     moments(G, rho, jx, jy, jz);
     float rI = fmaf(rho, inv_scale, 1.0f);
@@ -991,6 +1005,7 @@ __device__ __forceinline__ void nscbc(float (&G)[Q], int axis, int side, float i
 #pragma unroll
     for (int q = 0; q < Q; ++q)
     {
+        if (!inward<AXIS, SIDE>(q)) continue;
         float e = d0;
         if (ex(q)) e += mxx;
         if (ey(q)) e += myy;
@@ -1012,34 +1027,31 @@ __device__ __forceinline__ void store_moments(const float (&G)[Q], float4* out)
     *out = make_float4(rho, jx, jy, jz);
 }
 
-template <typename S>
-__global__ void __launch_bounds__(128) k_ghost(S* __restrict__ f, Layout L, GhostArgs a)
+// One face cell (two x-adjacent ones in FP16 y and z faces) of face (AXIS, SIDE).
+template <typename S, int AXIS, int SIDE>
+__device__ __forceinline__ void ghost_cell(S* __restrict__ f, const Layout& L, const GhostArgs& a, const GhostFace& F,
+                                           long long t, int lt)
 {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= a.total) return;
-    int fi = 0;
-    while (fi + 1 < a.nfaces && t >= a.face[fi + 1].first) ++fi;
-    const GhostFace F = a.face[fi];
-    const int lt = (int)(t - F.first);   // a face has fewer than 2^31 cells (nu, nv are ints of one grid)
     const int v = lt / F.nu, u = lt - v * F.nu;
     const float inv_scale = 1.0f / a.scale;
     float G[Q];
-    if (F.axis == 0)
+    if constexpr (AXIS == 0)
     {
         // x faces: compact export -> compact ghost, both coalesced along j
         const int j = 1 + u, k = 1 + v;
-        if (!LBM_IN(kChkGhost, a.xf.exp_index(F.side, 18, j, k, L.ny, L.nz), xexp_extent(L)) ||
-            !LBM_IN(kChkGhost, a.xf.gh_index(F.side, 18, j, k, L.ny, L.nz), xgh_extent(L)))
+        if (!LBM_IN(kChkGhost, a.xf.exp_index(SIDE, 18, j, k, L.ny, L.nz), xexp_extent(L)) ||
+            !LBM_IN(kChkGhost, a.xf.gh_index(SIDE, 18, j, k, L.ny, L.nz), xgh_extent(L)))
             return;
 #pragma unroll
-        for (int q = 0; q < Q; ++q) G[q] = a.xf.xexp[a.xf.exp_index(F.side, q, j, k, L.ny, L.nz)];
+        for (int q = 0; q < Q; ++q) G[q] = a.xf.xexp[a.xf.exp_index(SIDE, q, j, k, L.ny, L.nz)];
         if (a.face_mom) store_moments(G, a.face_mom + t);
-        nscbc(G, 0, F.side, inv_scale);
+        nscbc<AXIS, SIDE>(G, inv_scale);
 #pragma unroll
-        for (int q = 0; q < Q; ++q) a.xf.xgh[a.xf.gh_index(F.side, q, j, k, L.ny, L.nz)] = G[q];
+        for (int q = 0; q < Q; ++q)
+            if (inward<AXIS, SIDE>(q)) a.xf.xgh[a.xf.gh_index(SIDE, q, j, k, L.ny, L.nz)] = G[q];
         return;
     }
-    if constexpr (std::is_same<S, __half>::value)
+    else if constexpr (std::is_same<S, __half>::value)
     {
         // y and z faces in FP16: the first half of the face's threads take two
         // x-adjacent cells each, one half2 per direction (a 64-cell block
@@ -1050,8 +1062,8 @@ __global__ void __launch_bounds__(128) k_ghost(S* __restrict__ f, Layout L, Ghos
         const int vp = lt / npair, up = 2 * (lt - vp * npair);
         const bool two = up + 1 < F.nu;
         const int pi = 1 + up;
-        const int pj = F.axis == 1 ? (F.side ? L.ny : 1) : 1 + vp, pk = F.axis == 1 ? 1 + vp : (F.side ? L.nz : 1);
-        const int qj = F.axis == 1 ? (F.side ? L.ny + 1 : 0) : pj, qk = F.axis == 1 ? pk : (F.side ? L.nz + 1 : 0);
+        const int pj = AXIS == 1 ? (SIDE ? L.ny : 1) : 1 + vp, pk = AXIS == 1 ? 1 + vp : (SIDE ? L.nz : 1);
+        const int qj = AXIS == 1 ? (SIDE ? L.ny + 1 : 0) : pj, qk = AXIS == 1 ? pk : (SIDE ? L.nz + 1 : 0);
         constexpr int BCH = block_cells(sizeof(S));
         if (!LBM_IN(kChkGhost, L.elem(18, pi + (two ? 1 : 0), pj, pk), L.total) ||
             !LBM_IN(kChkGhost, L.elem(18, pi + (two ? 1 : 0), qj, qk), L.total))
@@ -1076,48 +1088,61 @@ __global__ void __launch_bounds__(128) k_ghost(S* __restrict__ f, Layout L, Ghos
         }
         const long long cell = F.first + (long long)vp * F.nu + up;   // the face enumeration of one cell a thread
         if (a.face_mom) store_moments(G, a.face_mom + cell);
-        nscbc(G, F.axis, F.side, inv_scale);
+        nscbc<AXIS, SIDE>(G, inv_scale);
         if (two)
         {
             if (a.face_mom) store_moments(G1, a.face_mom + cell + 1);
-            nscbc(G1, F.axis, F.side, inv_scale);
+            nscbc<AXIS, SIDE>(G1, inv_scale);
 #pragma unroll
-            for (int q = 0; q < Q; ++q) *reinterpret_cast<__half2*>(B + q * BCH) = __floats2half2_rn(G[q], G1[q]);
+            for (int q = 0; q < Q; ++q)
+                if (inward<AXIS, SIDE>(q)) *reinterpret_cast<__half2*>(B + q * BCH) = __floats2half2_rn(G[q], G1[q]);
         }
         else
         {
 #pragma unroll
-            for (int q = 0; q < Q; ++q) Io<S>::st(B + q * BCH, G[q]);
+            for (int q = 0; q < Q; ++q)
+                if (inward<AXIS, SIDE>(q)) Io<S>::st(B + q * BCH, G[q]);
         }
-        return;
-    }
-    int ci, cj, ck, gj, gk;
-    if (F.axis == 1)
-    {
-        ci = 1 + u;
-        ck = gk = 1 + v;
-        cj = F.side ? L.ny : 1;
-        gj = F.side ? L.ny + 1 : 0;
     }
     else
     {
-        ci = 1 + u;
-        cj = gj = 1 + v;
-        ck = F.side ? L.nz : 1;
-        gk = F.side ? L.nz + 1 : 0;
+        const int ci = 1 + u;
+        const int cj = AXIS == 1 ? (SIDE ? L.ny : 1) : 1 + v, gj = AXIS == 1 ? (SIDE ? L.ny + 1 : 0) : cj;
+        const int ck = AXIS == 1 ? 1 + v : (SIDE ? L.nz : 1), gk = AXIS == 1 ? ck : (SIDE ? L.nz + 1 : 0);
+        constexpr int BC = block_cells(sizeof(S));
+        if (!LBM_IN(kChkGhost, L.elem(18, ci, cj, ck), L.total) ||
+            !LBM_IN(kChkGhost, L.elem(18, ci, gj, gk), L.total) || !LBM_IN(kChkGhost, L.elem(0, ci, gj, gk), L.total))
+            return;
+        const S* I = f + L.elem(0, ci, cj, ck);
+        S* B = f + L.elem(0, ci, gj, gk);
+#pragma unroll
+        for (int q = 0; q < Q; ++q) G[q] = Io<S>::ld(I + q * BC);
+        if (a.face_mom) store_moments(G, a.face_mom + t);
+        nscbc<AXIS, SIDE>(G, inv_scale);
+#pragma unroll
+        for (int q = 0; q < Q; ++q)
+            if (inward<AXIS, SIDE>(q)) Io<S>::st(B + q * BC, G[q]);
     }
-    constexpr int BC = block_cells(sizeof(S));
-    if (!LBM_IN(kChkGhost, L.elem(18, ci, cj, ck), L.total) || !LBM_IN(kChkGhost, L.elem(18, ci, gj, gk), L.total) ||
-        !LBM_IN(kChkGhost, L.elem(0, ci, gj, gk), L.total))
-        return;
-    const S* I = f + L.elem(0, ci, cj, ck);
-    S* B = f + L.elem(0, ci, gj, gk);
-#pragma unroll
-    for (int q = 0; q < Q; ++q) G[q] = Io<S>::ld(I + q * BC);
-    if (a.face_mom) store_moments(G, a.face_mom + t);
-    nscbc(G, F.axis, F.side, inv_scale);
-#pragma unroll
-    for (int q = 0; q < Q; ++q) Io<S>::st(B + q * BC, G[q]);
+}
+
+template <typename S>
+__global__ void __launch_bounds__(128) k_ghost(S* __restrict__ f, Layout L, GhostArgs a)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= a.total) return;
+    int fi = 0;
+    while (fi + 1 < a.nfaces && t >= a.face[fi + 1].first) ++fi;
+    const GhostFace F = a.face[fi];
+    const int lt = (int)(t - F.first);   // a face has fewer than 2^31 cells (nu, nv are ints of one grid)
+    switch (F.axis * 2 + F.side)
+    {
+    case 0: ghost_cell<S, 0, 0>(f, L, a, F, t, lt); break;
+    case 1: ghost_cell<S, 0, 1>(f, L, a, F, t, lt); break;
+    case 2: ghost_cell<S, 1, 0>(f, L, a, F, t, lt); break;
+    case 3: ghost_cell<S, 1, 1>(f, L, a, F, t, lt); break;
+    case 4: ghost_cell<S, 2, 0>(f, L, a, F, t, lt); break;
+    default: ghost_cell<S, 2, 1>(f, L, a, F, t, lt); break;
+    }
 }
 
 // ---------------------------------------------------------------- probes
