@@ -320,7 +320,9 @@ int lbm_get_rho(lbm_handle* h, float* out, long capacity);
  * overwrites all the cells it returns, so nothing needs clearing. */
 int lbm_get_rho_noalloc(lbm_handle* h, float* out, long capacity);
 /* Populations f_q (FP64, w_q + deviation) in the reference's AoS,
- * halo-inclusive layout f[idx*19+q] (06:366, 06:206-209). */
+ * halo-inclusive layout f[idx*19+q] (06:366, 06:206-209).  In the ghost
+ * cells of open faces only the 5 directions the interior pulls from them are
+ * kept up to date (the reference fills all 19; the other 14 are never read). */
 int lbm_get_f(lbm_handle* h, double* out, long capacity);
 int lbm_set_f(lbm_handle* h, const double* in, long count);
 /* Scheme A: initial state at rest with density 1 + rho_minus_1 at every
