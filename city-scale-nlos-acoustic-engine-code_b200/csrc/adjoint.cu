@@ -153,44 +153,46 @@ __device__ __forceinline__ D4 nscbc_lam4(const LamMoments& A, D4 rho, D4 jx, D4 
 
 // J_ghost^T of every open-face ghost cell: lamHt at the ghost (what the
 // interior cells pulled from it) mapped onto the interior cell it was built
-// from.  One thread per face cell.
-__global__ void __launch_bounds__(128) k_adj_ghost(AdjGhostArgs a)
+// from.  One thread per face cell, the face (AXIS, SIDE) a template argument:
+// only the 5 directions pointing into the interior carry adjoint values.
+template <int AXIS, int SIDE>
+__host__ __device__ constexpr bool inward(int q)
 {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= a.ga.total) return;
-    int fi = 0;
-    while (fi + 1 < a.ga.nfaces && t >= a.ga.face[fi + 1].first) ++fi;
-    const GhostFace F = a.ga.face[fi];
-    const int lt = (int)(t - F.first);
+    return (AXIS == 0 ? ex(q) : AXIS == 1 ? ey(q) : ez(q)) == (SIDE ? -1 : 1);
+}
+
+template <int AXIS, int SIDE>
+__device__ __forceinline__ void adj_ghost_cell(const AdjGhostArgs& a, const GhostFace& F, long long t, int lt)
+{
     const int v = lt / F.nu, u = lt - v * F.nu;
     const Layout& L = a.L;
     // ghost cell g (the forward ghost kernel's enumeration of the face)
     int gi, gj, gk;
-    if (F.axis == 0)
+    if (AXIS == 0)
     {
-        gi = F.side ? L.nx + 1 : 0;
+        gi = SIDE ? L.nx + 1 : 0;
         gj = 1 + u;
         gk = 1 + v;
     }
-    else if (F.axis == 1)
+    else if (AXIS == 1)
     {
         gi = 1 + u;
-        gj = F.side ? L.ny + 1 : 0;
+        gj = SIDE ? L.ny + 1 : 0;
         gk = 1 + v;
     }
     else
     {
         gi = 1 + u;
         gj = 1 + v;
-        gk = F.side ? L.nz + 1 : 0;
+        gk = SIDE ? L.nz + 1 : 0;
     }
     // lamHt at the ghost: what the interior cells y = g + e_q pulled from it,
     // nothing when the ghost cell is SOLID (they bounced back instead).  Bit q
     // of y's links word is that solidity for every such y, so one word is
     // read: that of the interior neighbour along the inward normal.
-    const int qn = 1 + 2 * F.axis + F.side;
-    const int ni = F.axis == 0 ? 1 - 2 * F.side : 0, nj = F.axis == 1 ? 1 - 2 * F.side : 0,
-              nk = F.axis == 2 ? 1 - 2 * F.side : 0;
+    const int qn = 1 + 2 * AXIS + SIDE;
+    const int ni = AXIS == 0 ? 1 - 2 * SIDE : 0, nj = AXIS == 1 ? 1 - 2 * SIDE : 0,
+              nk = AXIS == 2 ? 1 - 2 * SIDE : 0;
     // (loaded beside the adjoint values, not before them: one memory round trip)
     const uint32_t lkn = __ldg(a.links + L.cell(gi + ni, gj + nj, gk + nk));
     float lh[Q];
@@ -198,12 +200,14 @@ __global__ void __launch_bounds__(128) k_adj_ghost(AdjGhostArgs a)
     for (int q = 0; q < Q; ++q)
     {
         const int di = gi + ex(q), dj = gj + ey(q), dk = gk + ez(q);
-        lh[q] = interior(L, di, dj, dk) ? __ldg(a.lam_in + L.elem(q, di, dj, dk)) : 0.f;
+        // only the directions pointing into the interior reach an interior cell
+        lh[q] = inward<AXIS, SIDE>(q) && interior(L, di, dj, dk) ? __ldg(a.lam_in + L.elem(q, di, dj, dk)) : 0.f;
     }
     if ((lkn >> qn) & 1u)
     {
 #pragma unroll
-        for (int q = 0; q < Q; ++q) lh[q] = 0.f;
+        for (int q = 0; q < Q; ++q)
+            if (inward<AXIS, SIDE>(q)) lh[q] = 0.f;
     }
     // moments of the interior cell the ghost was built from
     const float4 m = __ldg(a.face_mom + t);
@@ -212,6 +216,7 @@ __global__ void __launch_bounds__(128) k_adj_ghost(AdjGhostArgs a)
 #pragma unroll
     for (int q = 0; q < Q; ++q)
     {
+        if (!inward<AXIS, SIDE>(q)) continue;   // lh[q] = 0
         const float wl = wf(q) * lh[q];
         A.a0 += wl;
         if (ex(q)) A.a1[0] += ex(q) * wl;
@@ -225,12 +230,31 @@ __global__ void __launch_bounds__(128) k_adj_ghost(AdjGhostArgs a)
         if (ey(q) * ez(q)) A.a2[5] += ey(q) * ez(q) * wl;
     }
     const D4 S = nscbc_lam4(A, D4{m.x, {1.f, 0.f, 0.f, 0.f}}, D4{m.y, {0.f, 1.f, 0.f, 0.f}},
-                            D4{m.z, {0.f, 0.f, 1.f, 0.f}}, D4{m.w, {0.f, 0.f, 0.f, 1.f}}, F.axis, F.side);
+                            D4{m.z, {0.f, 0.f, 1.f, 0.f}}, D4{m.w, {0.f, 0.f, 0.f, 1.f}}, AXIS, SIDE);
     const float vk[4] = {S.d[0], S.d[1], S.d[2], S.d[3]};
-    const long long n = (long long)F.nu * F.nv, off = a.gadj_off[F.axis * 2 + F.side];
+    const long long n = (long long)F.nu * F.nv, off = a.gadj_off[AXIS * 2 + SIDE];
 #pragma unroll
     for (int p = 0; p < Q; ++p)
         a.gadj[off + (long long)p * n + lt] = lh[p] + vk[0] + ex(p) * vk[1] + ey(p) * vk[2] + ez(p) * vk[3];
+}
+
+__global__ void __launch_bounds__(128) k_adj_ghost(AdjGhostArgs a)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= a.ga.total) return;
+    int fi = 0;
+    while (fi + 1 < a.ga.nfaces && t >= a.ga.face[fi + 1].first) ++fi;
+    const GhostFace F = a.ga.face[fi];
+    const int lt = (int)(t - F.first);
+    switch (F.axis * 2 + F.side)
+    {
+    case 0: adj_ghost_cell<0, 0>(a, F, t, lt); break;
+    case 1: adj_ghost_cell<0, 1>(a, F, t, lt); break;
+    case 2: adj_ghost_cell<1, 0>(a, F, t, lt); break;
+    case 3: adj_ghost_cell<1, 1>(a, F, t, lt); break;
+    case 4: adj_ghost_cell<2, 0>(a, F, t, lt); break;
+    default: adj_ghost_cell<2, 1>(a, F, t, lt); break;
+    }
 }
 
 __device__ __forceinline__ uint32_t near_bits(const StepArgs& a, const Layout& L, int col, int j, int k)
