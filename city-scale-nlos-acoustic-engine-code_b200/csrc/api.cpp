@@ -131,8 +131,8 @@ struct lbm_handle
     void* slab_buf = nullptr;
     size_t slab_msg_bytes = 0;
     cudaEvent_t ev_packed = nullptr, ev_read = nullptr;
-    // lbm_adjoint_grad: a second stream for the small kernels that run beside a step
-    // (the forward pass's probe record, the reverse pass's source terms)
+    // a second stream for the small kernels that run beside a step (the batched step's
+    // probe record; in lbm_adjoint_grad also the source and the reverse pass's source terms)
     cudaStream_t side = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
 
@@ -930,6 +930,12 @@ extern "C" int lbm_init(lbm_handle* h)
 
     // Device buffers.
     if (!h->stream) CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    if (!h->side)
+    {
+        CK(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking), "side stream");
+        CK(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming), "side stream events");
+        CK(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming), "side stream events");
+    }
     const size_t esz = h->storage == LBM_STORE_F16 ? 2 : 4;
     const size_t pop_bytes = (size_t)L.total * esz;
     cudaError_t e = cudaSuccess;
@@ -1207,7 +1213,7 @@ int harvest_timing(lbm_handle* h)
 
 // One full time step on the device (source -> ghosts -> fused step ->
 // probes), reading the step index from the device control block.
-cudaError_t enqueue_batched_step(lbm_handle* h, int parity, int& kernels)
+cudaError_t enqueue_batched_step(lbm_handle* h, int parity, int& kernels, bool captured = false)
 {
     cudaError_t e = cudaSuccess;
     void* fc = h->f[parity];
@@ -1244,12 +1250,31 @@ cudaError_t enqueue_batched_step(lbm_handle* h, int parity, int& kernels)
         if (e != cudaSuccess) return e;
         kernels++;
     }
+    if (!captured)
+    {
+        e = timed_step_launch(h, parity, true, 0);
+        if (e != cudaSuccess) return e;
+        kernels++;
+        e = launch_probe(h->storage, fc, h->L, h->sa, probe_args(h, true, 0), h->stream);
+        kernels++;
+        return e;
+    }
+    // In the captured graph the probe record, which reads this step's input
+    // buffer and ghosts (the step only reads them) and advances the device step
+    // counter (no scheme-B step kernel reads it), is a branch beside the step,
+    // joined before the next step's source reads the counter.  (Direct launches
+    // keep one stream: the two event calls would cost more host time per step
+    // than the probe takes on small grids.)
+    e = cudaEventRecord(h->ev_fork, h->stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(h->side, h->ev_fork, 0);
+    if (e == cudaSuccess) e = launch_probe(h->storage, fc, h->L, h->sa, probe_args(h, true, 0), h->side);
+    if (e == cudaSuccess) e = cudaEventRecord(h->ev_join, h->side);
+    if (e != cudaSuccess) return e;
+    kernels++;
     e = timed_step_launch(h, parity, true, 0);
     if (e != cudaSuccess) return e;
     kernels++;
-    e = launch_probe(h->storage, fc, h->L, h->sa, probe_args(h, true, 0), h->stream);
-    kernels++;
-    return e;
+    return cudaStreamWaitEvent(h->stream, h->ev_join, 0);
 }
 
 int build_graph(lbm_handle* h)
@@ -1259,8 +1284,8 @@ int build_graph(lbm_handle* h)
     cudaError_t e = cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return h->cuda_fail(e, "begin capture");
     int k0 = 0, k1 = 0;
-    cudaError_t le = enqueue_batched_step(h, 0, k0);
-    if (le == cudaSuccess) le = enqueue_batched_step(h, 1, k1);
+    cudaError_t le = enqueue_batched_step(h, 0, k0, true);
+    if (le == cudaSuccess) le = enqueue_batched_step(h, 1, k1, true);
     e = cudaStreamEndCapture(h->stream, &g);
     if (le != cudaSuccess) e = le;
     if (e == cudaSuccess) e = cudaGraphInstantiate(&h->graph, g, 0);
@@ -2434,13 +2459,6 @@ extern "C" int lbm_adjoint_grad(lbm_handle* h, int nsteps, const double* observe
     };
     const auto ckpt_pos = [&](long long boundary) { return std::max(boundary - 1, 0LL); };
     const long long cnT = ckpt_pos(Tt);   // first step whose forward data the first pass stores
-
-    if (!h->side)
-    {
-        CK(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking), "adjoint side stream");
-        CK(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming), "adjoint events");
-        CK(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming), "adjoint events");
-    }
 
     // ---- forward pass: probe predictions, outer checkpoints G^{max(mK1-1,0)}
     // of the segments before the tail, and the tail's forward data

@@ -13,9 +13,10 @@
  * the cases the reference reports on stdout and then carries on (STL not
  * loaded, probe inside a solid).  No C++ exceptions cross this boundary.
  * A handle owns one CUDA stream and is not re-entrant: use one handle per
- * host thread.  (lbm_adjoint_grad also runs some small kernels on a second,
- * internal stream, joined back to the handle's stream before they could
- * matter and finished before the call returns.)
+ * host thread.  (The library also runs some small kernels, such as the probe
+ * record beside the step, on a second stream of the handle, joined back to
+ * the handle's stream before anything reads their results or overwrites
+ * their inputs, so work ordered on the handle's stream sees the same order.)
  *
  * Lattice: D3Q19 in the reference's family-B velocity order (06:21-31).
  * Populations are stored on the device as deviations g_q = f_q - w_q from the
