@@ -1262,9 +1262,8 @@ cudaError_t enqueue_batched_step(lbm_handle* h, int parity, int& kernels, bool c
     // In the captured graph the probe record, which reads this step's input
     // buffer and ghosts (the step only reads them) and advances the device step
     // counter (no scheme-B step kernel reads it), is a branch beside the step,
-    // joined before the next step's source reads the counter.  (Direct launches
-    // keep one stream: the two event calls would cost more host time per step
-    // than the probe takes on small grids.)
+    // joined before the next step's source reads the counter.  Direct launches
+    // of single steps keep one stream (no graph amortises the fork and join).
     e = cudaEventRecord(h->ev_fork, h->stream);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(h->side, h->ev_fork, 0);
     if (e == cudaSuccess) e = launch_probe(h->storage, fc, h->L, h->sa, probe_args(h, true, 0), h->side);
